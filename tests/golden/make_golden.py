@@ -1,0 +1,216 @@
+"""Generate golden vectors by running ZhenMode's own solver code.
+
+Run in a container that holds the ZhenMode source tree (default
+``/root/reference/src``; override with ``ZHENMODE_SRC``)::
+
+    python tests/golden/make_golden.py
+
+JAX is not installed here, so the unmodified reference modules are imported
+with the NumPy-backed stand-in under ``tests/golden/_jaxshim`` on
+``sys.path`` (float64, eager).  Outputs are ``tests/golden/*.npz``; the
+parity tests compare the float64 oracle (``oracle/``) and, on a GPU, the
+CUDA step against them.  This script is the only reader of the reference
+tree; nothing at test time needs it.
+"""
+from __future__ import annotations
+
+import dataclasses
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+REF_SRC = os.environ.get("ZHENMODE_SRC", "/root/reference/src")
+sys.path[:0] = [os.path.join(HERE, "_jaxshim"), REF_SRC, ROOT]
+
+import zhenmode.model.config as ref_config  # noqa: E402
+from zhenmode.model.solver.dynamics import barotropic as ref_bt  # noqa: E402
+from zhenmode.model.solver.dynamics import pressure as ref_pressure  # noqa: E402
+from zhenmode.model.solver.dynamics import tendencies as ref_tend  # noqa: E402
+from zhenmode.model.solver.dynamics import transport as ref_transport  # noqa: E402
+from zhenmode.model.solver.factory import make_solver_global  # noqa: E402
+from zhenmode.model.solver.numerics import horizontal as ref_h  # noqa: E402
+from zhenmode.model.solver.numerics import vertical as ref_v  # noqa: E402
+from zhenmode.model.solver.physics import vertical as ref_pv  # noqa: E402
+from zhenmode.model.solver.state import JaxStateG  # noqa: E402
+from zhenmode.model.solver.timestepping import step as ref_step  # noqa: E402
+
+from zhenmode_b200 import workloads  # noqa: E402
+
+
+def _physics(phys):
+    return ref_config.PhysicsConfig(**{f.name: getattr(phys, f.name)
+                                       for f in dataclasses.fields(phys)})
+
+
+def _np(x):
+    return np.array(np.asarray(x), dtype=np.float64)
+
+
+def _smooth_noise(rng, shape, passes=2):
+    a = rng.standard_normal(shape)
+    for _ in range(passes):
+        a = 0.25 * (np.roll(a, 1, 0) + 2 * a + np.roll(a, -1, 0))
+        a = 0.25 * (np.roll(a, 1, 1) + 2 * a + np.roll(a, -1, 1))
+    return a / np.std(a)
+
+
+def _moving_state(grid, T, S, seed, amp_u=0.05, amp_eta=0.05):
+    """Seeded nonzero wet-point velocity and free surface on top of T/S."""
+    rng = np.random.default_rng(seed)
+    wm = np.asarray(grid.wet_mask_3d)
+    nx, ny, nz = wm.shape
+    u = amp_u * _smooth_noise(rng, (nx, ny, nz)) * wm
+    v = amp_u * _smooth_noise(rng, (nx, ny, nz)) * wm
+    v[:, 0] = 0.0
+    v[:, -1] = 0.0
+    eta = amp_eta * _smooth_noise(rng, (nx, ny)) * np.asarray(grid.wet_mask)
+    T = T * wm + (1 - wm) * 15.0
+    S = S * wm + (1 - wm) * 35.0
+    return u, v, T, S, eta
+
+
+def _grid_arrays(grid):
+    return dict(grid_lon=np.asarray(grid.lon), grid_lat=np.asarray(grid.lat),
+                grid_dx_2d=np.asarray(grid.dx_2d), grid_dy=np.float64(grid.dy),
+                grid_cos_lat=np.asarray(grid.cos_lat), grid_f=np.asarray(grid.f),
+                grid_z=np.asarray(grid.z), grid_depth=np.asarray(grid.depth),
+                grid_wet_mask=np.asarray(grid.wet_mask),
+                grid_wet_mask_3d=np.asarray(grid.wet_mask_3d))
+
+
+def _digest(*arrays):
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(a, dtype=np.float64).tobytes())
+    return h.hexdigest()
+
+
+def _run_steps(step, state, nsteps):
+    outs = []
+    for _ in range(nsteps):
+        state = step(state)
+        outs.append(state)
+    return outs
+
+
+def make_step_case(name, nx, ny, nz, land_lat, physics, options, dt, dt_bt, restore_days,
+                   nsteps, moving, seed=7):
+    grid = workloads.build_grid(nx, ny, nz, land_lat=land_lat)
+    T, S = workloads.initial_fields(grid, perturb_sigma=0.2)
+    forcing = workloads.wind_forcing(grid)
+    kw = dict(options)
+    kw.update(forcing=forcing, dt_bt=dt_bt, dtype="float64")
+    if restore_days > 0:
+        kw.update(coastal_restore_mask=np.asarray(grid.wet_mask), coastal_restore_days=restore_days,
+                  coastal_restore_T=np.array(T[:, :, 0]))
+    step, init, _, params, _ = make_solver_global(grid, _physics(physics), dt, return_params=True, **kw)
+    st = init(T_init=T, S_init=S)
+    if moving:
+        u, v, T0, S0, eta = _moving_state(grid, T, S, seed)
+        st = JaxStateG(u, v, T0, S0, eta, np.zeros((nx, ny)))
+    outs = _run_steps(step, st, nsteps)
+    data = dict(_grid_arrays(grid))
+    data.update(in_u=_np(st.u), in_v=_np(st.v), in_T=_np(st.T), in_S=_np(st.S), in_eta=_np(st.eta),
+                dt=np.float64(dt), dt_bt=np.float64(dt_bt), restore_days=np.float64(restore_days),
+                nsteps=np.int64(nsteps), n_subcyc=np.int64(params.n_subcyc),
+                adv_nsub=np.int64(params.adv_nsub), conv_nsub=np.int64(params.conv_nsub),
+                physics=np.array(repr(dataclasses.asdict(physics))),
+                options=np.array(repr(options)))
+    for n, s in enumerate(outs, start=1):
+        if n == nsteps or (n == 1 and nsteps <= 2):
+            for key in ("u", "v", "T", "S", "eta"):
+                data[f"out{n}_{key}"] = _np(getattr(s, key))
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **data)
+    print(name, "saved", {k: v.shape for k, v in data.items() if hasattr(v, 'shape') and v.ndim > 1})
+
+
+def make_operator_case(seed=11):
+    """Single-operator goldens on a 24x16x6 grid with land blocks and a wet
+    polar band, random fields (reference functions called directly)."""
+    nx, ny, nz = 24, 16, 6
+    grid = workloads.build_grid(nx, ny, nz, land_lat=80.0)
+    wm = np.array(grid.wet_mask_3d)
+    wm[3:7, 6:9, :] = 0.0          # a land block
+    wm[12:15, 3:6, 3:] = 0.0       # a shallow shelf (ghost levels)
+    grid.wet_mask_3d = wm
+    grid.wet_mask = wm[:, :, 0].copy()
+    grid.ocean_mask = grid.wet_mask > 0.5
+    grid.land_mask = ~grid.ocean_mask
+    physics = workloads.PLAIN_PHYSICS
+    T, S = workloads.initial_fields(grid, perturb_sigma=0.2)
+    forcing = workloads.wind_forcing(grid)
+    results = {}
+    for limiter in ("fct", "monotone", "centered"):
+        kw = dict(workloads.PLAIN_OPTIONS)
+        kw.update(forcing=forcing, dt_bt=75.0, dtype="float64",
+                  fct_adv=(limiter == "fct"), monotone_adv=(limiter == "monotone"),
+                  coastal_restore_mask=np.asarray(grid.wet_mask), coastal_restore_days=30.0,
+                  coastal_restore_T=np.array(T[:, :, 0]))
+        _, _, _, p, _ = make_solver_global(grid, _physics(physics), 1800.0, return_params=True, **kw)
+        u, v, T0, S0, eta = _moving_state(grid, T, S, seed, amp_u=0.2, amp_eta=0.3)
+        st = JaxStateG(u, v, T0, S0, eta, np.zeros((nx, ny)))
+        Fz = ref_transport._vertical_transport_iface(u, v, p)
+        results[f"{limiter}_adv_T"] = _np(ref_transport._advection_scalar(T0, u, v, Fz, p))
+        results[f"{limiter}_tracer_residual_T"], results[f"{limiter}_tracer_residual_S"] = (
+            _np(a) for a in ref_tend._compute_tracer_residual(st, p))
+        if limiter != "fct":
+            continue
+        results["Fz"] = _np(Fz)
+        results["lap_u"] = _np(ref_h._laplacian_h(u, p))
+        results["bih_u"] = _np(ref_h._biharmonic_h(u, p))
+        results["hdiff_T"] = _np(ref_h._horizontal_tracer_diffusion(T0, p))
+        results["bihT_T"] = _np(ref_h._horizontal_biharmonic_tracer(T0, p))
+        results["d2z_T"] = _np(ref_v._d2_dz2(T0, p))
+        results["ddz_u"] = _np(ref_v._d_dz(ref_v._fill_ghost_bottom(u, p), p))
+        w = ref_transport._compute_vertical_velocity(st, p)
+        ax, ay = ref_transport._advection_flux_form(u, v, w, p)
+        results["madv_u"], results["madv_v"] = _np(ax), _np(ay)
+        results["dealias_u"] = _np(ref_h._dealias_h_fd(u, p))
+        gx, gy = ref_pressure._compute_pressure_gradient(st, p)
+        results["pgf_x"], results["pgf_y"] = _np(gx), _np(gy)
+        fx, fy = ref_pressure._compute_bt_rho_pgf(st, p)
+        results["btrho_x"], results["btrho_y"] = _np(fx), _np(fy)
+        col, unst = ref_pv._convective_mask(st, p)
+        results["conv_T"] = _np(ref_pv._conv_flux_tendency(T0, col, p.kappa_conv, p, unst))
+        mu, mv = ref_tend._compute_momentum_residual(st, p)
+        results["mom_residual_u"], results["mom_residual_v"] = _np(mu), _np(mv)
+        ubt, vbt = ref_transport._barotropic_velocity(u, v, p)
+        results["ubt"], results["vbt"] = _np(ubt), _np(vbt)
+        e1, u1, v1 = ref_bt._free_surface_step_fd(eta, ubt, vbt, p, fx, fy, dt_half=p.dt_bt)
+        results["fs_eta"], results["fs_ubt"], results["fs_vbt"] = _np(e1), _np(u1), _np(v1)
+        results["cap_T"] = _np(ref_h._apply_polar_cap(T0, p.wet_mask_z, p))
+        results["cap_eta"] = _np(ref_h._apply_polar_cap(eta, p.wet_mask, p))
+        lh = ref_step._linear_half_step(st, p, p.dt / 2)
+        for key in ("u", "v", "T", "S"):
+            results[f"lin_{key}"] = _np(getattr(lh, key))
+        nl = ref_step._explicit_full_step(st, p, p.dt)
+        for key in ("u", "v", "T", "S"):
+            results[f"nl_{key}"] = _np(getattr(nl, key))
+        results.update(in_u=u, in_v=v, in_T=T0, in_S=S0, in_eta=eta)
+    data = dict(_grid_arrays(grid))
+    data.update(results)
+    np.savez_compressed(os.path.join(HERE, "operators_24x16x6.npz"), **data)
+    print("operators saved", len(results), "arrays")
+
+
+def main():
+    make_operator_case()
+    # The 0.5 deg production option set, rescaled to a 7.5 deg x 7.5 deg grid
+    # whose polar bands are partly wet, from a moving state (2 steps).
+    make_step_case("step_plain_48x24x10", 48, 24, 10, 75.0, workloads.PLAIN_PHYSICS,
+                   workloads.PLAIN_OPTIONS, 1800.0, 75.0, 30.0, 2, moving=True)
+    # Same physics from rest on an all-land-polar grid (production geometry).
+    make_step_case("step_plain_rest_64x32x12", 64, 32, 12, 65.0, workloads.PLAIN_PHYSICS,
+                   workloads.PLAIN_OPTIONS, 1800.0, 75.0, 30.0, 1, moving=False)
+    # The CPU-runnable smoke configuration: 90x45x15, float64, 8 steps of 10 s.
+    wl = workloads.WORKLOADS["smoke"]
+    make_step_case("step_smoke_90x45x15", wl.nx, wl.ny, wl.nz, 65.0, wl.physics, wl.options,
+                   wl.dt, wl.dt_bt, 0.0, wl.steps, moving=False)
+
+
+if __name__ == "__main__":
+    main()

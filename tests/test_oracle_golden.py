@@ -1,0 +1,117 @@
+"""Pin the float64 oracle to golden vectors produced by ZhenMode's own step code.
+
+The fixtures come from ``tests/golden/make_golden.py`` (the reference solver
+run unmodified, float64).  Agreement is at round-off level: the oracle is a
+restatement of the same arithmetic, so anything above ~1e-12 relative is a
+transcription error, not precision.
+"""
+import numpy as np
+import pytest
+
+from oracle import params as oparams
+from oracle import step as ostep
+from tests.golden_io import case_inputs, grid_from, load, rel_l2
+
+TOL = 1e-11
+
+
+def _operator_params(data, limiter):
+    from zhenmode_b200 import workloads
+    grid = grid_from(data)
+    T = data["in_T"]
+    kw = dict(workloads.PLAIN_OPTIONS)
+    lat = np.radians(np.asarray(grid.lat))
+    tau_x = np.broadcast_to((0.1 * np.sin(2 * lat) * np.cos(lat))[None, :], (grid.nx, grid.ny)).copy()
+    zeros = np.zeros((grid.nx, grid.ny))
+    kw.update(forcing=(tau_x, zeros, zeros.copy()), dt_bt=75.0, dtype="float64",
+              fct_adv=(limiter == "fct"), monotone_adv=(limiter == "monotone"),
+              coastal_restore_mask=np.asarray(grid.wet_mask), coastal_restore_days=30.0,
+              coastal_restore_T=np.array(T[:, :, 0]))
+    return oparams.build_params(grid, workloads.PLAIN_PHYSICS, 1800.0, **kw)
+
+
+@pytest.fixture(scope="module")
+def ops():
+    return load("operators_24x16x6")
+
+
+def _check(name, got, want, tol=TOL):
+    err = rel_l2(got, want)
+    assert err < tol, f"{name}: rel L2 {err:.3e}"
+
+
+@pytest.mark.parametrize("limiter", ["fct", "monotone", "centered"])
+def test_tracer_advection_and_residual(ops, limiter):
+    p = _operator_params(ops, limiter)
+    u, v, T, S = ops["in_u"], ops["in_v"], ops["in_T"], ops["in_S"]
+    Fz = ostep.vertical_transport_iface(u, v, p)
+    _check("adv_T", ostep.tracer_advection(T, u, v, Fz, p), ops[f"{limiter}_adv_T"])
+    rT, rS = ostep.tracer_residual(u, v, T, S, p)
+    _check("res_T", rT, ops[f"{limiter}_tracer_residual_T"])
+    _check("res_S", rS, ops[f"{limiter}_tracer_residual_S"])
+
+
+def test_single_operators(ops):
+    p = _operator_params(ops, "fct")
+    u, v, T, S, eta = (ops["in_" + k] for k in ("u", "v", "T", "S", "eta"))
+    _check("Fz", ostep.vertical_transport_iface(u, v, p), ops["Fz"])
+    _check("lap", ostep.laplacian_h(u, p), ops["lap_u"])
+    _check("bih", ostep.biharmonic_h(u, p), ops["bih_u"])
+    _check("hdiff", ostep.horizontal_tracer_diffusion(T, p), ops["hdiff_T"])
+    _check("bihT", ostep.horizontal_biharmonic_tracer(T, p), ops["bihT_T"])
+    _check("d2z", ostep.d2_dz2(T, p), ops["d2z_T"])
+    _check("ddz", ostep.d_dz(ostep.fill_ghost_bottom(u, p), p), ops["ddz_u"])
+    w = ostep.vertical_velocity(u, v, p)
+    ax, ay = ostep.momentum_advection(u, v, w, p)
+    _check("madv_u", ax, ops["madv_u"])
+    _check("madv_v", ay, ops["madv_v"])
+    _check("dealias", ostep.dealias(u, p), ops["dealias_u"])
+    gx, gy = ostep.pressure_gradient(T, S, eta, p)
+    _check("pgf_x", gx, ops["pgf_x"])
+    _check("pgf_y", gy, ops["pgf_y"])
+    fx, fy = ostep.bt_rho_pgf(T, S, p)
+    _check("btrho_x", fx, ops["btrho_x"])
+    _check("btrho_y", fy, ops["btrho_y"])
+    col, unst = ostep.convective_gates(T, S, p)
+    _check("conv", ostep.convective_tendency(T, col, p.kappa_conv, p, unst), ops["conv_T"])
+    mu, mv = ostep.momentum_residual(u, v, T, S, eta, p)
+    _check("mres_u", mu, ops["mom_residual_u"])
+    _check("mres_v", mv, ops["mom_residual_v"])
+    ubt, vbt = ostep.barotropic_velocity(u, v, p)
+    _check("ubt", ubt, ops["ubt"])
+    _check("vbt", vbt, ops["vbt"])
+    e1, u1, v1 = ostep.free_surface_step(eta, ubt, vbt, p, fx, fy, p.dt_bt)
+    _check("fs_eta", e1, ops["fs_eta"])
+    _check("fs_ubt", u1, ops["fs_ubt"])
+    _check("fs_vbt", v1, ops["fs_vbt"])
+    _check("cap_T", ostep.polar_cap(T, p.wet_mask_z, p), ops["cap_T"])
+    _check("cap_eta", ostep.polar_cap(eta, p.wet_mask, p), ops["cap_eta"])
+    st = dict(u=u, v=v, T=T, S=S, eta=eta)
+    lh = ostep.linear_half_step(st, p, p.dt / 2)
+    for k in ("u", "v", "T", "S"):
+        _check("lin_" + k, lh[k], ops["lin_" + k])
+    nl = ostep.explicit_full_step(st, p)
+    for k in ("u", "v", "T", "S"):
+        _check("nl_" + k, nl[k], ops["nl_" + k])
+
+
+@pytest.mark.parametrize("name", ["step_plain_48x24x10", "step_plain_rest_64x32x12",
+                                  "step_smoke_90x45x15"])
+def test_full_step(name):
+    data = load(name)
+    grid, physics, dt, options, state = case_inputs(data)
+    p = oparams.build_params(grid, physics, dt, **options)
+    assert p.n_subcyc == int(data["n_subcyc"])
+    assert p.adv_nsub == int(data["adv_nsub"])
+    assert p.conv_nsub == int(data["conv_nsub"])
+    st = {k: np.array(v) for k, v in state.items()}
+    nsteps = int(data["nsteps"])
+    for n in range(1, nsteps + 1):
+        st = ostep.step(st, p)
+        if f"out{n}_u" in data:
+            for k in ("u", "v", "T", "S", "eta"):
+                want = data[f"out{n}_{k}"]
+                if np.linalg.norm(want) == 0:
+                    assert np.max(np.abs(st[k])) < 1e-14
+                else:
+                    _check(f"{name} step {n} {k}", st[k], want, tol=1e-10)
