@@ -1,0 +1,318 @@
+#!/usr/bin/env python
+"""Throughput of the B200 global ocean step on the 0.5-degree production
+workload: 720x360x50 levels, float32 fields, dt = 1800 s, 24 barotropic
+subcycles of 75 s, seeded synthetic bathymetry / thermocline / wind stress
+(the reference's ETOPO/WOA/NCEP inputs are not available).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One "step" is one baroclinic time step of the resident state.  `value` is
+simulated years per wall-clock day over all ranks (one independent replica
+per GPU: the step does not shard), timed with CUDA events on the launching
+stream; `e2e` is the same metric through the C ABI with host buffers (pinned
+host -> device copy of the state and device -> host copy of the result every
+step).  The per-step working set (~3 GB) is far larger than the 126 MB L2, so
+no flush is needed between iterations.
+
+`--impl reference` times the CPU restatement of the reference algorithm
+(``oracle/``, float64 NumPy, one thread) on a bounded sample: the same option
+set on a 180x90x50 grid, scaled per grid point to 720x360x50.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import platform
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SECONDS_PER_YEAR = 365.0 * 86400.0
+METRIC = "sim-years/day & ms/step at 720×360×50 on 1 B200: plain FP32 vs chosen form"
+WORKLOAD = "plain"
+SAMPLE_GRID = (180, 90, 50)
+
+# Algorithmic bytes per launch of each kernel class, in units of one float32
+# 3-D field (F = nx*ny*nz*4 bytes): distinct 3-D fields read + written.
+ALGO_FIELDS = {"nu_sub": 4, "inner_lap": 8, "lin_finish": 14, "fz": 3, "madv": 5, "dealias": 4,
+               "tracer_adv": 9, "tracer_rest": 10, "pgf": 10, "final": 12}
+# DRAM bytes per launch of the dominant kernel measured by ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum), recorded in profiles/; None until captured.
+NCU_TRAFFIC_BYTES = {}
+
+
+def sim_years_per_day(ms_per_step, dt):
+    return (86400.0 / (ms_per_step * 1e-3)) * dt / SECONDS_PER_YEAR
+
+
+def step_bytes(nx, ny, nz, n_nu, adv_nsub):
+    """Stage-structure algorithmic bytes of one step (two L half steps with
+    n_nu Laplacian sweeps, the N step, barotropic coupling and final pass)."""
+    F = 4.0 * nx * ny * nz
+    return (2 * (4 * n_nu + 10) + 46 + 12 * (adv_nsub - 1) + 8) * F
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            data = json.load(f)
+        return float(data["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for r in rows for q in range(4) if r[5 + q].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# Sample grids for the CPU timings (same option set), largest first; about
+# 5.4 us per grid point per step for the float64 NumPy step on one core.
+SAMPLE_GRIDS = ((180, 90, 50), (120, 60, 50), (90, 45, 50), (60, 30, 50), (48, 24, 50))
+CPU_US_PER_POINT = 5.4
+
+
+def sample_grid(total_steps, budget_s=150.0):
+    for g in SAMPLE_GRIDS:
+        if total_steps * g[0] * g[1] * g[2] * CPU_US_PER_POINT * 1e-6 <= budget_s:
+            return g
+    return SAMPLE_GRIDS[-1]
+
+
+def cpu_baseline(steps=2, warmup=1, grid_shape=SAMPLE_GRID):
+    """The float64 CPU restatement (oracle/) on a sample grid, scaled to the
+    full grid per point; returns (ms_per_full_step, description)."""
+    from oracle import params as oparams
+    from oracle import step as ostep
+    from zhenmode_b200 import workloads
+    nx, ny, nz = grid_shape
+    grid, physics, dt, kw, T, S = workloads.make_case(WORKLOAD, nx, ny, nz, dtype="float64")
+    kw = {k: v for k, v in kw.items() if k in oparams.SUPPORTED}
+    p = oparams.build_params(grid, physics, dt, **kw)
+    st = oparams.init_state(p, T, S)
+    for _ in range(warmup):
+        st = ostep.step(st, p)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        st = ostep.step(st, p)
+    sample_ms = (time.perf_counter() - t0) * 1e3 / steps
+    wl = workloads.WORKLOADS[WORKLOAD]
+    scale = (wl.nx * wl.ny * wl.nz) / float(nx * ny * nz)
+    desc = (f"float64 NumPy restatement of the reference step (oracle/), {steps} timed steps after {warmup} "
+            f"warm-up at {nx}x{ny}x{nz} with the 0.5-degree option set ({sample_ms:.0f} ms/step), scaled "
+            f"x{scale:.0f} per grid point to {wl.nx}x{wl.ny}x{wl.nz}")
+    return sample_ms * scale, desc
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from zhenmode_b200 import workloads
+    wl = workloads.WORKLOADS[WORKLOAD]
+    shape = sample_grid(args.steps + args.warmup)
+    ms, desc = cpu_baseline(steps=max(1, args.steps), warmup=max(0, args.warmup), grid_shape=shape)
+    value = sim_years_per_day(ms, wl.dt)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "sim-years/day",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded bathymetry, thermocline, wind stress)",
+            "config": {"workload": f"{wl.nx}x{wl.ny}x{wl.nz} 0.5-degree plain FP32 option set, dt={wl.dt:.0f} s",
+                       "sample": f"{shape[0]}x{shape[1]}x{shape[2]}"},
+            "cpu_baseline": {"value": value, "unit": "sim-years/day", "cores": 1, "kind": "port",
+                             "sample": desc, "cpu": platform.processor() or platform.machine(),
+                             "host_cores": len(os.sched_getaffinity(0))},
+            "e2e": {"value": value, "unit": "sim-years/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import ctypes
+
+    import torch
+    import torch.distributed as dist
+
+    from zhenmode_b200 import _native, make_solver_global, workloads
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+    wl = workloads.WORKLOADS[WORKLOAD]
+    grid, physics, dt, kw, T, S = workloads.make_case(WORKLOAD, dtype="float32")
+    step, init_state, _ = make_solver_global(grid, physics, dt, **kw)
+    solver = step.solver
+    st = init_state(T_init=T, S_init=S)
+    stream = torch.cuda.current_stream()
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    sin = _native.ZmState(*[t.data_ptr() for t in (st.u, st.v, st.T, st.S, st.eta)])
+    solver.check(solver.lib.zm_load_state(solver.handle, sptr, ctypes.byref(sin)), "zm_load_state")
+    solver.check(solver.lib.zm_advance(solver.handle, sptr, args.warmup), "zm_advance")
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    solver.check(solver.lib.zm_advance(solver.handle, sptr, args.steps), "zm_advance")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    code = ctypes.c_int32()
+    solver.check(solver.lib.zm_status(solver.handle, ctypes.byref(code)), "zm_status")
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    kernels_per_step = solver.kernels_per_step()
+
+    # per-kernel-class breakdown of one step (CUDA events around every launch)
+    prof = solver.profile(stream.cuda_stream)
+    total_prof = sum(v[0] for v in prof.values())
+    ranked = sorted(((v[0], k) for k, v in prof.items() if v[1] > 0), reverse=True)
+    dominant = next(k for _, k in ranked if k in ALGO_FIELDS)
+    dom_ms, dom_launches = prof[dominant]
+    F = 4.0 * wl.nx * wl.ny * wl.nz
+    algo = ALGO_FIELDS[dominant] * F
+    achieved = algo / (dom_ms / dom_launches * 1e-3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = NCU_TRAFFIC_BYTES.get(dominant)
+    bstep = step_bytes(wl.nx, wl.ny, wl.nz, solver.n_nu, solver.adv_nsub)
+
+    # end to end through the C ABI with pinned host buffers
+    e2e = None
+    if args.e2e_steps > 0:
+        host = [t.cpu().pin_memory() for t in (st.u, st.v, st.T, st.S, st.eta)]
+        hout = [torch.empty_like(h).pin_memory() for h in host]
+        hin = _native.ZmState(*[h.data_ptr() for h in host])
+        hres = _native.ZmState(*[h.data_ptr() for h in hout])
+        solver.check(solver.lib.zm_step_host(solver.handle, sptr, ctypes.byref(hin), ctypes.byref(hres), 1),
+                     "zm_step_host")
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        e2 = torch.cuda.Event(enable_timing=True)
+        e3 = torch.cuda.Event(enable_timing=True)
+        e2.record(stream)
+        for _ in range(args.e2e_steps):
+            solver.check(solver.lib.zm_step_host(solver.handle, sptr, ctypes.byref(hin), ctypes.byref(hres), 1),
+                         "zm_step_host")
+        e3.record(stream)
+        torch.cuda.synchronize()
+        ems = e2.elapsed_time(e3) / args.e2e_steps
+        if world > 1:
+            t = torch.tensor([ems], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        nbytes = sum(h.numel() * h.element_size() for h in host)
+        e2e = {"value": world * sim_years_per_day(ems, wl.dt), "unit": "sim-years/day", "ms_per_step": ems,
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cms, desc = cpu_baseline()
+        cpu = {"value": sim_years_per_day(cms, wl.dt), "unit": "sim-years/day", "cores": 1, "kind": "port",
+               "sample": desc, "ms_per_step": cms, "host_cores": len(os.sched_getaffinity(0))}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": world * sim_years_per_day(ms, wl.dt), "unit": "sim-years/day",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded bathymetry, thermocline, wind stress)",
+                "config": {"workload": f"{wl.nx}x{wl.ny}x{wl.nz} 0.5-degree plain FP32 option set, dt={wl.dt:.0f} s, "
+                                       f"{solver.n_subcyc} barotropic subcycles, {solver.n_nu} nu_h subcycles",
+                           "parallelism": f"replicas x{world}", "l2": "per-step working set >> L2 (no flush)",
+                           "monitor_code": int(code.value)},
+                "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
+                             "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                             "traffic": traffic, "algorithmic_bytes_per_launch": algo,
+                             "launch_ms": dom_ms / dom_launches,
+                             "step_stage_bytes": bstep, "step_frac": bstep / (ms * 1e-3) / 1e9 / peak},
+                "kernel_ms_per_step": {k: round(v[0], 4) for k, v in prof.items() if v[1] > 0},
+                "kernel_ms_unrolled_total": total_prof,
+                "gpu_launches": args.steps * kernels_per_step + 1,
+                "clocks": clk, "e2e": e2e, "cpu_baseline": cpu}
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,169 @@
+/* C ABI of the B200 (sm_100a) global ocean step.
+ *
+ * Drop-in boundary for ZhenMode's production solver step.  The reference's
+ * boundary is the Python factory
+ *   make_solver_global(grid, physics, dt, **options) -> (step, init_state, diagnostics[, ...])
+ * (src/zhenmode/model/solver/factory.py:30-68, 721-799), whose `step` is a
+ * jax.jit closure over `_step_impl` (src/zhenmode/model/solver/timestepping/step.py:341-458).
+ * The reference has no C or FFI layer; these entry points are what a jax.ffi
+ * custom call or a ctypes/cffi binding of that factory binds.
+ *
+ * Conventions
+ *  - Every array crossing this ABI uses the reference layout: 2-D fields are
+ *    (nx, ny) and 3-D fields (nx, ny, nz), C order, longitude periodic on the
+ *    first axis (src/zhenmode/model/solver/state.py:10-12).
+ *  - State arrays are float32 (the reference's dtype='float32' mode); grid and
+ *    parameter arrays are float64 host arrays, copied to the device once.
+ *  - Functions return 0 on success or one of the ZM_ERR_* codes; the message of
+ *    the last failure is available from zm_last_error().
+ *  - A handle is used by one host thread at a time; handles share nothing.
+ */
+#ifndef ZM_B200_H
+#define ZM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ZM_OK 0
+#define ZM_ERR_INVALID 1      /* invalid argument or configuration (the reference's ValueError) */
+#define ZM_ERR_UNSUPPORTED 2  /* an option the B200 path does not implement */
+#define ZM_ERR_CUDA 3         /* a CUDA runtime failure */
+#define ZM_ERR_TIMEOUT 4      /* a bounded device wait gave up */
+#define ZM_ERR_MONITOR 5      /* the device state monitor tripped */
+
+#define ZM_VDIFF_EXPLICIT 0
+#define ZM_VDIFF_IMPLICIT 1
+
+#define ZM_LIMITER_CENTERED 0
+#define ZM_LIMITER_DONOR 1    /* monotone_adv */
+#define ZM_LIMITER_MINMOD 2   /* fct_adv */
+
+typedef struct zm_solver zm_solver;
+
+/* GlobalOceanGrid fields (src/zhenmode/model/solver/geometry/grid.py:13-61). */
+typedef struct {
+  int32_t nx, ny, nz;
+  double dy;                  /* meridional spacing [m] */
+  const double* dx_2d;        /* (nx, ny) zonal spacing [m] */
+  const double* cos_lat;      /* (ny) */
+  const double* f;            /* (nx, ny) Coriolis parameter [1/s] */
+  const double* z;            /* (nz) level depths, negative downward */
+  const double* dz;           /* (nz-1) layer thicknesses */
+  const double* wet_mask;     /* (nx, ny) 1 ocean, 0 land */
+  const double* wet_mask_3d;  /* (nx, ny, nz) or NULL: column-uniform from wet_mask */
+} zm_grid;
+
+/* PhysicsConfig coefficients (src/zhenmode/model/config.py:86-140) and the
+ * make_solver_global options of the mode-split production path
+ * (src/zhenmode/model/solver/factory.py:30-68, 397-695). */
+typedef struct {
+  double dt, dt_bt;
+  double nu_h, nu_v, kappa_h, kappa_v, kappa_conv, nu_bi, kappa_bi;
+  double T_ref, S_ref, r_bot;
+  double lambda_bulk, restore_coef_S, ice_salt_flux, ice_freeze_temp_c;
+  int32_t nu_nsub;            /* 0: legacy count (= n_subcyc) */
+  int32_t polar_cap_rows, polar_cap_taper;
+  int32_t limiter;            /* ZM_LIMITER_* */
+  int32_t localize_conv, conservative_kv, freeze_adv_vel;
+  int32_t vertical_diffusion; /* ZM_VDIFF_* */
+  /* (nx, ny) float64 fields; NULL means zeros */
+  const double* tau_x;
+  const double* tau_y;
+  const double* q_heat;
+  const double* t_atm;               /* bulk target; used only with lambda_bulk > 0 */
+  const double* s_ref;               /* SSS restore target */
+  const double* coastal_restore_coef;/* 1/s */
+  const double* coastal_restore_t;
+  const double* coastal_bulk_lambda;
+  const double* coastal_kappa_h;
+  const double* coastal_kappa_v;
+} zm_params;
+
+/* JaxStateG fields u, v, T, S, eta (float32, reference layout); device
+ * pointers unless a function says host pointers. */
+typedef struct {
+  float* u;
+  float* v;
+  float* T;
+  float* S;
+  float* eta;
+} zm_state;
+
+/* Build a solver for one grid and parameter set: validates, derives the
+ * metric, subcycle counts and filter plans, copies everything to the current
+ * CUDA device and allocates the work buffers (replaces the parameter
+ * assembly of factory.py:397-718). */
+int zm_create(const zm_grid* grid, const zm_params* params, zm_solver** out);
+
+/* Derived counts: out[0] n_subcyc, out[1] nu subcycles, out[2] adv_nsub,
+ * out[3] conv_nsub, out[4] row pitch, out[5] device MiB held, out[6] kernel
+ * launches in one captured step (0 before the first zm_advance).
+ * Writes min(n, 7) values. */
+int zm_info(const zm_solver* s, int32_t* out, int32_t n);
+
+/* Copy a device state (reference layout) into the solver's resident state. */
+int zm_load_state(zm_solver* s, void* stream, const zm_state* in);
+
+/* Advance the resident state nsteps baroclinic steps (step.py:341-458), each
+ * one replay of a captured CUDA graph; stream ordered, no host sync. */
+int zm_advance(zm_solver* s, void* stream, int32_t nsteps);
+
+/* Copy the resident state out (reference layout, device pointers). */
+int zm_store_state(zm_solver* s, void* stream, zm_state* out);
+
+/* The jit `step` of factory.py:724-726 applied nsteps times: load, advance,
+ * store.  in and out may alias. */
+int zm_step(zm_solver* s, void* stream, const zm_state* in, zm_state* out, int32_t nsteps);
+
+/* As zm_step with HOST pointers (pinned memory gives full copy bandwidth);
+ * returns after the result is in `out`. */
+int zm_step_host(zm_solver* s, void* stream, const zm_state* in, zm_state* out, int32_t nsteps);
+
+/* Replace the 2-D forcing fields (device float32 arrays, (nx, ny)); the
+ * `step_dyn` path of factory.py:735-750.  NULL keeps a field. */
+int zm_set_forcing(zm_solver* s, void* stream, const float* tau_x, const float* tau_y, const float* q_heat);
+
+/* Run one stage of the step on a device state, for stage-level checks:
+ * 1 = linear half step L(dt/2) (step.py:76-187), 2 = nonlinear step N(dt)
+ * (step.py:249-320), 3 = one full step. */
+int zm_run_stage(zm_solver* s, void* stream, int32_t stage, const zm_state* in, zm_state* out);
+
+/* Kernel classes reported by zm_profile. */
+#define ZM_K_NU_SUB 0        /* nu_h Laplacian subcycles */
+#define ZM_K_INNER_LAP 1     /* inner Laplacians of the biharmonic operators */
+#define ZM_K_LIN_FINISH 2    /* rest of the linear half step */
+#define ZM_K_IMPLICIT 3      /* implicit vertical diffusion */
+#define ZM_K_FZ 4            /* interface transport Fz */
+#define ZM_K_MADV 5          /* momentum advection + latitude filter */
+#define ZM_K_DEALIAS 6       /* longitude FFT filter */
+#define ZM_K_TRACER_ADV 7    /* tracer advection substeps */
+#define ZM_K_TRACER_REST 8   /* convection, surface sources, tracer RK combine */
+#define ZM_K_PGF 9           /* pressure gradient, momentum RK combine, BT forcing */
+#define ZM_K_BAROTROPIC 10   /* barotropic subcycle */
+#define ZM_K_FINAL 11        /* projection, polar cap, land hold */
+#define ZM_K_COUNT 12
+
+/* Advance the resident state by one step without the CUDA graph, timing
+ * every kernel launch with CUDA events on `stream`; ms[c] and launches[c]
+ * receive the summed time and launch count of class c (n >= ZM_K_COUNT).
+ * Synchronizes the stream. */
+int zm_profile(zm_solver* s, void* stream, float* ms, int32_t* launches, int32_t n);
+
+/* Monitor of the resident state after the last zm_advance (runtime/monitor.py:20-30):
+ * 0 accepted, 1 non-finite, 3 velocity above 10 m/s, 4 |eta| above 15 m.
+ * Synchronizes the stream given to zm_advance. */
+int zm_status(zm_solver* s, int32_t* monitor_code);
+
+/* Message of the last failure on this handle ("" if none). */
+const char* zm_last_error(const zm_solver* s);
+
+void zm_destroy(zm_solver* s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ZM_B200_H */

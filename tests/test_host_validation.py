@@ -1,0 +1,62 @@
+"""Host-side behaviour of the drop-in factory that needs no GPU: invalid
+configurations raise ValueError before anything is built (as the reference
+factory does, src/zhenmode/model/solver/factory.py:166-395), and options the
+B200 path lacks raise UnsupportedOption (a ValueError subclass)."""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from zhenmode_b200 import UnsupportedOption, make_solver_global, workloads
+
+
+@pytest.fixture(scope="module")
+def case():
+    return workloads.make_case("plain", 24, 12, 6, dtype="float32")
+
+
+def _call(case, **over):
+    grid, physics, dt, kw, _, _ = case
+    kw = dict(kw)
+    kw.update(over)
+    return make_solver_global(grid, physics, dt, **kw)
+
+
+@pytest.mark.parametrize("over", [dict(dt_bt=0.0), dict(dt_bt=float("nan")), dict(polar_cap_rows=-1),
+                                  dict(polar_cap_rows=4, polar_cap_taper=3), dict(dtype="float16"),
+                                  dict(nu_nsub=0), dict(lambda_bulk=-1.0), dict(process_time_scheme="bogus"),
+                                  dict(column_geometry="bogus"), dict(vertical_diffusion="crank"),
+                                  dict(projection_max_refinements=3)])
+def test_invalid_configuration_raises_value_error(case, over):
+    with pytest.raises(ValueError):
+        _call(case, **over)
+
+
+def test_invalid_dt_and_physics(case):
+    grid, physics, dt, kw, _, _ = case
+    with pytest.raises(ValueError):
+        make_solver_global(grid, physics, -1.0, **kw)
+    with pytest.raises(ValueError):
+        make_solver_global(grid, dataclasses.replace(physics, nu_h=-1.0), dt, **kw)
+
+
+def test_invalid_grid(case):
+    grid, physics, dt, kw, _, _ = case
+    bad = dataclasses.replace(grid, z=np.asarray(grid.z)[::-1].copy())
+    with pytest.raises(ValueError):
+        make_solver_global(bad, physics, dt, **kw)
+
+
+@pytest.mark.parametrize("over", [dict(mode_split=False), dict(dtype="float64"), dict(project_adv_vel=True),
+                                  dict(sponge_days=10.0, sponge_cells=3), dict(dynamic_ice=True),
+                                  dict(mixed_layer_depth_m=50.0)])
+def test_unsupported_options(case, over):
+    with pytest.raises(UnsupportedOption):
+        _call(case, **over)
+
+
+def test_unknown_scheme_keyword(case):
+    with pytest.raises(TypeError):
+        _call(case, not_an_option=1)
+    with pytest.raises(ValueError):
+        _call(case, vertical_tracer_scheme="bogus")

@@ -1,0 +1,986 @@
+// Stencil, column and barotropic kernels of the global ocean step.
+//
+// Each kernel names the reference operator it computes (paths relative to the
+// ZhenMode source tree).  Layout and masks: see zm_internal.cuh.
+#include "zm_kernels.cuh"
+
+namespace zm {
+
+// ------------------------------------------------------------------ helpers
+struct Nb {  // horizontal neighbour indices of (j, i)
+  int i, j, ie, iw, jn, js;
+};
+__device__ __forceinline__ Nb nb(const Dev& d, int j, int i) {
+  return Nb{i, j, east(d, i), west(d, i), north(d, j), south(j)};
+}
+
+// Horizontal Laplacian on the sphere, legacy branch
+// (numerics/horizontal.py:181-215): face-gated d2/dx2, mirror-ghost face-gated
+// d2/dy2, metric term -(tan(lat)/R) d/dy on the unmasked centred difference.
+__device__ __forceinline__ float lap_h(const Dev& d, const float* __restrict__ a, int k, const Nb& n) {
+  const long long b = (long long)k * d.plane;
+  const float a0 = ld(a, b + idx2(d, n.j, n.i));
+  const float ae = ld(a, b + idx2(d, n.j, n.ie));
+  const float aw = ld(a, b + idx2(d, n.j, n.iw));
+  const float an = ld(a, b + idx2(d, n.jn, n.i));
+  const float as = ld(a, b + idx2(d, n.js, n.i));
+  const float w0 = wetf(wb(d, n.j, n.i), k), we = wetf(wb(d, n.j, n.ie), k);
+  const float ww = wetf(wb(d, n.j, n.iw), k), wn = wetf(wb(d, n.jn, n.i), k);
+  const float ws = wetf(wb(d, n.js, n.i), k);
+  const float d2x = ((ae - a0) * w0 * we - (a0 - aw) * w0 * ww) * __ldg(d.inv_dx2 + idx2(d, n.j, n.i));
+  const float d2y = ((an - a0) * wn * w0 - (a0 - as) * w0 * ws) * d.inv_dy2;
+  const float ddy = (an - as) * (0.5f * d.inv_dy);
+  return d2x + d2y + (-ddy * __ldg(d.tanR + n.j));
+}
+
+// Wet-face flux-form diffusion (numerics/horizontal.py:217-243); kap == nullptr
+// means unit diffusivity (the biharmonic tracer operator, :245-249).
+__device__ __forceinline__ float hdiff(const Dev& d, const float* __restrict__ c, const float* __restrict__ kap,
+                                       int k, const Nb& n) {
+  const long long b = (long long)k * d.plane;
+  const float c0 = ld(c, b + idx2(d, n.j, n.i));
+  const float ce = ld(c, b + idx2(d, n.j, n.ie));
+  const float cw = ld(c, b + idx2(d, n.j, n.iw));
+  const float w0 = wetf(wb(d, n.j, n.i), k), we = wetf(wb(d, n.j, n.ie), k), ww = wetf(wb(d, n.j, n.iw), k);
+  float kc = 1.f, ke = 1.f, kw = 1.f, kn = 1.f, ks = 1.f;
+  if (kap) {
+    kc = __ldg(kap + idx2(d, n.j, n.i));
+    ke = __ldg(kap + idx2(d, n.j, n.ie));
+    kw = __ldg(kap + idx2(d, n.j, n.iw));
+    kn = __ldg(kap + idx2(d, n.jn, n.i));
+    ks = __ldg(kap + idx2(d, n.js, n.i));
+  }
+  const float fe = 0.5f * (kc + ke) * (ce - c0) * __ldg(d.inv_dx + idx2(d, n.j, n.i)) * w0 * we;
+  const float fw = 0.5f * (kw + kc) * (c0 - cw) * __ldg(d.inv_dx + idx2(d, n.j, n.iw)) * ww * w0;
+  float fn = 0.f, fs = 0.f;
+  if (n.j < d.ny - 1) {
+    const float cn = ld(c, b + idx2(d, n.jn, n.i));
+    const float wn = wetf(wb(d, n.jn, n.i), k);
+    fn = 0.5f * (kc + kn) * (cn - c0) * d.inv_dy * w0 * wn * __ldg(d.cfp + n.j);
+  }
+  if (n.j > 0) {
+    const float cs = ld(c, b + idx2(d, n.js, n.i));
+    const float ws = wetf(wb(d, n.js, n.i), k);
+    fs = 0.5f * (ks + kc) * (c0 - cs) * d.inv_dy * ws * w0 * __ldg(d.cfp + n.js);
+  }
+  return (fe - fw) * __ldg(d.inv_dx + idx2(d, n.j, n.i)) + (fn - fs) * d.inv_dy * __ldg(d.inv_cos + n.j);
+}
+
+// Ghost-filled value of a column at level k (numerics/vertical.py:122-135).
+__device__ __forceinline__ float colv(const float* __restrict__ a, long long base, long long plane, int k, int kb) {
+  return ld(a, base + (long long)(k < kb ? k : kb) * plane);
+}
+
+// Node-form d2/dz2 with zero-flux ends on the ghost-filled column
+// (numerics/vertical.py:275-293).
+__device__ __forceinline__ float d2z(const Dev& d, const float* __restrict__ a, long long base, int k, int kb) {
+  if (k == 0) {
+    if (d.nz < 2) return 0.f;
+    return d.vc.d2_top * (colv(a, base, d.plane, 1, kb) - colv(a, base, d.plane, 0, kb));
+  }
+  if (k == d.nz - 1)
+    return d.vc.d2_bot * (colv(a, base, d.plane, k - 1, kb) - colv(a, base, d.plane, k, kb));
+  const float a0 = colv(a, base, d.plane, k, kb);
+  return d.vc.d2_hi[k] * (colv(a, base, d.plane, k + 1, kb) - a0) +
+         d.vc.d2_lo[k] * (colv(a, base, d.plane, k - 1, kb) - a0);
+}
+
+// Interface-flux vertical diffusion (numerics/vertical.py:317-332), the
+// conservative_kv form.
+__device__ __forceinline__ float d2z_flux(const Dev& d, const float* __restrict__ a, long long base, int k,
+                                          uint64_t bits, float kappa) {
+  const int kb = kbot_of(bits);
+  float up = 0.f, dn = 0.f;
+  if (k > 0 && wetb(bits, k - 1) && wetb(bits, k))
+    up = -kappa * (colv(a, base, d.plane, k, kb) - colv(a, base, d.plane, k - 1, kb)) * d.vc.inv_dz_iface[k - 1];
+  if (k < d.nz - 1 && wetb(bits, k) && wetb(bits, k + 1))
+    dn = -kappa * (colv(a, base, d.plane, k + 1, kb) - colv(a, base, d.plane, k, kb)) * d.vc.inv_dz_iface[k];
+  return (up - dn) * d.vc.inv_dz_node[k] * wetf(bits, k);
+}
+
+__device__ __forceinline__ float vdiff_tracer(const Dev& d, const float* __restrict__ a, long long base, int k,
+                                              uint64_t bits, float kv) {
+  if (d.conservative_kv) return d2z_flux(d, a, base, k, bits, kv);
+  return kv * d2z(d, a, base, k, kbot_of(bits));
+}
+
+#define ZM_POINT_IDX                                   \
+  const int i = blockIdx.x * blockDim.x + threadIdx.x; \
+  const int j = blockIdx.y * blockDim.y + threadIdx.y; \
+  const int k = blockIdx.z;                            \
+  if (i >= d.nx || j >= d.ny) return;                  \
+  const long long id = idx3(d, k, j, i);
+
+// ------------------------------------------------------------------ L half step
+// One nu_h Laplacian subcycle on (u, v) (timestepping/step.py:94-107).
+__global__ void __launch_bounds__(256) k_nu_sub(Dev d, const float* __restrict__ u, const float* __restrict__ v,
+                                                float* __restrict__ uo, float* __restrict__ vo, float dts) {
+  ZM_POINT_IDX
+  const Nb n = nb(d, j, i);
+  uo[id] = ld(u, id) + d.nu_h * lap_h(d, u, k, n) * dts;
+  vo[id] = ld(v, id) + d.nu_h * lap_h(d, v, k, n) * dts;
+}
+
+// Inner Laplacians for the biharmonic operators: velocity (horizontal.py:251)
+// and the unit-diffusivity tracer flux operator (horizontal.py:245-249).
+__global__ void __launch_bounds__(256) k_inner_lap(Dev d, const float* __restrict__ u, const float* __restrict__ v,
+                                                   const float* __restrict__ T, const float* __restrict__ S,
+                                                   float* __restrict__ Lu, float* __restrict__ Lv,
+                                                   float* __restrict__ LT, float* __restrict__ LS, int do_uv, int do_ts) {
+  ZM_POINT_IDX
+  const Nb n = nb(d, j, i);
+  if (do_uv) {
+    Lu[id] = lap_h(d, u, k, n);
+    Lv[id] = lap_h(d, v, k, n);
+  }
+  if (do_ts) {
+    LT[id] = hdiff(d, T, nullptr, k, n);
+    LS[id] = hdiff(d, S, nullptr, k, n);
+  }
+}
+
+// Rest of the linear half step (timestepping/step.py:108-173, legacy,
+// mode split): biharmonic and vertical diffusion from the start-of-step
+// state, land/ghost hold, exact Coriolis rotation by f dt/2.
+__global__ void __launch_bounds__(256) k_lin_finish(Dev d, const float* __restrict__ usub, const float* __restrict__ vsub,
+                                                    const float* __restrict__ u0, const float* __restrict__ v0,
+                                                    const float* __restrict__ T0, const float* __restrict__ S0,
+                                                    const float* __restrict__ Lu, const float* __restrict__ Lv,
+                                                    const float* __restrict__ LT, const float* __restrict__ LS,
+                                                    float* __restrict__ uo, float* __restrict__ vo,
+                                                    float* __restrict__ To, float* __restrict__ So, float dth,
+                                                    int implicit_v) {
+  ZM_POINT_IDX
+  const Nb n = nb(d, j, i);
+  const uint64_t bits = wb(d, j, i);
+  const int kb = kbot_of(bits);
+  const long long base = idx2(d, j, i);
+  const bool wet = wetb(bits, k);
+  const float kv = __ldg(d.kv2 + base);
+  // tracers
+  float T = ld(T0, id) + hdiff(d, T0, d.kh2, k, n) * dth;
+  float S = ld(S0, id) + hdiff(d, S0, d.kh2, k, n) * dth;
+  if (d.kappa_bi > 0.f) {
+    T = T - d.kappa_bi * hdiff(d, LT, nullptr, k, n) * dth;
+    S = S - d.kappa_bi * hdiff(d, LS, nullptr, k, n) * dth;
+  }
+  float u = ld(usub, id), v = ld(vsub, id);
+  if (d.nu_bi > 0.f) {
+    u = u - d.nu_bi * lap_h(d, Lu, k, n) * dth;
+    v = v - d.nu_bi * lap_h(d, Lv, k, n) * dth;
+  }
+  if (!implicit_v) {
+    u = u + d.nu_v * d2z(d, u0, base, k, kb) * dth;
+    v = v + d.nu_v * d2z(d, v0, base, k, kb) * dth;
+    T = T + vdiff_tracer(d, T0, base, k, bits, kv) * dth;
+    S = S + vdiff_tracer(d, S0, base, k, bits, kv) * dth;
+  }
+  if (!wet) {
+    u = ld(u0, id);
+    v = ld(v0, id);
+    T = ld(T0, id);
+    S = ld(S0, id);
+  }
+  To[id] = T;
+  So[id] = S;
+  if (implicit_v) {  // rotation happens after the column solve
+    uo[id] = u;
+    vo[id] = v;
+    return;
+  }
+  const float c = __ldg(d.rot_c + base), s = __ldg(d.rot_s + base);
+  uo[id] = c * u + s * v;
+  vo[id] = -s * u + c * v;
+}
+
+// Backward-Euler vertical diffusion, one column per thread (extension: the
+// implicit replacement of the explicit L-step vertical diffusion).  The
+// matrix is (I - s D2) with D2 the node-form operator of d2z on the wet
+// levels 0..kbot (ghost fill below); Thomas algorithm in FP32 plus one step of
+// iterative refinement, residual formed in FP32 against the original
+// right-hand side.  Rows below the deepest wet level are untouched.
+__device__ __forceinline__ void vcoef(const Dev& d, int k, int kb, float s, float& a, float& b, float& c) {
+  a = 0.f; c = 0.f; b = 1.f;
+  if (k == 0) { b += s * d.vc.d2_top; c = -s * d.vc.d2_top; return; }
+  if (k == d.nz - 1) { a = -s * d.vc.d2_bot; b += s * d.vc.d2_bot; return; }
+  a = -s * d.vc.d2_lo[k];
+  b += s * (d.vc.d2_lo[k] + d.vc.d2_hi[k]);
+  if (k < kb) c = -s * d.vc.d2_hi[k]; else b -= s * d.vc.d2_hi[k];
+}
+
+__device__ void thomas(const Dev& d, int n, int kb, float s, const float* rhs, float* x, float* cp) {
+  float a, b, c;
+  vcoef(d, 0, kb, s, a, b, c);
+  float inv = 1.f / b;
+  cp[0] = c * inv;
+  x[0] = rhs[0] * inv;
+  for (int k = 1; k < n; ++k) {
+    vcoef(d, k, kb, s, a, b, c);
+    inv = 1.f / (b - a * cp[k - 1]);
+    cp[k] = c * inv;
+    x[k] = (rhs[k] - a * x[k - 1]) * inv;
+  }
+  for (int k = n - 2; k >= 0; --k) x[k] -= cp[k] * x[k + 1];
+}
+
+__device__ void implicit_column(const Dev& d, float* __restrict__ f, long long base, uint64_t bits, float s) {
+  const int kb = kbot_of(bits);
+  if (kb == 0) return;  // a single wet node: the zero-flux operator vanishes
+  const int n = kb + 1;
+  float rhs[ZM_MAXZ], x[ZM_MAXZ], e[ZM_MAXZ], cp[ZM_MAXZ];
+  for (int k = 0; k < n; ++k) rhs[k] = f[base + (long long)k * d.plane];
+  thomas(d, n, kb, s, rhs, x, cp);
+  for (int k = 0; k < n; ++k) {  // residual of the FP32 solution
+    float a, b, c;
+    vcoef(d, k, kb, s, a, b, c);
+    float ax = b * x[k];
+    if (k > 0) ax += a * x[k - 1];
+    if (k + 1 < n) ax += c * x[k + 1];
+    e[k] = rhs[k] - ax;
+  }
+  thomas(d, n, kb, s, e, rhs, cp);
+  for (int k = 0; k < n; ++k) f[base + (long long)k * d.plane] = x[k] + rhs[k];
+}
+
+__global__ void __launch_bounds__(128) k_implicit_vdiff(Dev d, float* __restrict__ u, float* __restrict__ v,
+                                                        float* __restrict__ T, float* __restrict__ S,
+                                                        const float* __restrict__ u0, const float* __restrict__ v0,
+                                                        const float* __restrict__ T0, const float* __restrict__ S0,
+                                                        float dth) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= d.nx || j >= d.ny) return;
+  const long long base = idx2(d, j, i);
+  const uint64_t bits = wb(d, j, i);
+  implicit_column(d, u, base, bits, d.nu_v * dth);
+  implicit_column(d, v, base, bits, d.nu_v * dth);
+  const float kv = __ldg(d.kv2 + base);
+  implicit_column(d, T, base, bits, kv * dth);
+  implicit_column(d, S, base, bits, kv * dth);
+  // land/ghost hold, then the exact Coriolis rotation
+  const float c = __ldg(d.rot_c + base), s = __ldg(d.rot_s + base);
+  for (int k = 0; k < d.nz; ++k) {
+    const long long id = base + (long long)k * d.plane;
+    float uu = u[id], vv = v[id];
+    if (!wetb(bits, k)) {
+      uu = ld(u0, id); vv = ld(v0, id);
+      T[id] = ld(T0, id); S[id] = ld(S0, id);
+    }
+    u[id] = c * uu + s * vv;
+    v[id] = -s * uu + c * vv;
+  }
+}
+
+// ------------------------------------------------------------------ transport
+// Interface volume transport Fz[k] = sum_{m>=k} div_h[m] dz_node[m]
+// (dynamics/transport.py:110-133 with the face-flux divergence of
+// numerics/horizontal.py:255-281); Fz[nz] = 0 is implicit.
+__global__ void __launch_bounds__(128) k_fz(Dev d, const float* __restrict__ u, const float* __restrict__ v,
+                                            float* __restrict__ Fz) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= d.nx || j >= d.ny) return;
+  const Nb n = nb(d, j, i);
+  const uint64_t m0 = wb(d, j, i), me = wb(d, j, n.ie), mw = wb(d, j, n.iw);
+  const uint64_t mn = wb(d, n.jn, i), ms = wb(d, n.js, i);
+  const float idx_c = __ldg(d.inv_dx + idx2(d, j, i));
+  const float cf_n = __ldg(d.cfp + j), cf_s = j > 0 ? __ldg(d.cfp + j - 1) : 0.f;
+  const float yscale = d.inv_dy * __ldg(d.inv_cos + j);
+  float acc = 0.f;
+  for (int k = d.nz - 1; k >= 0; --k) {
+    const long long b = (long long)k * d.plane;
+    const float uc = ld(u, b + idx2(d, j, i)), ue = ld(u, b + idx2(d, j, n.ie)), uw = ld(u, b + idx2(d, j, n.iw));
+    const float w0 = wetf(m0, k);
+    const float fxe = 0.5f * (uc + ue) * w0 * wetf(me, k);
+    const float fxw = 0.5f * (uw + uc) * wetf(mw, k) * w0;
+    float fyn = 0.f, fys = 0.f;
+    const float vc = ld(v, b + idx2(d, j, i));
+    if (j < d.ny - 1) fyn = 0.5f * (vc + ld(v, b + idx2(d, n.jn, i))) * w0 * wetf(mn, k) * cf_n;
+    if (j > 0) fys = 0.5f * (ld(v, b + idx2(d, n.js, i)) + vc) * wetf(ms, k) * w0 * cf_s;
+    const float div = (fxe - fxw) * idx_c + (fyn - fys) * yscale;
+    acc += div * d.vc.dz_node[k];
+    Fz[b + idx2(d, j, i)] = acc;
+  }
+}
+
+// Raw advective-form momentum advection -(u d/dx + v d/dy + w d/dz) of u and
+// v (dynamics/transport.py:169-197 before its filter) with the latitude half
+// of the dealias filter, [1,4,6,4,1]/16 on edge-held rows
+// (numerics/horizontal.py:283-305).  The longitude 2/3-rule half runs in the
+// FFT kernel; the two filters act on different axes and commute.
+constexpr int MADV_TY = 8;
+__device__ __forceinline__ void adv_point(const Dev& d, const float* __restrict__ u, const float* __restrict__ v,
+                                          const float* __restrict__ Fz, int k, int j, int i, float& au, float& av) {
+  const Nb n = nb(d, j, i);
+  const long long b = (long long)k * d.plane;
+  const uint64_t m0 = wb(d, j, i);
+  const float w0 = wetf(m0, k);
+  if (w0 == 0.f) { au = 0.f; av = 0.f; return; }
+  const float we = wetf(wb(d, j, n.ie), k), ww = wetf(wb(d, j, n.iw), k);
+  const float wn = wetf(wb(d, n.jn, i), k), ws = wetf(wb(d, n.js, i), k);
+  const long long c = b + idx2(d, j, i);
+  const float uc = ld(u, c), vc = ld(v, c);
+  const float ue = ld(u, b + idx2(d, j, n.ie)), uw = ld(u, b + idx2(d, j, n.iw));
+  const float un = ld(u, b + idx2(d, n.jn, i)), us = ld(u, b + idx2(d, n.js, i));
+  const float ve = ld(v, b + idx2(d, j, n.ie)), vw = ld(v, b + idx2(d, j, n.iw));
+  const float vn = ld(v, b + idx2(d, n.jn, i)), vs = ld(v, b + idx2(d, n.js, i));
+  const float hx = __ldg(d.inv_dx + idx2(d, j, i)) * 0.5f, hy = d.inv_dy * 0.5f;
+  const float dudx = hx * ((ue - uc) * w0 * we + (uc - uw) * w0 * ww);
+  const float dvdx = hx * ((ve - vc) * w0 * we + (vc - vw) * w0 * ww);
+  const float dudy = hy * ((un - uc) * wn * w0 + (uc - us) * w0 * ws);
+  const float dvdy = hy * ((vn - vc) * wn * w0 + (vc - vs) * w0 * ws);
+  // d/dz of the ghost-filled column (numerics/vertical.py:267-272)
+  const int kb = kbot_of(m0);
+  const long long base = idx2(d, j, i);
+  float dudz, dvdz;
+  if (k == 0) {
+    const float inv = d.vc.ddz_inv[0];
+    dudz = (colv(u, base, d.plane, 1, kb) - colv(u, base, d.plane, 0, kb)) * inv;
+    dvdz = (colv(v, base, d.plane, 1, kb) - colv(v, base, d.plane, 0, kb)) * inv;
+  } else if (k == d.nz - 1) {
+    const float inv = d.vc.ddz_inv[k];
+    dudz = (colv(u, base, d.plane, k, kb) - colv(u, base, d.plane, k - 1, kb)) * inv;
+    dvdz = (colv(v, base, d.plane, k, kb) - colv(v, base, d.plane, k - 1, kb)) * inv;
+  } else {
+    const float inv = d.vc.ddz_inv[k];
+    dudz = (colv(u, base, d.plane, k + 1, kb) - colv(u, base, d.plane, k - 1, kb)) * inv;
+    dvdz = (colv(v, base, d.plane, k + 1, kb) - colv(v, base, d.plane, k - 1, kb)) * inv;
+  }
+  const float w = -ld(Fz, c) * w0;  // dynamics/transport.py:149-166
+  au = -(uc * dudx + vc * dudy + w * dudz);
+  av = -(uc * dvdx + vc * dvdy + w * dvdz);
+}
+
+__global__ void __launch_bounds__(256) k_madv(Dev d, const float* __restrict__ u, const float* __restrict__ v,
+                                              const float* __restrict__ Fz, float* __restrict__ Ayu,
+                                              float* __restrict__ Ayv) {
+  __shared__ float su[MADV_TY + 4][32];
+  __shared__ float sv[MADV_TY + 4][32];
+  const int i = blockIdx.x * 32 + threadIdx.x;
+  const int j0 = blockIdx.y * MADV_TY;
+  const int k = blockIdx.z;
+  for (int r = threadIdx.y; r < MADV_TY + 4; r += blockDim.y) {
+    int jj = j0 - 2 + r;
+    jj = jj < 0 ? 0 : (jj >= d.ny ? d.ny - 1 : jj);
+    float au = 0.f, av = 0.f;
+    if (i < d.nx) adv_point(d, u, v, Fz, k, jj, i, au, av);
+    su[r][threadIdx.x] = au;
+    sv[r][threadIdx.x] = av;
+  }
+  __syncthreads();
+  const int j = j0 + threadIdx.y;
+  if (i >= d.nx || j >= d.ny) return;
+  // rows j-2..j+2 clamped to the domain: with the tile loaded on clamped rows
+  // the clamp is already applied at the tile edges except inside the tile.
+  auto row = [&](int jj) { jj = jj < 0 ? 0 : (jj >= d.ny ? d.ny - 1 : jj); return jj - (j0 - 2); };
+  const int t = threadIdx.x;
+  const float fu = (su[row(j - 2)][t] + 4.f * su[row(j - 1)][t] + 6.f * su[row(j)][t] + 4.f * su[row(j + 1)][t] +
+                    su[row(j + 2)][t]) / 16.f;
+  const float fv = (sv[row(j - 2)][t] + 4.f * sv[row(j - 1)][t] + 6.f * sv[row(j)][t] + 4.f * sv[row(j + 1)][t] +
+                    sv[row(j + 2)][t]) / 16.f;
+  const long long id = idx3(d, k, j, i);
+  Ayu[id] = fu;
+  Ayv[id] = fv;
+}
+
+// Minmod slope over wet neighbours (dynamics/transport.py:199-213).
+__device__ __forceinline__ float minmod_slope(float cm, float c0, float cp, float wm, float w0, float wp) {
+  const float l = c0 - cm, r = cp - c0;
+  const float sg = (float)((l > 0.f) - (l < 0.f)) + (float)((r > 0.f) - (r < 0.f));
+  return 0.5f * sg * fminf(fabsf(l), fabsf(r)) * w0 * wm * wp;
+}
+
+// Zonal tracer flux through face i+1/2 (dynamics/transport.py:224-290).
+__device__ __forceinline__ float flux_x(const Dev& d, const float* __restrict__ c, const float* __restrict__ u,
+                                        long long b, int k, int j, int i) {
+  const int ie = east(d, i);
+  const float w0 = wetf(wb(d, j, i), k), we = wetf(wb(d, j, ie), k);
+  const float gate = w0 * we;
+  const float ux = 0.5f * (ld(u, b + idx2(d, j, i)) + ld(u, b + idx2(d, j, ie)));
+  const float c0 = ld(c, b + idx2(d, j, i)), ce = ld(c, b + idx2(d, j, ie));
+  float cf;
+  if (d.limiter == 2) {
+    if (ux >= 0.f) {
+      const int iw = west(d, i);
+      const float sx = minmod_slope(ld(c, b + idx2(d, j, iw)), c0, ce, wetf(wb(d, j, iw), k), w0, we);
+      cf = c0 + 0.5f * sx;
+    } else {
+      const int iee = east(d, ie);
+      const float sx = minmod_slope(c0, ce, ld(c, b + idx2(d, j, iee)), w0, we, wetf(wb(d, j, iee), k));
+      cf = ce - 0.5f * sx;
+    }
+  } else if (d.limiter == 1) {
+    cf = ux >= 0.f ? c0 : ce;
+  } else {
+    cf = 0.5f * (c0 + ce);
+  }
+  return ux * cf * gate;
+}
+
+// Meridional tracer flux through face j+1/2 (closed at the north wall).
+__device__ __forceinline__ float flux_y(const Dev& d, const float* __restrict__ c, const float* __restrict__ v,
+                                        long long b, int k, int j, int i) {
+  if (j >= d.ny - 1) return 0.f;
+  const int jn = j + 1;
+  const float w0 = wetf(wb(d, j, i), k), wn = wetf(wb(d, jn, i), k);
+  const float vy = 0.5f * (ld(v, b + idx2(d, j, i)) + ld(v, b + idx2(d, jn, i)));
+  const float c0 = ld(c, b + idx2(d, j, i)), cn = ld(c, b + idx2(d, jn, i));
+  float cf;
+  if (d.limiter == 2) {
+    if (vy >= 0.f) {
+      const int js = south(j);
+      const float sy = minmod_slope(ld(c, b + idx2(d, js, i)), c0, cn, wetf(wb(d, js, i), k), w0, wn);
+      cf = c0 + 0.5f * sy;
+    } else {
+      const int jnn = north(d, jn);
+      const float sy = minmod_slope(c0, cn, ld(c, b + idx2(d, jnn, i)), w0, wn, wetf(wb(d, jnn, i), k));
+      cf = cn - 0.5f * sy;
+    }
+  } else if (d.limiter == 1) {
+    cf = vy >= 0.f ? c0 : cn;
+  } else {
+    cf = 0.5f * (c0 + cn);
+  }
+  return vy * cf * (w0 * wn) * __ldg(d.cfp + j);
+}
+
+// Flux-form tracer advection tendency (dynamics/transport.py:365-475, legacy
+// donor-cell vertical flux with the rigid-lid top flux Fz[0] c[0]).
+__device__ __forceinline__ float tracer_adv(const Dev& d, const float* __restrict__ c, const float* __restrict__ u,
+                                            const float* __restrict__ v, const float* __restrict__ Fz, int k, int j,
+                                            int i, uint64_t bits) {
+  const float w0 = wetf(bits, k);
+  if (w0 == 0.f) return 0.f;
+  const long long b = (long long)k * d.plane;
+  const float fxe = flux_x(d, c, u, b, k, j, i);
+  const float fxw = flux_x(d, c, u, b, k, j, west(d, i));
+  const float fyn = flux_y(d, c, v, b, k, j, i);
+  const float fys = j > 0 ? flux_y(d, c, v, b, k, j - 1, i) : 0.f;
+  const float hdiv = (fxe - fxw) * __ldg(d.inv_dx + idx2(d, j, i)) + (fyn - fys) * d.inv_dy * __ldg(d.inv_cos + j);
+  const long long base = idx2(d, j, i);
+  const int kb = kbot_of(bits);
+  const float ck = ld(c, base + b);
+  float up, dn = 0.f;
+  const float fz_k = ld(Fz, base + b);
+  if (k == 0) {
+    up = fz_k * ck;
+  } else {
+    const float donor = fz_k > 0.f ? ld(c, base + b - d.plane) : ck;  // k <= kb here since node k is wet
+    up = fz_k * donor * (wetf(bits, k - 1) * w0);
+  }
+  if (k < d.nz - 1) {
+    const float fz_n = ld(Fz, base + b + d.plane);
+    const float donor = fz_n > 0.f ? ck : colv(c, base, d.plane, k + 1, kb);
+    dn = fz_n * donor * (w0 * wetf(bits, k + 1));
+  }
+  return -(hdiv + (dn - up) * d.vc.inv_dz_node[k]) * w0;
+}
+
+// One advection substep of T and S with frozen (u, v, Fz)
+// (dynamics/tendencies.py:111-140): accumulates the rate and advances the
+// substep state.
+__global__ void __launch_bounds__(256) k_tracer_adv(Dev d, const float* __restrict__ T, const float* __restrict__ S,
+                                                    const float* __restrict__ u, const float* __restrict__ v,
+                                                    const float* __restrict__ Fz, float* __restrict__ accT,
+                                                    float* __restrict__ accS, float* __restrict__ Tn,
+                                                    float* __restrict__ Sn, float dts, int first, int last) {
+  ZM_POINT_IDX
+  const uint64_t bits = wb(d, j, i);
+  const float aT = tracer_adv(d, T, u, v, Fz, k, j, i, bits);
+  const float aS = tracer_adv(d, S, u, v, Fz, k, j, i, bits);
+  accT[id] = first ? aT : accT[id] + aT;
+  accS[id] = first ? aS : accS[id] + aS;
+  if (!last) {
+    Tn[id] = ld(T, id) + aT * dts;
+    Sn[id] = ld(S, id) + aS * dts;
+  }
+}
+
+// Tracer residual of the N step (dynamics/tendencies.py:94-245) without the
+// diffusion pair that the residual adds and removes again: mean advection
+// rate + interface-flux convective mixing (physics/vertical.py:13-37, 63-82)
+// + surface sources at k = 0.  One column per thread.
+//   stage 1: dT1 = r(T1), Tp = T1 + dt dT1
+//   stage 2: T2 = T1 + dt (dT1 + r(Tp)) / 2
+
+
+__device__ __forceinline__ void rest_store(const Dev& d, const RestArgs& a, long long id, long long base, int k,
+                                           float w, float rT, float rS) {
+  if (k == 0) {  // surface sources (dynamics/tendencies.py:167-207, physics/surface.py:8-20)
+    const float sst = ld(a.Tev, id), sss = ld(a.Sev, id);
+    const float hf = w / (d.dz_surface * kRho0 * kCp);
+    const float tatm = __ldg(d.tatm + base);
+    rT += __ldg(d.qheat + base) * hf + d.lambda_bulk * (tatm - sst) * hf + __ldg(d.cbulk + base) * (tatm - sst) * hf +
+          __ldg(d.rest_c + base) * (__ldg(d.rest_T + base) - sst);
+    rS += d.restore_S * (__ldg(d.sref + base) - sss) + (sst <= d.ice_freeze ? d.ice_salt : 0.f);
+  }
+  rT *= w;
+  rS *= w;
+  if (a.stage == 1) {
+    a.dT1[id] = rT;
+    a.dS1[id] = rS;
+    a.To[id] = ld(a.Tbase, id) + rT * a.dt;
+    a.So[id] = ld(a.Sbase, id) + rS * a.dt;
+  } else {
+    a.To[id] = ld(a.Tbase, id) + 0.5f * (ld(a.dT1, id) + rT) * a.dt;
+    a.So[id] = ld(a.Sbase, id) + 0.5f * (ld(a.dS1, id) + rS) * a.dt;
+  }
+}
+
+__global__ void __launch_bounds__(128) k_tracer_rest(Dev d, RestArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= d.nx || j >= d.ny) return;
+  const long long base = idx2(d, j, i);
+  const uint64_t bits = wb(d, j, i);
+  const int nz = d.nz;
+  // static-instability gates of the evaluation state, in difference form:
+  // rho[m] > rho[m+1]  <=>  beta (S[m]-S[m+1]) > alpha (T[m]-T[m+1]).
+  uint64_t unstable = 0ull, wetpair = 0ull;
+  float Tu = ld(a.Tev, base), Su = ld(a.Sev, base);
+  for (int m = 0; m + 1 < nz; ++m) {
+    const long long idn = base + (long long)(m + 1) * d.plane;
+    const float Tl = ld(a.Tev, idn), Sl = ld(a.Sev, idn);
+    if (wetb(bits, m) && wetb(bits, m + 1)) {
+      wetpair |= 1ull << m;
+      if (kBeta * (Su - Sl) > kAlpha * (Tu - Tl)) unstable |= 1ull << m;
+    }
+    Tu = Tl;
+    Su = Sl;
+  }
+  uint64_t allow = 0ull;
+  if (unstable && d.kappa_conv > 0.f) allow = d.localize_conv ? unstable : wetpair;
+  if (a.nc == 1 || allow == 0ull) {
+    const float kc = d.kappa_conv;
+    float fT = 0.f, fS = 0.f;
+    float cT = ld(a.Tev, base), cS = ld(a.Sev, base);
+    for (int k = 0; k < nz; ++k) {
+      const long long id = base + (long long)k * d.plane;
+      float nT = 0.f, nS = 0.f, gT = 0.f, gS = 0.f;
+      if (k + 1 < nz) {
+        nT = ld(a.Tev, id + d.plane);
+        nS = ld(a.Sev, id + d.plane);
+        if ((allow >> k) & 1ull) {
+          gT = -kc * (nT - cT) * d.vc.inv_dz_iface[k];
+          gS = -kc * (nS - cS) * d.vc.inv_dz_iface[k];
+        }
+      }
+      const float w = wetf(bits, k);
+      const float convT = (fT - gT) * d.vc.inv_dz_node[k] * w;
+      const float convS = (fS - gS) * d.vc.inv_dz_node[k] * w;
+      rest_store(d, a, id, base, k, w, ld(a.accT, id) * a.inv_na + convT, ld(a.accS, id) * a.inv_na + convS);
+      fT = gT; fS = gS; cT = nT; cS = nS;
+    }
+    return;
+  }
+  // several convective substeps (legacy: kappa and time both divided by nc)
+  float cT[ZM_MAXZ], cS[ZM_MAXZ], sT[ZM_MAXZ], sS[ZM_MAXZ];
+  for (int k = 0; k < nz; ++k) {
+    cT[k] = ld(a.Tev, base + (long long)k * d.plane);
+    cS[k] = ld(a.Sev, base + (long long)k * d.plane);
+    sT[k] = 0.f;
+    sS[k] = 0.f;
+  }
+  const float kc = d.kappa_conv / a.nc;
+  const float hc = a.dt / a.nc;
+  for (int s = 0; s < a.nc; ++s) {
+    float fT = 0.f, fS = 0.f;
+    for (int k = 0; k < nz; ++k) {
+      float gT = 0.f, gS = 0.f;
+      if (k + 1 < nz && ((allow >> k) & 1ull)) {
+        gT = -kc * (cT[k + 1] - cT[k]) * d.vc.inv_dz_iface[k];
+        gS = -kc * (cS[k + 1] - cS[k]) * d.vc.inv_dz_iface[k];
+      }
+      const float w = wetf(bits, k);
+      const float tT = (fT - gT) * d.vc.inv_dz_node[k] * w;
+      const float tS = (fS - gS) * d.vc.inv_dz_node[k] * w;
+      sT[k] += tT;
+      sS[k] += tS;
+      fT = gT;
+      fS = gS;
+      // node k is not read again in this substep: the flux below it used the
+      // pre-update values of k and k+1.
+      cT[k] += tT * hc;
+      cS[k] += tS * hc;
+    }
+  }
+  const float inv_nc = 1.f / (float)a.nc;
+  for (int k = 0; k < nz; ++k) {
+    const long long id = base + (long long)k * d.plane;
+    rest_store(d, a, id, base, k, wetf(bits, k), ld(a.accT, id) * a.inv_na + sT[k] * inv_nc,
+               ld(a.accS, id) * a.inv_na + sS[k] * inv_nc);
+  }
+}
+
+// ------------------------------------------------------------------ pressure
+// Baroclinic pressure-gradient force and its barotropic (layer-averaged)
+// part, one column per thread (dynamics/pressure.py:32-42, 86-97, 144-180).
+// The horizontal pressure differences p[e]-p[c] are accumulated down the
+// column from the density differences (the same trapezoid sums as
+// differencing the integrated pressure, with less cancellation in FP32).
+//   mode 0: F_rho and the barotropic velocity (ubt0, vbt0; transport.py:135-143)
+//   mode 1: P = wm (pgf - F_rho); up = u1 + dt (A + P)
+//   mode 2: u2 = (u1 + dt/2 ((A + Pp) + (A + P))) * exp(-r_bot dt) at k = nz-1
+
+
+__device__ __forceinline__ float drho(const Dev& d, float Ta, float Sa, float wa, float Tb, float Sb, float wb_) {
+  // rho'(a) wa - rho'(b) wb in difference form when both are wet
+  if (wa != 0.f && wb_ != 0.f) return kRho0 * (-kAlpha * (Ta - Tb) + kBeta * (Sa - Sb));
+  return rho_anom(Ta, Sa) * wa - rho_anom(Tb, Sb) * wb_;
+}
+
+__global__ void __launch_bounds__(128) k_pgf(Dev d, PgfArgs a) {
+  extern __shared__ float smem[];
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const int nt = blockDim.x * blockDim.y;
+  float* gxs = smem;
+  float* gys = smem + d.nz * nt;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= d.nx || j >= d.ny) return;
+  const Nb n = nb(d, j, i);
+  const uint64_t m0 = wb(d, j, i), me = wb(d, j, n.ie), mw = wb(d, j, n.iw), mn = wb(d, n.jn, i),
+                 ms = wb(d, n.js, i);
+  const long long cc = idx2(d, j, i), ce = idx2(d, j, n.ie), cw = idx2(d, j, n.iw), cn = idx2(d, n.jn, i),
+                  cs = idx2(d, n.js, i);
+  const float hx = __ldg(d.inv_dx + cc) * 0.5f;
+  const float hy = d.inv_dy * __ldg(d.inv_cos + j) * 0.5f;
+  const float cfp = __ldg(d.cfp + j), cfm = __ldg(d.cfm + j);
+  const bool has_n = j < d.ny - 1, has_s = j > 0;
+  float pe = 0.f, pw = 0.f, pn = 0.f, ps = 0.f;       // p[e]-p[c], p[c]-p[w], p[n]-p[c], p[c]-p[s]
+  float de0 = 0.f, dw0 = 0.f, dn0 = 0.f, ds0 = 0.f;   // density differences at the level above
+  float gx_prev = 0.f, gy_prev = 0.f, fx = 0.f, fy = 0.f;
+  for (int k = 0; k < d.nz; ++k) {
+    const long long b = (long long)k * d.plane;
+    const float w0 = wetf(m0, k), we = wetf(me, k), ww = wetf(mw, k), wn = wetf(mn, k), ws = wetf(ms, k);
+    const float Tc = ld(a.T, b + cc), Sc = ld(a.S, b + cc);
+    const float de = drho(d, ld(a.T, b + ce), ld(a.S, b + ce), we, Tc, Sc, w0);
+    const float dw = drho(d, Tc, Sc, w0, ld(a.T, b + cw), ld(a.S, b + cw), ww);
+    const float dn = drho(d, ld(a.T, b + cn), ld(a.S, b + cn), wn, Tc, Sc, w0);
+    const float ds = drho(d, Tc, Sc, w0, ld(a.T, b + cs), ld(a.S, b + cs), ws);
+    if (k > 0) {
+      const float h = kG * 0.5f * d.vc.dz3d[k - 1];
+      pe += (de0 + de) * h;
+      pw += (dw0 + dw) * h;
+      pn += (dn0 + dn) * h;
+      ps += (ds0 + ds) * h;
+    }
+    de0 = de; dw0 = dw; dn0 = dn; ds0 = ds;
+    const float gx = hx * (pe * w0 * we + pw * w0 * ww);
+    const float gy = hy * ((has_n ? pn * w0 * wn : 0.f) * cfp + (has_s ? ps * w0 * ws : 0.f) * cfm);
+    if (k > 0) {
+      const float wif = wetf(m0, k - 1) * w0 * d.vc.dz3d[k - 1];
+      fx += 0.5f * (gx_prev + gx) * wif;
+      fy += 0.5f * (gy_prev + gy) * wif;
+    }
+    gx_prev = gx;
+    gy_prev = gy;
+    if (a.mode != 0) {
+      gxs[k * nt + tid] = -gx / kRho0;
+      gys[k * nt + tid] = -gy / kRho0;
+    }
+  }
+  const float Fx = -fx / (kRho0 * d.H_sw);
+  const float Fy = -fy / (kRho0 * d.H_sw);
+  if (a.mode == 0) {
+    a.frx[cc] = Fx;
+    a.fry[cc] = Fy;
+    double su = 0.0, sv = 0.0;
+    float u_prev = ld(a.u1, cc), v_prev = ld(a.v1, cc);
+    for (int k = 1; k < d.nz; ++k) {
+      const float uk = ld(a.u1, (long long)k * d.plane + cc), vk = ld(a.v1, (long long)k * d.plane + cc);
+      su += (double)(0.5f * (u_prev + uk) * d.vc.dznorm[k - 1]);
+      sv += (double)(0.5f * (v_prev + vk) * d.vc.dznorm[k - 1]);
+      u_prev = uk;
+      v_prev = vk;
+    }
+    a.ubt0[cc] = su;
+    a.vbt0[cc] = sv;
+    return;
+  }
+  for (int k = 0; k < d.nz; ++k) {
+    const long long id = (long long)k * d.plane + cc;
+    const float w = wetf(m0, k);
+    const float Pu = (gxs[k * nt + tid] - Fx) * w;
+    const float Pv = (gys[k * nt + tid] - Fy) * w;
+    const float Au = ld(a.Au, id), Av = ld(a.Av, id);
+    const float u1 = ld(a.u1, id), v1 = ld(a.v1, id);
+    if (a.mode == 1) {
+      a.Pu[id] = Pu;
+      a.Pv[id] = Pv;
+      a.uo[id] = u1 + (Au + Pu) * a.dt;
+      a.vo[id] = v1 + (Av + Pv) * a.dt;
+    } else {
+      const float dec = (k == d.nz - 1 && w != 0.f) ? a.bottom_decay : 1.f;
+      a.uo[id] = (u1 + 0.5f * ((Au + ld(a.Ppu, id)) + (Au + Pu)) * a.dt) * dec;
+      a.vo[id] = (v1 + 0.5f * ((Av + ld(a.Ppv, id)) + (Av + Pv)) * a.dt) * dec;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ barotropic mode (float64)
+// Free-surface continuity (dynamics/barotropic.py:129-145, 331-347):
+// eta <- (eta - dt H div(ubt wm, vbt wm)) wm with the flux-form divergence
+// of numerics/horizontal.py:69-97.
+__global__ void __launch_bounds__(256) k_bt_eta(Dev d, const double* __restrict__ eta, const double* __restrict__ ubt,
+                                                const double* __restrict__ vbt, double* __restrict__ eta_o,
+                                                double dtH) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= d.nx || j >= d.ny) return;
+  const Nb n = nb(d, j, i);
+  const int c = idx2(d, j, i);
+  const double w0 = __ldg(d.wet2 + c);
+  const double we = __ldg(d.wet2 + idx2(d, j, n.ie)), ww = __ldg(d.wet2 + idx2(d, j, n.iw));
+  const double u0 = ubt[c] * w0, ue = ubt[idx2(d, j, n.ie)] * we, uw = ubt[idx2(d, j, n.iw)] * ww;
+  const double fe = 0.5 * (u0 + ue) * (w0 * we);
+  const double fw = 0.5 * (uw + u0) * (ww * w0);
+  const double div_x = (fe - fw) * __ldg(d.inv_dx_d + c);
+  double fn = 0.0, fs = 0.0;
+  const double v0 = vbt[c] * w0;
+  if (j < d.ny - 1) {
+    const double wn = __ldg(d.wet2 + idx2(d, j + 1, i));
+    fn = 0.5 * (v0 + vbt[idx2(d, j + 1, i)] * wn) * (w0 * wn) * (double)__ldg(d.cfp + j);
+  }
+  if (j > 0) {
+    const double ws = __ldg(d.wet2 + idx2(d, j - 1, i));
+    fs = 0.5 * (vbt[idx2(d, j - 1, i)] * ws + v0) * (ws * w0) * (double)__ldg(d.cfp + j - 1);
+  }
+  const double div = div_x + (fn - fs) * d.inv_dy_d / (double)__ldg(d.cosl + j);
+  eta_o[c] = (eta[c] - dtH * div) * w0;
+}
+
+// Barotropic momentum (dynamics/barotropic.py:389-428, legacy): new-eta
+// pressure gradient (the adjoint gradient of numerics/horizontal.py:99-124),
+// forcing, backward-Euler Coriolis, implicit linear drag, wet mask.
+__global__ void __launch_bounds__(256) k_bt_vel(Dev d, const double* __restrict__ eta, const double* __restrict__ ubt,
+                                                const double* __restrict__ vbt, const double* __restrict__ Fx,
+                                                const double* __restrict__ Fy, double* __restrict__ ubt_o,
+                                                double* __restrict__ vbt_o, double dtb, double drag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= d.nx || j >= d.ny) return;
+  const Nb n = nb(d, j, i);
+  const int c = idx2(d, j, i);
+  const double w0 = __ldg(d.wet2 + c);
+  const double we = __ldg(d.wet2 + idx2(d, j, n.ie)), ww = __ldg(d.wet2 + idx2(d, j, n.iw));
+  const double e0 = eta[c];
+  const double gx = __ldg(d.inv_dx_d + c) * 0.5 *
+                    ((eta[idx2(d, j, n.ie)] - e0) * (w0 * we) + (e0 - eta[idx2(d, j, n.iw)]) * (w0 * ww));
+  double dyp = 0.0, dym = 0.0;
+  if (j < d.ny - 1) dyp = (eta[idx2(d, j + 1, i)] - e0) * (w0 * __ldg(d.wet2 + idx2(d, j + 1, i))) * (double)__ldg(d.cfp + j);
+  if (j > 0) dym = (e0 - eta[idx2(d, j - 1, i)]) * (w0 * __ldg(d.wet2 + idx2(d, j - 1, i))) * (double)__ldg(d.cfm + j);
+  const double gy = (d.inv_dy_d / (double)__ldg(d.cosl + j)) * 0.5 * (dyp + dym);
+  const double us = ubt[c] + dtb * (-9.81 * gx + Fx[c]);
+  const double vs = vbt[c] + dtb * (-9.81 * gy + Fy[c]);
+  const double fd = __ldg(d.fcor_d + c) * dtb;
+  const double den = 1.0 + fd * fd;
+  ubt_o[c] = (us + fd * vs) / den * drag * w0;
+  vbt_o[c] = (vs - fd * us) / den * drag * w0;
+}
+
+// Total barotropic forcing F_rho + tau / (rho0 H) in float64.
+__global__ void k_bt_forcing(Dev d, const float* __restrict__ frx, const float* __restrict__ fry,
+                             double* __restrict__ Fx, double* __restrict__ Fy, const float* __restrict__ eta32,
+                             double* __restrict__ eta64) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= d.nx || j >= d.ny) return;
+  const int c = idx2(d, j, i);
+  const double scale = 1.0 / (1025.0 * (double)d.H_sw);
+  Fx[c] = (double)frx[c] + (double)__ldg(d.tau_x + c) * scale;
+  Fy[c] = (double)fry[c] + (double)__ldg(d.tau_y + c) * scale;
+  eta64[c] = (double)eta32[c];
+}
+
+// Polar cap of 2-D float64 fields (numerics/horizontal.py:387-451, legacy
+// branch): one block per band row; wet-point zonal mean blended with the
+// pole-inward weight; band land points come back zero.
+__global__ void __launch_bounds__(256) k_cap2d(Dev d, double* f0, double* f1, const float* __restrict__ wts, int nb_rows) {
+  __shared__ double red[2][256];
+  const int r = blockIdx.x;          // 0..2*nb_rows-1
+  double* f = blockIdx.y == 0 ? f0 : f1;
+  if (!f) return;
+  const int j = r < nb_rows ? r : d.ny - 2 * nb_rows + r;
+  const float wt = r < nb_rows ? wts[r] : wts[2 * nb_rows - 1 - r];
+  double s = 0.0, cnt = 0.0;
+  for (int i = threadIdx.x; i < d.nx; i += blockDim.x) {
+    const double w = __ldg(d.wet2 + idx2(d, j, i));
+    s += f[idx2(d, j, i)] * w;
+    cnt += w;
+  }
+  red[0][threadIdx.x] = s;
+  red[1][threadIdx.x] = cnt;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      red[0][threadIdx.x] += red[0][threadIdx.x + o];
+      red[1][threadIdx.x] += red[1][threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  const double mean = red[0][0] / fmax(red[1][0], 1.0);
+  const double wb_ = (double)wt;
+  for (int i = threadIdx.x; i < d.nx; i += blockDim.x) {
+    const double w = __ldg(d.wet2 + idx2(d, j, i));
+    const double val = f[idx2(d, j, i)] * w;
+    f[idx2(d, j, i)] = wb_ * (mean * w) + (1.0 - wb_) * val;
+  }
+}
+
+// Wet-point zonal means of the band rows of the projected 3-D fields
+// (u + dubt, v + dvbt, T, S) for the final polar cap.
+__global__ void __launch_bounds__(256) k_cap3_means(Dev d, const float* __restrict__ u, const float* __restrict__ v,
+                                                    const float* __restrict__ T, const float* __restrict__ S,
+                                                    const double* __restrict__ ubt, const double* __restrict__ ubt0,
+                                                    const double* __restrict__ vbt, const double* __restrict__ vbt0,
+                                                    float* __restrict__ means, int nb_rows) {
+  __shared__ float red[5][256];
+  const int r = blockIdx.x;  // band row index
+  const int k = blockIdx.y;
+  const int j = r < nb_rows ? r : d.ny - 2 * nb_rows + r;
+  float s[4] = {0.f, 0.f, 0.f, 0.f}, cnt = 0.f;
+  for (int i = threadIdx.x; i < d.nx; i += blockDim.x) {
+    const int c = idx2(d, j, i);
+    const float w = wetf(wb(d, j, i), k);
+    const long long id = idx3(d, k, j, i);
+    s[0] += (ld(u, id) + (float)(ubt[c] - ubt0[c])) * w;
+    s[1] += (ld(v, id) + (float)(vbt[c] - vbt0[c])) * w;
+    s[2] += ld(T, id) * w;
+    s[3] += ld(S, id) * w;
+    cnt += w;
+  }
+  for (int q = 0; q < 4; ++q) red[q][threadIdx.x] = s[q];
+  red[4][threadIdx.x] = cnt;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+      for (int q = 0; q < 5; ++q) red[q][threadIdx.x] += red[q][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x < 4) {
+    const float c = fmaxf(red[4][0], 1.f);
+    means[((size_t)threadIdx.x * 2 * nb_rows + r) * d.nz + k] = red[threadIdx.x][0] / c;
+  }
+}
+
+// Uniform barotropic projection, polar cap, land/ghost hold and the no-flux
+// wall on v (timestepping/step.py:419-450).
+__global__ void __launch_bounds__(256) k_final(Dev d, const float* __restrict__ u3, const float* __restrict__ v3,
+                                               const float* __restrict__ T3, const float* __restrict__ S3,
+                                               const double* __restrict__ ubt, const double* __restrict__ ubt0,
+                                               const double* __restrict__ vbt, const double* __restrict__ vbt0,
+                                               const float* __restrict__ u0, const float* __restrict__ v0,
+                                               const float* __restrict__ T0, const float* __restrict__ S0,
+                                               const float* __restrict__ means, const float* __restrict__ wts,
+                                               int nb_rows, float* __restrict__ uo, float* __restrict__ vo,
+                                               float* __restrict__ To, float* __restrict__ So) {
+  ZM_POINT_IDX
+  const int c = idx2(d, j, i);
+  const bool wet = wetb(wb(d, j, i), k);
+  if (!wet) {
+    uo[id] = ld(u0, id);
+    vo[id] = (j == 0 || j == d.ny - 1) ? 0.f : ld(v0, id);
+    To[id] = ld(T0, id);
+    So[id] = ld(S0, id);
+    return;
+  }
+  float u = ld(u3, id) + (float)(ubt[c] - ubt0[c]);
+  float v = ld(v3, id) + (float)(vbt[c] - vbt0[c]);
+  float T = ld(T3, id), S = ld(S3, id);
+  int r = -1;
+  if (nb_rows > 0) {
+    if (j < nb_rows) r = j;
+    else if (j >= d.ny - nb_rows) r = j - (d.ny - 2 * nb_rows);
+  }
+  if (r >= 0) {
+    const float wt = r < nb_rows ? wts[r] : wts[2 * nb_rows - 1 - r];
+    const size_t stride = (size_t)2 * nb_rows * d.nz;
+    const size_t o = (size_t)r * d.nz + k;
+    u = wt * means[o] + (1.f - wt) * u;
+    v = wt * means[stride + o] + (1.f - wt) * v;
+    T = wt * means[2 * stride + o] + (1.f - wt) * T;
+    S = wt * means[3 * stride + o] + (1.f - wt) * S;
+  }
+  uo[id] = u;
+  vo[id] = (j == 0 || j == d.ny - 1) ? 0.f : v;
+  To[id] = T;
+  So[id] = S;
+}
+
+// ------------------------------------------------------------------ layout conversion
+// Reference layout (nx, ny, nz) C order  <->  internal [nz][ny][P].
+__global__ void k_ref_to_int3(Dev d, const float* __restrict__ src, float* __restrict__ dst, float offset) {
+  __shared__ float tile[32][33];
+  const int j = blockIdx.z;
+  const int i0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = i0 + r, k = k0 + threadIdx.x;
+    if (i < d.nx && k < d.nz) tile[r][threadIdx.x] = src[((long long)i * d.ny + j) * d.nz + k] - offset;
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int k = k0 + r, i = i0 + threadIdx.x;
+    if (i < d.nx && k < d.nz) dst[idx3(d, k, j, i)] = tile[threadIdx.x][r];
+  }
+}
+
+__global__ void k_int_to_ref3(Dev d, const float* __restrict__ src, float* __restrict__ dst, float offset) {
+  __shared__ float tile[32][33];
+  const int j = blockIdx.z;
+  const int i0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int k = k0 + r, i = i0 + threadIdx.x;
+    if (i < d.nx && k < d.nz) tile[r][threadIdx.x] = src[idx3(d, k, j, i)];
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = i0 + r, k = k0 + threadIdx.x;
+    if (i < d.nx && k < d.nz) dst[((long long)i * d.ny + j) * d.nz + k] = tile[threadIdx.x][r] + offset;
+  }
+}
+
+__global__ void k_ref_to_int2(Dev d, const float* __restrict__ src, float* __restrict__ dst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i < d.nx && j < d.ny) dst[idx2(d, j, i)] = src[(long long)i * d.ny + j];
+}
+
+__global__ void k_int_to_ref2(Dev d, const float* __restrict__ src, float* __restrict__ dst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i < d.nx && j < d.ny) dst[(long long)i * d.ny + j] = src[idx2(d, j, i)];
+}
+
+__global__ void k_eta_to_float(Dev d, const double* __restrict__ e64, float* __restrict__ e32) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i < d.nx && j < d.ny) e32[idx2(d, j, i)] = (float)e64[idx2(d, j, i)];
+}
+
+// ------------------------------------------------------------------ monitor
+// Device-side state classification (runtime/monitor.py:20-30): bit 0 non-finite,
+// bit 1 |u| or |v| above the velocity limit, bit 2 |eta| above its limit.
+__global__ void __launch_bounds__(256) k_monitor(Dev d, const float* __restrict__ u, const float* __restrict__ v,
+                                                 const float* __restrict__ T, const float* __restrict__ S,
+                                                 const float* __restrict__ eta, float umax, float etamax,
+                                                 unsigned int* __restrict__ flags) {
+  const long long n3 = (long long)d.nz * d.plane;
+  unsigned int f = 0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n3; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % d.P);
+    if (i >= d.nx) continue;
+    const float a = u[t], b = v[t], c = T[t], e = S[t];
+    if (!isfinite(a) || !isfinite(b) || !isfinite(c) || !isfinite(e)) f |= 1u;
+    if (fabsf(a) > umax || fabsf(b) > umax) f |= 2u;
+    if (t < d.plane) {
+      const float h = eta[t];
+      if (!isfinite(h)) f |= 1u;
+      if (fabsf(h) > etamax) f |= 4u;
+    }
+  }
+  f = __reduce_or_sync(0xffffffffu, f);
+  if ((threadIdx.x & 31) == 0 && f) atomicOr(flags, f);
+}
+
+}  // namespace zm

@@ -1,0 +1,65 @@
+// Declarations shared by the kernel translation units and the solver.
+#pragma once
+
+#include "zm_internal.cuh"
+
+namespace zm {
+
+struct FftPlan {
+  int n, nstages, keep;
+  int radix[24];
+  const float2* tw;  // exp(-2 pi i m / n), m < n
+};
+
+struct PgfArgs {
+  const float *T, *S, *u1, *v1, *Au, *Av, *Ppu, *Ppv;
+  float *Pu, *Pv, *uo, *vo, *frx, *fry;
+  double *ubt0, *vbt0;
+  float dt, bottom_decay;
+  int mode;
+};
+
+struct RestArgs {
+  const float *Tev, *Sev, *accT, *accS, *Tbase, *Sbase;
+  float *dT1, *dS1, *To, *So;
+  float dt, inv_na;
+  int nc, stage;
+};
+
+__global__ void k_nu_sub(Dev d, const float* u, const float* v, float* uo, float* vo, float dts);
+__global__ void k_inner_lap(Dev d, const float* u, const float* v, const float* T, const float* S, float* Lu,
+                            float* Lv, float* LT, float* LS, int do_uv, int do_ts);
+__global__ void k_lin_finish(Dev d, const float* usub, const float* vsub, const float* u0, const float* v0,
+                             const float* T0, const float* S0, const float* Lu, const float* Lv, const float* LT,
+                             const float* LS, float* uo, float* vo, float* To, float* So, float dth, int implicit_v);
+__global__ void k_implicit_vdiff(Dev d, float* u, float* v, float* T, float* S, const float* u0, const float* v0,
+                                 const float* T0, const float* S0, float dth);
+__global__ void k_fz(Dev d, const float* u, const float* v, float* Fz);
+__global__ void k_madv(Dev d, const float* u, const float* v, const float* Fz, float* Ayu, float* Ayv);
+__global__ void k_dealias_lon(Dev d, FftPlan plan, const float* Ayu, const float* Ayv, float* Au, float* Av,
+                              int lines_per_block);
+__global__ void k_tracer_adv(Dev d, const float* T, const float* S, const float* u, const float* v, const float* Fz,
+                             float* accT, float* accS, float* Tn, float* Sn, float dts, int first, int last);
+__global__ void k_tracer_rest(Dev d, RestArgs a);
+__global__ void k_pgf(Dev d, PgfArgs a);
+__global__ void k_bt_forcing(Dev d, const float* frx, const float* fry, double* Fx, double* Fy, const float* eta32,
+                             double* eta64);
+__global__ void k_bt_eta(Dev d, const double* eta, const double* ubt, const double* vbt, double* eta_o, double dtH);
+__global__ void k_bt_vel(Dev d, const double* eta, const double* ubt, const double* vbt, const double* Fx,
+                         const double* Fy, double* ubt_o, double* vbt_o, double dtb, double drag);
+__global__ void k_cap2d(Dev d, double* f0, double* f1, const float* wts, int nb_rows);
+__global__ void k_cap3_means(Dev d, const float* u, const float* v, const float* T, const float* S, const double* ubt,
+                             const double* ubt0, const double* vbt, const double* vbt0, float* means, int nb_rows);
+__global__ void k_final(Dev d, const float* u3, const float* v3, const float* T3, const float* S3, const double* ubt,
+                        const double* ubt0, const double* vbt, const double* vbt0, const float* u0, const float* v0,
+                        const float* T0, const float* S0, const float* means, const float* wts, int nb_rows,
+                        float* uo, float* vo, float* To, float* So);
+__global__ void k_ref_to_int3(Dev d, const float* src, float* dst, float offset);
+__global__ void k_int_to_ref3(Dev d, const float* src, float* dst, float offset);
+__global__ void k_ref_to_int2(Dev d, const float* src, float* dst);
+__global__ void k_int_to_ref2(Dev d, const float* src, float* dst);
+__global__ void k_eta_to_float(Dev d, const double* e64, float* e32);
+__global__ void k_monitor(Dev d, const float* u, const float* v, const float* T, const float* S, const float* eta,
+                          float umax, float etamax, unsigned int* flags);
+
+}  // namespace zm

@@ -1,0 +1,789 @@
+// Host side of the B200 global ocean step: parameter derivation, device
+// buffers, the kernel sequence of one step, CUDA-graph replay and the C ABI
+// declared in include/zm_b200.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/zm_b200.h"
+#include "zm_kernels.cuh"
+
+using namespace zm;
+
+namespace {
+
+constexpr double kOmega = 7.2921e-5;
+constexpr double kREarth = 6371.0e3;
+constexpr double kPi = 3.14159265358979323846;
+
+struct Err {
+  int code;
+  std::string msg;
+};
+
+#define ZM_CUDA(call)                                                             \
+  do {                                                                            \
+    cudaError_t e__ = (call);                                                     \
+    if (e__ != cudaSuccess) throw Err{ZM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e__)}; \
+  } while (0)
+
+struct Fields4 {
+  float *u = nullptr, *v = nullptr, *T = nullptr, *S = nullptr;
+};
+
+}  // namespace
+
+struct zm_solver {
+  Dev d{};
+  int device = 0;
+  int nx = 0, ny = 0, nz = 0, P = 0;
+  size_t n2 = 0, n3 = 0;
+  int n_subcyc = 1, n_nu = 1, adv_nsub = 1, conv_nsub = 1;
+  double dt = 0, dt_bt = 0;
+  int cap_rows = 0, cap_nb = 0;
+  int vdiff = 0, freeze = 0;
+  float bottom_decay = 1.f;
+  double bt_drag = 1.0;
+  FftPlan fft{};
+  int fft_lines = 1;
+  size_t fft_smem = 0;
+  std::vector<void*> allocs;
+  size_t bytes = 0;
+  // resident states (ping-pong) and their free surfaces
+  Fields4 st[2];
+  float* eta[2] = {nullptr, nullptr};
+  int cur = 0;
+  // work fields
+  Fields4 s1, s2, W1, W2, L;
+  float *Fz = nullptr, *Ayu = nullptr, *Ayv = nullptr, *Au = nullptr, *Av = nullptr;
+  float *accT = nullptr, *accS = nullptr, *TsA = nullptr, *SsA = nullptr, *TsB = nullptr, *SsB = nullptr;
+  float *dT1 = nullptr, *dS1 = nullptr, *Tp = nullptr, *Sp = nullptr, *Pu = nullptr, *Pv = nullptr;
+  float *up = nullptr, *vp = nullptr;
+  float *frx = nullptr, *fry = nullptr, *means = nullptr, *wts = nullptr;
+  double *ubt0 = nullptr, *vbt0 = nullptr, *ubt[2] = {nullptr, nullptr}, *vbt[2] = {nullptr, nullptr};
+  double *eta64[2] = {nullptr, nullptr}, *Fx = nullptr, *Fy = nullptr, *wts_d = nullptr;
+  // reference-layout staging (zm_step_host)
+  Fields4 ref;
+  float* ref_eta = nullptr;
+  // mutable forcing fields
+  float *tau_x = nullptr, *tau_y = nullptr, *qheat = nullptr;
+  unsigned int* flags = nullptr;
+  cudaStream_t cap_stream = nullptr;  // graphs are captured here, launched on the caller's stream
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  bool graphs_ready = false;
+  int kernels_per_step = 0;
+  std::string last_error;
+  // launch accounting: every kernel launch of the step is bracketed by
+  // pb()/pe(); with profiling on, CUDA events time each launch class
+  int launch_count = 0;
+  bool profiling = false;
+  struct ProfEv { int cls; cudaEvent_t a, b; };
+  std::vector<ProfEv> prof;
+  void pb(int cls, cudaStream_t s) {
+    ++launch_count;
+    if (!profiling) return;
+    ProfEv e{cls, nullptr, nullptr};
+    ZM_CUDA(cudaEventCreate(&e.a));
+    ZM_CUDA(cudaEventCreate(&e.b));
+    ZM_CUDA(cudaEventRecord(e.a, s));
+    prof.push_back(e);
+  }
+  void pe(cudaStream_t s) {
+    if (profiling) ZM_CUDA(cudaEventRecord(prof.back().b, s));
+  }
+
+  template <class T>
+  T* alloc(size_t count) {
+    void* p = nullptr;
+    ZM_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    ZM_CUDA(cudaMemset(p, 0, count * sizeof(T)));
+    allocs.push_back(p);
+    bytes += count * sizeof(T);
+    return static_cast<T*>(p);
+  }
+  float* f3() { return alloc<float>(n3); }
+  float* f2() { return alloc<float>(n2); }
+  Fields4 four() { return Fields4{f3(), f3(), f3(), f3()}; }
+
+  template <class T>
+  T* upload(const std::vector<T>& h) {
+    T* p = alloc<T>(h.size());
+    ZM_CUDA(cudaMemcpy(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return p;
+  }
+
+  ~zm_solver() {
+    for (int g = 0; g < 2; ++g)
+      if (graph[g]) cudaGraphExecDestroy(graph[g]);
+    if (cap_stream) cudaStreamDestroy(cap_stream);
+    for (void* p : allocs) cudaFree(p);
+  }
+
+  dim3 grid3(dim3 b) const { return dim3((nx + b.x - 1) / b.x, (ny + b.y - 1) / b.y, nz); }
+  dim3 grid2(dim3 b) const { return dim3((nx + b.x - 1) / b.x, (ny + b.y - 1) / b.y, 1); }
+
+  void check_launch() {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) throw Err{ZM_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e)};
+  }
+
+  // ---------------------------------------------------------------- stages
+  // Linear half step L(dt/2): src -> dst (dst must not alias src).
+  void linear_half(cudaStream_t s, const Fields4& src, const Fields4& dst) {
+    const dim3 b(32, 8);
+    const float dth = (float)(dt / 2.0);
+    const float* usub = src.u;
+    const float* vsub = src.v;
+    if (d.nu_h != 0.f) {
+      const float dts = (float)(dt / 2.0 / n_nu);
+      const float* a = src.u;
+      const float* c = src.v;
+      for (int n = 0; n < n_nu; ++n) {
+        const Fields4& o = (n % 2 == 0) ? W1 : W2;
+        pb(ZM_K_NU_SUB, s);
+        k_nu_sub<<<grid3(b), b, 0, s>>>(d, a, c, o.u, o.v, dts);
+        pe(s);
+        a = o.u;
+        c = o.v;
+      }
+      usub = a;
+      vsub = c;
+    }
+    const int do_uv = d.nu_bi > 0.f, do_ts = d.kappa_bi > 0.f;
+    if (do_uv || do_ts) {
+      pb(ZM_K_INNER_LAP, s);
+      k_inner_lap<<<grid3(b), b, 0, s>>>(d, src.u, src.v, src.T, src.S, L.u, L.v, L.T, L.S, do_uv, do_ts);
+      pe(s);
+    }
+    pb(ZM_K_LIN_FINISH, s);
+    k_lin_finish<<<grid3(b), b, 0, s>>>(d, usub, vsub, src.u, src.v, src.T, src.S, L.u, L.v, L.T, L.S, dst.u,
+                                        dst.v, dst.T, dst.S, dth, vdiff);
+    pe(s);
+    if (vdiff) {
+      const dim3 c(32, 4);
+      pb(ZM_K_IMPLICIT, s);
+      k_implicit_vdiff<<<grid2(c), c, 0, s>>>(d, dst.u, dst.v, dst.T, dst.S, src.u, src.v, src.T, src.S, dth);
+      pe(s);
+    }
+    check_launch();
+  }
+
+  // Tracer residual at the evaluation state (u, v, T, S) with transport Fz.
+  void tracer_residual(cudaStream_t s, int stage, const float* u, const float* v, const float* T, const float* S,
+                       const float* Tbase, const float* Sbase, float* To, float* So) {
+    const dim3 b(32, 8);
+    const float dts = (float)(dt / adv_nsub);
+    const float* cT = T;
+    const float* cS = S;
+    for (int n = 0; n < adv_nsub; ++n) {
+      float* nT = (n % 2 == 0) ? TsA : TsB;
+      float* nS = (n % 2 == 0) ? SsA : SsB;
+      pb(ZM_K_TRACER_ADV, s);
+      k_tracer_adv<<<grid3(b), b, 0, s>>>(d, cT, cS, u, v, Fz, accT, accS, nT, nS, dts, n == 0, n == adv_nsub - 1);
+      pe(s);
+      cT = nT;
+      cS = nS;
+    }
+    RestArgs a{T, S, accT, accS, Tbase, Sbase, dT1, dS1, To, So, (float)dt, 1.f / (float)adv_nsub, conv_nsub, stage};
+    const dim3 c(32, 4);
+    pb(ZM_K_TRACER_REST, s);
+    k_tracer_rest<<<grid2(c), c, 0, s>>>(d, a);
+    pe(s);
+    check_launch();
+  }
+
+  void pgf(cudaStream_t s, PgfArgs a) {
+    const dim3 c(32, 2);
+    const size_t smem = a.mode == 0 ? 0 : (size_t)2 * nz * c.x * c.y * sizeof(float);
+    pb(ZM_K_PGF, s);
+    k_pgf<<<grid2(c), c, smem, s>>>(d, a);
+    pe(s);
+    check_launch();
+  }
+
+  // Nonlinear RK2 step N(dt): src -> dst.
+  void nonlinear(cudaStream_t s, const Fields4& src, const Fields4& dst) {
+    const dim3 c(32, 4);
+    pb(ZM_K_FZ, s);
+    k_fz<<<grid2(c), c, 0, s>>>(d, src.u, src.v, Fz);
+    pe(s);
+    const dim3 m(32, 8);
+    pb(ZM_K_MADV, s);
+    k_madv<<<dim3((nx + 31) / 32, (ny + 7) / 8, nz), m, 0, s>>>(d, src.u, src.v, Fz, Ayu, Ayv);
+    pe(s);
+    const int nlines = ny * nz;
+    pb(ZM_K_DEALIAS, s);
+    k_dealias_lon<<<(nlines + fft_lines - 1) / fft_lines, 256, fft_smem, s>>>(d, fft, Ayu, Ayv, Au, Av, fft_lines);
+    pe(s);
+    check_launch();
+    // stage 1: tracers at the old velocity, momentum with the predicted tracers
+    tracer_residual(s, 1, src.u, src.v, src.T, src.S, src.T, src.S, Tp, Sp);
+    PgfArgs a{};
+    a.T = Tp; a.S = Sp; a.u1 = src.u; a.v1 = src.v; a.Au = Au; a.Av = Av;
+    a.Pu = Pu; a.Pv = Pv; a.uo = up; a.vo = vp; a.dt = (float)dt; a.mode = 1;
+    pgf(s, a);
+    // stage 2: tracers at the predicted velocity (or the old one if frozen)
+    const float* u2 = src.u;
+    const float* v2 = src.v;
+    if (!freeze) {
+      pb(ZM_K_FZ, s);
+      k_fz<<<grid2(c), c, 0, s>>>(d, up, vp, Fz);
+      pe(s);
+      u2 = up;
+      v2 = vp;
+    }
+    tracer_residual(s, 2, u2, v2, Tp, Sp, src.T, src.S, dst.T, dst.S);
+    PgfArgs b{};
+    b.T = dst.T; b.S = dst.S; b.u1 = src.u; b.v1 = src.v; b.Au = Au; b.Av = Av; b.Ppu = Pu; b.Ppv = Pv;
+    b.uo = dst.u; b.vo = dst.v; b.dt = (float)dt; b.bottom_decay = bottom_decay; b.mode = 2;
+    pgf(s, b);
+  }
+
+  // Barotropic subcycle and the final projection/cap/hold.
+  void barotropic_and_final(cudaStream_t s, const Fields4& s3, const float* eta_in, const Fields4& held,
+                            const Fields4& out, float* eta_out) {
+    PgfArgs a{};
+    a.T = s3.T; a.S = s3.S; a.u1 = s3.u; a.v1 = s3.v; a.frx = frx; a.fry = fry; a.ubt0 = ubt0; a.vbt0 = vbt0;
+    a.mode = 0;
+    pgf(s, a);
+    const dim3 c(32, 8);
+    pb(ZM_K_BAROTROPIC, s);
+    k_bt_forcing<<<grid2(c), c, 0, s>>>(d, frx, fry, Fx, Fy, eta_in, eta64[0]);
+    pe(s);
+    ZM_CUDA(cudaMemcpyAsync(ubt[0], ubt0, n2 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    ZM_CUDA(cudaMemcpyAsync(vbt[0], vbt0, n2 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    const double dtH = dt_bt * (double)d.H_sw;
+    for (int n = 0; n < n_subcyc; ++n) {
+      const int a0 = n % 2, a1 = 1 - a0;
+      pb(ZM_K_BAROTROPIC, s);
+      k_bt_eta<<<grid2(c), c, 0, s>>>(d, eta64[a0], ubt[a0], vbt[a0], eta64[a1], dtH);
+      pe(s);
+      if (cap_rows > 0) {
+        pb(ZM_K_BAROTROPIC, s);
+        k_cap2d<<<dim3(2 * cap_nb, 1), 256, 0, s>>>(d, eta64[a1], nullptr, wts, cap_nb);
+        pe(s);
+      }
+      pb(ZM_K_BAROTROPIC, s);
+      k_bt_vel<<<grid2(c), c, 0, s>>>(d, eta64[a1], ubt[a0], vbt[a0], Fx, Fy, ubt[a1], vbt[a1], dt_bt, bt_drag);
+      pe(s);
+      if (cap_rows > 0) {
+        pb(ZM_K_BAROTROPIC, s);
+        k_cap2d<<<dim3(2 * cap_nb, 2), 256, 0, s>>>(d, ubt[a1], vbt[a1], wts, cap_nb);
+        pe(s);
+      }
+    }
+    const int fin = n_subcyc % 2;
+    pb(ZM_K_BAROTROPIC, s);
+    k_eta_to_float<<<grid2(c), c, 0, s>>>(d, eta64[fin], eta_out);
+    pe(s);
+    if (cap_rows > 0) {
+      pb(ZM_K_FINAL, s);
+      k_cap3_means<<<dim3(2 * cap_nb, nz), 256, 0, s>>>(d, s3.u, s3.v, s3.T, s3.S, ubt[fin], ubt0, vbt[fin], vbt0,
+                                                       means, cap_nb);
+      pe(s);
+    }
+    pb(ZM_K_FINAL, s);
+    k_final<<<grid3(c), c, 0, s>>>(d, s3.u, s3.v, s3.T, s3.S, ubt[fin], ubt0, vbt[fin], vbt0, held.u, held.v,
+                                   held.T, held.S, means, wts, cap_rows > 0 ? cap_nb : 0, out.u, out.v, out.T,
+                                   out.S);
+    pe(s);
+    check_launch();
+  }
+
+  void full_step(cudaStream_t s, int from, int to) {
+    const Fields4& in = st[from];
+    linear_half(s, in, s1);
+    nonlinear(s, s1, s2);
+    linear_half(s, s2, s1);
+    barotropic_and_final(s, s1, eta[from], in, st[to], eta[to]);
+  }
+
+  void monitor(cudaStream_t s, int which) {
+    ZM_CUDA(cudaMemsetAsync(flags, 0, sizeof(unsigned int), s));
+    k_monitor<<<4 * 148, 256, 0, s>>>(d, st[which].u, st[which].v, st[which].T, st[which].S, eta[which], 10.f, 15.f,
+                                      flags);
+    check_launch();
+  }
+
+  void build_graphs() {
+    cudaStream_t s = cap_stream;
+    for (int g = 0; g < 2; ++g) {
+      cudaGraph_t graph_def = nullptr;
+      ZM_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      const int before = launch_count;
+      try {
+        full_step(s, g, 1 - g);
+        kernels_per_step = launch_count - before;
+      } catch (...) {
+        cudaStreamEndCapture(s, &graph_def);
+        if (graph_def) cudaGraphDestroy(graph_def);
+        throw;
+      }
+      ZM_CUDA(cudaStreamEndCapture(s, &graph_def));
+      ZM_CUDA(cudaGraphInstantiate(&graph[g], graph_def, 0));
+      cudaGraphDestroy(graph_def);
+    }
+    graphs_ready = true;
+  }
+
+  // layout conversion between reference arrays and internal fields
+  void to_int3(cudaStream_t s, const float* src, float* dst, float offset) {
+    k_ref_to_int3<<<dim3((nx + 31) / 32, (nz + 31) / 32, ny), dim3(32, 8), 0, s>>>(d, src, dst, offset);
+  }
+  void to_ref3(cudaStream_t s, const float* src, float* dst, float offset) {
+    k_int_to_ref3<<<dim3((nx + 31) / 32, (nz + 31) / 32, ny), dim3(32, 8), 0, s>>>(d, src, dst, offset);
+  }
+  // tracers enter as anomalies from (T_ref, S_ref)
+  void load(cudaStream_t s, const zm_state* in, const Fields4& f, float* e) {
+    to_int3(s, in->u, f.u, 0.f);
+    to_int3(s, in->v, f.v, 0.f);
+    to_int3(s, in->T, f.T, d.T_ref);
+    to_int3(s, in->S, f.S, d.S_ref);
+    const dim3 c(32, 8);
+    k_ref_to_int2<<<grid2(c), c, 0, s>>>(d, in->eta, e);
+    check_launch();
+  }
+  void store(cudaStream_t s, const Fields4& f, const float* e, zm_state* out) {
+    to_ref3(s, f.u, out->u, 0.f);
+    to_ref3(s, f.v, out->v, 0.f);
+    to_ref3(s, f.T, out->T, d.T_ref);
+    to_ref3(s, f.S, out->S, d.S_ref);
+    const dim3 c(32, 8);
+    k_int_to_ref2<<<grid2(c), c, 0, s>>>(d, e, out->eta);
+    check_launch();
+  }
+};
+
+namespace {
+
+void require(bool ok, int code, const std::string& msg) {
+  if (!ok) throw Err{code, msg};
+}
+
+bool fft_factor(int n, FftPlan& plan) {
+  plan.n = n;
+  plan.nstages = 0;
+  int m = n;
+  const int radices[4] = {4, 2, 3, 5};
+  for (int r : radices) {
+    while (m % r == 0) {
+      if (plan.nstages >= 24) return false;
+      plan.radix[plan.nstages++] = r;
+      m /= r;
+    }
+  }
+  return m == 1;
+}
+
+std::vector<float> to_int2(const double* src, int nx, int ny, int P, double fill) {
+  std::vector<float> out((size_t)ny * P, 0.f);
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i) out[(size_t)j * P + i] = (float)(src ? src[(size_t)i * ny + j] : fill);
+  return out;
+}
+
+void build(zm_solver* s, const zm_grid* g, const zm_params* p) {
+  require(g && p, ZM_ERR_INVALID, "null grid or params");
+  const int nx = g->nx, ny = g->ny, nz = g->nz;
+  require(nx >= 2 && ny >= 2 && nz >= 2, ZM_ERR_INVALID, "nx, ny and nz must be at least 2");
+  require(nz <= ZM_MAXZ, ZM_ERR_UNSUPPORTED, "nz above 64 levels is not supported");
+  require(g->dx_2d && g->cos_lat && g->f && g->z && g->dz && g->wet_mask, ZM_ERR_INVALID, "missing grid array");
+  require(std::isfinite(g->dy) && g->dy > 0, ZM_ERR_INVALID, "dy must be positive and finite");
+  require(std::isfinite(p->dt) && p->dt > 0, ZM_ERR_INVALID, "dt must be positive and finite");
+  require(std::isfinite(p->dt_bt) && p->dt_bt > 0, ZM_ERR_INVALID, "dt_bt must be positive and finite");
+  for (int k = 0; k + 1 < nz; ++k)
+    require(g->z[k + 1] < g->z[k] && g->dz[k] > 0, ZM_ERR_INVALID, "z must be strictly descending");
+  const int nb = p->polar_cap_rows + p->polar_cap_taper;
+  require(p->polar_cap_rows >= 0 && p->polar_cap_taper >= 0, ZM_ERR_INVALID, "polar cap counts must be >= 0");
+  require(!(p->polar_cap_rows > 0 && 2 * nb > ny), ZM_ERR_INVALID,
+          "polar cap bands must not overlap; reduce rows/taper or disable the cap");
+  require(p->limiter >= 0 && p->limiter <= 2, ZM_ERR_INVALID, "unknown limiter");
+  FftPlan plan{};
+  require(fft_factor(nx, plan), ZM_ERR_UNSUPPORTED, "nx must be a product of 2, 3 and 5 (longitude FFT filter)");
+
+  cudaGetDevice(&s->device);
+  s->nx = nx; s->ny = ny; s->nz = nz;
+  s->P = (nx + 3) / 4 * 4;
+  const int P = s->P;
+  s->n2 = (size_t)ny * P;
+  s->n3 = s->n2 * nz;
+  s->dt = p->dt;
+  s->n_subcyc = std::max(1, (int)std::nearbyint(p->dt / p->dt_bt));
+  s->dt_bt = p->dt / s->n_subcyc;
+  s->n_nu = std::max(1, p->nu_nsub > 0 ? (int)p->nu_nsub : s->n_subcyc);
+  double dzmin = g->dz[0];
+  for (int k = 0; k + 1 < nz; ++k) dzmin = std::min(dzmin, g->dz[k]);
+  s->conv_nsub = std::max(1, (int)std::ceil(p->kappa_conv * p->dt / (0.4 * dzmin * dzmin)));
+  s->adv_nsub = std::max(1, (int)std::ceil(p->dt * 4.0e-3 / (0.5 * dzmin)));
+  s->cap_rows = p->polar_cap_rows;
+  s->cap_nb = nb;
+  s->vdiff = p->vertical_diffusion;
+  s->freeze = p->freeze_adv_vel;
+  s->bottom_decay = (float)std::exp(-p->r_bot * p->dt);
+  s->bt_drag = 1.0 / (1.0 + p->r_bot * s->dt_bt);
+
+  Dev& d = s->d;
+  d.nx = nx; d.ny = ny; d.nz = nz; d.P = P;
+  d.plane = (long long)s->n2;
+  // ---- per-row metric
+  std::vector<float> cosl(ny), inv_cos(ny), cfp(ny), cfm(ny), tanR(ny);
+  for (int j = 0; j < ny; ++j) {
+    const double c = g->cos_lat[j];
+    cosl[j] = (float)c;
+    inv_cos[j] = (float)(1.0 / c);
+    cfp[j] = (float)(0.5 * (c + g->cos_lat[(j + 1) % ny]));
+    cfm[j] = (float)(0.5 * (c + g->cos_lat[(j - 1 + ny) % ny]));
+    const double sin_row = g->f[j] / (2.0 * kOmega);   // f[0, j]
+    tanR[j] = (float)((sin_row / c) / kREarth);
+  }
+  d.cosl = s->upload(cosl); d.inv_cos = s->upload(inv_cos); d.cfp = s->upload(cfp); d.cfm = s->upload(cfm);
+  d.tanR = s->upload(tanR);
+  // ---- 2-D fields
+  std::vector<float> inv_dx(s->n2, 1.f), inv_dx2(s->n2, 1.f), fc(s->n2, 0.f), rc(s->n2, 1.f), rs(s->n2, 0.f);
+  std::vector<double> inv_dx_d(s->n2, 1.0), fc_d(s->n2, 0.0);
+  std::vector<uint64_t> bits(s->n2, 0ull);
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i) {
+      const size_t r = (size_t)i * ny + j, c = (size_t)j * P + i;
+      const double dx = g->dx_2d[r];
+      require(std::isfinite(dx) && dx > 0, ZM_ERR_INVALID, "dx_2d must be positive and finite");
+      inv_dx[c] = (float)(1.0 / dx);
+      inv_dx2[c] = (float)(1.0 / (dx * dx));
+      inv_dx_d[c] = 1.0 / dx;
+      fc[c] = (float)g->f[r];
+      fc_d[c] = g->f[r];
+      const double ang = g->f[r] * (p->dt / 2.0);
+      rc[c] = (float)std::cos(ang);
+      rs[c] = (float)std::sin(ang);
+      uint64_t b = 0;
+      for (int k = 0; k < nz; ++k) {
+        const double w = g->wet_mask_3d ? g->wet_mask_3d[r * nz + k] : g->wet_mask[r];
+        require(w == 0.0 || w == 1.0, ZM_ERR_UNSUPPORTED, "wet masks must be 0 or 1");
+        if (w == 1.0) b |= 1ull << k;
+      }
+      bits[c] = b;
+    }
+  d.inv_dx = s->upload(inv_dx); d.inv_dx2 = s->upload(inv_dx2); d.fcor = s->upload(fc);
+  d.rot_c = s->upload(rc); d.rot_s = s->upload(rs);
+  d.inv_dx_d = s->upload(inv_dx_d); d.fcor_d = s->upload(fc_d);
+  d.wbits = s->upload(bits);
+  d.wet2 = s->upload(to_int2(g->wet_mask, nx, ny, P, 0.0));
+  {
+    std::vector<float> kh = to_int2(p->coastal_kappa_h, nx, ny, P, 0.0);
+    std::vector<float> kv = to_int2(p->coastal_kappa_v, nx, ny, P, 0.0);
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        const size_t r = (size_t)i * ny + j, c = (size_t)j * P + i;
+        kh[c] = (float)(p->kappa_h + (p->coastal_kappa_h ? p->coastal_kappa_h[r] : 0.0));
+        kv[c] = (float)(p->kappa_v + (p->coastal_kappa_v ? p->coastal_kappa_v[r] : 0.0));
+      }
+    d.kh2 = s->upload(kh);
+    d.kv2 = s->upload(kv);
+  }
+  s->tau_x = s->upload(to_int2(p->tau_x, nx, ny, P, 0.0));
+  s->tau_y = s->upload(to_int2(p->tau_y, nx, ny, P, 0.0));
+  s->qheat = s->upload(to_int2(p->q_heat, nx, ny, P, 0.0));
+  d.tau_x = s->tau_x; d.tau_y = s->tau_y; d.qheat = s->qheat;
+  // temperature / salinity targets, shifted like the tracers
+  std::vector<float> tatm = to_int2(p->lambda_bulk > 0 ? p->t_atm : nullptr, nx, ny, P, 0.0);
+  std::vector<float> rest_t = to_int2(p->coastal_restore_t, nx, ny, P, 0.0);
+  std::vector<float> sref = to_int2(p->s_ref, nx, ny, P, 0.0);
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i) {
+      const size_t r = (size_t)i * ny + j, c = (size_t)j * P + i;
+      tatm[c] = (float)(((p->lambda_bulk > 0 && p->t_atm) ? p->t_atm[r] : 0.0) - p->T_ref);
+      rest_t[c] = (float)((p->coastal_restore_t ? p->coastal_restore_t[r] : 0.0) - p->T_ref);
+      sref[c] = (float)((p->s_ref ? p->s_ref[r] : 0.0) - p->S_ref);
+    }
+  d.tatm = s->upload(tatm);
+  d.cbulk = s->upload(to_int2(p->coastal_bulk_lambda, nx, ny, P, 0.0));
+  d.rest_c = s->upload(to_int2(p->coastal_restore_coef, nx, ny, P, 0.0));
+  d.rest_T = s->upload(rest_t);
+  d.sref = s->upload(sref);
+  // ---- scalars
+  d.inv_dy = (float)(1.0 / g->dy);
+  d.inv_dy2 = (float)(1.0 / (g->dy * g->dy));
+  d.inv_dy_d = 1.0 / g->dy;
+  d.nu_h = (float)p->nu_h; d.nu_v = (float)p->nu_v; d.nu_bi = (float)p->nu_bi; d.kappa_bi = (float)p->kappa_bi;
+  d.kappa_conv = (float)p->kappa_conv; d.r_bot = (float)p->r_bot; d.T_ref = (float)p->T_ref;
+  d.S_ref = (float)p->S_ref;
+  double H = 0.0;
+  for (int k = 0; k + 1 < nz; ++k) H += g->dz[k];
+  d.H_sw = (float)H;
+  d.dz_surface = (float)std::fabs(g->z[0] - g->z[1]);
+  d.lambda_bulk = (float)(p->t_atm ? p->lambda_bulk : 0.0);
+  d.restore_S = (float)p->restore_coef_S;
+  d.ice_salt = (float)p->ice_salt_flux;
+  d.ice_freeze = (float)(p->ice_freeze_temp_c - p->T_ref);
+  d.localize_conv = p->localize_conv;
+  d.limiter = p->limiter;
+  d.conservative_kv = p->conservative_kv;
+  // ---- vertical coefficients (fd_metrics.py:55-98)
+  Vert& vc = d.vc;
+  const double* z = g->z;
+  std::vector<double> gap(nz - 1);
+  for (int k = 0; k + 1 < nz; ++k) gap[k] = std::fabs(z[k + 1] - z[k]);
+  for (int k = 0; k < nz; ++k) {
+    double node;
+    if (k == 0) node = gap[0];
+    else if (k == nz - 1) node = gap[nz - 2];
+    else node = 0.5 * (gap[k - 1] + gap[k]);
+    vc.dz_node[k] = (float)node;
+    vc.inv_dz_node[k] = (float)(1.0 / node);
+  }
+  for (int k = 0; k + 1 < nz; ++k) {
+    vc.inv_dz_iface[k] = (float)(1.0 / gap[k]);
+    vc.dz3d[k] = (float)g->dz[k];
+    vc.dznorm[k] = (float)(g->dz[k] / H);
+  }
+  for (int k = 1; k + 1 < nz; ++k) {
+    const double hm = std::fabs(z[k - 1] - z[k]), hp = std::fabs(z[k + 1] - z[k]);
+    const double den = hm * hp * (hm + hp) / 2.0;
+    vc.d2_hi[k] = (float)(hm / den);
+    vc.d2_lo[k] = (float)(hp / den);
+    vc.ddz_inv[k] = (float)(1.0 / ((z[k] - z[k - 1]) + (z[k + 1] - z[k])));
+  }
+  vc.ddz_inv[0] = (float)(1.0 / (z[1] - z[0]));
+  vc.ddz_inv[nz - 1] = (float)(1.0 / (z[nz - 1] - z[nz - 2]));
+  vc.d2_top = (float)(2.0 / (gap[0] * gap[0]));
+  vc.d2_bot = (float)(2.0 / (gap[nz - 2] * gap[nz - 2]));
+  // ---- polar cap weights (numerics/horizontal.py:362-385), pole-inward
+  std::vector<float> w(std::max(nb, 1), 0.f);
+  for (int r = 0; r < p->polar_cap_rows; ++r) w[r] = 1.f;
+  for (int t = 0; t < p->polar_cap_taper; ++t) {
+    const double x = (kPi / 2.0) * (t + 1) / (p->polar_cap_taper + 1);
+    w[p->polar_cap_rows + t] = (float)(std::cos(x) * std::cos(x));
+  }
+  s->wts = s->upload(w);
+  // ---- FFT plan for the longitude dealias (factory.py:529-533)
+  plan.keep = std::max(1, (int)((double)(nx / 2) * 2.0 / 3.0));
+  std::vector<float2> tw(nx);
+  for (int m = 0; m < nx; ++m) {
+    const double a = -2.0 * kPi * m / nx;
+    tw[m] = make_float2((float)std::cos(a), (float)std::sin(a));
+  }
+  plan.tw = s->upload(tw);
+  s->fft = plan;
+  s->fft_lines = std::max(1, std::min(8, (int)((200 * 1024 / sizeof(float2) - nx) / (2 * nx))));
+  s->fft_smem = ((size_t)nx + (size_t)2 * s->fft_lines * nx) * sizeof(float2);
+  require(s->fft_smem <= 227 * 1024, ZM_ERR_UNSUPPORTED, "nx too large for the shared-memory FFT filter");
+  ZM_CUDA(cudaFuncSetAttribute(k_dealias_lon, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->fft_smem));
+  ZM_CUDA(cudaFuncSetAttribute(k_pgf, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * nz * 64 * (int)sizeof(float)));
+  // ---- buffers
+  for (int q = 0; q < 2; ++q) {
+    s->st[q] = s->four();
+    s->eta[q] = s->f2();
+  }
+  s->s1 = s->four(); s->s2 = s->four(); s->W1 = s->four(); s->W2 = s->four(); s->L = s->four();
+  s->Fz = s->f3(); s->Ayu = s->f3(); s->Ayv = s->f3(); s->Au = s->f3(); s->Av = s->f3();
+  s->accT = s->f3(); s->accS = s->f3(); s->TsA = s->f3(); s->SsA = s->f3(); s->TsB = s->f3(); s->SsB = s->f3();
+  s->dT1 = s->f3(); s->dS1 = s->f3(); s->Tp = s->f3(); s->Sp = s->f3(); s->Pu = s->f3(); s->Pv = s->f3();
+  s->up = s->f3(); s->vp = s->f3();
+  s->frx = s->f2(); s->fry = s->f2();
+  s->means = s->alloc<float>((size_t)4 * 2 * std::max(nb, 1) * nz);
+  s->ubt0 = s->alloc<double>(s->n2); s->vbt0 = s->alloc<double>(s->n2);
+  for (int q = 0; q < 2; ++q) {
+    s->ubt[q] = s->alloc<double>(s->n2);
+    s->vbt[q] = s->alloc<double>(s->n2);
+    s->eta64[q] = s->alloc<double>(s->n2);
+  }
+  s->Fx = s->alloc<double>(s->n2); s->Fy = s->alloc<double>(s->n2);
+  const size_t nref3 = (size_t)nx * ny * nz;
+  s->ref = Fields4{s->alloc<float>(nref3), s->alloc<float>(nref3), s->alloc<float>(nref3), s->alloc<float>(nref3)};
+  s->ref_eta = s->alloc<float>((size_t)nx * ny);
+  s->flags = s->alloc<unsigned int>(1);
+  ZM_CUDA(cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking));
+  ZM_CUDA(cudaDeviceSynchronize());
+}
+
+int fail(zm_solver* s, const Err& e) {
+  if (s) s->last_error = e.msg;
+  return e.code;
+}
+
+}  // namespace
+
+extern "C" {
+
+int zm_create(const zm_grid* grid, const zm_params* params, zm_solver** out) {
+  if (!out) return ZM_ERR_INVALID;
+  *out = nullptr;
+  zm_solver* s = new zm_solver();
+  try {
+    build(s, grid, params);
+  } catch (const Err& e) {
+    std::fprintf(stderr, "zm_create: %s\n", e.msg.c_str());
+    const int code = e.code;
+    delete s;
+    return code;
+  }
+  *out = s;
+  return ZM_OK;
+}
+
+int zm_info(const zm_solver* s, int32_t* out, int32_t n) {
+  if (!s || !out) return ZM_ERR_INVALID;
+  const int32_t v[7] = {s->n_subcyc, s->n_nu, s->adv_nsub, s->conv_nsub, s->P, (int32_t)(s->bytes >> 20),
+                        s->kernels_per_step};
+  for (int q = 0; q < n && q < 7; ++q) out[q] = v[q];
+  return ZM_OK;
+}
+
+int zm_load_state(zm_solver* s, void* stream, const zm_state* in) {
+  if (!s || !in || !in->u || !in->v || !in->T || !in->S || !in->eta) return ZM_ERR_INVALID;
+  try {
+    s->load((cudaStream_t)stream, in, s->st[s->cur], s->eta[s->cur]);
+  } catch (const Err& e) {
+    return fail(s, e);
+  }
+  return ZM_OK;
+}
+
+int zm_store_state(zm_solver* s, void* stream, zm_state* out) {
+  if (!s || !out || !out->u || !out->v || !out->T || !out->S || !out->eta) return ZM_ERR_INVALID;
+  try {
+    s->store((cudaStream_t)stream, s->st[s->cur], s->eta[s->cur], out);
+  } catch (const Err& e) {
+    return fail(s, e);
+  }
+  return ZM_OK;
+}
+
+int zm_advance(zm_solver* s, void* stream, int32_t nsteps) {
+  if (!s || nsteps < 0) return ZM_ERR_INVALID;
+  cudaStream_t st = (cudaStream_t)stream;
+  try {
+    if (!s->graphs_ready) s->build_graphs();
+    for (int n = 0; n < nsteps; ++n) {
+      ZM_CUDA(cudaGraphLaunch(s->graph[s->cur], st));
+      s->cur = 1 - s->cur;
+    }
+    s->monitor(st, s->cur);
+  } catch (const Err& e) {
+    return fail(s, e);
+  }
+  return ZM_OK;
+}
+
+int zm_step(zm_solver* s, void* stream, const zm_state* in, zm_state* out, int32_t nsteps) {
+  int rc = zm_load_state(s, stream, in);
+  if (rc) return rc;
+  rc = zm_advance(s, stream, nsteps);
+  if (rc) return rc;
+  return zm_store_state(s, stream, out);
+}
+
+int zm_step_host(zm_solver* s, void* stream, const zm_state* in, zm_state* out, int32_t nsteps) {
+  if (!s || !in || !out) return ZM_ERR_INVALID;
+  cudaStream_t st = (cudaStream_t)stream;
+  try {
+    const size_t b3 = (size_t)s->nx * s->ny * s->nz * sizeof(float), b2 = (size_t)s->nx * s->ny * sizeof(float);
+    ZM_CUDA(cudaMemcpyAsync(s->ref.u, in->u, b3, cudaMemcpyHostToDevice, st));
+    ZM_CUDA(cudaMemcpyAsync(s->ref.v, in->v, b3, cudaMemcpyHostToDevice, st));
+    ZM_CUDA(cudaMemcpyAsync(s->ref.T, in->T, b3, cudaMemcpyHostToDevice, st));
+    ZM_CUDA(cudaMemcpyAsync(s->ref.S, in->S, b3, cudaMemcpyHostToDevice, st));
+    ZM_CUDA(cudaMemcpyAsync(s->ref_eta, in->eta, b2, cudaMemcpyHostToDevice, st));
+    zm_state dev{s->ref.u, s->ref.v, s->ref.T, s->ref.S, s->ref_eta};
+    s->load(st, &dev, s->st[s->cur], s->eta[s->cur]);
+    int rc = zm_advance(s, stream, nsteps);
+    if (rc) return rc;
+    s->store(st, s->st[s->cur], s->eta[s->cur], &dev);
+    ZM_CUDA(cudaMemcpyAsync(out->u, s->ref.u, b3, cudaMemcpyDeviceToHost, st));
+    ZM_CUDA(cudaMemcpyAsync(out->v, s->ref.v, b3, cudaMemcpyDeviceToHost, st));
+    ZM_CUDA(cudaMemcpyAsync(out->T, s->ref.T, b3, cudaMemcpyDeviceToHost, st));
+    ZM_CUDA(cudaMemcpyAsync(out->S, s->ref.S, b3, cudaMemcpyDeviceToHost, st));
+    ZM_CUDA(cudaMemcpyAsync(out->eta, s->ref_eta, b2, cudaMemcpyDeviceToHost, st));
+    ZM_CUDA(cudaStreamSynchronize(st));
+  } catch (const Err& e) {
+    return fail(s, e);
+  }
+  return ZM_OK;
+}
+
+int zm_set_forcing(zm_solver* s, void* stream, const float* tau_x, const float* tau_y, const float* q_heat) {
+  if (!s) return ZM_ERR_INVALID;
+  cudaStream_t st = (cudaStream_t)stream;
+  try {
+    const dim3 c(32, 8);
+    if (tau_x) k_ref_to_int2<<<s->grid2(c), c, 0, st>>>(s->d, tau_x, s->tau_x);
+    if (tau_y) k_ref_to_int2<<<s->grid2(c), c, 0, st>>>(s->d, tau_y, s->tau_y);
+    if (q_heat) k_ref_to_int2<<<s->grid2(c), c, 0, st>>>(s->d, q_heat, s->qheat);
+    s->check_launch();
+  } catch (const Err& e) {
+    return fail(s, e);
+  }
+  return ZM_OK;
+}
+
+int zm_run_stage(zm_solver* s, void* stream, int32_t stage, const zm_state* in, zm_state* out) {
+  if (!s || !in || !out || stage < 1 || stage > 3) return ZM_ERR_INVALID;
+  cudaStream_t st = (cudaStream_t)stream;
+  try {
+    s->load(st, in, s->st[s->cur], s->eta[s->cur]);
+    const int a = s->cur, b = 1 - s->cur;
+    if (stage == 1) {
+      s->linear_half(st, s->st[a], s->st[b]);
+    } else if (stage == 2) {
+      s->nonlinear(st, s->st[a], s->st[b]);
+    } else {
+      s->full_step(st, a, b);
+    }
+    if (stage != 3)
+      ZM_CUDA(cudaMemcpyAsync(s->eta[b], s->eta[a], s->n2 * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    s->store(st, s->st[b], s->eta[b], out);
+  } catch (const Err& e) {
+    return fail(s, e);
+  }
+  return ZM_OK;
+}
+
+int zm_profile(zm_solver* s, void* stream, float* ms, int32_t* launches, int32_t n) {
+  if (!s || !ms || !launches || n < ZM_K_COUNT) return ZM_ERR_INVALID;
+  cudaStream_t st = (cudaStream_t)stream;
+  try {
+    for (int c = 0; c < ZM_K_COUNT; ++c) { ms[c] = 0.f; launches[c] = 0; }
+    s->profiling = true;
+    s->prof.clear();
+    try {
+      s->full_step(st, s->cur, 1 - s->cur);
+    } catch (...) {
+      s->profiling = false;
+      throw;
+    }
+    s->profiling = false;
+    s->cur = 1 - s->cur;
+    ZM_CUDA(cudaStreamSynchronize(st));
+    for (auto& e : s->prof) {
+      float t = 0.f;
+      ZM_CUDA(cudaEventElapsedTime(&t, e.a, e.b));
+      ms[e.cls] += t;
+      launches[e.cls] += 1;
+      cudaEventDestroy(e.a);
+      cudaEventDestroy(e.b);
+    }
+    s->prof.clear();
+  } catch (const Err& e) {
+    return fail(s, e);
+  }
+  return ZM_OK;
+}
+
+int zm_status(zm_solver* s, int32_t* monitor_code) {
+  if (!s || !monitor_code) return ZM_ERR_INVALID;
+  unsigned int f = 0;
+  cudaError_t e = cudaMemcpy(&f, s->flags, sizeof(f), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return fail(s, Err{ZM_ERR_CUDA, std::string("zm_status: ") + cudaGetErrorString(e)});
+  *monitor_code = (f & 1u) ? 1 : (f & 2u) ? 3 : (f & 4u) ? 4 : 0;
+  return ZM_OK;
+}
+
+const char* zm_last_error(const zm_solver* s) { return s ? s->last_error.c_str() : "null solver"; }
+
+void zm_destroy(zm_solver* s) { delete s; }
+
+}  // extern "C"

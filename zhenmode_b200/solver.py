@@ -1,0 +1,436 @@
+"""Drop-in ``make_solver_global`` for the B200 global ocean step.
+
+Mirrors ``make_solver_global`` of ``src/zhenmode/model/solver/factory.py:30-799``
+for the production mode-split path: same positional/keyword arguments, the
+same ``ValueError`` on invalid configurations raised before any array is
+built, and the same return arity ``(step, init_state, diagnostics[, params,
+terms_fn][, step_dyn])`` (factory.py:793-799).  ``step`` accepts and returns a
+``JaxStateG`` whose arrays are either CUDA ``torch`` tensors (device-resident,
+stream ordered on torch's current stream) or NumPy arrays (host path).
+
+The arithmetic runs in the CUDA library ``libzm_b200.so`` (float32 fields,
+float64 barotropic mode); options that path does not implement raise
+:class:`UnsupportedOption` (a ``ValueError``).
+"""
+from __future__ import annotations
+
+import collections
+import ctypes
+import math
+import numbers
+
+import numpy as np
+
+from . import _native
+from .config import RHO_0
+
+JaxStateG = collections.namedtuple("JaxStateG", ["u", "v", "T", "S", "eta", "ice"])
+JaxStateG.__new__.__defaults__ = (0.0,)
+
+
+class UnsupportedOption(ValueError):
+    """A reference option the B200 path does not implement (C-ABI status 2)."""
+
+
+def _finite(name, value, *, positive=False, nonnegative=False):
+    """config.py finite_number: a finite real scalar with an optional sign."""
+    if isinstance(value, bool) or not isinstance(value, numbers.Real) or not math.isfinite(float(value)):
+        raise ValueError(f"{name} must be a finite number")
+    if positive and value <= 0:
+        raise ValueError(f"{name} must be positive")
+    if nonnegative and value < 0:
+        raise ValueError(f"{name} must be nonnegative")
+
+
+def _count(name, value, minimum=0):
+    """config.py integer_count."""
+    if isinstance(value, (bool, np.bool_)) or not isinstance(value, (int, np.integer)) or value < minimum:
+        raise ValueError(f"{name} must be an integer >= {minimum}")
+
+
+_DEFAULTS = dict(
+    external_mode_scheme='forward_backward', meridional_boundary_scheme='clamped_nodes',
+    pressure_continuity_scheme='centered_second', tracer_transport_scheme='centered_second',
+    hydrostatic_surface_scheme='reference_plane', density_rotation_scheme='split_sources',
+    vertical_tracer_scheme='donor_cell', hydrostatic_integral_scheme='trapezoidal',
+    column_mean_scheme='nodal_capacity', tracer_flux_arithmetic='legacy',
+    momentum_vertical_velocity_scheme='dual_face_v1', material_point_gradient_scheme='minmod_v1',
+    momentum_tangent_filter_scheme='binomial_v1', column_geometry='legacy',
+    process_time_scheme='legacy')
+
+_KNOWN = dict(
+    external_mode_scheme=('forward_backward', 'symmetric'),
+    meridional_boundary_scheme=('clamped_nodes', 'closed_faces'),
+    pressure_continuity_scheme=('centered_second', 'centered_fourth'),
+    tracer_transport_scheme=('centered_second', 'product_fourth', 'paired_product_fourth'),
+    hydrostatic_surface_scheme=('reference_plane', 'linear_density'),
+    density_rotation_scheme=('split_sources', 'joint_shear'),
+    vertical_tracer_scheme=('donor_cell', 'muscl_nodal_v1', 'muscl_endpoint_v2', 'muscl_band_v3',
+                            'material_point_v4'),
+    hydrostatic_integral_scheme=('trapezoidal', 'cubic_uniform_v1'),
+    column_mean_scheme=('nodal_capacity', 'cubic_consistent_v1'),
+    tracer_flux_arithmetic=('legacy', 'integrated_reference_v1'),
+    momentum_vertical_velocity_scheme=('dual_face_v1', 'point_primitive_v1'),
+    material_point_gradient_scheme=('minmod_v1', 'fourth_uniform_v1'),
+    momentum_tangent_filter_scheme=('binomial_v1', 'gram_fourth_v1'),
+    column_geometry=('legacy', 'nodal_dual_v1', 'fixed_partial_v1'),
+    process_time_scheme=('legacy', 'consistent_split_v1', 'subcycled_rk2_v2', 'symmetric_fast_v3'))
+
+
+def _validate_grid(grid):
+    """grid.py:384-398 validate_grid."""
+    for name in ("nx", "ny", "nz"):
+        _count(name, getattr(grid, name), minimum=2)
+    _finite("dy", grid.dy, positive=True)
+    widths = np.asarray(grid.dx_2d, dtype=np.float64)
+    depths = np.asarray(grid.z, dtype=np.float64)
+    spacing = np.asarray(grid.dz, dtype=np.float64)
+    if widths.shape != (grid.nx, grid.ny) or not np.all(np.isfinite(widths) & (widths > 0.)):
+        raise ValueError("dx_2d must have grid shape and positive finite spacing")
+    if depths.shape != (grid.nz,) or not np.all(np.isfinite(depths)) or not np.all(np.diff(depths) < 0.):
+        raise ValueError("z must contain finite, strictly descending nodes")
+    if (spacing.shape != (grid.nz - 1,) or not np.all(np.isfinite(spacing) & (spacing > 0.))
+            or not np.allclose(spacing, -np.diff(depths), rtol=1e-12, atol=0.)):
+        raise ValueError("dz must match the positive distances between z nodes")
+
+
+def _f64(a, shape=None):
+    out = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+    if shape is not None and out.shape != shape:
+        raise ValueError(f"expected an array of shape {shape}, got {out.shape}")
+    return out
+
+
+class _Solver:
+    """Owns one native solver handle and the host arrays handed to it."""
+
+    def __init__(self, grid, physics, dt, opts):
+        self.lib = _native.load()
+        nx, ny, nz = int(grid.nx), int(grid.ny), int(grid.nz)
+        self.shape = (nx, ny, nz)
+        keep = []
+
+        def arr(a, shape):
+            if a is None:
+                return None
+            out = _f64(a, shape)
+            keep.append(out)
+            return out
+
+        g = _native.ZmGrid()
+        g.nx, g.ny, g.nz = nx, ny, nz
+        g.dy = float(grid.dy)
+        for name, value, shape in (("dx_2d", grid.dx_2d, (nx, ny)), ("cos_lat", grid.cos_lat, (ny,)),
+                                   ("f", grid.f, (nx, ny)), ("z", grid.z, (nz,)), ("dz", grid.dz, (nz - 1,)),
+                                   ("wet_mask", grid.wet_mask, (nx, ny))):
+            setattr(g, name, _native.dptr(arr(value, shape)))
+        wet3 = getattr(grid, "wet_mask_3d", None)
+        g.wet_mask_3d = _native.dptr(arr(wet3, (nx, ny, nz))) if wet3 is not None else None
+
+        p = _native.ZmParams()
+        p.dt = float(dt)
+        p.dt_bt = float(opts["dt_bt"])
+        for name in ("nu_h", "nu_v", "kappa_h", "kappa_v", "kappa_conv", "nu_bi", "kappa_bi", "T_ref",
+                     "S_ref", "r_bot"):
+            setattr(p, name, float(getattr(physics, name)))
+        p.lambda_bulk = opts["lambda_bulk"]
+        p.restore_coef_S = opts["restore_coef_S"]
+        p.ice_salt_flux = float(opts["ice_salt_flux"])
+        p.ice_freeze_temp_c = float(opts["ice_freeze_temp_c"])
+        p.nu_nsub = int(opts["nu_nsub"] or 0)
+        p.polar_cap_rows = int(opts["polar_cap_rows"])
+        p.polar_cap_taper = int(opts["polar_cap_taper"])
+        p.limiter = 2 if opts["fct_adv"] else (1 if opts["monotone_adv"] else 0)
+        p.localize_conv = int(bool(opts["localize_conv"]))
+        p.conservative_kv = int(bool(opts["conservative_kv"]))
+        p.freeze_adv_vel = int(bool(opts["freeze_adv_vel"]))
+        p.vertical_diffusion = 1 if opts["vertical_diffusion"] == "implicit" else 0
+        for name in ("tau_x", "tau_y", "q_heat", "t_atm", "s_ref", "coastal_restore_coef",
+                     "coastal_restore_t", "coastal_bulk_lambda", "coastal_kappa_h", "coastal_kappa_v"):
+            setattr(p, name, _native.dptr(arr(opts["fields"].get(name), (nx, ny))))
+        self._keep = keep
+        handle = ctypes.c_void_p()
+        rc = self.lib.zm_create(ctypes.byref(g), ctypes.byref(p), ctypes.byref(handle))
+        if rc == _native.ZM_ERR_UNSUPPORTED:
+            raise UnsupportedOption("configuration not supported by the B200 step (see stderr)")
+        if rc == _native.ZM_ERR_INVALID:
+            raise ValueError("invalid configuration (see stderr)")
+        if rc != _native.ZM_OK:
+            raise RuntimeError(f"zm_create failed with status {rc}")
+        self.handle = handle
+        info = (ctypes.c_int32 * 7)()
+        self.lib.zm_info(handle, info, 7)
+        self.n_subcyc, self.n_nu, self.adv_nsub, self.conv_nsub, self.pitch, self.mib, _ = list(info)
+
+    def kernels_per_step(self):
+        info = (ctypes.c_int32 * 7)()
+        self.lib.zm_info(self.handle, info, 7)
+        return int(info[6])
+
+    def profile(self, stream=None):
+        """Per-class (ms, launches) of one un-graphed step of the resident state."""
+        n = len(_native.KERNEL_CLASSES)
+        ms = (ctypes.c_float * n)()
+        cnt = (ctypes.c_int32 * n)()
+        self.check(self.lib.zm_profile(self.handle, ctypes.c_void_p(stream or 0), ms, cnt, n), "zm_profile")
+        return {name: (float(ms[i]), int(cnt[i])) for i, name in enumerate(_native.KERNEL_CLASSES)}
+
+    def check(self, rc, what):
+        if rc != _native.ZM_OK:
+            msg = self.lib.zm_last_error(self.handle)
+            raise RuntimeError(f"{what} failed (status {rc}): {msg.decode() if msg else ''}")
+
+    def __del__(self):
+        handle = getattr(self, "handle", None)
+        if handle:
+            self.lib.zm_destroy(handle)
+            self.handle = None
+
+
+def _torch_state_ptrs(state, shape):
+    import torch
+    nx, ny, nz = shape
+    fields = []
+    for name, want in (("u", shape), ("v", shape), ("T", shape), ("S", shape), ("eta", (nx, ny))):
+        t = getattr(state, name)
+        if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float32
+                and tuple(t.shape) == want and t.is_contiguous()):
+            raise ValueError(f"state.{name} must be a contiguous CUDA float32 tensor of shape {want}")
+        fields.append(t)
+    return fields
+
+
+def make_solver_global(grid, physics, dt, forcing=None,
+                       T_atm=None, lambda_bulk=0.0,
+                       mixed_layer_depth_m=None, mixed_layer_mask=None,
+                       mixed_layer_depth_2d=None,
+                       ice_freeze_temp_c=-1.8, ice_salt_flux=0.0,
+                       dynamic_ice=False, ice_insulation_scale_m=1.0,
+                       S_ref_surf=None, sss_restore_days=0.0,
+                       coastal_restore_mask=None, coastal_restore_days=0.0,
+                       coastal_bulk_mask=None, coastal_bulk_lambda=0.0,
+                       coastal_kappa_h_mask=None, coastal_kappa_h=0.0,
+                       coastal_kappa_v_mask=None, coastal_kappa_v=0.0,
+                       coastal_restore_T=None,
+                       sponge_days=0.0, sponge_cells=0,
+                       T_init=None, S_init=None,
+                       polar_cap_rows=2, polar_cap_taper=3, return_params=False,
+                       eta_relax_days=0.0, eta_relax_box=None,
+                       eta_relax_buffer=1.0, dynamic_forcing=False,
+                       mode_split=False, dt_bt=150.0, nu_nsub=None,
+                       dtype='float64', use_scan=False, freeze_adv_vel=False,
+                       conservative_kv=False, project_adv_vel=False,
+                       localize_conv=False, monotone_adv=False,
+                       fct_adv=False, projection_niter=None,
+                       projection_rtol=None, projection_preconditioner='none',
+                       projection_max_refinements=2, column_geometry='legacy',
+                       match_barotropic_transport=False, process_time_scheme='legacy',
+                       eos_pressure_dbar=None, surface_pressure_pa=None,
+                       vertical_diffusion='explicit', **schemes):
+    """Build the B200 step; the argument list is the reference factory's.
+
+    ``vertical_diffusion='implicit'`` (not a reference option) replaces the
+    explicit L-step vertical diffusion by a per-column backward-Euler solve.
+    """
+    # ---- validation, in the reference's order where it matters (factory.py:166-395)
+    _finite('dt', dt, positive=True)
+    _finite('dt_bt', dt_bt, positive=True)
+    for name, value in schemes.items():
+        if name not in _KNOWN:
+            raise TypeError(f"make_solver_global() got an unexpected keyword argument '{name}'")
+        if value not in _KNOWN[name]:
+            raise ValueError(f"unknown {name}")
+    for name in ('column_geometry', 'process_time_scheme'):
+        value = locals()[name]
+        if value not in _KNOWN[name]:
+            raise ValueError(f"unknown {name}")
+    _validate_grid(grid)
+    if dtype not in {'float32', 'float64'}:
+        raise ValueError('dtype must be float32 or float64')
+    if physics.thermodynamics not in {'linear', 'teos10_reference'}:
+        raise ValueError('unknown thermodynamics definition')
+    if physics.thermodynamics == 'linear' and eos_pressure_dbar is not None:
+        raise ValueError('linear EOS does not accept an unused TEOS pressure field')
+    for name in ('nu_h', 'nu_v', 'nu_bi', 'kappa_h', 'kappa_v', 'kappa_bi', 'kappa_conv', 'kappa_gm',
+                 'kappa_redi', 'r_bot', 'cd'):
+        _finite(name, getattr(physics, name), nonnegative=True)
+    for name, value in (('lambda_bulk', lambda_bulk), ('sss_restore_days', sss_restore_days),
+                        ('coastal_restore_days', coastal_restore_days), ('coastal_bulk_lambda', coastal_bulk_lambda),
+                        ('coastal_kappa_h', coastal_kappa_h), ('coastal_kappa_v', coastal_kappa_v),
+                        ('sponge_days', sponge_days), ('eta_relax_days', eta_relax_days)):
+        _finite(name, value, nonnegative=True)
+    for name, value in (('polar_cap_rows', polar_cap_rows), ('polar_cap_taper', polar_cap_taper),
+                        ('sponge_cells', sponge_cells)):
+        _count(name, value)
+    if nu_nsub is not None and not (isinstance(nu_nsub, str) and nu_nsub == 'cfl'):
+        _count('nu_nsub', nu_nsub, minimum=1)
+    if match_barotropic_transport and (not mode_split or column_geometry not in {'nodal_dual_v1', 'fixed_partial_v1'}):
+        raise ValueError("match_barotropic_transport requires mode_split=True and reference column geometry")
+    if process_time_scheme != 'legacy' and not match_barotropic_transport:
+        raise ValueError(f"{process_time_scheme} requires match_barotropic_transport=True")
+    if column_geometry in {'nodal_dual_v1', 'fixed_partial_v1'} and (not conservative_kv or not localize_conv):
+        raise ValueError("reference column geometry requires conservative_kv=True and localize_conv=True")
+    if polar_cap_rows > 0 and 2 * (polar_cap_rows + polar_cap_taper) > grid.ny:
+        raise ValueError('polar cap bands must not overlap; reduce rows/taper or disable the cap')
+    if projection_niter is not None and (isinstance(projection_niter, (bool, np.bool_))
+                                         or not isinstance(projection_niter, (int, np.integer))
+                                         or projection_niter <= 0):
+        raise ValueError('projection_niter must be a positive integer')
+    if projection_rtol is not None and (not np.isfinite(projection_rtol) or projection_rtol <= 0.):
+        raise ValueError('projection_rtol must be finite and positive')
+    if projection_preconditioner not in {'none', 'jacobi'}:
+        raise ValueError('projection_preconditioner must be none or jacobi')
+    if (isinstance(projection_max_refinements, (bool, np.bool_))
+            or not isinstance(projection_max_refinements, (int, np.integer))
+            or not 0 <= projection_max_refinements <= 2):
+        raise ValueError('projection_max_refinements must be an integer from 0 to 2')
+    if mixed_layer_depth_m is not None and (not np.isfinite(mixed_layer_depth_m) or mixed_layer_depth_m < 0.):
+        raise ValueError("mixed_layer_depth_m must be finite and nonnegative")
+    if vertical_diffusion not in ('explicit', 'implicit'):
+        raise ValueError("vertical_diffusion must be 'explicit' or 'implicit'")
+    nx, ny, nz = int(grid.nx), int(grid.ny), int(grid.nz)
+    if surface_pressure_pa is not None:
+        load = np.asarray(surface_pressure_pa)
+        if load.shape != (nx, ny) or not np.isfinite(load).all():
+            raise ValueError('surface pressure must be a finite (nx, ny) Pa field')
+
+    # ---- options outside the B200 path
+    unsupported = []
+    if not mode_split:
+        unsupported.append('mode_split=False (monolithic free surface)')
+    if dtype != 'float32':
+        unsupported.append("dtype='float64' (the B200 step computes in float32)")
+    if column_geometry != 'legacy' or process_time_scheme != 'legacy' or match_barotropic_transport:
+        unsupported.append('non-legacy column geometry or process time scheme')
+    if any(schemes.get(k, v) != v for k, v in _DEFAULTS.items() if k in schemes):
+        unsupported.append('non-default numerical scheme options')
+    if project_adv_vel:
+        unsupported.append('project_adv_vel (column-divergence projection)')
+    if physics.thermodynamics != 'linear':
+        unsupported.append('TEOS-10 thermodynamics')
+    if physics.kappa_gm > 0 or physics.kappa_redi > 0:
+        unsupported.append('GM/Redi closure')
+    if physics.bottom_friction != 'linear':
+        unsupported.append('quadratic bottom drag')
+    if dynamic_ice:
+        unsupported.append('dynamic ice')
+    if (mixed_layer_depth_m or 0.0) > 0.0 or mixed_layer_depth_2d is not None:
+        unsupported.append('mixed-layer heat deposition')
+    if sponge_days > 0.0 and sponge_cells > 0:
+        unsupported.append('lateral sponge')
+    if eta_relax_days > 0.0 and eta_relax_box is not None:
+        unsupported.append('eta relaxation box')
+    if surface_pressure_pa is not None:
+        unsupported.append('surface pressure load')
+    if nz > 64:
+        unsupported.append('more than 64 levels')
+    if unsupported:
+        raise UnsupportedOption('not implemented on the B200 path: ' + '; '.join(unsupported))
+
+    # ---- derived host fields (factory.py:397-457)
+    shape2 = (nx, ny)
+    if forcing is None:
+        tau_x = tau_y = q_heat = None
+    else:
+        tau_x, tau_y, q_heat = (_f64(a, shape2) for a in forcing)
+    fields = dict(tau_x=tau_x, tau_y=tau_y, q_heat=q_heat)
+    if T_atm is not None and lambda_bulk > 0.0:
+        fields['t_atm'] = _f64(T_atm, shape2)
+    else:
+        lambda_bulk = 0.0
+    restore_coef_S = 0.0
+    if S_ref_surf is not None and sss_restore_days > 0.0:
+        fields['s_ref'] = _f64(S_ref_surf, shape2)
+        restore_coef_S = 1.0 / (sss_restore_days * 86400.0)
+
+    def coastal(mask, coefficient):
+        return _f64(mask, shape2) * coefficient if mask is not None and coefficient > 0.0 else None
+
+    fields['coastal_kappa_v'] = coastal(coastal_kappa_v_mask, coastal_kappa_v)
+    fields['coastal_kappa_h'] = coastal(coastal_kappa_h_mask, coastal_kappa_h)
+    fields['coastal_bulk_lambda'] = coastal(coastal_bulk_mask, coastal_bulk_lambda)
+    if coastal_restore_mask is not None and coastal_restore_days > 0.0 and coastal_restore_T is not None:
+        fields['coastal_restore_coef'] = _f64(coastal_restore_mask, shape2) / (coastal_restore_days * 86400.0)
+        fields['coastal_restore_t'] = _f64(coastal_restore_T, shape2)
+    if nu_nsub == 'cfl':
+        inv_dx2_max = float(np.max(np.asarray(grid.dx_2d, dtype=np.float64) ** -2))
+        nu_nsub = max(1, int(np.ceil(physics.nu_h * (dt / 2.0) * (inv_dx2_max + 1.0 / float(grid.dy) ** 2) / 0.25)))
+    opts = dict(dt_bt=dt_bt, lambda_bulk=float(lambda_bulk), restore_coef_S=restore_coef_S,
+                ice_salt_flux=ice_salt_flux, ice_freeze_temp_c=ice_freeze_temp_c, nu_nsub=nu_nsub,
+                polar_cap_rows=polar_cap_rows, polar_cap_taper=polar_cap_taper, fct_adv=fct_adv,
+                monotone_adv=monotone_adv, localize_conv=localize_conv, conservative_kv=conservative_kv,
+                freeze_adv_vel=freeze_adv_vel, vertical_diffusion=vertical_diffusion, fields=fields)
+    solver = _Solver(grid, physics, dt, opts)
+    wet3 = np.asarray(getattr(grid, 'wet_mask_3d', None) if getattr(grid, 'wet_mask_3d', None) is not None
+                      else np.broadcast_to(np.asarray(grid.wet_mask)[:, :, None], (nx, ny, nz)), dtype=np.float64)
+    T_ref, S_ref = float(physics.T_ref), float(physics.S_ref)
+
+    def _run(state, nsteps):
+        import torch
+        if isinstance(state.u, np.ndarray):
+            host = [np.ascontiguousarray(getattr(state, k), dtype=np.float32) for k in ("u", "v", "T", "S", "eta")]
+            out = [np.empty_like(a) for a in host]
+            sin = _native.ZmState(*[a.ctypes.data for a in host])
+            sout = _native.ZmState(*[a.ctypes.data for a in out])
+            solver.check(solver.lib.zm_step_host(solver.handle, None, ctypes.byref(sin), ctypes.byref(sout),
+                                                 int(nsteps)), "zm_step_host")
+            return JaxStateG(*out, state.ice)
+        fin = _torch_state_ptrs(state, solver.shape)
+        out = [torch.empty_like(t) for t in fin]
+        stream = torch.cuda.current_stream(fin[0].device).cuda_stream
+        sin = _native.ZmState(*[t.data_ptr() for t in fin])
+        sout = _native.ZmState(*[t.data_ptr() for t in out])
+        solver.check(solver.lib.zm_step(solver.handle, ctypes.c_void_p(stream), ctypes.byref(sin),
+                                        ctypes.byref(sout), int(nsteps)), "zm_step")
+        return JaxStateG(*out, state.ice)
+
+    def step(state):
+        """One baroclinic step (factory.py:724-726)."""
+        return _run(state, 1)
+
+    def init_state(T_init=None, S_init=None):
+        """Rest state with the land/ghost T_ref/S_ref sentinel (factory.py:766-788)."""
+        import torch
+        shape = solver.shape
+        T = np.full(shape, T_ref) if T_init is None else np.asarray(T_init, dtype=np.float64)
+        S = (np.full(shape, S_ref) if S_init is None else np.asarray(S_init, dtype=np.float64)) \
+            if T_init is not None else np.full(shape, S_ref)
+        T = T * wet3 + (1.0 - wet3) * T_ref
+        S = S * wet3 + (1.0 - wet3) * S_ref
+        dev = torch.device('cuda')
+        as_t = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float32), device=dev)
+        zeros3 = torch.zeros(shape, dtype=torch.float32, device=dev)
+        return JaxStateG(zeros3, zeros3.clone(), as_t(T), as_t(S),
+                         torch.zeros(shape[:2], dtype=torch.float32, device=dev),
+                         torch.zeros(shape[:2], dtype=torch.float32, device=dev))
+
+    def diagnostics(state, surface_pressure_pa=None):
+        raise NotImplementedError("diagnostics (rho, pressure, w) are not implemented on the B200 path yet")
+
+    step.solver = solver
+    step.advance = _run
+    result = [step, init_state, diagnostics]
+    if return_params:
+        params = dict(n_subcyc=solver.n_subcyc, nu_nsub=solver.n_nu, adv_nsub=solver.adv_nsub,
+                      conv_nsub=solver.conv_nsub, dt_bt=float(dt) / solver.n_subcyc, H_sw=float(np.sum(grid.dz)),
+                      rho0=RHO_0)
+
+        def terms_fn(state):
+            raise NotImplementedError("tracer term decomposition is not implemented on the B200 path")
+
+        result += [params, terms_fn]
+    if dynamic_forcing:
+        def step_dyn(state, tau_x, tau_y, q_heat, T_atm_3d=None, surface_pressure_pa=None):
+            """Step with runtime 2-D forcing (factory.py:735-750)."""
+            import torch
+            if T_atm_3d is not None or surface_pressure_pa is not None:
+                raise UnsupportedOption('runtime T_atm / surface pressure are not implemented on the B200 path')
+            fs = [torch.as_tensor(np.asarray(a, dtype=np.float32) if not isinstance(a, torch.Tensor) else a,
+                                  dtype=torch.float32, device='cuda').contiguous() for a in (tau_x, tau_y, q_heat)]
+            stream = torch.cuda.current_stream().cuda_stream
+            solver.check(solver.lib.zm_set_forcing(solver.handle, ctypes.c_void_p(stream),
+                                                   *[ctypes.c_void_p(t.data_ptr()) for t in fs]), "zm_set_forcing")
+            return step(state)
+
+        result.append(step_dyn)
+    return tuple(result)
