@@ -128,7 +128,14 @@ int zm_set_forcing(zm_solver* s, void* stream, const float* tau_x, const float* 
 
 /* Run one stage of the step on a device state, for stage-level checks:
  * 1 = linear half step L(dt/2) (step.py:76-187), 2 = nonlinear step N(dt)
- * (step.py:249-320), 3 = one full step. */
+ * (step.py:249-320), 3 = one full step, 4 = the velocity-only part of the
+ * momentum residual into out->u/v (dealiased advection + surface wind -
+ * barotropic wind, wet-masked; tendencies.py:39-72, 247-319), 5 = its
+ * density part (baroclinic pressure-gradient force minus its barotropic
+ * layer average, wet-masked; pressure.py:86-97, 144-180) into out->u/v,
+ * 6 = the advection of stage 4 before its longitude filter (latitude
+ * filter applied, no wind, no mask) into out->u/v.
+ * out->T/S/eta receive the input fields for stages 4 to 6. */
 int zm_run_stage(zm_solver* s, void* stream, int32_t stage, const zm_state* in, zm_state* out);
 
 /* Kernel classes reported by zm_profile. */

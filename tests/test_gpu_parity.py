@@ -108,3 +108,48 @@ def test_implicit_vertical_diffusion_matches_oracle():
     want = ostep.linear_half_step(dict(state), p, p.dt / 2)
     errs = gu.errors(got, want, ("u", "v", "T", "S"))
     assert max(errs.values()) < STAGE_TOL, errs
+
+
+def _moving(p, T, S, seed=5, amp=0.1):
+    rng = np.random.default_rng(seed)
+    from oracle.params import init_state
+    st = gu.f32(init_state(p, T, S))
+    wm = p.wet_mask_z
+    st["u"] = gu.f32({k: amp * rng.standard_normal(wm.shape) * wm for k in gu.FIELDS})["u"]
+    st["v"] = gu.f32({k: amp * rng.standard_normal(wm.shape) * wm for k in gu.FIELDS})["v"]
+    st["v"][:, 0] = 0.0
+    st["v"][:, -1] = 0.0
+    return st
+
+
+@pytest.mark.parametrize("shape", [(24, 16, 6), (90, 45, 15), (180, 24, 10)])
+def test_momentum_advection_part_matches_oracle(shape):
+    """Dealiased advection + wind part of the momentum residual (stage 4),
+    including grids whose longitude mask drops the +-nx/3 bins."""
+    from oracle.params import RHO_0
+    grid, physics, dt, kw, T, S = workloads.make_case("plain", *shape, dtype="float32")
+    gpu, p = gu.build_pair(grid, physics, dt, kw)
+    st = _moving(p, T, S)
+    w = ostep.vertical_velocity(st["u"], st["v"], p)
+    ax, ay = ostep.momentum_advection(st["u"], st["v"], w, p)
+    wind = lambda tau: (tau[:, :, None] * p.surface_mask / (RHO_0 * p.dz_surface)
+                        - (tau / (RHO_0 * p.H_sw))[:, :, None]) * p.wet_mask_z
+    got = gu.run_stage(gpu, 4, st)
+    err_u = gu.rel_l2(got["u"] - wind(p.tau_x_2d), ax)
+    err_v = gu.rel_l2(got["v"] - wind(p.tau_y_2d), ay)
+    assert max(err_u, err_v) < 1e-5, (err_u, err_v)
+
+
+@pytest.mark.parametrize("shape", [(24, 16, 6), (90, 45, 15)])
+def test_pressure_part_matches_oracle(shape):
+    """Baroclinic pressure-gradient force minus its barotropic layer mean (stage 5)."""
+    from oracle.params import RHO_0
+    grid, physics, dt, kw, T, S = workloads.make_case("plain", *shape, dtype="float32")
+    gpu, p = gu.build_pair(grid, physics, dt, kw)
+    st = _moving(p, T, S)
+    gx, gy = ostep.gradient_conservative_3d(ostep.baroclinic_pressure(st["T"], st["S"], p), p)
+    fx, fy = ostep.bt_rho_pgf(st["T"], st["S"], p)
+    got = gu.run_stage(gpu, 5, st)
+    err_u = gu.rel_l2(got["u"], (-gx / RHO_0 - fx[:, :, None]) * p.wet_mask_z)
+    err_v = gu.rel_l2(got["v"], (-gy / RHO_0 - fy[:, :, None]) * p.wet_mask_z)
+    assert max(err_u, err_v) < 1e-5, (err_u, err_v)

@@ -1,6 +1,10 @@
 // Longitude half of the momentum-advection dealias filter
-// (numerics/horizontal.py:283-305): FFT along each periodic x-line, zero every
-// bin with |k| > floor(nx/2 * 2/3) (factory.py:529-533), inverse FFT, real part.
+// (numerics/horizontal.py:283-305): FFT along each periodic x-line, zero the
+// bins outside the 2/3-rule mask (factory.py:529-533), inverse FFT, real part.
+// The mask is the reference's own floating-point expression evaluated on the
+// host, bin by bin: |fftfreq(nx) * nx| <= floor(nx/2 * 2/3) drops the
+// boundary bins +-nx/3 for nx = 90, 180, 360, 720 because the product rounds
+// just above the integer.
 //
 // The two advection fields of a line are packed as one complex signal
 // (adv_u + i adv_v); the filter mask is real and even, so the filtered real
@@ -133,12 +137,11 @@ __global__ void __launch_bounds__(256) k_dealias_lon(Dev d, FftPlan plan, const 
   __syncthreads();
   float2* spec = fft_lines(bufa, bufb, tw, plan, lines);
   float2* other = spec == bufa ? bufb : bufa;
-  // 2/3 rule: keep |k| <= keep; conjugate for the inverse transform
+  // 2/3 rule with the reference's bin mask; conjugate for the inverse transform
   for (int t = threadIdx.x; t < lines * n; t += blockDim.x) {
     const int m = t % n;
-    const int km = m < n - m ? m : n - m;
     float2 z = spec[t];
-    spec[t] = km <= plan.keep ? make_float2(z.x, -z.y) : make_float2(0.f, 0.f);
+    spec[t] = __ldg(plan.keepbin + m) ? make_float2(z.x, -z.y) : make_float2(0.f, 0.f);
   }
   __syncthreads();
   float2* res = fft_lines(spec, other, tw, plan, lines);

@@ -112,13 +112,124 @@ __device__ __forceinline__ float vdiff_tracer(const Dev& d, const float* __restr
   const long long id = idx3(d, k, j, i);
 
 // ------------------------------------------------------------------ L half step
-// One nu_h Laplacian subcycle on (u, v) (timestepping/step.py:94-107).
-__global__ void __launch_bounds__(256) k_nu_sub(Dev d, const float* __restrict__ u, const float* __restrict__ v,
-                                                float* __restrict__ uo, float* __restrict__ vo, float dts) {
-  ZM_POINT_IDX
-  const Nb n = nb(d, j, i);
-  uo[id] = ld(u, id) + d.nu_h * lap_h(d, u, k, n) * dts;
-  vo[id] = ld(v, id) + d.nu_h * lap_h(d, v, k, n) * dts;
+// nu_h Laplacian subcycles on (u, v) (timestepping/step.py:94-107), several
+// subcycles per pass.  Each block holds a NB_W x NB_W tile of one level in
+// shared memory; every thread owns one column of the tile and keeps a strip of
+// NB_R rows of u and v in registers.  A subcycle reads the x neighbours and
+// the strip-end y neighbours from shared memory and the inner y neighbours
+// from registers.  Values at the tile edge use themselves as missing
+// neighbours, so garbage enters one cell per subcycle: after nsub <= NB_T
+// subcycles the inner (NB_W - 2 NB_T)^2 points are exact.  The closed
+// latitude walls use the mirror ghost (the wall row is its own outer
+// neighbour); longitude wraps.  Face gates are kept as bits, the metric
+// factors per row of the strip, so two blocks fit on an SM.
+__global__ void __launch_bounds__(NB_W * NB_W / NB_R, 2)
+k_nu_tb(Dev d, const float* __restrict__ u, const float* __restrict__ v, float* __restrict__ uo,
+        float* __restrict__ vo, float c, int nsub) {
+  extern __shared__ float nb_smem[];
+  float(*su)[NB_W] = reinterpret_cast<float(*)[NB_W]>(nb_smem);
+  float(*sv)[NB_W] = reinterpret_cast<float(*)[NB_W]>(nb_smem + NB_W * NB_W);
+  float(*sx2)[NB_W] = reinterpret_cast<float(*)[NB_W]>(nb_smem + 2 * NB_W * NB_W);
+  float* stR = nb_smem + 3 * NB_W * NB_W;
+  unsigned char(*sw)[NB_W] = reinterpret_cast<unsigned char(*)[NB_W]>(nb_smem + 3 * NB_W * NB_W + NB_W);
+  constexpr int TI = NB_W - 2 * NB_T;
+  const int k = blockIdx.z;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int gx0 = blockIdx.x * TI - NB_T, gy0 = blockIdx.y * TI - NB_T;
+  int gi = (gx0 + tx) % d.nx;
+  if (gi < 0) gi += d.nx;
+  const long long kb = (long long)k * d.plane;
+  const int r0 = ty * NB_R;
+  if (ty == 0) {
+    int gj = gy0 + tx;
+    gj = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
+    stR[tx] = 0.5f * d.inv_dy * __ldg(d.tanR + gj);
+  }
+  float au[NB_R], av[NB_R];
+#pragma unroll
+  for (int q = 0; q < NB_R; ++q) {
+    int gj = gy0 + r0 + q;
+    gj = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
+    const long long id = kb + (long long)gj * d.P + gi;
+    au[q] = ld(u, id);
+    av[q] = ld(v, id);
+    su[r0 + q][tx] = au[q];
+    sv[r0 + q][tx] = av[q];
+    sw[r0 + q][tx] = (unsigned char)wetb(wb(d, gj, gi), k);
+    sx2[r0 + q][tx] = __ldg(d.inv_dx2 + idx2(d, gj, gi));
+  }
+  __syncthreads();
+  // gate bits per point q: 6q+0 east, +1 west, +2 north, +3 south face open;
+  // +4 north neighbour exists, +5 south neighbour exists
+  unsigned long long g = 0ull;
+#pragma unroll
+  for (int q = 0; q < NB_R; ++q) {
+    const int r = r0 + q;
+    const int gj = gy0 + r;
+    const bool w0 = sw[r][tx];
+    const bool we = tx + 1 < NB_W && sw[r][tx + 1];
+    const bool ww = tx > 0 && sw[r][tx - 1];
+    const bool n_ok = gj < d.ny - 1 && r + 1 < NB_W;
+    const bool s_ok = gj > 0 && r > 0;
+    const bool wn = n_ok && sw[r + 1][tx];
+    const bool ws = s_ok && sw[r - 1][tx];
+    const unsigned long long bits = (unsigned long long)((w0 && we) | ((w0 && ww) << 1) | ((w0 && wn) << 2) |
+                                                         ((w0 && ws) << 3) | (n_ok << 4) | (s_ok << 5));
+    g |= bits << (6 * q);
+  }
+  const float idy2 = d.inv_dy2;
+  const float cn = d.nu_h * c;
+  for (int s = 0; s < nsub; ++s) {
+    // the strip is updated in place; pu/pv keep the pre-update value of the
+    // row above for the next row's south neighbour
+    float pu = 0.f, pv = 0.f;
+#pragma unroll
+    for (int q = 0; q < NB_R; ++q) {
+      const int r = r0 + q;
+      const unsigned b = (unsigned)(g >> (6 * q)) & 63u;
+      const float u0 = au[q], v0 = av[q];
+      const float ue = tx + 1 < NB_W ? su[r][tx + 1] : u0, uw = tx > 0 ? su[r][tx - 1] : u0;
+      const float ve = tx + 1 < NB_W ? sv[r][tx + 1] : v0, vw = tx > 0 ? sv[r][tx - 1] : v0;
+      float un = u0, vn = v0, us = u0, vs = v0;
+      if (b & 16u) {
+        un = q + 1 < NB_R ? au[q + 1] : su[r + 1][tx];
+        vn = q + 1 < NB_R ? av[q + 1] : sv[r + 1][tx];
+      }
+      if (b & 32u) {
+        us = q > 0 ? pu : su[r - 1][tx];
+        vs = q > 0 ? pv : sv[r - 1][tx];
+      }
+      const float ix2 = sx2[r][tx];
+      const float cE = (b & 1u) ? ix2 : 0.f, cW = (b & 2u) ? ix2 : 0.f;
+      const float cN = (b & 4u) ? idy2 : 0.f, cS = (b & 8u) ? idy2 : 0.f;
+      const float tr = stR[r];
+      const float lu = cE * (ue - u0) - cW * (u0 - uw) + cN * (un - u0) - cS * (u0 - us) - tr * (un - us);
+      const float lv = cE * (ve - v0) - cW * (v0 - vw) + cN * (vn - v0) - cS * (v0 - vs) - tr * (vn - vs);
+      pu = u0;
+      pv = v0;
+      au[q] = u0 + lu * cn;
+      av[q] = v0 + lv * cn;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < NB_R; ++q) {
+      su[r0 + q][tx] = au[q];
+      sv[r0 + q][tx] = av[q];
+    }
+    __syncthreads();
+  }
+  // write the exact interior
+  const int ix = gx0 + tx;
+  if (tx < NB_T || tx >= NB_W - NB_T || ix >= d.nx) return;
+#pragma unroll
+  for (int q = 0; q < NB_R; ++q) {
+    const int r = r0 + q;
+    const int gj = gy0 + r;
+    if (r < NB_T || r >= NB_W - NB_T || gj >= d.ny) continue;
+    const long long id = kb + (long long)gj * d.P + ix;
+    uo[id] = au[q];
+    vo[id] = av[q];
+  }
 }
 
 // Inner Laplacians for the biharmonic operators: velocity (horizontal.py:251)

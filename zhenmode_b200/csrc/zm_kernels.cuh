@@ -8,7 +8,8 @@ namespace zm {
 struct FftPlan {
   int n, nstages, keep;
   int radix[24];
-  const float2* tw;  // exp(-2 pi i m / n), m < n
+  const float2* tw;             // exp(-2 pi i m / n), m < n
+  const unsigned char* keepbin; // 1 where bin m survives the 2/3 rule, m < n
 };
 
 struct PgfArgs {
@@ -26,7 +27,12 @@ struct RestArgs {
   int nc, stage;
 };
 
-__global__ void k_nu_sub(Dev d, const float* u, const float* v, float* uo, float* vo, float dts);
+// temporally blocked nu_h subcycles: tile width, rows per thread, subcycles per pass
+constexpr int NB_W = 64;
+constexpr int NB_R = 8;
+constexpr int NB_T = 6;
+constexpr size_t NB_SMEM = (size_t)(3 * NB_W * NB_W + NB_W) * sizeof(float) + (size_t)NB_W * NB_W;
+__global__ void k_nu_tb(Dev d, const float* u, const float* v, float* uo, float* vo, float c, int nsub);
 __global__ void k_inner_lap(Dev d, const float* u, const float* v, const float* T, const float* S, float* Lu,
                             float* Lv, float* LT, float* LS, int do_uv, int do_ts);
 __global__ void k_lin_finish(Dev d, const float* usub, const float* vsub, const float* u0, const float* v0,

@@ -143,13 +143,20 @@ struct zm_solver {
       const float dts = (float)(dt / 2.0 / n_nu);
       const float* a = src.u;
       const float* c = src.v;
-      for (int n = 0; n < n_nu; ++n) {
-        const Fields4& o = (n % 2 == 0) ? W1 : W2;
+      constexpr int TI = NB_W - 2 * NB_T;
+      const dim3 blk(NB_W, NB_W / NB_R);
+      const dim3 grd((nx + TI - 1) / TI, (ny + TI - 1) / TI, nz);
+      int done = 0, pass = 0;
+      while (done < n_nu) {
+        const int nsub = std::min(NB_T, n_nu - done);
+        const Fields4& o = (pass % 2 == 0) ? W1 : W2;
         pb(ZM_K_NU_SUB, s);
-        k_nu_sub<<<grid3(b), b, 0, s>>>(d, a, c, o.u, o.v, dts);
+        k_nu_tb<<<grd, blk, NB_SMEM, s>>>(d, a, c, o.u, o.v, dts, nsub);
         pe(s);
         a = o.u;
         c = o.v;
+        done += nsub;
+        ++pass;
       }
       usub = a;
       vsub = c;
@@ -206,8 +213,9 @@ struct zm_solver {
     check_launch();
   }
 
-  // Nonlinear RK2 step N(dt): src -> dst.
-  void nonlinear(cudaStream_t s, const Fields4& src, const Fields4& dst) {
+  // T/S-independent part of the momentum residual, A = wm (dealiased
+  // advection + surface wind - barotropic wind), into Au/Av.
+  void momentum_advection_part(cudaStream_t s, const Fields4& src) {
     const dim3 c(32, 4);
     pb(ZM_K_FZ, s);
     k_fz<<<grid2(c), c, 0, s>>>(d, src.u, src.v, Fz);
@@ -221,6 +229,30 @@ struct zm_solver {
     k_dealias_lon<<<(nlines + fft_lines - 1) / fft_lines, 256, fft_smem, s>>>(d, fft, Ayu, Ayv, Au, Av, fft_lines);
     pe(s);
     check_launch();
+  }
+
+  // Pressure part P = wm (pgf_bc - F_rho) of the state's T/S, into Pu/Pv
+  // (diagnostic stage; the step itself fuses it with the RK combination).
+  void pressure_part(cudaStream_t s, const Fields4& src) {
+    ZM_CUDA(cudaMemsetAsync(Au, 0, n3 * sizeof(float), s));
+    ZM_CUDA(cudaMemsetAsync(Av, 0, n3 * sizeof(float), s));
+    PgfArgs a{};
+    a.T = src.T; a.S = src.S; a.u1 = src.u; a.v1 = src.v; a.Au = Au; a.Av = Av;
+    a.Pu = Pu; a.Pv = Pv; a.uo = up; a.vo = vp; a.dt = (float)dt; a.mode = 1;
+    pgf(s, a);
+  }
+
+  void copy_uv(cudaStream_t s, const float* a, const float* b, const Fields4& src, const Fields4& dst) {
+    ZM_CUDA(cudaMemcpyAsync(dst.u, a, n3 * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    ZM_CUDA(cudaMemcpyAsync(dst.v, b, n3 * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    ZM_CUDA(cudaMemcpyAsync(dst.T, src.T, n3 * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    ZM_CUDA(cudaMemcpyAsync(dst.S, src.S, n3 * sizeof(float), cudaMemcpyDeviceToDevice, s));
+  }
+
+  // Nonlinear RK2 step N(dt): src -> dst.
+  void nonlinear(cudaStream_t s, const Fields4& src, const Fields4& dst) {
+    const dim3 c(32, 4);
+    momentum_advection_part(s, src);
     // stage 1: tracers at the old velocity, momentum with the predicted tracers
     tracer_residual(s, 1, src.u, src.v, src.T, src.S, src.T, src.S, Tp, Sp);
     PgfArgs a{};
@@ -568,11 +600,25 @@ void build(zm_solver* s, const zm_grid* g, const zm_params* p) {
     tw[m] = make_float2((float)std::cos(a), (float)std::sin(a));
   }
   plan.tw = s->upload(tw);
+  // 2/3-rule bin mask exactly as the reference forms it: numpy's
+  // fftfreq(nx) * nx in float64, |.| <= keep
+  std::vector<unsigned char> keepbin(nx);
+  {
+    const int half = (nx - 1) / 2 + 1;
+    const double val = 1.0 / (double)nx;
+    for (int m = 0; m < nx; ++m) {
+      const int ms = m < half ? m : m - nx;
+      const double kidx = ((double)ms * val) * (double)nx;
+      keepbin[m] = std::fabs(kidx) <= (double)plan.keep ? 1 : 0;
+    }
+  }
+  plan.keepbin = s->upload(keepbin);
   s->fft = plan;
   s->fft_lines = std::max(1, std::min(8, (int)((200 * 1024 / sizeof(float2) - nx) / (2 * nx))));
   s->fft_smem = ((size_t)nx + (size_t)2 * s->fft_lines * nx) * sizeof(float2);
   require(s->fft_smem <= 227 * 1024, ZM_ERR_UNSUPPORTED, "nx too large for the shared-memory FFT filter");
   ZM_CUDA(cudaFuncSetAttribute(k_dealias_lon, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->fft_smem));
+  ZM_CUDA(cudaFuncSetAttribute(k_nu_tb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)NB_SMEM));
   ZM_CUDA(cudaFuncSetAttribute(k_pgf, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * nz * 64 * (int)sizeof(float)));
   // ---- buffers
   for (int q = 0; q < 2; ++q) {
@@ -721,7 +767,7 @@ int zm_set_forcing(zm_solver* s, void* stream, const float* tau_x, const float* 
 }
 
 int zm_run_stage(zm_solver* s, void* stream, int32_t stage, const zm_state* in, zm_state* out) {
-  if (!s || !in || !out || stage < 1 || stage > 3) return ZM_ERR_INVALID;
+  if (!s || !in || !out || stage < 1 || stage > 7) return ZM_ERR_INVALID;
   cudaStream_t st = (cudaStream_t)stream;
   try {
     s->load(st, in, s->st[s->cur], s->eta[s->cur]);
@@ -730,8 +776,23 @@ int zm_run_stage(zm_solver* s, void* stream, int32_t stage, const zm_state* in, 
       s->linear_half(st, s->st[a], s->st[b]);
     } else if (stage == 2) {
       s->nonlinear(st, s->st[a], s->st[b]);
-    } else {
+    } else if (stage == 3) {
       s->full_step(st, a, b);
+    } else if (stage == 4) {
+      s->momentum_advection_part(st, s->st[a]);
+      s->copy_uv(st, s->Au, s->Av, s->st[a], s->st[b]);
+    } else if (stage == 5) {
+      s->pressure_part(st, s->st[a]);
+      s->copy_uv(st, s->Pu, s->Pv, s->st[a], s->st[b]);
+    } else if (stage == 6) {
+      s->momentum_advection_part(st, s->st[a]);
+      s->copy_uv(st, s->Ayu, s->Ayv, s->st[a], s->st[b]);
+    } else {
+      const int nlines = s->ny * s->nz;
+      k_dealias_lon<<<(nlines + s->fft_lines - 1) / s->fft_lines, 256, s->fft_smem, st>>>(
+          s->d, s->fft, s->st[a].u, s->st[a].v, s->Au, s->Av, s->fft_lines);
+      s->check_launch();
+      s->copy_uv(st, s->Au, s->Av, s->st[a], s->st[b]);
     }
     if (stage != 3)
       ZM_CUDA(cudaMemcpyAsync(s->eta[b], s->eta[a], s->n2 * sizeof(float), cudaMemcpyDeviceToDevice, st));
