@@ -164,6 +164,31 @@ int zm_profile(zm_solver* s, void* stream, float* ms, int32_t* launches, int32_t
  * Synchronizes the stream given to zm_advance. */
 int zm_status(zm_solver* s, int32_t* monitor_code);
 
+/* Classify a float32 state held in the caller's device arrays (reference
+ * layout) without allocating any device memory.  No counterpart in the
+ * reference: its classify_state (runtime/monitor.py:20-30) runs inside JAX,
+ * which owns all device memory.  This is for callers that cannot call
+ * cudaMalloc: a runtime whose memory pool already holds the GPU (XLA
+ * preallocates most of it), a check made after a blow-up exhausted that pool,
+ * or a coupler working within a fixed memory budget.
+ *
+ * metrics (host, 4 floats): max |u|, max(|u|, |v|), max |eta| (over finite
+ * values) and 1 if every value is finite else 0; *code: 0 accepted,
+ * 1 non-finite, 3 velocity above velocity_limit, 4 |eta| above eta_limit
+ * (>= with inclusive != 0).  Synchronizes `stream`.
+ *
+ * Its only scratch is a fixed ZM_NOALLOC_SCRATCH_BYTES array inside the
+ * library, held by every GPU that loads it until exit.  Fields of more than
+ * ZM_NOALLOC_MAX_POINTS points are rejected with ZM_ERR_INVALID.  The first
+ * call on a device looks up the array's device address; make that first call
+ * before any stream capture.  All calls on a device share the array: calls
+ * whose work overlaps on the GPU race, so order them. */
+#define ZM_NOALLOC_SCRATCH_BYTES 33024
+#define ZM_NOALLOC_MAX_POINTS 134217728LL
+int zm_classify_state_noalloc(void* stream, int32_t nx, int32_t ny, int32_t nz, const float* u, const float* v,
+                              const float* T, const float* S, const float* eta, float velocity_limit,
+                              float eta_limit, int32_t inclusive, float* metrics, int32_t* code);
+
 /* Message of the last failure on this handle ("" if none). */
 const char* zm_last_error(const zm_solver* s);
 
