@@ -185,6 +185,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grid", default=None, help="NXxNYxNZ: same option set on another grid (profiling cases)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -207,7 +208,11 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
 
     wl = workloads.WORKLOADS[WORKLOAD]
-    grid, physics, dt, kw, T, S = workloads.make_case(WORKLOAD, dtype="float32")
+    if args.grid:
+        import dataclasses
+        gnx, gny, gnz = (int(x) for x in args.grid.lower().split("x"))
+        wl = dataclasses.replace(wl, nx=gnx, ny=gny, nz=gnz)
+    grid, physics, dt, kw, T, S = workloads.make_case(WORKLOAD, wl.nx, wl.ny, wl.nz, dtype="float32")
     step, init_state, _ = make_solver_global(grid, physics, dt, **kw)
     solver = step.solver
     st = init_state(T_init=T, S_init=S)

@@ -114,108 +114,97 @@ __device__ __forceinline__ float vdiff_tracer(const Dev& d, const float* __restr
 // ------------------------------------------------------------------ L half step
 // nu_h Laplacian subcycles on (u, v) (timestepping/step.py:94-107), several
 // subcycles per pass.  Each block holds a NB_W x NB_W tile of one level in
-// shared memory; every thread owns one column of the tile and keeps a strip of
-// NB_R rows of u and v in registers.  A subcycle reads the x neighbours and
-// the strip-end y neighbours from shared memory and the inner y neighbours
-// from registers.  Values at the tile edge use themselves as missing
-// neighbours, so garbage enters one cell per subcycle: after nsub <= NB_T
-// subcycles the inner (NB_W - 2 NB_T)^2 points are exact.  The closed
-// latitude walls use the mirror ghost (the wall row is its own outer
-// neighbour); longitude wraps.  Face gates are kept as bits, the metric
-// factors per row of the strip, so two blocks fit on an SM.
+// shared memory as interleaved (u, v) pairs with a one-cell border; every
+// thread owns one column of the tile and keeps a strip of NB_R rows in
+// registers.  Values at the tile edge read the border (zeros), so garbage
+// enters one cell per subcycle: after nsub <= NB_T subcycles the inner
+// (NB_W - 2 NB_T)^2 points are exact.
+//
+// The Laplacian of numerics/horizontal.py:181-215 is rewritten per point as
+//   lap = aE (uE - u0) + aW (uW - u0) + aN (uN - u0) + aS (uS - u0)
+// with aE/aW the gated x faces times 1/dx^2, aN = cN - t, aS = cS + t
+// (cN/cS the gated y faces times 1/dy^2, t = tan(lat)/(2 R dy) from the
+// metric term -(tan(lat)/R) du/dy), and the mirror ghost of the closed
+// walls folded in: at j = ny-1 the north neighbour equals u0, so aN = 0; at
+// j = 0, aS = 0.  The coefficients, scaled by nu_h dt_sub, are formed once
+// per pass.  Longitude wraps.
 __global__ void __launch_bounds__(NB_W * NB_W / NB_R, 2)
 k_nu_tb(Dev d, const float* __restrict__ u, const float* __restrict__ v, float* __restrict__ uo,
         float* __restrict__ vo, float c, int nsub) {
-  extern __shared__ float nb_smem[];
-  float(*su)[NB_W] = reinterpret_cast<float(*)[NB_W]>(nb_smem);
-  float(*sv)[NB_W] = reinterpret_cast<float(*)[NB_W]>(nb_smem + NB_W * NB_W);
-  float(*sx2)[NB_W] = reinterpret_cast<float(*)[NB_W]>(nb_smem + 2 * NB_W * NB_W);
-  float* stR = nb_smem + 3 * NB_W * NB_W;
-  unsigned char(*sw)[NB_W] = reinterpret_cast<unsigned char(*)[NB_W]>(nb_smem + 3 * NB_W * NB_W + NB_W);
+  extern __shared__ float4 nb_smem4[];
+  constexpr int PW = NB_W + 2;
+  float4* coef = nb_smem4;                                                  // [NB_W][NB_W]
+  float2* suv = reinterpret_cast<float2*>(nb_smem4 + NB_W * NB_W);          // [PW][PW]
+  unsigned char* sw = reinterpret_cast<unsigned char*>(suv + PW * PW);      // [NB_W][NB_W]
   constexpr int TI = NB_W - 2 * NB_T;
   const int k = blockIdx.z;
   const int tx = threadIdx.x, ty = threadIdx.y;
+  const int nt = blockDim.x * blockDim.y, tid = ty * blockDim.x + tx;
   const int gx0 = blockIdx.x * TI - NB_T, gy0 = blockIdx.y * TI - NB_T;
   int gi = (gx0 + tx) % d.nx;
   if (gi < 0) gi += d.nx;
   const long long kb = (long long)k * d.plane;
   const int r0 = ty * NB_R;
-  if (ty == 0) {
-    int gj = gy0 + tx;
-    gj = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
-    stR[tx] = 0.5f * d.inv_dy * __ldg(d.tanR + gj);
+  // zero the border ring
+  for (int e = tid; e < 4 * PW; e += nt) {
+    const int side = e / PW, p = e - side * PW;
+    const int rr = side == 0 ? 0 : (side == 1 ? PW - 1 : p);
+    const int cc = side == 0 || side == 1 ? p : (side == 2 ? 0 : PW - 1);
+    suv[rr * PW + cc] = make_float2(0.f, 0.f);
   }
-  float au[NB_R], av[NB_R];
+  float2 a[NB_R];
 #pragma unroll
   for (int q = 0; q < NB_R; ++q) {
     int gj = gy0 + r0 + q;
     gj = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
     const long long id = kb + (long long)gj * d.P + gi;
-    au[q] = ld(u, id);
-    av[q] = ld(v, id);
-    su[r0 + q][tx] = au[q];
-    sv[r0 + q][tx] = av[q];
-    sw[r0 + q][tx] = (unsigned char)wetb(wb(d, gj, gi), k);
-    sx2[r0 + q][tx] = __ldg(d.inv_dx2 + idx2(d, gj, gi));
+    a[q] = make_float2(ld(u, id), ld(v, id));
+    suv[(r0 + q + 1) * PW + tx + 1] = a[q];
+    sw[(r0 + q) * NB_W + tx] = (unsigned char)wetb(wb(d, gj, gi), k);
   }
   __syncthreads();
-  // gate bits per point q: 6q+0 east, +1 west, +2 north, +3 south face open;
-  // +4 north neighbour exists, +5 south neighbour exists
-  unsigned long long g = 0ull;
+  const float cn = d.nu_h * c;
 #pragma unroll
   for (int q = 0; q < NB_R; ++q) {
     const int r = r0 + q;
     const int gj = gy0 + r;
-    const bool w0 = sw[r][tx];
-    const bool we = tx + 1 < NB_W && sw[r][tx + 1];
-    const bool ww = tx > 0 && sw[r][tx - 1];
-    const bool n_ok = gj < d.ny - 1 && r + 1 < NB_W;
-    const bool s_ok = gj > 0 && r > 0;
-    const bool wn = n_ok && sw[r + 1][tx];
-    const bool ws = s_ok && sw[r - 1][tx];
-    const unsigned long long bits = (unsigned long long)((w0 && we) | ((w0 && ww) << 1) | ((w0 && wn) << 2) |
-                                                         ((w0 && ws) << 3) | (n_ok << 4) | (s_ok << 5));
-    g |= bits << (6 * q);
+    const int gjc = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
+    const bool w0 = sw[r * NB_W + tx];
+    const bool we = tx + 1 < NB_W && sw[r * NB_W + tx + 1];
+    const bool ww = tx > 0 && sw[r * NB_W + tx - 1];
+    const bool n_in = gj < d.ny - 1;   // north neighbour inside the domain
+    const bool s_in = gj > 0;
+    const bool wn = n_in && r + 1 < NB_W && sw[(r + 1) * NB_W + tx];
+    const bool ws = s_in && r > 0 && sw[(r - 1) * NB_W + tx];
+    const float ix2 = __ldg(d.inv_dx2 + idx2(d, gjc, gi));
+    const float t = 0.5f * d.inv_dy * __ldg(d.tanR + gjc);
+    const float cN = (w0 && wn) ? d.inv_dy2 : 0.f, cS = (w0 && ws) ? d.inv_dy2 : 0.f;
+    float4 cf;
+    cf.x = (w0 && we) ? ix2 * cn : 0.f;
+    cf.y = (w0 && ww) ? ix2 * cn : 0.f;
+    cf.z = n_in ? (cN - t) * cn : 0.f;
+    cf.w = s_in ? (cS + t) * cn : 0.f;
+    coef[r * NB_W + tx] = cf;
   }
-  const float idy2 = d.inv_dy2;
-  const float cn = d.nu_h * c;
   for (int s = 0; s < nsub; ++s) {
-    // the strip is updated in place; pu/pv keep the pre-update value of the
-    // row above for the next row's south neighbour
-    float pu = 0.f, pv = 0.f;
+    float2 above = suv[r0 * PW + tx + 1];  // row r0-1
 #pragma unroll
     for (int q = 0; q < NB_R; ++q) {
       const int r = r0 + q;
-      const unsigned b = (unsigned)(g >> (6 * q)) & 63u;
-      const float u0 = au[q], v0 = av[q];
-      const float ue = tx + 1 < NB_W ? su[r][tx + 1] : u0, uw = tx > 0 ? su[r][tx - 1] : u0;
-      const float ve = tx + 1 < NB_W ? sv[r][tx + 1] : v0, vw = tx > 0 ? sv[r][tx - 1] : v0;
-      float un = u0, vn = v0, us = u0, vs = v0;
-      if (b & 16u) {
-        un = q + 1 < NB_R ? au[q + 1] : su[r + 1][tx];
-        vn = q + 1 < NB_R ? av[q + 1] : sv[r + 1][tx];
-      }
-      if (b & 32u) {
-        us = q > 0 ? pu : su[r - 1][tx];
-        vs = q > 0 ? pv : sv[r - 1][tx];
-      }
-      const float ix2 = sx2[r][tx];
-      const float cE = (b & 1u) ? ix2 : 0.f, cW = (b & 2u) ? ix2 : 0.f;
-      const float cN = (b & 4u) ? idy2 : 0.f, cS = (b & 8u) ? idy2 : 0.f;
-      const float tr = stR[r];
-      const float lu = cE * (ue - u0) - cW * (u0 - uw) + cN * (un - u0) - cS * (u0 - us) - tr * (un - us);
-      const float lv = cE * (ve - v0) - cW * (v0 - vw) + cN * (vn - v0) - cS * (v0 - vs) - tr * (vn - vs);
-      pu = u0;
-      pv = v0;
-      au[q] = u0 + lu * cn;
-      av[q] = v0 + lv * cn;
+      const float4 cf = coef[r * NB_W + tx];
+      const float2 e = suv[(r + 1) * PW + tx + 2];
+      const float2 w = suv[(r + 1) * PW + tx];
+      const float2 nn = q + 1 < NB_R ? a[q + 1] : suv[(r + 2) * PW + tx + 1];
+      const float2 c0 = a[q];
+      float2 out;
+      out.x = c0.x + cf.x * (e.x - c0.x) + cf.y * (w.x - c0.x) + cf.z * (nn.x - c0.x) + cf.w * (above.x - c0.x);
+      out.y = c0.y + cf.x * (e.y - c0.y) + cf.y * (w.y - c0.y) + cf.z * (nn.y - c0.y) + cf.w * (above.y - c0.y);
+      above = c0;
+      a[q] = out;
     }
     __syncthreads();
 #pragma unroll
-    for (int q = 0; q < NB_R; ++q) {
-      su[r0 + q][tx] = au[q];
-      sv[r0 + q][tx] = av[q];
-    }
+    for (int q = 0; q < NB_R; ++q) suv[(r0 + q + 1) * PW + tx + 1] = a[q];
     __syncthreads();
   }
   // write the exact interior
@@ -227,81 +216,169 @@ k_nu_tb(Dev d, const float* __restrict__ u, const float* __restrict__ v, float* 
     const int gj = gy0 + r;
     if (r < NB_T || r >= NB_W - NB_T || gj >= d.ny) continue;
     const long long id = kb + (long long)gj * d.P + ix;
-    uo[id] = au[q];
-    vo[id] = av[q];
+    uo[id] = a[q].x;
+    vo[id] = a[q].y;
   }
 }
 
-// Inner Laplacians for the biharmonic operators: velocity (horizontal.py:251)
-// and the unit-diffusivity tracer flux operator (horizontal.py:245-249).
-__global__ void __launch_bounds__(256) k_inner_lap(Dev d, const float* __restrict__ u, const float* __restrict__ v,
-                                                   const float* __restrict__ T, const float* __restrict__ S,
-                                                   float* __restrict__ Lu, float* __restrict__ Lv,
-                                                   float* __restrict__ LT, float* __restrict__ LS, int do_uv, int do_ts) {
-  ZM_POINT_IDX
-  const Nb n = nb(d, j, i);
-  if (do_uv) {
-    Lu[id] = lap_h(d, u, k, n);
-    Lv[id] = lap_h(d, v, k, n);
+// Whole linear half step except the nu_h subcycles, on one level tile
+// (timestepping/step.py:108-173, legacy, mode split).  u0, v0, T0, S0 of the
+// level with a two-cell halo sit in shared memory; the inner Laplacians of
+// the biharmonic operators (numerics/horizontal.py:245-253) are formed on the
+// one-cell ring, the outer ones at the tile interior.  Rows beyond the closed
+// walls load the clamped row (the edge padding of horizontal.py:14-25); the
+// outer biharmonic applies the mirror to the inner Laplacian field, whose
+// edge row is padded by itself in the reference.  Vertical diffusion reads
+// the column neighbours directly; then land/ghost hold and the exact
+// Coriolis rotation by f dt/2.
+constexpr int LT_X = LT_TX, LT_Y = LT_TY, LT_H = 2;
+constexpr int LT_PX = LT_X + 2 * LT_H, LT_PY = LT_Y + 2 * LT_H;
+
+struct LtTile {
+  float u[LT_PY][LT_PX], v[LT_PY][LT_PX], T[LT_PY][LT_PX], S[LT_PY][LT_PX];
+  float Lu[LT_PY][LT_PX], Lv[LT_PY][LT_PX], LT[LT_PY][LT_PX], LS[LT_PY][LT_PX];
+  float w[LT_PY][LT_PX], kh[LT_PY][LT_PX], ix[LT_PY][LT_PX], ix2[LT_PY][LT_PX];
+  float tanR[LT_PY], cfp[LT_PY], icos[LT_PY];
+  int gj[LT_PY];
+};
+
+// Laplacian of a tile field at (r, c) (horizontal.py:181-215); `mirror`
+// replaces the outer neighbour at a wall row by the row itself.
+__device__ __forceinline__ float lap_s(const Dev& d, const LtTile& t, const float (*a)[LT_PX], int r, int c,
+                                      bool mirror) {
+  const float a0 = a[r][c], ae = a[r][c + 1], aw = a[r][c - 1];
+  float an = a[r + 1][c], as = a[r - 1][c];
+  if (mirror) {
+    if (t.gj[r] == d.ny - 1) an = a0;
+    if (t.gj[r] == 0) as = a0;
   }
-  if (do_ts) {
-    LT[id] = hdiff(d, T, nullptr, k, n);
-    LS[id] = hdiff(d, S, nullptr, k, n);
-  }
+  const float w0 = t.w[r][c];
+  const float d2x = ((ae - a0) * w0 * t.w[r][c + 1] - (a0 - aw) * w0 * t.w[r][c - 1]) * t.ix2[r][c];
+  const float d2y = ((an - a0) * t.w[r + 1][c] * w0 - (a0 - as) * w0 * t.w[r - 1][c]) * d.inv_dy2;
+  const float ddy = (an - as) * (0.5f * d.inv_dy);
+  return d2x + d2y + (-ddy * t.tanR[r]);
 }
 
-// Rest of the linear half step (timestepping/step.py:108-173, legacy,
-// mode split): biharmonic and vertical diffusion from the start-of-step
-// state, land/ghost hold, exact Coriolis rotation by f dt/2.
-__global__ void __launch_bounds__(256) k_lin_finish(Dev d, const float* __restrict__ usub, const float* __restrict__ vsub,
-                                                    const float* __restrict__ u0, const float* __restrict__ v0,
-                                                    const float* __restrict__ T0, const float* __restrict__ S0,
-                                                    const float* __restrict__ Lu, const float* __restrict__ Lv,
-                                                    const float* __restrict__ LT, const float* __restrict__ LS,
-                                                    float* __restrict__ uo, float* __restrict__ vo,
-                                                    float* __restrict__ To, float* __restrict__ So, float dth,
-                                                    int implicit_v) {
-  ZM_POINT_IDX
-  const Nb n = nb(d, j, i);
-  const uint64_t bits = wb(d, j, i);
-  const int kb = kbot_of(bits);
+// Wet-face flux diffusion of a tile field at (r, c) (horizontal.py:217-243);
+// unit diffusivity when `unit`.  The wall faces are closed explicitly.
+__device__ __forceinline__ float hdiff_s(const Dev& d, const LtTile& t, const float (*a)[LT_PX], int r, int c,
+                                        bool unit) {
+  const float a0 = a[r][c];
+  const float k0 = unit ? 1.f : t.kh[r][c];
+  const float ke = unit ? 1.f : t.kh[r][c + 1], kw = unit ? 1.f : t.kh[r][c - 1];
+  const float kn = unit ? 1.f : t.kh[r + 1][c], ks = unit ? 1.f : t.kh[r - 1][c];
+  const float w0 = t.w[r][c];
+  const float fe = 0.5f * (k0 + ke) * (a[r][c + 1] - a0) * t.ix[r][c] * w0 * t.w[r][c + 1];
+  const float fw = 0.5f * (kw + k0) * (a0 - a[r][c - 1]) * t.ix[r][c - 1] * t.w[r][c - 1] * w0;
+  const int gj = t.gj[r];
+  float fn = 0.f, fs = 0.f;
+  if (gj < d.ny - 1) fn = 0.5f * (k0 + kn) * (a[r + 1][c] - a0) * d.inv_dy * w0 * t.w[r + 1][c] * t.cfp[r];
+  if (gj > 0) fs = 0.5f * (ks + k0) * (a0 - a[r - 1][c]) * d.inv_dy * t.w[r - 1][c] * w0 * t.cfp[r - 1];
+  return (fe - fw) * t.ix[r][c] + (fn - fs) * d.inv_dy * t.icos[r];
+}
+
+size_t lin_tile_smem() { return sizeof(LtTile); }
+
+__global__ void __launch_bounds__(LT_X * LT_Y) k_lin_t(Dev d, const float* __restrict__ usub,
+                                                      const float* __restrict__ vsub, const float* __restrict__ u0,
+                                                      const float* __restrict__ v0, const float* __restrict__ T0,
+                                                      const float* __restrict__ S0, float* __restrict__ uo,
+                                                      float* __restrict__ vo, float* __restrict__ To,
+                                                      float* __restrict__ So, float dth, int implicit_v) {
+  extern __shared__ float lt_smem[];
+  LtTile& t = *reinterpret_cast<LtTile*>(lt_smem);
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = ty * LT_X + tx, nt = LT_X * LT_Y;
+  const int i0 = blockIdx.x * LT_X, j0 = blockIdx.y * LT_Y, k = blockIdx.z;
+  const long long kb = (long long)k * d.plane;
+  constexpr int NCELL = LT_PX * LT_PY;
+  for (int e = tid; e < NCELL; e += nt) {
+    const int r = e / LT_PX, cc = e - r * LT_PX;
+    int gj = j0 - LT_H + r;
+    gj = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
+    int gi = (i0 - LT_H + cc) % d.nx;
+    if (gi < 0) gi += d.nx;
+    const int c2 = idx2(d, gj, gi);
+    const long long g = kb + c2;
+    t.u[r][cc] = ld(u0, g);
+    t.v[r][cc] = ld(v0, g);
+    t.T[r][cc] = ld(T0, g);
+    t.S[r][cc] = ld(S0, g);
+    t.w[r][cc] = wetf(__ldg(d.wbits + c2), k);
+    t.kh[r][cc] = __ldg(d.kh2 + c2);
+    t.ix[r][cc] = __ldg(d.inv_dx + c2);
+    t.ix2[r][cc] = __ldg(d.inv_dx2 + c2);
+  }
+  if (tid < LT_PY) {
+    int gj = j0 - LT_H + tid;
+    gj = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
+    t.gj[tid] = gj;
+    t.tanR[tid] = __ldg(d.tanR + gj);
+    t.cfp[tid] = __ldg(d.cfp + gj);
+    t.icos[tid] = __ldg(d.inv_cos + gj);
+  }
+  __syncthreads();
+  const bool do_uv = d.nu_bi > 0.f, do_ts = d.kappa_bi > 0.f;
+  if (do_uv || do_ts) {
+    constexpr int RX = LT_X + 2, RY = LT_Y + 2;   // the one-cell ring around the interior
+    for (int e = tid; e < RX * RY; e += nt) {
+      const int r = 1 + e / RX, cc = 1 + e % RX;
+      if (do_uv) {
+        t.Lu[r][cc] = lap_s(d, t, t.u, r, cc, false);
+        t.Lv[r][cc] = lap_s(d, t, t.v, r, cc, false);
+      }
+      if (do_ts) {
+        t.LT[r][cc] = hdiff_s(d, t, t.T, r, cc, true);
+        t.LS[r][cc] = hdiff_s(d, t, t.S, r, cc, true);
+      }
+    }
+    __syncthreads();
+  }
+  const int i = i0 + tx, j = j0 + ty;
+  if (i >= d.nx || j >= d.ny) return;
+  const int r = ty + LT_H, cc = tx + LT_H;
   const long long base = idx2(d, j, i);
+  const long long id = kb + base;
+  const uint64_t bits = __ldg(d.wbits + base);
   const bool wet = wetb(bits, k);
-  const float kv = __ldg(d.kv2 + base);
-  // tracers
-  float T = ld(T0, id) + hdiff(d, T0, d.kh2, k, n) * dth;
-  float S = ld(S0, id) + hdiff(d, S0, d.kh2, k, n) * dth;
-  if (d.kappa_bi > 0.f) {
-    T = T - d.kappa_bi * hdiff(d, LT, nullptr, k, n) * dth;
-    S = S - d.kappa_bi * hdiff(d, LS, nullptr, k, n) * dth;
-  }
-  float u = ld(usub, id), v = ld(vsub, id);
-  if (d.nu_bi > 0.f) {
-    u = u - d.nu_bi * lap_h(d, Lu, k, n) * dth;
-    v = v - d.nu_bi * lap_h(d, Lv, k, n) * dth;
-  }
-  if (!implicit_v) {
-    u = u + d.nu_v * d2z(d, u0, base, k, kb) * dth;
-    v = v + d.nu_v * d2z(d, v0, base, k, kb) * dth;
-    T = T + vdiff_tracer(d, T0, base, k, bits, kv) * dth;
-    S = S + vdiff_tracer(d, S0, base, k, bits, kv) * dth;
-  }
+  float u, v, T, S;
   if (!wet) {
-    u = ld(u0, id);
-    v = ld(v0, id);
-    T = ld(T0, id);
-    S = ld(S0, id);
+    u = t.u[r][cc];
+    v = t.v[r][cc];
+    T = t.T[r][cc];
+    S = t.S[r][cc];
+  } else {
+    T = t.T[r][cc] + hdiff_s(d, t, t.T, r, cc, false) * dth;
+    S = t.S[r][cc] + hdiff_s(d, t, t.S, r, cc, false) * dth;
+    if (do_ts) {
+      T = T - d.kappa_bi * hdiff_s(d, t, t.LT, r, cc, true) * dth;
+      S = S - d.kappa_bi * hdiff_s(d, t, t.LS, r, cc, true) * dth;
+    }
+    u = ld(usub, id);
+    v = ld(vsub, id);
+    if (do_uv) {
+      u = u - d.nu_bi * lap_s(d, t, t.Lu, r, cc, true) * dth;
+      v = v - d.nu_bi * lap_s(d, t, t.Lv, r, cc, true) * dth;
+    }
+    if (!implicit_v) {
+      const int kbt = kbot_of(bits);
+      const float kv = __ldg(d.kv2 + base);
+      u = u + d.nu_v * d2z(d, u0, base, k, kbt) * dth;
+      v = v + d.nu_v * d2z(d, v0, base, k, kbt) * dth;
+      T = T + vdiff_tracer(d, T0, base, k, bits, kv) * dth;
+      S = S + vdiff_tracer(d, S0, base, k, bits, kv) * dth;
+    }
   }
   To[id] = T;
   So[id] = S;
-  if (implicit_v) {  // rotation happens after the column solve
+  if (implicit_v) {  // the column solve and the rotation follow
     uo[id] = u;
     vo[id] = v;
     return;
   }
-  const float c = __ldg(d.rot_c + base), s = __ldg(d.rot_s + base);
-  uo[id] = c * u + s * v;
-  vo[id] = -s * u + c * v;
+  const float c = __ldg(d.rot_c + base), sn = __ldg(d.rot_s + base);
+  uo[id] = c * u + sn * v;
+  vo[id] = -sn * u + c * v;
 }
 
 // Backward-Euler vertical diffusion, one column per thread (extension: the
@@ -501,109 +578,131 @@ __device__ __forceinline__ float minmod_slope(float cm, float c0, float cp, floa
   return 0.5f * sg * fminf(fabsf(l), fabsf(r)) * w0 * wm * wp;
 }
 
-// Zonal tracer flux through face i+1/2 (dynamics/transport.py:224-290).
-__device__ __forceinline__ float flux_x(const Dev& d, const float* __restrict__ c, const float* __restrict__ u,
-                                        long long b, int k, int j, int i) {
-  const int ie = east(d, i);
-  const float w0 = wetf(wb(d, j, i), k), we = wetf(wb(d, j, ie), k);
-  const float gate = w0 * we;
-  const float ux = 0.5f * (ld(u, b + idx2(d, j, i)) + ld(u, b + idx2(d, j, ie)));
-  const float c0 = ld(c, b + idx2(d, j, i)), ce = ld(c, b + idx2(d, j, ie));
+// Tracer advection substep on one level tile (dynamics/tendencies.py:111-140
+// with _advection_scalar, dynamics/transport.py:365-475): each block owns a
+// TA_X x TA_Y tile of one level; T, S, u, v of that level with a two-cell halo
+// (for the minmod slopes of the face states) and the level's wet flags sit in
+// shared memory.  Rows beyond the closed walls are loaded from the clamped row,
+// which is the edge padding of transport.py:199-290; longitude wraps.  The
+// vertical donor-cell flux reads the column neighbours directly.
+constexpr int TA_H = 2;
+constexpr int TA_PX = TA_X + 2 * TA_H, TA_PY = TA_Y + 2 * TA_H;
+
+struct TaTile {
+  float T[TA_PY][TA_PX];
+  float S[TA_PY][TA_PX];
+  float u[TA_PY][TA_PX];
+  float v[TA_PY][TA_PX];
+  float w[TA_PY][TA_PX];
+};
+
+__device__ __forceinline__ float ta_face_x(const Dev& d, const float (*c)[TA_PX], const TaTile& t, int r, int cc) {
+  // face between tile columns cc and cc+1 of row r
+  const float w0 = t.w[r][cc], we = t.w[r][cc + 1];
+  const float ux = 0.5f * (t.u[r][cc] + t.u[r][cc + 1]);
+  const float c0 = c[r][cc], ce = c[r][cc + 1];
   float cf;
   if (d.limiter == 2) {
-    if (ux >= 0.f) {
-      const int iw = west(d, i);
-      const float sx = minmod_slope(ld(c, b + idx2(d, j, iw)), c0, ce, wetf(wb(d, j, iw), k), w0, we);
-      cf = c0 + 0.5f * sx;
-    } else {
-      const int iee = east(d, ie);
-      const float sx = minmod_slope(c0, ce, ld(c, b + idx2(d, j, iee)), w0, we, wetf(wb(d, j, iee), k));
-      cf = ce - 0.5f * sx;
-    }
+    if (ux >= 0.f) cf = c0 + 0.5f * minmod_slope(c[r][cc - 1], c0, ce, t.w[r][cc - 1], w0, we);
+    else cf = ce - 0.5f * minmod_slope(c0, ce, c[r][cc + 2], w0, we, t.w[r][cc + 2]);
   } else if (d.limiter == 1) {
     cf = ux >= 0.f ? c0 : ce;
   } else {
     cf = 0.5f * (c0 + ce);
   }
-  return ux * cf * gate;
+  return ux * cf * (w0 * we);
 }
 
-// Meridional tracer flux through face j+1/2 (closed at the north wall).
-__device__ __forceinline__ float flux_y(const Dev& d, const float* __restrict__ c, const float* __restrict__ v,
-                                        long long b, int k, int j, int i) {
-  if (j >= d.ny - 1) return 0.f;
-  const int jn = j + 1;
-  const float w0 = wetf(wb(d, j, i), k), wn = wetf(wb(d, jn, i), k);
-  const float vy = 0.5f * (ld(v, b + idx2(d, j, i)) + ld(v, b + idx2(d, jn, i)));
-  const float c0 = ld(c, b + idx2(d, j, i)), cn = ld(c, b + idx2(d, jn, i));
+__device__ __forceinline__ float ta_face_y(const Dev& d, const float (*c)[TA_PX], const TaTile& t, int r, int cc,
+                                           int gj) {
+  // face between tile rows r and r+1 (global rows gj, gj+1); closed at the north wall
+  if (gj >= d.ny - 1) return 0.f;
+  const float w0 = t.w[r][cc], wn = t.w[r + 1][cc];
+  const float vy = 0.5f * (t.v[r][cc] + t.v[r + 1][cc]);
+  const float c0 = c[r][cc], cn = c[r + 1][cc];
   float cf;
   if (d.limiter == 2) {
-    if (vy >= 0.f) {
-      const int js = south(j);
-      const float sy = minmod_slope(ld(c, b + idx2(d, js, i)), c0, cn, wetf(wb(d, js, i), k), w0, wn);
-      cf = c0 + 0.5f * sy;
-    } else {
-      const int jnn = north(d, jn);
-      const float sy = minmod_slope(c0, cn, ld(c, b + idx2(d, jnn, i)), w0, wn, wetf(wb(d, jnn, i), k));
-      cf = cn - 0.5f * sy;
-    }
+    if (vy >= 0.f) cf = c0 + 0.5f * minmod_slope(c[r - 1][cc], c0, cn, t.w[r - 1][cc], w0, wn);
+    else cf = cn - 0.5f * minmod_slope(c0, cn, c[r + 2][cc], w0, wn, t.w[r + 2][cc]);
   } else if (d.limiter == 1) {
     cf = vy >= 0.f ? c0 : cn;
   } else {
     cf = 0.5f * (c0 + cn);
   }
-  return vy * cf * (w0 * wn) * __ldg(d.cfp + j);
+  return vy * cf * (w0 * wn) * __ldg(d.cfp + gj);
 }
 
-// Flux-form tracer advection tendency (dynamics/transport.py:365-475, legacy
-// donor-cell vertical flux with the rigid-lid top flux Fz[0] c[0]).
-__device__ __forceinline__ float tracer_adv(const Dev& d, const float* __restrict__ c, const float* __restrict__ u,
-                                            const float* __restrict__ v, const float* __restrict__ Fz, int k, int j,
-                                            int i, uint64_t bits) {
-  const float w0 = wetf(bits, k);
-  if (w0 == 0.f) return 0.f;
-  const long long b = (long long)k * d.plane;
-  const float fxe = flux_x(d, c, u, b, k, j, i);
-  const float fxw = flux_x(d, c, u, b, k, j, west(d, i));
-  const float fyn = flux_y(d, c, v, b, k, j, i);
-  const float fys = j > 0 ? flux_y(d, c, v, b, k, j - 1, i) : 0.f;
-  const float hdiv = (fxe - fxw) * __ldg(d.inv_dx + idx2(d, j, i)) + (fyn - fys) * d.inv_dy * __ldg(d.inv_cos + j);
+__global__ void __launch_bounds__(TA_X * TA_Y) k_tracer_adv_t(Dev d, const float* __restrict__ T,
+                                                              const float* __restrict__ S, const float* __restrict__ u,
+                                                              const float* __restrict__ v, const float* __restrict__ Fz,
+                                                              float* __restrict__ accT, float* __restrict__ accS,
+                                                              float* __restrict__ Tn, float* __restrict__ Sn,
+                                                              float dts, int first, int last) {
+  __shared__ TaTile t;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = ty * TA_X + tx, nt = TA_X * TA_Y;
+  const int i0 = blockIdx.x * TA_X, j0 = blockIdx.y * TA_Y, k = blockIdx.z;
+  const long long kb = (long long)k * d.plane;
+  constexpr int NCELL = TA_PX * TA_PY;
+  for (int e = tid; e < NCELL; e += nt) {
+    const int r = e / TA_PX, cc = e - r * TA_PX;
+    int gj = j0 - TA_H + r;
+    gj = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
+    int gi = (i0 - TA_H + cc) % d.nx;
+    if (gi < 0) gi += d.nx;
+    const long long g = kb + (long long)gj * d.P + gi;
+    t.T[r][cc] = ld(T, g);
+    t.S[r][cc] = ld(S, g);
+    t.u[r][cc] = ld(u, g);
+    t.v[r][cc] = ld(v, g);
+    t.w[r][cc] = wetf(__ldg(d.wbits + idx2(d, gj, gi)), k);
+  }
+  __syncthreads();
+  const int i = i0 + tx, j = j0 + ty;
+  if (i >= d.nx || j >= d.ny) return;
+  const int r = ty + TA_H, cc = tx + TA_H;
   const long long base = idx2(d, j, i);
-  const int kb = kbot_of(bits);
-  const float ck = ld(c, base + b);
-  float up, dn = 0.f;
-  const float fz_k = ld(Fz, base + b);
-  if (k == 0) {
-    up = fz_k * ck;
-  } else {
-    const float donor = fz_k > 0.f ? ld(c, base + b - d.plane) : ck;  // k <= kb here since node k is wet
-    up = fz_k * donor * (wetf(bits, k - 1) * w0);
+  const long long id = kb + base;
+  const float w0 = t.w[r][cc];
+  const float ck = t.T[r][cc], sk = t.S[r][cc];
+  float aT = 0.f, aS = 0.f;
+  if (w0 != 0.f) {
+    const uint64_t bits = __ldg(d.wbits + base);
+    const float fxeT = ta_face_x(d, t.T, t, r, cc), fxwT = ta_face_x(d, t.T, t, r, cc - 1);
+    const float fxeS = ta_face_x(d, t.S, t, r, cc), fxwS = ta_face_x(d, t.S, t, r, cc - 1);
+    const float fynT = ta_face_y(d, t.T, t, r, cc, j), fynS = ta_face_y(d, t.S, t, r, cc, j);
+    const float fysT = j > 0 ? ta_face_y(d, t.T, t, r - 1, cc, j - 1) : 0.f;
+    const float fysS = j > 0 ? ta_face_y(d, t.S, t, r - 1, cc, j - 1) : 0.f;
+    const float ix = __ldg(d.inv_dx + base), ysc = d.inv_dy * __ldg(d.inv_cos + j);
+    const float hT = (fxeT - fxwT) * ix + (fynT - fysT) * ysc;
+    const float hS = (fxeS - fxwS) * ix + (fynS - fysS) * ysc;
+    const float fz_k = ld(Fz, id);
+    float upT, upS, dnT = 0.f, dnS = 0.f;
+    if (k == 0) {
+      upT = fz_k * ck;
+      upS = fz_k * sk;
+    } else {
+      const float g = wetf(bits, k - 1) * w0;
+      upT = fz_k * (fz_k > 0.f ? ld(T, id - d.plane) : ck) * g;
+      upS = fz_k * (fz_k > 0.f ? ld(S, id - d.plane) : sk) * g;
+    }
+    if (k + 1 < d.nz) {
+      const float g = w0 * wetf(bits, k + 1);
+      const float fz_n = ld(Fz, id + d.plane);
+      // ghost fill below the deepest wet level: node k+1 carries node k's value
+      const bool below = k + 1 <= kbot_of(bits);
+      const float tn = below ? ld(T, id + d.plane) : ck, sn = below ? ld(S, id + d.plane) : sk;
+      dnT = fz_n * (fz_n > 0.f ? ck : tn) * g;
+      dnS = fz_n * (fz_n > 0.f ? sk : sn) * g;
+    }
+    aT = -(hT + (dnT - upT) * d.vc.inv_dz_node[k]) * w0;
+    aS = -(hS + (dnS - upS) * d.vc.inv_dz_node[k]) * w0;
   }
-  if (k < d.nz - 1) {
-    const float fz_n = ld(Fz, base + b + d.plane);
-    const float donor = fz_n > 0.f ? ck : colv(c, base, d.plane, k + 1, kb);
-    dn = fz_n * donor * (w0 * wetf(bits, k + 1));
-  }
-  return -(hdiv + (dn - up) * d.vc.inv_dz_node[k]) * w0;
-}
-
-// One advection substep of T and S with frozen (u, v, Fz)
-// (dynamics/tendencies.py:111-140): accumulates the rate and advances the
-// substep state.
-__global__ void __launch_bounds__(256) k_tracer_adv(Dev d, const float* __restrict__ T, const float* __restrict__ S,
-                                                    const float* __restrict__ u, const float* __restrict__ v,
-                                                    const float* __restrict__ Fz, float* __restrict__ accT,
-                                                    float* __restrict__ accS, float* __restrict__ Tn,
-                                                    float* __restrict__ Sn, float dts, int first, int last) {
-  ZM_POINT_IDX
-  const uint64_t bits = wb(d, j, i);
-  const float aT = tracer_adv(d, T, u, v, Fz, k, j, i, bits);
-  const float aS = tracer_adv(d, S, u, v, Fz, k, j, i, bits);
   accT[id] = first ? aT : accT[id] + aT;
   accS[id] = first ? aS : accS[id] + aS;
   if (!last) {
-    Tn[id] = ld(T, id) + aT * dts;
-    Sn[id] = ld(S, id) + aS * dts;
+    Tn[id] = ck + aT * dts;
+    Sn[id] = sk + aS * dts;
   }
 }
 

@@ -27,25 +27,28 @@ struct RestArgs {
   int nc, stage;
 };
 
+// 2.5-D tracer advection tile
+constexpr int TA_X = 32, TA_Y = 16;
 // temporally blocked nu_h subcycles: tile width, rows per thread, subcycles per pass
 constexpr int NB_W = 64;
 constexpr int NB_R = 8;
 constexpr int NB_T = 6;
-constexpr size_t NB_SMEM = (size_t)(3 * NB_W * NB_W + NB_W) * sizeof(float) + (size_t)NB_W * NB_W;
+constexpr size_t NB_SMEM = (size_t)NB_W * NB_W * sizeof(float4) + (size_t)(NB_W + 2) * (NB_W + 2) * sizeof(float2) +
+                           (size_t)NB_W * NB_W;
 __global__ void k_nu_tb(Dev d, const float* u, const float* v, float* uo, float* vo, float c, int nsub);
-__global__ void k_inner_lap(Dev d, const float* u, const float* v, const float* T, const float* S, float* Lu,
-                            float* Lv, float* LT, float* LS, int do_uv, int do_ts);
-__global__ void k_lin_finish(Dev d, const float* usub, const float* vsub, const float* u0, const float* v0,
-                             const float* T0, const float* S0, const float* Lu, const float* Lv, const float* LT,
-                             const float* LS, float* uo, float* vo, float* To, float* So, float dth, int implicit_v);
+__global__ void k_lin_t(Dev d, const float* usub, const float* vsub, const float* u0, const float* v0, const float* T0,
+                        const float* S0, float* uo, float* vo, float* To, float* So, float dth, int implicit_v);
+// tile of k_lin_t
+constexpr int LT_TX = 32, LT_TY = 16;
+size_t lin_tile_smem();
 __global__ void k_implicit_vdiff(Dev d, float* u, float* v, float* T, float* S, const float* u0, const float* v0,
                                  const float* T0, const float* S0, float dth);
 __global__ void k_fz(Dev d, const float* u, const float* v, float* Fz);
 __global__ void k_madv(Dev d, const float* u, const float* v, const float* Fz, float* Ayu, float* Ayv);
 __global__ void k_dealias_lon(Dev d, FftPlan plan, const float* Ayu, const float* Ayv, float* Au, float* Av,
                               int lines_per_block);
-__global__ void k_tracer_adv(Dev d, const float* T, const float* S, const float* u, const float* v, const float* Fz,
-                             float* accT, float* accS, float* Tn, float* Sn, float dts, int first, int last);
+__global__ void k_tracer_adv_t(Dev d, const float* T, const float* S, const float* u, const float* v, const float* Fz,
+                               float* accT, float* accS, float* Tn, float* Sn, float dts, int first, int last);
 __global__ void k_tracer_rest(Dev d, RestArgs a);
 __global__ void k_pgf(Dev d, PgfArgs a);
 __global__ void k_bt_forcing(Dev d, const float* frx, const float* fry, double* Fx, double* Fy, const float* eta32,

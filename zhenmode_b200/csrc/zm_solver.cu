@@ -135,7 +135,6 @@ struct zm_solver {
   // ---------------------------------------------------------------- stages
   // Linear half step L(dt/2): src -> dst (dst must not alias src).
   void linear_half(cudaStream_t s, const Fields4& src, const Fields4& dst) {
-    const dim3 b(32, 8);
     const float dth = (float)(dt / 2.0);
     const float* usub = src.u;
     const float* vsub = src.v;
@@ -161,15 +160,9 @@ struct zm_solver {
       usub = a;
       vsub = c;
     }
-    const int do_uv = d.nu_bi > 0.f, do_ts = d.kappa_bi > 0.f;
-    if (do_uv || do_ts) {
-      pb(ZM_K_INNER_LAP, s);
-      k_inner_lap<<<grid3(b), b, 0, s>>>(d, src.u, src.v, src.T, src.S, L.u, L.v, L.T, L.S, do_uv, do_ts);
-      pe(s);
-    }
     pb(ZM_K_LIN_FINISH, s);
-    k_lin_finish<<<grid3(b), b, 0, s>>>(d, usub, vsub, src.u, src.v, src.T, src.S, L.u, L.v, L.T, L.S, dst.u,
-                                        dst.v, dst.T, dst.S, dth, vdiff);
+    k_lin_t<<<dim3((nx + LT_TX - 1) / LT_TX, (ny + LT_TY - 1) / LT_TY, nz), dim3(LT_TX, LT_TY), lin_tile_smem(), s>>>(
+        d, usub, vsub, src.u, src.v, src.T, src.S, dst.u, dst.v, dst.T, dst.S, dth, vdiff);
     pe(s);
     if (vdiff) {
       const dim3 c(32, 4);
@@ -183,7 +176,6 @@ struct zm_solver {
   // Tracer residual at the evaluation state (u, v, T, S) with transport Fz.
   void tracer_residual(cudaStream_t s, int stage, const float* u, const float* v, const float* T, const float* S,
                        const float* Tbase, const float* Sbase, float* To, float* So) {
-    const dim3 b(32, 8);
     const float dts = (float)(dt / adv_nsub);
     const float* cT = T;
     const float* cS = S;
@@ -191,7 +183,8 @@ struct zm_solver {
       float* nT = (n % 2 == 0) ? TsA : TsB;
       float* nS = (n % 2 == 0) ? SsA : SsB;
       pb(ZM_K_TRACER_ADV, s);
-      k_tracer_adv<<<grid3(b), b, 0, s>>>(d, cT, cS, u, v, Fz, accT, accS, nT, nS, dts, n == 0, n == adv_nsub - 1);
+      k_tracer_adv_t<<<dim3((nx + TA_X - 1) / TA_X, (ny + TA_Y - 1) / TA_Y, nz), dim3(TA_X, TA_Y), 0, s>>>(
+          d, cT, cS, u, v, Fz, accT, accS, nT, nS, dts, n == 0, n == adv_nsub - 1);
       pe(s);
       cT = nT;
       cS = nS;
@@ -619,6 +612,7 @@ void build(zm_solver* s, const zm_grid* g, const zm_params* p) {
   require(s->fft_smem <= 227 * 1024, ZM_ERR_UNSUPPORTED, "nx too large for the shared-memory FFT filter");
   ZM_CUDA(cudaFuncSetAttribute(k_dealias_lon, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->fft_smem));
   ZM_CUDA(cudaFuncSetAttribute(k_nu_tb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)NB_SMEM));
+  ZM_CUDA(cudaFuncSetAttribute(k_lin_t, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lin_tile_smem()));
   ZM_CUDA(cudaFuncSetAttribute(k_pgf, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * nz * 64 * (int)sizeof(float)));
   // ---- buffers
   for (int q = 0; q < 2; ++q) {
