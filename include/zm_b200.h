@@ -56,6 +56,14 @@ typedef struct {
   const double* wet_mask_3d;  /* (nx, ny, nz) or NULL: column-uniform from wet_mask */
 } zm_grid;
 
+/* Barotropic subcycle kernels: AUTO takes the resident kernel (every tile in
+ * shared memory, one cooperative launch) when all tiles fit on the GPU at
+ * once and the streaming kernels (three launches per subcycle) otherwise;
+ * RESIDENT fails zm_create with ZM_ERR_UNSUPPORTED when they do not fit. */
+#define ZM_BT_AUTO 0
+#define ZM_BT_RESIDENT 1
+#define ZM_BT_STREAMING 2
+
 /* PhysicsConfig coefficients (src/zhenmode/model/config.py:86-140) and the
  * make_solver_global options of the mode-split production path
  * (src/zhenmode/model/solver/factory.py:30-68, 397-695). */
@@ -69,6 +77,8 @@ typedef struct {
   int32_t limiter;            /* ZM_LIMITER_* */
   int32_t localize_conv, conservative_kv, freeze_adv_vel;
   int32_t vertical_diffusion; /* ZM_VDIFF_* */
+  int32_t bt_kernel;          /* ZM_BT_* barotropic kernel choice */
+  int32_t reserved0;          /* explicit padding to the pointers; set 0 */
   /* (nx, ny) float64 fields; NULL means zeros */
   const double* tau_x;
   const double* tau_y;
@@ -100,8 +110,10 @@ int zm_create(const zm_grid* grid, const zm_params* params, zm_solver** out);
 
 /* Derived counts: out[0] n_subcyc, out[1] nu subcycles, out[2] adv_nsub,
  * out[3] conv_nsub, out[4] row pitch, out[5] device MiB held, out[6] kernel
- * launches in one captured step (0 before the first zm_advance).
- * Writes min(n, 7) values. */
+ * launches in one captured step (0 before the first zm_advance), out[7]
+ * barotropic blocks of the resident kernel (0: streaming kernels), out[8] 1
+ * when the polar cap of the barotropic mode is active (a band row is wet).
+ * Writes min(n, 9) values. */
 int zm_info(const zm_solver* s, int32_t* out, int32_t n);
 
 /* Copy a device state (reference layout) into the solver's resident state. */
@@ -159,9 +171,17 @@ int zm_run_stage(zm_solver* s, void* stream, int32_t stage, const zm_state* in, 
  * Synchronizes the stream. */
 int zm_profile(zm_solver* s, void* stream, float* ms, int32_t* launches, int32_t n);
 
+/* Exercise the bounded grid barrier of the barotropic kernel: `blocks` blocks
+ * each wait for `expected` arrivals, polling at most max_polls times.  With
+ * expected == blocks the barrier completes (ZM_OK); with expected > blocks
+ * the polls run out and ZM_ERR_TIMEOUT is returned with the context intact.
+ * 1 <= blocks <= the SM count, expected >= blocks.  Synchronizes. */
+int zm_barrier_probe(zm_solver* s, void* stream, int32_t blocks, int32_t expected, int32_t max_polls);
+
 /* Monitor of the resident state after the last zm_advance (runtime/monitor.py:20-30):
  * 0 accepted, 1 non-finite, 3 velocity above 10 m/s, 4 |eta| above 15 m.
- * Synchronizes the stream given to zm_advance. */
+ * Returns ZM_ERR_TIMEOUT if a grid barrier of the barotropic kernel gave up
+ * (the state is then not a valid step result).  Synchronizes the device. */
 int zm_status(zm_solver* s, int32_t* monitor_code);
 
 /* Classify a float32 state held in the caller's device arrays (reference

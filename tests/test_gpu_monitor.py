@@ -55,3 +55,14 @@ def test_monitor_clears_between_calls(solver_state):
     bad["u"][0, 0, 0] = np.nan
     assert _code(solver, bad) == 1
     assert _code(solver, base) == 0
+
+
+def test_barrier_timeout_is_reported_and_context_survives(solver_state):
+    """A grid barrier waiting for more blocks than exist gives up after its
+    poll limit and reports ZM_ERR_TIMEOUT; the solver keeps working."""
+    import torch
+    solver, base = solver_state
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    assert solver.lib.zm_barrier_probe(solver.handle, stream, 8, 8, 1 << 20) == _native.ZM_OK
+    assert solver.lib.zm_barrier_probe(solver.handle, stream, 8, 9, 20000) == _native.ZM_ERR_TIMEOUT
+    assert _code(solver, base) == 0

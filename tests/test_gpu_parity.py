@@ -153,3 +153,56 @@ def test_pressure_part_matches_oracle(shape):
     err_u = gu.rel_l2(got["u"], (-gx / RHO_0 - fx[:, :, None]) * p.wet_mask_z)
     err_v = gu.rel_l2(got["v"], (-gy / RHO_0 - fy[:, :, None]) * p.wet_mask_z)
     assert max(err_u, err_v) < 1e-5, (err_u, err_v)
+
+
+
+def _polar_case(nx, ny, nz, land_lat, barotropic_kernel="auto"):
+    """The 0.5-degree option set on a grid whose polar cap band rows are all
+    land (land_lat = 65: the barotropic polar cap is the identity) or partly
+    ocean (land_lat = 87 on a 1.9-degree grid: the cap averages wet band
+    rows), with a moving state."""
+    wl = workloads.WORKLOADS["plain"]
+    grid = workloads.build_grid(nx, ny, nz, land_lat=land_lat)
+    T, S = workloads.initial_fields(grid, perturb_sigma=wl.perturb_sigma)
+    kw = dict(wl.options)
+    kw.update(forcing=workloads.wind_forcing(grid), dt_bt=wl.dt_bt,
+              coastal_restore_mask=np.asarray(grid.wet_mask), coastal_restore_days=wl.restore_days,
+              coastal_restore_T=np.array(T[:, :, 0]), barotropic_kernel=barotropic_kernel)
+    gpu, p = gu.build_pair(grid, wl.physics, wl.dt, kw)
+    from oracle.params import init_state
+    st = init_state(p, T, S)
+    lon = np.radians(np.asarray(grid.lon))[:, None, None]
+    lat = np.radians(np.asarray(grid.lat))[None, :, None]
+    wet3 = np.asarray(grid.wet_mask_3d)
+    st["u"] = 0.1 * np.cos(lat) * np.sin(3 * lon) * wet3
+    st["v"] = 0.05 * np.sin(2 * lon) * np.cos(lat) ** 2 * wet3
+    st["eta"] = 0.2 * np.sin(lon[:, :, 0]) * np.cos(lat[:, :, 0]) * np.asarray(grid.wet_mask)
+    return gpu, p, gu.f32(st)
+
+
+@pytest.mark.parametrize("land_lat,kernel,resident,cap", [
+    (87.0, "auto", True, True),          # resident tiles, cap active
+    (87.0, "streaming", False, True),    # streaming kernels, cap active
+    (65.0, "streaming", False, False),   # streaming kernels, cap the identity
+])
+def test_barotropic_paths_match_oracle(land_lat, kernel, resident, cap):
+    gpu, p, st = _polar_case(192, 96, 8, land_lat, kernel)
+    solver = gpu.solver
+    assert (solver.bt_blocks > 0) == resident
+    assert bool(solver.bt_cap_active) == cap
+    want = ostep.step(dict(st), p)
+    got = gu.run_steps(gpu, st, 1)
+    errs = gu.errors(got, want)
+    assert max(errs.values()) < STEP_TOL, errs
+
+
+def test_barotropic_kernel_choice_follows_grid_size():
+    """More tiles than the GPU holds at once: 'auto' streams, 'resident' is refused."""
+    from zhenmode_b200 import UnsupportedOption, make_solver_global
+    wl = workloads.WORKLOADS["plain"]
+    grid = workloads.build_grid(2048, 1024, 3)
+    kw = dict(wl.options, dt_bt=wl.dt_bt, dtype="float32")
+    step = make_solver_global(grid, wl.physics, wl.dt, **kw)[0]
+    assert step.solver.bt_blocks == 0
+    with pytest.raises(UnsupportedOption):
+        make_solver_global(grid, wl.physics, wl.dt, barotropic_kernel="resident", **kw)

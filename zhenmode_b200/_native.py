@@ -44,6 +44,7 @@ class ZmParams(ctypes.Structure):
                 ("polar_cap_taper", ctypes.c_int32), ("limiter", ctypes.c_int32),
                 ("localize_conv", ctypes.c_int32), ("conservative_kv", ctypes.c_int32),
                 ("freeze_adv_vel", ctypes.c_int32), ("vertical_diffusion", ctypes.c_int32),
+                ("bt_kernel", ctypes.c_int32), ("reserved0", ctypes.c_int32),
                 ("tau_x", _dp), ("tau_y", _dp), ("q_heat", _dp), ("t_atm", _dp), ("s_ref", _dp),
                 ("coastal_restore_coef", _dp), ("coastal_restore_t", _dp),
                 ("coastal_bulk_lambda", _dp), ("coastal_kappa_h", _dp), ("coastal_kappa_v", _dp)]
@@ -70,6 +71,8 @@ EXPORTS = {
                                     ctypes.POINTER(ZmState)]),
     "zm_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_float),
                                   ctypes.POINTER(ctypes.c_int32), ctypes.c_int32]),
+    "zm_barrier_probe": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                        ctypes.c_int32]),
     "zm_status": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
     "zm_classify_state_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,

@@ -929,66 +929,6 @@ __global__ void __launch_bounds__(128) k_pgf(Dev d, PgfArgs a) {
 }
 
 // ------------------------------------------------------------------ barotropic mode (float64)
-// Free-surface continuity (dynamics/barotropic.py:129-145, 331-347):
-// eta <- (eta - dt H div(ubt wm, vbt wm)) wm with the flux-form divergence
-// of numerics/horizontal.py:69-97.
-__global__ void __launch_bounds__(256) k_bt_eta(Dev d, const double* __restrict__ eta, const double* __restrict__ ubt,
-                                                const double* __restrict__ vbt, double* __restrict__ eta_o,
-                                                double dtH) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= d.nx || j >= d.ny) return;
-  const Nb n = nb(d, j, i);
-  const int c = idx2(d, j, i);
-  const double w0 = __ldg(d.wet2 + c);
-  const double we = __ldg(d.wet2 + idx2(d, j, n.ie)), ww = __ldg(d.wet2 + idx2(d, j, n.iw));
-  const double u0 = ubt[c] * w0, ue = ubt[idx2(d, j, n.ie)] * we, uw = ubt[idx2(d, j, n.iw)] * ww;
-  const double fe = 0.5 * (u0 + ue) * (w0 * we);
-  const double fw = 0.5 * (uw + u0) * (ww * w0);
-  const double div_x = (fe - fw) * __ldg(d.inv_dx_d + c);
-  double fn = 0.0, fs = 0.0;
-  const double v0 = vbt[c] * w0;
-  if (j < d.ny - 1) {
-    const double wn = __ldg(d.wet2 + idx2(d, j + 1, i));
-    fn = 0.5 * (v0 + vbt[idx2(d, j + 1, i)] * wn) * (w0 * wn) * (double)__ldg(d.cfp + j);
-  }
-  if (j > 0) {
-    const double ws = __ldg(d.wet2 + idx2(d, j - 1, i));
-    fs = 0.5 * (vbt[idx2(d, j - 1, i)] * ws + v0) * (ws * w0) * (double)__ldg(d.cfp + j - 1);
-  }
-  const double div = div_x + (fn - fs) * d.inv_dy_d / (double)__ldg(d.cosl + j);
-  eta_o[c] = (eta[c] - dtH * div) * w0;
-}
-
-// Barotropic momentum (dynamics/barotropic.py:389-428, legacy): new-eta
-// pressure gradient (the adjoint gradient of numerics/horizontal.py:99-124),
-// forcing, backward-Euler Coriolis, implicit linear drag, wet mask.
-__global__ void __launch_bounds__(256) k_bt_vel(Dev d, const double* __restrict__ eta, const double* __restrict__ ubt,
-                                                const double* __restrict__ vbt, const double* __restrict__ Fx,
-                                                const double* __restrict__ Fy, double* __restrict__ ubt_o,
-                                                double* __restrict__ vbt_o, double dtb, double drag) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= d.nx || j >= d.ny) return;
-  const Nb n = nb(d, j, i);
-  const int c = idx2(d, j, i);
-  const double w0 = __ldg(d.wet2 + c);
-  const double we = __ldg(d.wet2 + idx2(d, j, n.ie)), ww = __ldg(d.wet2 + idx2(d, j, n.iw));
-  const double e0 = eta[c];
-  const double gx = __ldg(d.inv_dx_d + c) * 0.5 *
-                    ((eta[idx2(d, j, n.ie)] - e0) * (w0 * we) + (e0 - eta[idx2(d, j, n.iw)]) * (w0 * ww));
-  double dyp = 0.0, dym = 0.0;
-  if (j < d.ny - 1) dyp = (eta[idx2(d, j + 1, i)] - e0) * (w0 * __ldg(d.wet2 + idx2(d, j + 1, i))) * (double)__ldg(d.cfp + j);
-  if (j > 0) dym = (e0 - eta[idx2(d, j - 1, i)]) * (w0 * __ldg(d.wet2 + idx2(d, j - 1, i))) * (double)__ldg(d.cfm + j);
-  const double gy = (d.inv_dy_d / (double)__ldg(d.cosl + j)) * 0.5 * (dyp + dym);
-  const double us = ubt[c] + dtb * (-9.81 * gx + Fx[c]);
-  const double vs = vbt[c] + dtb * (-9.81 * gy + Fy[c]);
-  const double fd = __ldg(d.fcor_d + c) * dtb;
-  const double den = 1.0 + fd * fd;
-  ubt_o[c] = (us + fd * vs) / den * drag * w0;
-  vbt_o[c] = (vs - fd * us) / den * drag * w0;
-}
-
 // Total barotropic forcing F_rho + tau / (rho0 H) in float64.
 __global__ void k_bt_forcing(Dev d, const float* __restrict__ frx, const float* __restrict__ fry,
                              double* __restrict__ Fx, double* __restrict__ Fy, const float* __restrict__ eta32,
@@ -1001,41 +941,6 @@ __global__ void k_bt_forcing(Dev d, const float* __restrict__ frx, const float* 
   Fx[c] = (double)frx[c] + (double)__ldg(d.tau_x + c) * scale;
   Fy[c] = (double)fry[c] + (double)__ldg(d.tau_y + c) * scale;
   eta64[c] = (double)eta32[c];
-}
-
-// Polar cap of 2-D float64 fields (numerics/horizontal.py:387-451, legacy
-// branch): one block per band row; wet-point zonal mean blended with the
-// pole-inward weight; band land points come back zero.
-__global__ void __launch_bounds__(256) k_cap2d(Dev d, double* f0, double* f1, const float* __restrict__ wts, int nb_rows) {
-  __shared__ double red[2][256];
-  const int r = blockIdx.x;          // 0..2*nb_rows-1
-  double* f = blockIdx.y == 0 ? f0 : f1;
-  if (!f) return;
-  const int j = r < nb_rows ? r : d.ny - 2 * nb_rows + r;
-  const float wt = r < nb_rows ? wts[r] : wts[2 * nb_rows - 1 - r];
-  double s = 0.0, cnt = 0.0;
-  for (int i = threadIdx.x; i < d.nx; i += blockDim.x) {
-    const double w = __ldg(d.wet2 + idx2(d, j, i));
-    s += f[idx2(d, j, i)] * w;
-    cnt += w;
-  }
-  red[0][threadIdx.x] = s;
-  red[1][threadIdx.x] = cnt;
-  __syncthreads();
-  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-    if (threadIdx.x < o) {
-      red[0][threadIdx.x] += red[0][threadIdx.x + o];
-      red[1][threadIdx.x] += red[1][threadIdx.x + o];
-    }
-    __syncthreads();
-  }
-  const double mean = red[0][0] / fmax(red[1][0], 1.0);
-  const double wb_ = (double)wt;
-  for (int i = threadIdx.x; i < d.nx; i += blockDim.x) {
-    const double w = __ldg(d.wet2 + idx2(d, j, i));
-    const double val = f[idx2(d, j, i)] * w;
-    f[idx2(d, j, i)] = wb_ * (mean * w) + (1.0 - wb_) * val;
-  }
 }
 
 // Wet-point zonal means of the band rows of the projected 3-D fields
@@ -1160,12 +1065,6 @@ __global__ void k_int_to_ref2(Dev d, const float* __restrict__ src, float* __res
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i < d.nx && j < d.ny) dst[(long long)i * d.ny + j] = src[idx2(d, j, i)];
-}
-
-__global__ void k_eta_to_float(Dev d, const double* __restrict__ e64, float* __restrict__ e32) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i < d.nx && j < d.ny) e32[idx2(d, j, i)] = (float)e64[idx2(d, j, i)];
 }
 
 // ------------------------------------------------------------------ monitor

@@ -35,6 +35,31 @@ constexpr int NB_R = 8;
 constexpr int NB_T = 6;
 constexpr size_t NB_SMEM = (size_t)NB_W * NB_W * sizeof(float4) + (size_t)(NB_W + 2) * (NB_W + 2) * sizeof(float2) +
                            (size_t)NB_W * NB_W;
+// persistent barotropic subcycle
+#define ZM_BT_MAX_NB 64
+#define ZM_BT_BARRIER_POLLS (1u << 24)
+#define ZM_BT_ERR_BARRIER 1u
+// barotropic tile of the resident kernel: owned cells, halo width, threads
+constexpr int BT_TX = 32, BT_TY = 16, BT_H = 2, BT_THREADS = 128;
+struct BtArgs {
+  const double *eta0, *ubt0, *vbt0, *Fx, *Fy, *count;
+  double *pub_e[2], *pub_u[2], *pub_v[2];  // published fields by subcycle parity
+  double *ubt_out, *vbt_out;
+  double *part_e[2], *part_u[2], *part_v[2];
+  float* eta_out;
+  const float* wts;
+  unsigned *bar, *err;
+  int ntx, nb, nsub, cap_active;
+  double dtH, dtb, drag;
+};
+size_t bt_tile_smem();
+__global__ void k_bt_loop(Dev d, BtArgs a);
+__global__ void k_bt_eta(Dev d, const double* eta, const double* ubt, const double* vbt, double* eta_o, double dtH);
+__global__ void k_bt_vel(Dev d, const double* eta, const double* ubt, const double* vbt, const double* Fx,
+                         const double* Fy, double* ubt_o, double* vbt_o, double dtb, double drag);
+__global__ void k_cap2d(Dev d, double* f0, double* f1, const float* wts, const double* count, int nb_rows);
+__global__ void k_eta_to_float(Dev d, const double* e64, float* e32);
+__global__ void k_barrier_probe(unsigned* bar, unsigned* err, unsigned expected, unsigned max_polls);
 __global__ void k_nu_tb(Dev d, const float* u, const float* v, float* uo, float* vo, float c, int nsub);
 __global__ void k_lin_t(Dev d, const float* usub, const float* vsub, const float* u0, const float* v0, const float* T0,
                         const float* S0, float* uo, float* vo, float* To, float* So, float dth, int implicit_v);
@@ -53,10 +78,6 @@ __global__ void k_tracer_rest(Dev d, RestArgs a);
 __global__ void k_pgf(Dev d, PgfArgs a);
 __global__ void k_bt_forcing(Dev d, const float* frx, const float* fry, double* Fx, double* Fy, const float* eta32,
                              double* eta64);
-__global__ void k_bt_eta(Dev d, const double* eta, const double* ubt, const double* vbt, double* eta_o, double dtH);
-__global__ void k_bt_vel(Dev d, const double* eta, const double* ubt, const double* vbt, const double* Fx,
-                         const double* Fy, double* ubt_o, double* vbt_o, double dtb, double drag);
-__global__ void k_cap2d(Dev d, double* f0, double* f1, const float* wts, int nb_rows);
 __global__ void k_cap3_means(Dev d, const float* u, const float* v, const float* T, const float* S, const double* ubt,
                              const double* ubt0, const double* vbt, const double* vbt0, float* means, int nb_rows);
 __global__ void k_final(Dev d, const float* u3, const float* v3, const float* T3, const float* S3, const double* ubt,
@@ -67,7 +88,6 @@ __global__ void k_ref_to_int3(Dev d, const float* src, float* dst, float offset)
 __global__ void k_int_to_ref3(Dev d, const float* src, float* dst, float offset);
 __global__ void k_ref_to_int2(Dev d, const float* src, float* dst);
 __global__ void k_int_to_ref2(Dev d, const float* src, float* dst);
-__global__ void k_eta_to_float(Dev d, const double* e64, float* e32);
 __global__ void k_monitor(Dev d, const float* u, const float* v, const float* T, const float* S, const float* eta,
                           float umax, float etamax, unsigned int* flags);
 

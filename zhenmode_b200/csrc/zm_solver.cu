@@ -67,6 +67,9 @@ struct zm_solver {
   float *frx = nullptr, *fry = nullptr, *means = nullptr, *wts = nullptr;
   double *ubt0 = nullptr, *vbt0 = nullptr, *ubt[2] = {nullptr, nullptr}, *vbt[2] = {nullptr, nullptr};
   double *eta64[2] = {nullptr, nullptr}, *Fx = nullptr, *Fy = nullptr, *wts_d = nullptr;
+  BtArgs bt{};          // persistent barotropic kernel arguments
+  int bt_blocks = 0;
+  unsigned* bt_sync = nullptr;  // [0..1] barrier counter/generation, [2] error flags
   // reference-layout staging (zm_step_host)
   Fields4 ref;
   float* ref_eta = nullptr;
@@ -280,40 +283,63 @@ struct zm_solver {
     pb(ZM_K_BAROTROPIC, s);
     k_bt_forcing<<<grid2(c), c, 0, s>>>(d, frx, fry, Fx, Fy, eta_in, eta64[0]);
     pe(s);
-    ZM_CUDA(cudaMemcpyAsync(ubt[0], ubt0, n2 * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    ZM_CUDA(cudaMemcpyAsync(vbt[0], vbt0, n2 * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    const double dtH = dt_bt * (double)d.H_sw;
-    for (int n = 0; n < n_subcyc; ++n) {
-      const int a0 = n % 2, a1 = 1 - a0;
+    double *ubt_fin, *vbt_fin;
+    if (bt_blocks > 0) {
+      BtArgs a2 = bt;
+      a2.eta_out = eta_out;
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(bt_blocks);
+      cfg.blockDim = dim3(BT_THREADS);
+      cfg.dynamicSmemBytes = bt_tile_smem();
+      cfg.stream = s;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeCooperative;
+      attr[0].val.cooperative = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
       pb(ZM_K_BAROTROPIC, s);
-      k_bt_eta<<<grid2(c), c, 0, s>>>(d, eta64[a0], ubt[a0], vbt[a0], eta64[a1], dtH);
+      ZM_CUDA(cudaLaunchKernelEx(&cfg, k_bt_loop, d, a2));
       pe(s);
-      if (cap_rows > 0) {
+      ubt_fin = bt.ubt_out;
+      vbt_fin = bt.vbt_out;
+    } else {
+      ZM_CUDA(cudaMemcpyAsync(ubt[0], ubt0, n2 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      ZM_CUDA(cudaMemcpyAsync(vbt[0], vbt0, n2 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      const bool cap = bt.cap_active != 0;
+      for (int n = 0; n < n_subcyc; ++n) {
+        const int a0 = n % 2, a1 = 1 - a0;
         pb(ZM_K_BAROTROPIC, s);
-        k_cap2d<<<dim3(2 * cap_nb, 1), 256, 0, s>>>(d, eta64[a1], nullptr, wts, cap_nb);
+        k_bt_eta<<<grid2(c), c, 0, s>>>(d, eta64[a0], ubt[a0], vbt[a0], eta64[a1], bt.dtH);
         pe(s);
+        if (cap) {
+          pb(ZM_K_BAROTROPIC, s);
+          k_cap2d<<<dim3(2 * cap_nb, 1), 256, 0, s>>>(d, eta64[a1], nullptr, wts, bt.count, cap_nb);
+          pe(s);
+        }
+        pb(ZM_K_BAROTROPIC, s);
+        k_bt_vel<<<grid2(c), c, 0, s>>>(d, eta64[a1], ubt[a0], vbt[a0], Fx, Fy, ubt[a1], vbt[a1], dt_bt, bt_drag);
+        pe(s);
+        if (cap) {
+          pb(ZM_K_BAROTROPIC, s);
+          k_cap2d<<<dim3(2 * cap_nb, 2), 256, 0, s>>>(d, ubt[a1], vbt[a1], wts, bt.count, cap_nb);
+          pe(s);
+        }
       }
+      const int fin = n_subcyc % 2;
       pb(ZM_K_BAROTROPIC, s);
-      k_bt_vel<<<grid2(c), c, 0, s>>>(d, eta64[a1], ubt[a0], vbt[a0], Fx, Fy, ubt[a1], vbt[a1], dt_bt, bt_drag);
+      k_eta_to_float<<<grid2(c), c, 0, s>>>(d, eta64[fin], eta_out);
       pe(s);
-      if (cap_rows > 0) {
-        pb(ZM_K_BAROTROPIC, s);
-        k_cap2d<<<dim3(2 * cap_nb, 2), 256, 0, s>>>(d, ubt[a1], vbt[a1], wts, cap_nb);
-        pe(s);
-      }
+      ubt_fin = ubt[fin];
+      vbt_fin = vbt[fin];
     }
-    const int fin = n_subcyc % 2;
-    pb(ZM_K_BAROTROPIC, s);
-    k_eta_to_float<<<grid2(c), c, 0, s>>>(d, eta64[fin], eta_out);
-    pe(s);
     if (cap_rows > 0) {
       pb(ZM_K_FINAL, s);
-      k_cap3_means<<<dim3(2 * cap_nb, nz), 256, 0, s>>>(d, s3.u, s3.v, s3.T, s3.S, ubt[fin], ubt0, vbt[fin], vbt0,
+      k_cap3_means<<<dim3(2 * cap_nb, nz), 256, 0, s>>>(d, s3.u, s3.v, s3.T, s3.S, ubt_fin, ubt0, vbt_fin, vbt0,
                                                        means, cap_nb);
       pe(s);
     }
     pb(ZM_K_FINAL, s);
-    k_final<<<grid3(c), c, 0, s>>>(d, s3.u, s3.v, s3.T, s3.S, ubt[fin], ubt0, vbt[fin], vbt0, held.u, held.v,
+    k_final<<<grid3(c), c, 0, s>>>(d, s3.u, s3.v, s3.T, s3.S, ubt_fin, ubt0, vbt_fin, vbt0, held.u, held.v,
                                    held.T, held.S, means, wts, cap_rows > 0 ? cap_nb : 0, out.u, out.v, out.T,
                                    out.S);
     pe(s);
@@ -633,6 +659,67 @@ void build(zm_solver* s, const zm_grid* g, const zm_params* p) {
     s->eta64[q] = s->alloc<double>(s->n2);
   }
   s->Fx = s->alloc<double>(s->n2); s->Fy = s->alloc<double>(s->n2);
+  // ---- barotropic subcycle: resident tiles when they all fit on the GPU at
+  // once, else the streaming kernels
+  {
+    require(nb <= ZM_BT_MAX_NB, ZM_ERR_UNSUPPORTED, "polar cap band wider than 64 rows");
+    BtArgs& a = s->bt;
+    a.nb = p->polar_cap_rows > 0 ? nb : 0;
+    a.nsub = s->n_subcyc;
+    a.dtH = s->dt_bt * (double)d.H_sw;
+    a.dtb = s->dt_bt;
+    a.drag = s->bt_drag;
+    // wet counts of the band rows, max(count, 1); the cap is the identity when
+    // every band row is land
+    std::vector<double> cnt(std::max(1, 2 * a.nb), 1.0);
+    a.cap_active = 0;
+    for (int b = 0; b < 2 * a.nb; ++b) {
+      const int j = b < a.nb ? b : ny - 2 * a.nb + b;
+      double c = 0.0;
+      for (int i = 0; i < nx; ++i) c += g->wet_mask[(size_t)i * ny + j];
+      if (c > 0.0) a.cap_active = 1;
+      cnt[b] = std::max(c, 1.0);
+    }
+    a.count = s->upload(cnt);
+    a.wts = s->wts;
+    a.eta0 = s->eta64[0];
+    a.ubt0 = s->ubt0;
+    a.vbt0 = s->vbt0;
+    a.Fx = s->Fx;
+    a.Fy = s->Fy;
+    const size_t smem = bt_tile_smem();
+    ZM_CUDA(cudaFuncSetAttribute(k_bt_loop, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0, sms = 0, coop = 0;
+    ZM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bt_loop, BT_THREADS, smem));
+    ZM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
+    ZM_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, s->device));
+    a.ntx = (nx + BT_TX - 1) / BT_TX;
+    const int nty = (ny + BT_TY - 1) / BT_TY;
+    const long long tiles = (long long)a.ntx * nty;
+    require(p->bt_kernel >= ZM_BT_AUTO && p->bt_kernel <= ZM_BT_STREAMING, ZM_ERR_INVALID, "unknown bt_kernel");
+    const bool fits = coop && tiles <= (long long)per_sm * sms;
+    require(fits || p->bt_kernel != ZM_BT_RESIDENT, ZM_ERR_UNSUPPORTED,
+            "barotropic tiles do not fit on the GPU at once (bt_kernel = ZM_BT_RESIDENT)");
+    s->bt_blocks = (fits && p->bt_kernel != ZM_BT_STREAMING) ? (int)tiles : 0;
+    if (s->bt_blocks > 0) {
+      for (int q = 0; q < 2; ++q) {
+        a.pub_e[q] = s->alloc<double>(s->n2);
+        a.pub_u[q] = s->alloc<double>(s->n2);
+        a.pub_v[q] = s->alloc<double>(s->n2);
+      }
+      a.ubt_out = s->alloc<double>(s->n2);
+      a.vbt_out = s->alloc<double>(s->n2);
+      const size_t np = (size_t)std::max(1, 2 * a.nb) * a.ntx;
+      for (int q = 0; q < 2; ++q) {
+        a.part_e[q] = s->alloc<double>(np);
+        a.part_u[q] = s->alloc<double>(np);
+        a.part_v[q] = s->alloc<double>(np);
+      }
+    }
+    s->bt_sync = s->alloc<unsigned>(4);
+    a.bar = s->bt_sync;
+    a.err = s->bt_sync + 2;
+  }
   const size_t nref3 = (size_t)nx * ny * nz;
   s->ref = Fields4{s->alloc<float>(nref3), s->alloc<float>(nref3), s->alloc<float>(nref3), s->alloc<float>(nref3)};
   s->ref_eta = s->alloc<float>((size_t)nx * ny);
@@ -668,15 +755,16 @@ int zm_create(const zm_grid* grid, const zm_params* params, zm_solver** out) {
 
 int zm_info(const zm_solver* s, int32_t* out, int32_t n) {
   if (!s || !out) return ZM_ERR_INVALID;
-  const int32_t v[7] = {s->n_subcyc, s->n_nu, s->adv_nsub, s->conv_nsub, s->P, (int32_t)(s->bytes >> 20),
-                        s->kernels_per_step};
-  for (int q = 0; q < n && q < 7; ++q) out[q] = v[q];
+  const int32_t v[9] = {s->n_subcyc, s->n_nu, s->adv_nsub, s->conv_nsub, s->P, (int32_t)(s->bytes >> 20),
+                        s->kernels_per_step, s->bt_blocks, s->bt.cap_active};
+  for (int q = 0; q < n && q < 9; ++q) out[q] = v[q];
   return ZM_OK;
 }
 
 int zm_load_state(zm_solver* s, void* stream, const zm_state* in) {
   if (!s || !in || !in->u || !in->v || !in->T || !in->S || !in->eta) return ZM_ERR_INVALID;
   try {
+    ZM_CUDA(cudaMemsetAsync(s->bt_sync, 0, 4 * sizeof(unsigned), (cudaStream_t)stream));
     s->load((cudaStream_t)stream, in, s->st[s->cur], s->eta[s->cur]);
   } catch (const Err& e) {
     return fail(s, e);
@@ -828,12 +916,38 @@ int zm_profile(zm_solver* s, void* stream, float* ms, int32_t* launches, int32_t
   return ZM_OK;
 }
 
+int zm_barrier_probe(zm_solver* s, void* stream, int32_t blocks, int32_t expected, int32_t max_polls) {
+  if (!s || blocks < 1 || expected < blocks || max_polls < 1) return ZM_ERR_INVALID;
+  cudaStream_t st = (cudaStream_t)stream;
+  try {
+    int sms = 0;
+    ZM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
+    if (blocks > sms) return fail(s, Err{ZM_ERR_INVALID, "barrier probe: more blocks than SMs"});
+    ZM_CUDA(cudaMemsetAsync(s->bt_sync, 0, 4 * sizeof(unsigned), st));
+    k_barrier_probe<<<blocks, 32, 0, st>>>(s->bt.bar, s->bt.err, (unsigned)expected, (unsigned)max_polls);
+    s->check_launch();
+    ZM_CUDA(cudaStreamSynchronize(st));
+    unsigned berr = 0;
+    ZM_CUDA(cudaMemcpy(&berr, s->bt.err, sizeof(berr), cudaMemcpyDeviceToHost));
+    ZM_CUDA(cudaMemsetAsync(s->bt_sync, 0, 4 * sizeof(unsigned), st));
+    ZM_CUDA(cudaStreamSynchronize(st));
+    if (berr) return fail(s, Err{ZM_ERR_TIMEOUT, "barrier probe timed out"});
+  } catch (const Err& e) {
+    return fail(s, e);
+  }
+  return ZM_OK;
+}
+
 int zm_status(zm_solver* s, int32_t* monitor_code) {
   if (!s || !monitor_code) return ZM_ERR_INVALID;
   unsigned int f = 0;
   cudaError_t e = cudaMemcpy(&f, s->flags, sizeof(f), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return fail(s, Err{ZM_ERR_CUDA, std::string("zm_status: ") + cudaGetErrorString(e)});
   *monitor_code = (f & 1u) ? 1 : (f & 2u) ? 3 : (f & 4u) ? 4 : 0;
+  unsigned berr = 0;
+  e = cudaMemcpy(&berr, s->bt.err, sizeof(berr), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return fail(s, Err{ZM_ERR_CUDA, std::string("zm_status: ") + cudaGetErrorString(e)});
+  if (berr) return fail(s, Err{ZM_ERR_TIMEOUT, "barotropic grid barrier timed out"});
   return ZM_OK;
 }
 

@@ -145,6 +145,7 @@ class _Solver:
         p.conservative_kv = int(bool(opts["conservative_kv"]))
         p.freeze_adv_vel = int(bool(opts["freeze_adv_vel"]))
         p.vertical_diffusion = 1 if opts["vertical_diffusion"] == "implicit" else 0
+        p.bt_kernel = _BT_KERNELS[opts["barotropic_kernel"]]
         for name in ("tau_x", "tau_y", "q_heat", "t_atm", "s_ref", "coastal_restore_coef",
                      "coastal_restore_t", "coastal_bulk_lambda", "coastal_kappa_h", "coastal_kappa_v"):
             setattr(p, name, _native.dptr(arr(opts["fields"].get(name), (nx, ny))))
@@ -158,9 +159,10 @@ class _Solver:
         if rc != _native.ZM_OK:
             raise RuntimeError(f"zm_create failed with status {rc}")
         self.handle = handle
-        info = (ctypes.c_int32 * 7)()
-        self.lib.zm_info(handle, info, 7)
-        self.n_subcyc, self.n_nu, self.adv_nsub, self.conv_nsub, self.pitch, self.mib, _ = list(info)
+        info = (ctypes.c_int32 * 9)()
+        self.lib.zm_info(handle, info, 9)
+        (self.n_subcyc, self.n_nu, self.adv_nsub, self.conv_nsub, self.pitch, self.mib, _,
+         self.bt_blocks, self.bt_cap_active) = list(info)
 
     def kernels_per_step(self):
         info = (ctypes.c_int32 * 7)()
@@ -200,6 +202,9 @@ def _torch_state_ptrs(state, shape):
     return fields
 
 
+_BT_KERNELS = {'auto': 0, 'resident': 1, 'streaming': 2}
+
+
 def make_solver_global(grid, physics, dt, forcing=None,
                        T_atm=None, lambda_bulk=0.0,
                        mixed_layer_depth_m=None, mixed_layer_mask=None,
@@ -226,11 +231,14 @@ def make_solver_global(grid, physics, dt, forcing=None,
                        projection_max_refinements=2, column_geometry='legacy',
                        match_barotropic_transport=False, process_time_scheme='legacy',
                        eos_pressure_dbar=None, surface_pressure_pa=None,
-                       vertical_diffusion='explicit', **schemes):
+                       vertical_diffusion='explicit', barotropic_kernel='auto', **schemes):
     """Build the B200 step; the argument list is the reference factory's.
 
-    ``vertical_diffusion='implicit'`` (not a reference option) replaces the
-    explicit L-step vertical diffusion by a per-column backward-Euler solve.
+    Two options are not the reference's: ``vertical_diffusion='implicit'``
+    replaces the explicit L-step vertical diffusion by a per-column
+    backward-Euler solve, and ``barotropic_kernel`` ('auto', 'resident',
+    'streaming') picks the CUDA kernels of the barotropic subcycle (same
+    arithmetic; 'auto' takes the resident kernel when the grid fits).
     """
     # ---- validation, in the reference's order where it matters (factory.py:166-395)
     _finite('dt', dt, positive=True)
@@ -288,6 +296,8 @@ def make_solver_global(grid, physics, dt, forcing=None,
         raise ValueError("mixed_layer_depth_m must be finite and nonnegative")
     if vertical_diffusion not in ('explicit', 'implicit'):
         raise ValueError("vertical_diffusion must be 'explicit' or 'implicit'")
+    if barotropic_kernel not in _BT_KERNELS:
+        raise ValueError("barotropic_kernel must be 'auto', 'resident' or 'streaming'")
     nx, ny, nz = int(grid.nx), int(grid.ny), int(grid.nz)
     if surface_pressure_pa is not None:
         load = np.asarray(surface_pressure_pa)
@@ -359,7 +369,8 @@ def make_solver_global(grid, physics, dt, forcing=None,
                 ice_salt_flux=ice_salt_flux, ice_freeze_temp_c=ice_freeze_temp_c, nu_nsub=nu_nsub,
                 polar_cap_rows=polar_cap_rows, polar_cap_taper=polar_cap_taper, fct_adv=fct_adv,
                 monotone_adv=monotone_adv, localize_conv=localize_conv, conservative_kv=conservative_kv,
-                freeze_adv_vel=freeze_adv_vel, vertical_diffusion=vertical_diffusion, fields=fields)
+                freeze_adv_vel=freeze_adv_vel, vertical_diffusion=vertical_diffusion,
+                barotropic_kernel=barotropic_kernel, fields=fields)
     solver = _Solver(grid, physics, dt, opts)
     wet3 = np.asarray(getattr(grid, 'wet_mask_3d', None) if getattr(grid, 'wet_mask_3d', None) is not None
                       else np.broadcast_to(np.asarray(grid.wet_mask)[:, :, None], (nx, ny, nz)), dtype=np.float64)
