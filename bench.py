@@ -41,12 +41,22 @@ WORKLOAD = "plain"
 SAMPLE_GRID = (180, 90, 50)
 
 # Algorithmic bytes per launch of each kernel class, in units of one float32
-# 3-D field (F = nx*ny*nz*4 bytes): distinct 3-D fields read + written.
-ALGO_FIELDS = {"nu_sub": 4, "inner_lap": 8, "lin_finish": 14, "fz": 3, "madv": 5, "dealias": 4,
+# 3-D field (F = nx*ny*nz*4 bytes): distinct 3-D fields read + written by the
+# stage the launch covers.  The nu_h class is counted per subcycle, as the
+# stage structure has it (R+W of u and v, 4F, for each of the 2*n_nu
+# subcycles of a step), however many subcycles one launch blocks together.
+ALGO_FIELDS = {"nu_sub": None, "lin_finish": 10, "fz": 3, "madv": 5, "dealias": 4,
                "tracer_adv": 9, "tracer_rest": 10, "pgf": 10, "final": 12}
-# DRAM bytes per launch of the dominant kernel measured by ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum), recorded in profiles/; None until captured.
-NCU_TRAFFIC_BYTES = {}
+PROFILE_STEPS = 5
+# DRAM bytes per launch measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum)
+# for a kernel class on a grid, as summarised under profiles/; null for others.
+NCU_TRAFFIC_BYTES = {((720, 360, 50), "nu_sub"): 106862080 + 64039680}   # k_nu_tb_720x360x50.md
+
+
+def algo_fields_per_launch(cls, launches_per_step, n_nu):
+    if cls == "nu_sub":
+        return 4.0 * 2 * n_nu / launches_per_step
+    return float(ALGO_FIELDS[cls])
 
 
 def sim_years_per_day(ms_per_step, dt):
@@ -248,16 +258,21 @@ def main():
     kernels_per_step = solver.kernels_per_step()
 
     # per-kernel-class breakdown of one step (CUDA events around every launch)
-    prof = solver.profile(stream.cuda_stream)
+    # (average of PROFILE_STEPS un-graphed steps, events on the launching stream)
+    prof = {}
+    for _ in range(PROFILE_STEPS):
+        for k, (pm, pc) in solver.profile(stream.cuda_stream).items():
+            am, ac = prof.get(k, (0.0, 0))
+            prof[k] = (am + pm / PROFILE_STEPS, pc)
     total_prof = sum(v[0] for v in prof.values())
     ranked = sorted(((v[0], k) for k, v in prof.items() if v[1] > 0), reverse=True)
     dominant = next(k for _, k in ranked if k in ALGO_FIELDS)
     dom_ms, dom_launches = prof[dominant]
     F = 4.0 * wl.nx * wl.ny * wl.nz
-    algo = ALGO_FIELDS[dominant] * F
+    algo = algo_fields_per_launch(dominant, dom_launches, solver.n_nu) * F
     achieved = algo / (dom_ms / dom_launches * 1e-3) / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = NCU_TRAFFIC_BYTES.get(dominant)
+    traffic = NCU_TRAFFIC_BYTES.get(((wl.nx, wl.ny, wl.nz), dominant))
     bstep = step_bytes(wl.nx, wl.ny, wl.nz, solver.n_nu, solver.adv_nsub)
 
     # end to end through the C ABI with pinned host buffers
@@ -308,7 +323,8 @@ def main():
                              "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                              "traffic": traffic, "algorithmic_bytes_per_launch": algo,
                              "launch_ms": dom_ms / dom_launches,
-                             "step_stage_bytes": bstep, "step_frac": bstep / (ms * 1e-3) / 1e9 / peak},
+                             "step_stage_bytes": bstep, "step_frac": bstep / (ms * 1e-3) / 1e9 / peak,
+                             "step_floor_bytes": 8 * F, "floor_frac": 8 * F / (ms * 1e-3) / 1e9 / peak},
                 "kernel_ms_per_step": {k: round(v[0], 4) for k, v in prof.items() if v[1] > 0},
                 "kernel_ms_unrolled_total": total_prof,
                 "gpu_launches": args.steps * kernels_per_step + 1,
