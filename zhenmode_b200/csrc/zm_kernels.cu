@@ -113,12 +113,14 @@ __device__ __forceinline__ float vdiff_tracer(const Dev& d, const float* __restr
 
 // ------------------------------------------------------------------ L half step
 // nu_h Laplacian subcycles on (u, v) (timestepping/step.py:94-107), several
-// subcycles per pass.  Each block holds a NB_W x NB_W tile of one level in
-// shared memory as interleaved (u, v) pairs with a one-cell border; every
-// thread owns one column of the tile and keeps a strip of NB_R rows in
-// registers.  Values at the tile edge read the border (zeros), so garbage
-// enters one cell per subcycle: after nsub <= NB_T subcycles the inner
-// (NB_W - 2 NB_T)^2 points are exact.
+// subcycles per pass on one level.  A block covers an NB_W x NB_W tile with
+// 32 x (NB_W / NB_R) threads: lane l of warp w holds columns 2l, 2l+1 of rows
+// NB_R w .. NB_R w + NB_R - 1 in registers, as (u, v) pairs, with their face
+// coefficients.  East/west neighbours move between lanes by shuffles; the
+// rows above and below a warp's strip pass through shared memory, double
+// buffered, so one barrier per subcycle suffices.  Values at the tile edge
+// are wrong, and the error enters one cell per subcycle: after nsub <= NB_T
+// subcycles the inner (NB_W - 2 NB_T)^2 points are exact.
 //
 // The Laplacian of numerics/horizontal.py:181-215 is rewritten per point as
 //   lap = aE (uE - u0) + aW (uW - u0) + aN (uN - u0) + aS (uS - u0)
@@ -128,96 +130,115 @@ __device__ __forceinline__ float vdiff_tracer(const Dev& d, const float* __restr
 // walls folded in: at j = ny-1 the north neighbour equals u0, so aN = 0; at
 // j = 0, aS = 0.  The coefficients, scaled by nu_h dt_sub, are formed once
 // per pass.  Longitude wraps.
-__global__ void __launch_bounds__(NB_W * NB_W / NB_R, 2)
+__global__ void __launch_bounds__(32 * (NB_W / NB_R), 2)
 k_nu_tb(Dev d, const float* __restrict__ u, const float* __restrict__ v, float* __restrict__ uo,
         float* __restrict__ vo, float c, int nsub) {
-  extern __shared__ float4 nb_smem4[];
-  constexpr int PW = NB_W + 2;
-  float4* coef = nb_smem4;                                                  // [NB_W][NB_W]
-  float2* suv = reinterpret_cast<float2*>(nb_smem4 + NB_W * NB_W);          // [PW][PW]
-  unsigned char* sw = reinterpret_cast<unsigned char*>(suv + PW * PW);      // [NB_W][NB_W]
+  constexpr int NW = NB_W / NB_R;                 // warps per block
   constexpr int TI = NB_W - 2 * NB_T;
+  __shared__ float4 edge[2][NW][2][32];           // [parity][warp][0 bottom row, 1 top row][lane]
+  __shared__ unsigned char sw[NB_W][NB_W + 4];    // wet flags (coefficient setup)
+  const int lane = threadIdx.x, wp = threadIdx.y;
   const int k = blockIdx.z;
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int nt = blockDim.x * blockDim.y, tid = ty * blockDim.x + tx;
   const int gx0 = blockIdx.x * TI - NB_T, gy0 = blockIdx.y * TI - NB_T;
-  int gi = (gx0 + tx) % d.nx;
-  if (gi < 0) gi += d.nx;
-  const long long kb = (long long)k * d.plane;
-  const int r0 = ty * NB_R;
-  // zero the border ring
-  for (int e = tid; e < 4 * PW; e += nt) {
-    const int side = e / PW, p = e - side * PW;
-    const int rr = side == 0 ? 0 : (side == 1 ? PW - 1 : p);
-    const int cc = side == 0 || side == 1 ? p : (side == 2 ? 0 : PW - 1);
-    suv[rr * PW + cc] = make_float2(0.f, 0.f);
+  const int c0 = 2 * lane, r0 = wp * NB_R;
+  int gi[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    int g = (gx0 + c0 + h) % d.nx;
+    gi[h] = g < 0 ? g + d.nx : g;
   }
-  float2 a[NB_R];
+  const long long kb = (long long)k * d.plane;
+  float2 a[NB_R][2];
 #pragma unroll
   for (int q = 0; q < NB_R; ++q) {
     int gj = gy0 + r0 + q;
     gj = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
-    const long long id = kb + (long long)gj * d.P + gi;
-    a[q] = make_float2(ld(u, id), ld(v, id));
-    suv[(r0 + q + 1) * PW + tx + 1] = a[q];
-    sw[(r0 + q) * NB_W + tx] = (unsigned char)wetb(wb(d, gj, gi), k);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const long long id = kb + (long long)gj * d.P + gi[h];
+      a[q][h] = make_float2(ld(u, id), ld(v, id));
+      sw[r0 + q][c0 + h] = (unsigned char)wetb(wb(d, gj, gi[h]), k);
+    }
   }
   __syncthreads();
   const float cn = d.nu_h * c;
+  float4 cf[NB_R][2];
 #pragma unroll
   for (int q = 0; q < NB_R; ++q) {
     const int r = r0 + q;
     const int gj = gy0 + r;
     const int gjc = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
-    const bool w0 = sw[r * NB_W + tx];
-    const bool we = tx + 1 < NB_W && sw[r * NB_W + tx + 1];
-    const bool ww = tx > 0 && sw[r * NB_W + tx - 1];
-    const bool n_in = gj < d.ny - 1;   // north neighbour inside the domain
+    const bool n_in = gj < d.ny - 1;  // north neighbour inside the domain
     const bool s_in = gj > 0;
-    const bool wn = n_in && r + 1 < NB_W && sw[(r + 1) * NB_W + tx];
-    const bool ws = s_in && r > 0 && sw[(r - 1) * NB_W + tx];
-    const float ix2 = __ldg(d.inv_dx2 + idx2(d, gjc, gi));
     const float t = 0.5f * d.inv_dy * __ldg(d.tanR + gjc);
-    const float cN = (w0 && wn) ? d.inv_dy2 : 0.f, cS = (w0 && ws) ? d.inv_dy2 : 0.f;
-    float4 cf;
-    cf.x = (w0 && we) ? ix2 * cn : 0.f;
-    cf.y = (w0 && ww) ? ix2 * cn : 0.f;
-    cf.z = n_in ? (cN - t) * cn : 0.f;
-    cf.w = s_in ? (cS + t) * cn : 0.f;
-    coef[r * NB_W + tx] = cf;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int col = c0 + h;
+      const bool w0 = sw[r][col];
+      const bool we = col + 1 < NB_W && sw[r][col + 1];
+      const bool ww = col > 0 && sw[r][col - 1];
+      const bool wn = n_in && r + 1 < NB_W && sw[r + 1][col];
+      const bool ws = s_in && r > 0 && sw[r - 1][col];
+      const float ix2 = __ldg(d.inv_dx2 + idx2(d, gjc, gi[h]));
+      const float cN = (w0 && wn) ? d.inv_dy2 : 0.f, cS = (w0 && ws) ? d.inv_dy2 : 0.f;
+      cf[q][h].x = (w0 && we) ? ix2 * cn : 0.f;
+      cf[q][h].y = (w0 && ww) ? ix2 * cn : 0.f;
+      cf[q][h].z = n_in ? (cN - t) * cn : 0.f;
+      cf[q][h].w = s_in ? (cS + t) * cn : 0.f;
+    }
   }
+  const unsigned full = 0xffffffffu;
   for (int s = 0; s < nsub; ++s) {
-    float2 above = suv[r0 * PW + tx + 1];  // row r0-1
+    const int p = s & 1;
+    edge[p][wp][0][lane] = make_float4(a[0][0].x, a[0][0].y, a[0][1].x, a[0][1].y);
+    edge[p][wp][1][lane] = make_float4(a[NB_R - 1][0].x, a[NB_R - 1][0].y, a[NB_R - 1][1].x, a[NB_R - 1][1].y);
+    __syncthreads();
+    // rows just outside the strip (the tile edge reuses the strip's own row)
+    const float4 nt = edge[p][wp + 1 < NW ? wp + 1 : wp][wp + 1 < NW ? 0 : 1][lane];
+    const float4 sb = edge[p][wp > 0 ? wp - 1 : wp][wp > 0 ? 1 : 0][lane];
+    float2 south[2] = {make_float2(sb.x, sb.y), make_float2(sb.z, sb.w)};
 #pragma unroll
     for (int q = 0; q < NB_R; ++q) {
-      const int r = r0 + q;
-      const float4 cf = coef[r * NB_W + tx];
-      const float2 e = suv[(r + 1) * PW + tx + 2];
-      const float2 w = suv[(r + 1) * PW + tx];
-      const float2 nn = q + 1 < NB_R ? a[q + 1] : suv[(r + 2) * PW + tx + 1];
-      const float2 c0 = a[q];
-      float2 out;
-      out.x = c0.x + cf.x * (e.x - c0.x) + cf.y * (w.x - c0.x) + cf.z * (nn.x - c0.x) + cf.w * (above.x - c0.x);
-      out.y = c0.y + cf.x * (e.y - c0.y) + cf.y * (w.y - c0.y) + cf.z * (nn.y - c0.y) + cf.w * (above.y - c0.y);
-      above = c0;
-      a[q] = out;
-    }
-    __syncthreads();
+      float2 north[2];
+      if (q + 1 < NB_R) {
+        north[0] = a[q + 1][0];
+        north[1] = a[q + 1][1];
+      } else {
+        north[0] = make_float2(nt.x, nt.y);
+        north[1] = make_float2(nt.z, nt.w);
+      }
+      // west of column 2l is column 2l+1 of lane l-1; east of 2l+1 is 2l of lane l+1
+      // (lanes 0 and 31 get their own values: tile-edge error)
+      const float2 west0 = make_float2(__shfl_up_sync(full, a[q][1].x, 1), __shfl_up_sync(full, a[q][1].y, 1));
+      const float2 east1 = make_float2(__shfl_down_sync(full, a[q][0].x, 1), __shfl_down_sync(full, a[q][0].y, 1));
+      const float2 ew[2][2] = {{a[q][1], west0}, {east1, a[q][0]}};
 #pragma unroll
-    for (int q = 0; q < NB_R; ++q) suv[(r0 + q + 1) * PW + tx + 1] = a[q];
-    __syncthreads();
+      for (int h = 0; h < 2; ++h) {
+        const float4 k4 = cf[q][h];
+        const float2 c0v = a[q][h], e = ew[h][0], w = ew[h][1], nn = north[h], ss = south[h];
+        float2 o;
+        o.x = c0v.x + k4.x * (e.x - c0v.x) + k4.y * (w.x - c0v.x) + k4.z * (nn.x - c0v.x) + k4.w * (ss.x - c0v.x);
+        o.y = c0v.y + k4.x * (e.y - c0v.y) + k4.y * (w.y - c0v.y) + k4.z * (nn.y - c0v.y) + k4.w * (ss.y - c0v.y);
+        south[h] = c0v;
+        a[q][h] = o;
+      }
+    }
   }
   // write the exact interior
-  const int ix = gx0 + tx;
-  if (tx < NB_T || tx >= NB_W - NB_T || ix >= d.nx) return;
 #pragma unroll
   for (int q = 0; q < NB_R; ++q) {
     const int r = r0 + q;
     const int gj = gy0 + r;
     if (r < NB_T || r >= NB_W - NB_T || gj >= d.ny) continue;
-    const long long id = kb + (long long)gj * d.P + ix;
-    uo[id] = a[q].x;
-    vo[id] = a[q].y;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int col = c0 + h;
+      const int ix = gx0 + col;
+      if (col < NB_T || col >= NB_W - NB_T || ix >= d.nx) continue;
+      const long long id = kb + (long long)gj * d.P + ix;
+      uo[id] = a[q][h].x;
+      vo[id] = a[q][h].y;
+    }
   }
 }
 

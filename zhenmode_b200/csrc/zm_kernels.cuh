@@ -33,8 +33,7 @@ constexpr int TA_X = 32, TA_Y = 16;
 constexpr int NB_W = 64;
 constexpr int NB_R = 8;
 constexpr int NB_T = 6;
-constexpr size_t NB_SMEM = (size_t)NB_W * NB_W * sizeof(float4) + (size_t)(NB_W + 2) * (NB_W + 2) * sizeof(float2) +
-                           (size_t)NB_W * NB_W;
+
 // persistent barotropic subcycle
 #define ZM_BT_MAX_NB 64
 #define ZM_BT_BARRIER_POLLS (1u << 24)

@@ -146,14 +146,14 @@ struct zm_solver {
       const float* a = src.u;
       const float* c = src.v;
       constexpr int TI = NB_W - 2 * NB_T;
-      const dim3 blk(NB_W, NB_W / NB_R);
+      const dim3 blk(32, NB_W / NB_R);
       const dim3 grd((nx + TI - 1) / TI, (ny + TI - 1) / TI, nz);
       int done = 0, pass = 0;
       while (done < n_nu) {
         const int nsub = std::min(NB_T, n_nu - done);
         const Fields4& o = (pass % 2 == 0) ? W1 : W2;
         pb(ZM_K_NU_SUB, s);
-        k_nu_tb<<<grd, blk, NB_SMEM, s>>>(d, a, c, o.u, o.v, dts, nsub);
+        k_nu_tb<<<grd, blk, 0, s>>>(d, a, c, o.u, o.v, dts, nsub);
         pe(s);
         a = o.u;
         c = o.v;
@@ -637,7 +637,6 @@ void build(zm_solver* s, const zm_grid* g, const zm_params* p) {
   s->fft_smem = ((size_t)nx + (size_t)2 * s->fft_lines * nx) * sizeof(float2);
   require(s->fft_smem <= 227 * 1024, ZM_ERR_UNSUPPORTED, "nx too large for the shared-memory FFT filter");
   ZM_CUDA(cudaFuncSetAttribute(k_dealias_lon, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->fft_smem));
-  ZM_CUDA(cudaFuncSetAttribute(k_nu_tb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)NB_SMEM));
   ZM_CUDA(cudaFuncSetAttribute(k_lin_t, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lin_tile_smem()));
   ZM_CUDA(cudaFuncSetAttribute(k_pgf, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * nz * 64 * (int)sizeof(float)));
   // ---- buffers
