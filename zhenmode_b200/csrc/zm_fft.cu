@@ -9,8 +9,9 @@
 // The two advection fields of a line are packed as one complex signal
 // (adv_u + i adv_v); the filter mask is real and even, so the filtered real
 // and imaginary parts are the filtered fields.  Each block keeps several lines
-// in shared memory and runs a mixed-radix (2, 3, 4, 5) Stockham FFT with a
-// float64-derived twiddle table.  The epilogue adds the surface wind stress
+// in shared memory and runs a mixed-radix (2, 3, 4, 5) Stockham FFT whose
+// per-stage output indices and twiddles (float64-derived) are tabulated on
+// the host.  The epilogue adds the surface wind stress
 // and removes its barotropic part (dynamics/tendencies.py:59-62, 307-310) and
 // applies the wet mask, producing the T/S-independent part of the momentum
 // residual.
@@ -70,43 +71,55 @@ __device__ __forceinline__ void dft5(float2* v) {
   v[3] = cadd(r2, mul_pi(q2));
 }
 
-// One Stockham pass of radix R over `lines` lines of length n.
+// One Stockham pass of radix R over `lines` lines of length n (ns = product of
+// the earlier radices).  Butterfly jj reads x[jj + r m] (m = n / R), applies
+// the twiddles of its k = jj mod ns, and writes y[base + r ns] with
+// base = (jj / ns) ns R + k; the bases and twiddles come from the plan's
+// tables, and one thread runs the same butterfly on every line of the block.
 template <int R>
 __device__ __forceinline__ void stockham_pass(const float2* __restrict__ in, float2* __restrict__ out,
-                                              const float2* __restrict__ tw, int n, int ns, int lines) {
+                                              const int* __restrict__ base_tab, const float2* __restrict__ twt,
+                                              int n, int ns, int lines) {
   const int m = n / R;
-  const int stride = n / (ns * R);
-  for (int t = threadIdx.x; t < lines * m; t += blockDim.x) {
-    const int l = t / m, jj = t - l * m;
-    const float2* src = in + l * n;
-    float2* dst = out + l * n;
-    const int k = jj % ns;
-    float2 v[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = src[jj + r * m];
+  for (int jj = threadIdx.x; jj < m; jj += blockDim.x) {
+    const int base = __ldg(base_tab + jj);
+    float2 w[R - 1];
     if (ns > 1) {
 #pragma unroll
-      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], tw[(k * r * stride) % n]);
+      for (int r = 1; r < R; ++r) w[r - 1] = __ldg(twt + (r - 1) * m + jj);
     }
-    if (R == 2) dft2(v);
-    if (R == 3) dft3(v);
-    if (R == 4) dft4(v);
-    if (R == 5) dft5(v);
-    const int base = (jj / ns) * ns * R + k;
+#pragma unroll 4
+    for (int l = 0; l < lines; ++l) {
+      const float2* src = in + l * n;
+      float2* dst = out + l * n;
+      float2 v[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) dst[base + r * ns] = v[r];
+      for (int r = 0; r < R; ++r) v[r] = src[jj + r * m];
+      if (ns > 1) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) v[r] = cmul(v[r], w[r - 1]);
+      }
+      if (R == 2) dft2(v);
+      if (R == 3) dft3(v);
+      if (R == 4) dft4(v);
+      if (R == 5) dft5(v);
+#pragma unroll
+      for (int r = 0; r < R; ++r) dst[base + r * ns] = v[r];
+    }
   }
 }
 
 // Forward FFT of all lines; returns the buffer holding the result.
-__device__ float2* fft_lines(float2* a, float2* b, const float2* tw, const FftPlan& plan, int lines) {
+__device__ float2* fft_lines(float2* a, float2* b, const FftPlan& plan, int lines) {
   int ns = 1;
   for (int s = 0; s < plan.nstages; ++s) {
     const int R = plan.radix[s];
-    if (R == 4) stockham_pass<4>(a, b, tw, plan.n, ns, lines);
-    else if (R == 2) stockham_pass<2>(a, b, tw, plan.n, ns, lines);
-    else if (R == 3) stockham_pass<3>(a, b, tw, plan.n, ns, lines);
-    else stockham_pass<5>(a, b, tw, plan.n, ns, lines);
+    const int* bt = plan.base_tab + plan.tab_off[s];
+    const float2* tw = plan.stage_tw + plan.tw_off[s];
+    if (R == 4) stockham_pass<4>(a, b, bt, tw, plan.n, ns, lines);
+    else if (R == 2) stockham_pass<2>(a, b, bt, tw, plan.n, ns, lines);
+    else if (R == 3) stockham_pass<3>(a, b, bt, tw, plan.n, ns, lines);
+    else stockham_pass<5>(a, b, bt, tw, plan.n, ns, lines);
     __syncthreads();
     float2* t = a; a = b; b = t;
     ns *= R;
@@ -119,49 +132,49 @@ __global__ void __launch_bounds__(256) k_dealias_lon(Dev d, FftPlan plan, const 
                                                      float* __restrict__ Av, int lines_per_block) {
   extern __shared__ float2 fsm[];
   const int n = plan.n;
-  float2* tw = fsm;
-  float2* bufa = fsm + n;
+  float2* bufa = fsm;
   float2* bufb = bufa + (size_t)lines_per_block * n;
-  for (int t = threadIdx.x; t < n; t += blockDim.x) tw[t] = plan.tw[t];
   const int total = d.ny * d.nz;
   const int first = blockIdx.x * lines_per_block;
   const int lines = min(lines_per_block, total - first);
   if (lines <= 0) return;
-  for (int t = threadIdx.x; t < lines * n; t += blockDim.x) {
-    const int l = t / n, i = t - l * n;
+  for (int l = 0; l < lines; ++l) {
     const int line = first + l;
     const int k = line / d.ny, j = line - k * d.ny;
-    const long long id = idx3(d, k, j, i);
-    bufa[t] = make_float2(ld(Ayu, id), ld(Ayv, id));
+    const long long row = idx3(d, k, j, 0);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) bufa[l * n + i] = make_float2(ld(Ayu, row + i), ld(Ayv, row + i));
   }
   __syncthreads();
-  float2* spec = fft_lines(bufa, bufb, tw, plan, lines);
+  float2* spec = fft_lines(bufa, bufb, plan, lines);
   float2* other = spec == bufa ? bufb : bufa;
   // 2/3 rule with the reference's bin mask; conjugate for the inverse transform
-  for (int t = threadIdx.x; t < lines * n; t += blockDim.x) {
-    const int m = t % n;
-    float2 z = spec[t];
-    spec[t] = __ldg(plan.keepbin + m) ? make_float2(z.x, -z.y) : make_float2(0.f, 0.f);
+  for (int m = threadIdx.x; m < n; m += blockDim.x) {
+    const bool keep = __ldg(plan.keepbin + m) != 0;
+    for (int l = 0; l < lines; ++l) {
+      const float2 z = spec[l * n + m];
+      spec[l * n + m] = keep ? make_float2(z.x, -z.y) : make_float2(0.f, 0.f);
+    }
   }
   __syncthreads();
-  float2* res = fft_lines(spec, other, tw, plan, lines);
+  float2* res = fft_lines(spec, other, plan, lines);
   const float inv_n = 1.f / (float)n;
   const float wind_s = 1.f / (kRho0 * d.dz_surface);
   const float wind_bt = 1.f / (kRho0 * d.H_sw);
-  for (int t = threadIdx.x; t < lines * n; t += blockDim.x) {
-    const int l = t / n, i = t - l * n;
+  for (int l = 0; l < lines; ++l) {
     const int line = first + l;
     const int k = line / d.ny, j = line - k * d.ny;
-    const long long id = idx3(d, k, j, i);
-    const int c = idx2(d, j, i);
-    const float w = wetf(wb(d, j, i), k);
-    const float2 z = res[t];
-    const float fu = z.x * inv_n, fv = -z.y * inv_n;   // conj of the forward transform of conj(X)
-    const float tx = __ldg(d.tau_x + c), ty = __ldg(d.tau_y + c);
-    const float su = (k == 0 ? tx * wind_s : 0.f) - tx * wind_bt;
-    const float sv = (k == 0 ? ty * wind_s : 0.f) - ty * wind_bt;
-    Au[id] = (fu + su) * w;
-    Av[id] = (fv + sv) * w;
+    const long long row = idx3(d, k, j, 0);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const int c = idx2(d, j, i);
+      const float w = wetf(wb(d, j, i), k);
+      const float2 z = res[l * n + i];
+      const float fu = z.x * inv_n, fv = -z.y * inv_n;   // conj of the forward transform of conj(X)
+      const float tx = __ldg(d.tau_x + c), ty = __ldg(d.tau_y + c);
+      const float su = (k == 0 ? tx * wind_s : 0.f) - tx * wind_bt;
+      const float sv = (k == 0 ? ty * wind_s : 0.f) - ty * wind_bt;
+      Au[row + i] = (fu + su) * w;
+      Av[row + i] = (fv + sv) * w;
+    }
   }
 }
 

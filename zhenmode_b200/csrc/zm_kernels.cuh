@@ -8,7 +8,10 @@ namespace zm {
 struct FftPlan {
   int n, nstages, keep;
   int radix[24];
-  const float2* tw;             // exp(-2 pi i m / n), m < n
+  int tab_off[24];              // stage s: output bases at base_tab + tab_off[s] (n / R entries)
+  int tw_off[24];               // stage s: twiddles at stage_tw + tw_off[s], [r - 1][butterfly]
+  const int* base_tab;          // Stockham output base of each butterfly
+  const float2* stage_tw;       // exp(-2 pi i (k r n / (ns R) mod n) / n) per butterfly and r >= 1
   const unsigned char* keepbin; // 1 where bin m survives the 2/3 rule, m < n
 };
 

@@ -613,12 +613,27 @@ void build(zm_solver* s, const zm_grid* g, const zm_params* p) {
   s->wts = s->upload(w);
   // ---- FFT plan for the longitude dealias (factory.py:529-533)
   plan.keep = std::max(1, (int)((double)(nx / 2) * 2.0 / 3.0));
-  std::vector<float2> tw(nx);
-  for (int m = 0; m < nx; ++m) {
-    const double a = -2.0 * kPi * m / nx;
-    tw[m] = make_float2((float)std::cos(a), (float)std::sin(a));
+  {
+    std::vector<int> bases;
+    std::vector<float2> stw;
+    int ns = 1;
+    for (int st = 0; st < plan.nstages; ++st) {
+      const int R = plan.radix[st], m = nx / R, stride = nx / (ns * R);
+      plan.tab_off[st] = (int)bases.size();
+      plan.tw_off[st] = (int)stw.size();
+      for (int jj = 0; jj < m; ++jj) bases.push_back((jj / ns) * ns * R + jj % ns);
+      for (int r = 1; r < R; ++r)
+        for (int jj = 0; jj < m; ++jj) {
+          const long long e = ((long long)(jj % ns) * r * stride) % nx;
+          const double a = -2.0 * kPi * (double)e / nx;
+          stw.push_back(make_float2((float)std::cos(a), (float)std::sin(a)));
+        }
+      ns *= R;
+    }
+    if (stw.empty()) stw.push_back(make_float2(1.f, 0.f));
+    plan.base_tab = s->upload(bases);
+    plan.stage_tw = s->upload(stw);
   }
-  plan.tw = s->upload(tw);
   // 2/3-rule bin mask exactly as the reference forms it: numpy's
   // fftfreq(nx) * nx in float64, |.| <= keep
   std::vector<unsigned char> keepbin(nx);
@@ -633,8 +648,8 @@ void build(zm_solver* s, const zm_grid* g, const zm_params* p) {
   }
   plan.keepbin = s->upload(keepbin);
   s->fft = plan;
-  s->fft_lines = std::max(1, std::min(8, (int)((200 * 1024 / sizeof(float2) - nx) / (2 * nx))));
-  s->fft_smem = ((size_t)nx + (size_t)2 * s->fft_lines * nx) * sizeof(float2);
+  s->fft_lines = std::max(1, std::min(8, (int)((200 * 1024 / sizeof(float2)) / (2 * nx))));
+  s->fft_smem = (size_t)2 * s->fft_lines * nx * sizeof(float2);
   require(s->fft_smem <= 227 * 1024, ZM_ERR_UNSUPPORTED, "nx too large for the shared-memory FFT filter");
   ZM_CUDA(cudaFuncSetAttribute(k_dealias_lon, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->fft_smem));
   ZM_CUDA(cudaFuncSetAttribute(k_lin_t, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lin_tile_smem()));
