@@ -594,18 +594,21 @@ __global__ void __launch_bounds__(256) k_madv(Dev d, const float* __restrict__ u
 
 // Minmod slope over wet neighbours (dynamics/transport.py:199-213).
 __device__ __forceinline__ float minmod_slope(float cm, float c0, float cp, float wm, float w0, float wp) {
+  // 0.5 (sign l + sign r) min(|l|, |r|): +-min when l and r share a sign, else 0
   const float l = c0 - cm, r = cp - c0;
-  const float sg = (float)((l > 0.f) - (l < 0.f)) + (float)((r > 0.f) - (r < 0.f));
-  return 0.5f * sg * fminf(fabsf(l), fabsf(r)) * w0 * wm * wp;
+  const float m = fminf(fabsf(l), fabsf(r));
+  const float s = (l > 0.f && r > 0.f) ? m : ((l < 0.f && r < 0.f) ? -m : 0.f);
+  return s * w0 * wm * wp;
 }
 
-// Tracer advection substep on one level tile (dynamics/tendencies.py:111-140
-// with _advection_scalar, dynamics/transport.py:365-475): each block owns a
-// TA_X x TA_Y tile of one level; T, S, u, v of that level with a two-cell halo
-// (for the minmod slopes of the face states) and the level's wet flags sit in
-// shared memory.  Rows beyond the closed walls are loaded from the clamped row,
-// which is the edge padding of transport.py:199-290; longitude wraps.  The
-// vertical donor-cell flux reads the column neighbours directly.
+// Tracer advection substep (dynamics/tendencies.py:111-140 with
+// _advection_scalar, dynamics/transport.py:365-475) on one level tile: each
+// block owns a TA_X x TA_Y tile of one level; T, S, u, v of that level with a
+// two-cell halo (for the minmod slopes of the face states) and the level's wet
+// flags sit in shared memory.  Each thread forms the four faces of its point,
+// T and S together.  Rows beyond the closed walls are loaded from the clamped
+// row, which is the edge padding of transport.py:199-290; longitude wraps.
+// The vertical donor-cell flux reads the column neighbours directly.
 constexpr int TA_H = 2;
 constexpr int TA_PX = TA_X + 2 * TA_H, TA_PY = TA_Y + 2 * TA_H;
 
@@ -617,48 +620,66 @@ struct TaTile {
   float w[TA_PY][TA_PX];
 };
 
-__device__ __forceinline__ float ta_face_x(const Dev& d, const float (*c)[TA_PX], const TaTile& t, int r, int cc) {
-  // face between tile columns cc and cc+1 of row r
+// Limited face value of one tracer (transport.py:199-290).  With the upwind
+// triple (a, b, c) = (c-, c0, c1) for a flow towards +, (c+, c1, c0) towards -,
+// the minmod face state is b + 0.5 minmod(a, b, c): for the negative
+// direction minmod(c+, c1, c0) = -minmod(c0, c1, c+) exactly, so this is
+// c1 - 0.5 minmod(c0, c1, c+) without a divergent branch.
+__device__ __forceinline__ float ta_face_value(int limiter, bool pos, float cm, float c0, float c1, float cp, float wm,
+                                               float w0, float w1, float wp) {
+  if (limiter == 2) {
+    const float a = pos ? cm : cp, b = pos ? c0 : c1, c = pos ? c1 : c0;
+    const float wa = pos ? wm : wp, wb = pos ? w0 : w1, wc = pos ? w1 : w0;
+    return b + 0.5f * minmod_slope(a, b, c, wa, wb, wc);
+  }
+  if (limiter == 1) return pos ? c0 : c1;
+  return 0.5f * (c0 + c1);
+}
+
+// T and S fluxes through the x face between tile columns cc and cc+1 of row r
+__device__ __forceinline__ void ta_faces_x(int limiter, const TaTile& t, int r, int cc, float& fT, float& fS) {
   const float w0 = t.w[r][cc], we = t.w[r][cc + 1];
   const float ux = 0.5f * (t.u[r][cc] + t.u[r][cc + 1]);
-  const float c0 = c[r][cc], ce = c[r][cc + 1];
-  float cf;
-  if (d.limiter == 2) {
-    if (ux >= 0.f) cf = c0 + 0.5f * minmod_slope(c[r][cc - 1], c0, ce, t.w[r][cc - 1], w0, we);
-    else cf = ce - 0.5f * minmod_slope(c0, ce, c[r][cc + 2], w0, we, t.w[r][cc + 2]);
-  } else if (d.limiter == 1) {
-    cf = ux >= 0.f ? c0 : ce;
-  } else {
-    cf = 0.5f * (c0 + ce);
-  }
-  return ux * cf * (w0 * we);
+  const bool pos = ux >= 0.f;
+  const float wm = t.w[r][cc - 1], wp = t.w[r][cc + 2];
+  const float cT = ta_face_value(limiter, pos, t.T[r][cc - 1], t.T[r][cc], t.T[r][cc + 1], t.T[r][cc + 2], wm, w0,
+                                 we, wp);
+  const float cS = ta_face_value(limiter, pos, t.S[r][cc - 1], t.S[r][cc], t.S[r][cc + 1], t.S[r][cc + 2], wm, w0,
+                                 we, wp);
+  const float g = w0 * we;
+  fT = ux * cT * g;
+  fS = ux * cS * g;
 }
 
-__device__ __forceinline__ float ta_face_y(const Dev& d, const float (*c)[TA_PX], const TaTile& t, int r, int cc,
-                                           int gj) {
-  // face between tile rows r and r+1 (global rows gj, gj+1); closed at the north wall
-  if (gj >= d.ny - 1) return 0.f;
+// T and S fluxes through the y face between tile rows r and r+1 (global rows
+// gj, gj+1); zero through the closed walls
+__device__ __forceinline__ void ta_faces_y(const Dev& d, const TaTile& t, int r, int cc, int gj, float& fT,
+                                           float& fS) {
+  if (gj < 0 || gj >= d.ny - 1) {
+    fT = fS = 0.f;
+    return;
+  }
   const float w0 = t.w[r][cc], wn = t.w[r + 1][cc];
   const float vy = 0.5f * (t.v[r][cc] + t.v[r + 1][cc]);
-  const float c0 = c[r][cc], cn = c[r + 1][cc];
-  float cf;
-  if (d.limiter == 2) {
-    if (vy >= 0.f) cf = c0 + 0.5f * minmod_slope(c[r - 1][cc], c0, cn, t.w[r - 1][cc], w0, wn);
-    else cf = cn - 0.5f * minmod_slope(c0, cn, c[r + 2][cc], w0, wn, t.w[r + 2][cc]);
-  } else if (d.limiter == 1) {
-    cf = vy >= 0.f ? c0 : cn;
-  } else {
-    cf = 0.5f * (c0 + cn);
-  }
-  return vy * cf * (w0 * wn) * __ldg(d.cfp + gj);
+  const bool pos = vy >= 0.f;
+  const float wm = t.w[r - 1][cc], wp = t.w[r + 2][cc];
+  const float cT = ta_face_value(d.limiter, pos, t.T[r - 1][cc], t.T[r][cc], t.T[r + 1][cc], t.T[r + 2][cc], wm, w0,
+                                 wn, wp);
+  const float cS = ta_face_value(d.limiter, pos, t.S[r - 1][cc], t.S[r][cc], t.S[r + 1][cc], t.S[r + 2][cc], wm, w0,
+                                 wn, wp);
+  const float g = w0 * wn, cf = __ldg(d.cfp + gj);
+  fT = vy * cT * g * cf;
+  fS = vy * cS * g * cf;
 }
 
-__global__ void __launch_bounds__(TA_X * TA_Y) k_tracer_adv_t(Dev d, const float* __restrict__ T,
-                                                              const float* __restrict__ S, const float* __restrict__ u,
-                                                              const float* __restrict__ v, const float* __restrict__ Fz,
-                                                              float* __restrict__ accT, float* __restrict__ accS,
-                                                              float* __restrict__ Tn, float* __restrict__ Sn,
-                                                              float dts, int first, int last) {
+__global__ void __launch_bounds__(TA_X * TA_Y, 4) k_tracer_adv_t(Dev d, const float* __restrict__ T,
+                                                                 const float* __restrict__ S,
+                                                                 const float* __restrict__ u,
+                                                                 const float* __restrict__ v,
+                                                                 const float* __restrict__ Fz,
+                                                                 float* __restrict__ accT, float* __restrict__ accS,
+                                                                 float* __restrict__ Tn, float* __restrict__ Sn,
+                                                                 float dts, int first, int last) {
   __shared__ TaTile t;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = ty * TA_X + tx, nt = TA_X * TA_Y;
@@ -669,14 +690,15 @@ __global__ void __launch_bounds__(TA_X * TA_Y) k_tracer_adv_t(Dev d, const float
     const int r = e / TA_PX, cc = e - r * TA_PX;
     int gj = j0 - TA_H + r;
     gj = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
-    int gi = (i0 - TA_H + cc) % d.nx;
-    if (gi < 0) gi += d.nx;
-    const long long g = kb + (long long)gj * d.P + gi;
+    int gi = i0 - TA_H + cc;
+    if (gi < 0 || gi >= d.nx) gi = ((gi % d.nx) + d.nx) % d.nx;
+    const int c2 = idx2(d, gj, gi);
+    const long long g = kb + c2;
     t.T[r][cc] = ld(T, g);
     t.S[r][cc] = ld(S, g);
     t.u[r][cc] = ld(u, g);
     t.v[r][cc] = ld(v, g);
-    t.w[r][cc] = wetf(__ldg(d.wbits + idx2(d, gj, gi)), k);
+    t.w[r][cc] = wetf(__ldg(d.wbits + c2), k);
   }
   __syncthreads();
   const int i = i0 + tx, j = j0 + ty;
@@ -689,11 +711,11 @@ __global__ void __launch_bounds__(TA_X * TA_Y) k_tracer_adv_t(Dev d, const float
   float aT = 0.f, aS = 0.f;
   if (w0 != 0.f) {
     const uint64_t bits = __ldg(d.wbits + base);
-    const float fxeT = ta_face_x(d, t.T, t, r, cc), fxwT = ta_face_x(d, t.T, t, r, cc - 1);
-    const float fxeS = ta_face_x(d, t.S, t, r, cc), fxwS = ta_face_x(d, t.S, t, r, cc - 1);
-    const float fynT = ta_face_y(d, t.T, t, r, cc, j), fynS = ta_face_y(d, t.S, t, r, cc, j);
-    const float fysT = j > 0 ? ta_face_y(d, t.T, t, r - 1, cc, j - 1) : 0.f;
-    const float fysS = j > 0 ? ta_face_y(d, t.S, t, r - 1, cc, j - 1) : 0.f;
+    float fxeT, fxeS, fxwT, fxwS, fynT, fynS, fysT, fysS;
+    ta_faces_x(d.limiter, t, r, cc, fxeT, fxeS);
+    ta_faces_x(d.limiter, t, r, cc - 1, fxwT, fxwS);
+    ta_faces_y(d, t, r, cc, j, fynT, fynS);
+    ta_faces_y(d, t, r - 1, cc, j - 1, fysT, fysS);
     const float ix = __ldg(d.inv_dx + base), ysc = d.inv_dy * __ldg(d.inv_cos + j);
     const float hT = (fxeT - fxwT) * ix + (fynT - fysT) * ysc;
     const float hS = (fxeS - fxwS) * ix + (fynS - fysS) * ysc;
@@ -860,12 +882,31 @@ __device__ __forceinline__ float drho(const Dev& d, float Ta, float Sa, float wa
   return rho_anom(Ta, Sa) * wa - rho_anom(Tb, Sb) * wb_;
 }
 
+// Pressure-gradient kernel (physics/pressure.py:32-97, legacy trapezoid form,
+// in differences), one column per thread.  Modes: 0 the barotropic forcing
+// F_rho and the depth-mean velocity; 1 and 2 the P part of the momentum
+// residual with the RK combination of the first and second stage.  The march
+// down the column keeps the density differences to the four neighbours and
+// their downward accumulation in registers, with the next level's ten T/S
+// values loaded while the current level computes.  Modes 1 and 2 need the
+// depth integral before the first output level, so the per-level gradient
+// goes to a scratch field (read back by the same thread, normally from L2).
+struct PgLevel {
+  float Tc, Sc, Te, Se, Tw, Sw, Tn, Sn, Ts, Ss;
+};
+
+__device__ __forceinline__ PgLevel pg_load(const float* __restrict__ T, const float* __restrict__ S, long long b,
+                                           long long cc, long long ce, long long cw, long long cn, long long cs) {
+  PgLevel L;
+  L.Tc = ld(T, b + cc); L.Sc = ld(S, b + cc);
+  L.Te = ld(T, b + ce); L.Se = ld(S, b + ce);
+  L.Tw = ld(T, b + cw); L.Sw = ld(S, b + cw);
+  L.Tn = ld(T, b + cn); L.Sn = ld(S, b + cn);
+  L.Ts = ld(T, b + cs); L.Ss = ld(S, b + cs);
+  return L;
+}
+
 __global__ void __launch_bounds__(128) k_pgf(Dev d, PgfArgs a) {
-  extern __shared__ float smem[];
-  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-  const int nt = blockDim.x * blockDim.y;
-  float* gxs = smem;
-  float* gys = smem + d.nz * nt;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= d.nx || j >= d.ny) return;
@@ -881,14 +922,15 @@ __global__ void __launch_bounds__(128) k_pgf(Dev d, PgfArgs a) {
   float pe = 0.f, pw = 0.f, pn = 0.f, ps = 0.f;       // p[e]-p[c], p[c]-p[w], p[n]-p[c], p[c]-p[s]
   float de0 = 0.f, dw0 = 0.f, dn0 = 0.f, ds0 = 0.f;   // density differences at the level above
   float gx_prev = 0.f, gy_prev = 0.f, fx = 0.f, fy = 0.f;
+  PgLevel nxt = pg_load(a.T, a.S, 0, cc, ce, cw, cn, cs);
   for (int k = 0; k < d.nz; ++k) {
-    const long long b = (long long)k * d.plane;
+    const PgLevel L = nxt;
+    if (k + 1 < d.nz) nxt = pg_load(a.T, a.S, (long long)(k + 1) * d.plane, cc, ce, cw, cn, cs);
     const float w0 = wetf(m0, k), we = wetf(me, k), ww = wetf(mw, k), wn = wetf(mn, k), ws = wetf(ms, k);
-    const float Tc = ld(a.T, b + cc), Sc = ld(a.S, b + cc);
-    const float de = drho(d, ld(a.T, b + ce), ld(a.S, b + ce), we, Tc, Sc, w0);
-    const float dw = drho(d, Tc, Sc, w0, ld(a.T, b + cw), ld(a.S, b + cw), ww);
-    const float dn = drho(d, ld(a.T, b + cn), ld(a.S, b + cn), wn, Tc, Sc, w0);
-    const float ds = drho(d, Tc, Sc, w0, ld(a.T, b + cs), ld(a.S, b + cs), ws);
+    const float de = drho(d, L.Te, L.Se, we, L.Tc, L.Sc, w0);
+    const float dw = drho(d, L.Tc, L.Sc, w0, L.Tw, L.Sw, ww);
+    const float dn = drho(d, L.Tn, L.Sn, wn, L.Tc, L.Sc, w0);
+    const float ds = drho(d, L.Tc, L.Sc, w0, L.Ts, L.Ss, ws);
     if (k > 0) {
       const float h = kG * 0.5f * d.vc.dz3d[k - 1];
       pe += (de0 + de) * h;
@@ -907,8 +949,9 @@ __global__ void __launch_bounds__(128) k_pgf(Dev d, PgfArgs a) {
     gx_prev = gx;
     gy_prev = gy;
     if (a.mode != 0) {
-      gxs[k * nt + tid] = -gx / kRho0;
-      gys[k * nt + tid] = -gy / kRho0;
+      const long long id = (long long)k * d.plane + cc;
+      a.gsx[id] = -gx / kRho0;
+      a.gsy[id] = -gy / kRho0;
     }
   }
   const float Fx = -fx / (kRho0 * d.H_sw);
@@ -932,8 +975,8 @@ __global__ void __launch_bounds__(128) k_pgf(Dev d, PgfArgs a) {
   for (int k = 0; k < d.nz; ++k) {
     const long long id = (long long)k * d.plane + cc;
     const float w = wetf(m0, k);
-    const float Pu = (gxs[k * nt + tid] - Fx) * w;
-    const float Pv = (gys[k * nt + tid] - Fy) * w;
+    const float Pu = (a.gsx[id] - Fx) * w;
+    const float Pv = (a.gsy[id] - Fy) * w;
     const float Au = ld(a.Au, id), Av = ld(a.Av, id);
     const float u1 = ld(a.u1, id), v1 = ld(a.v1, id);
     if (a.mode == 1) {

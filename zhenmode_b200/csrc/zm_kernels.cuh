@@ -18,6 +18,7 @@ struct FftPlan {
 struct PgfArgs {
   const float *T, *S, *u1, *v1, *Au, *Av, *Ppu, *Ppv;
   float *Pu, *Pv, *uo, *vo, *frx, *fry;
+  float *gsx, *gsy;  // per-level gradient scratch (modes 1 and 2)
   double *ubt0, *vbt0;
   float dt, bottom_decay;
   int mode;

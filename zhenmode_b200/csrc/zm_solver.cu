@@ -63,6 +63,7 @@ struct zm_solver {
   float *Fz = nullptr, *Ayu = nullptr, *Ayv = nullptr, *Au = nullptr, *Av = nullptr;
   float *accT = nullptr, *accS = nullptr, *TsA = nullptr, *SsA = nullptr, *TsB = nullptr, *SsB = nullptr;
   float *dT1 = nullptr, *dS1 = nullptr, *Tp = nullptr, *Sp = nullptr, *Pu = nullptr, *Pv = nullptr;
+  float *gsx = nullptr, *gsy = nullptr;  // pressure-gradient scratch
   float *up = nullptr, *vp = nullptr;
   float *frx = nullptr, *fry = nullptr, *means = nullptr, *wts = nullptr;
   double *ubt0 = nullptr, *vbt0 = nullptr, *ubt[2] = {nullptr, nullptr}, *vbt[2] = {nullptr, nullptr};
@@ -201,10 +202,11 @@ struct zm_solver {
   }
 
   void pgf(cudaStream_t s, PgfArgs a) {
-    const dim3 c(32, 2);
-    const size_t smem = a.mode == 0 ? 0 : (size_t)2 * nz * c.x * c.y * sizeof(float);
+    const dim3 c(32, 4);
+    a.gsx = gsx;
+    a.gsy = gsy;
     pb(ZM_K_PGF, s);
-    k_pgf<<<grid2(c), c, smem, s>>>(d, a);
+    k_pgf<<<grid2(c), c, 0, s>>>(d, a);
     pe(s);
     check_launch();
   }
@@ -653,7 +655,6 @@ void build(zm_solver* s, const zm_grid* g, const zm_params* p) {
   require(s->fft_smem <= 227 * 1024, ZM_ERR_UNSUPPORTED, "nx too large for the shared-memory FFT filter");
   ZM_CUDA(cudaFuncSetAttribute(k_dealias_lon, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->fft_smem));
   ZM_CUDA(cudaFuncSetAttribute(k_lin_t, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lin_tile_smem()));
-  ZM_CUDA(cudaFuncSetAttribute(k_pgf, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * nz * 64 * (int)sizeof(float)));
   // ---- buffers
   for (int q = 0; q < 2; ++q) {
     s->st[q] = s->four();
@@ -663,6 +664,7 @@ void build(zm_solver* s, const zm_grid* g, const zm_params* p) {
   s->Fz = s->f3(); s->Ayu = s->f3(); s->Ayv = s->f3(); s->Au = s->f3(); s->Av = s->f3();
   s->accT = s->f3(); s->accS = s->f3(); s->TsA = s->f3(); s->SsA = s->f3(); s->TsB = s->f3(); s->SsB = s->f3();
   s->dT1 = s->f3(); s->dS1 = s->f3(); s->Tp = s->f3(); s->Sp = s->f3(); s->Pu = s->f3(); s->Pv = s->f3();
+  s->gsx = s->f3(); s->gsy = s->f3();
   s->up = s->f3(); s->vp = s->f3();
   s->frx = s->f2(); s->fry = s->f2();
   s->means = s->alloc<float>((size_t)4 * 2 * std::max(nb, 1) * nz);
