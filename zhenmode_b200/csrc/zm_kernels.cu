@@ -317,8 +317,8 @@ __global__ void __launch_bounds__(LT_X * LT_Y) k_lin_t(Dev d, const float* __res
     const int r = e / LT_PX, cc = e - r * LT_PX;
     int gj = j0 - LT_H + r;
     gj = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
-    int gi = (i0 - LT_H + cc) % d.nx;
-    if (gi < 0) gi += d.nx;
+    int gi = i0 - LT_H + cc;
+    if (gi < 0 || gi >= d.nx) gi = ((gi % d.nx) + d.nx) % d.nx;
     const int c2 = idx2(d, gj, gi);
     const long long g = kb + c2;
     t.u[r][cc] = ld(u0, g);
@@ -791,6 +791,7 @@ __global__ void __launch_bounds__(128) k_tracer_rest(Dev d, RestArgs a) {
   // rho[m] > rho[m+1]  <=>  beta (S[m]-S[m+1]) > alpha (T[m]-T[m+1]).
   uint64_t unstable = 0ull, wetpair = 0ull;
   float Tu = ld(a.Tev, base), Su = ld(a.Sev, base);
+#pragma unroll 8
   for (int m = 0; m + 1 < nz; ++m) {
     const long long idn = base + (long long)(m + 1) * d.plane;
     const float Tl = ld(a.Tev, idn), Sl = ld(a.Sev, idn);
@@ -807,6 +808,7 @@ __global__ void __launch_bounds__(128) k_tracer_rest(Dev d, RestArgs a) {
     const float kc = d.kappa_conv;
     float fT = 0.f, fS = 0.f;
     float cT = ld(a.Tev, base), cS = ld(a.Sev, base);
+#pragma unroll 4
     for (int k = 0; k < nz; ++k) {
       const long long id = base + (long long)k * d.plane;
       float nT = 0.f, nS = 0.f, gT = 0.f, gS = 0.f;

@@ -650,7 +650,7 @@ void build(zm_solver* s, const zm_grid* g, const zm_params* p) {
   }
   plan.keepbin = s->upload(keepbin);
   s->fft = plan;
-  s->fft_lines = std::max(1, std::min(8, (int)((200 * 1024 / sizeof(float2)) / (2 * nx))));
+  s->fft_lines = std::max(1, std::min(4, (int)((200 * 1024 / sizeof(float2)) / (2 * nx))));
   s->fft_smem = (size_t)2 * s->fft_lines * nx * sizeof(float2);
   require(s->fft_smem <= 227 * 1024, ZM_ERR_UNSUPPORTED, "nx too large for the shared-memory FFT filter");
   ZM_CUDA(cudaFuncSetAttribute(k_dealias_lon, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->fft_smem));
