@@ -184,6 +184,26 @@ int zm_barrier_probe(zm_solver* s, void* stream, int32_t blocks, int32_t expecte
  * (the state is then not a valid step result).  Synchronizes the device. */
 int zm_status(zm_solver* s, int32_t* monitor_code);
 
+/* The diagnostics closure of make_solver_global (factory.py:752-760) on a
+ * state in the caller's device arrays, reference layout (nx, ny, nz) float32:
+ * rho = rho0 + rho'(T, S), the hydrostatic pressure rho0 g eta (+ the optional
+ * (nx, ny) surface_pressure_pa, NULL for none) + the trapezoid integral of the
+ * wet-masked density anomaly (dynamics/pressure.py:32-42, 62-74), and the
+ * vertical velocity -Fz wet (dynamics/transport.py:149-166).  Outputs are
+ * (nx, ny, nz) float32 device arrays.  Stream ordered, no host sync; uses the
+ * handle's work buffers, so it must not overlap a step of the same handle. */
+int zm_diagnostics(zm_solver* s, void* stream, const zm_state* in, const float* surface_pressure_pa, float* rho,
+                   float* pressure, float* w);
+
+/* Global heat/salt/volume snapshot of a state (compute_budget_diagnostics,
+ * diagnostics/snapshot.py:67-128, legacy node thickness, linear
+ * thermodynamics): T and S are (nx, ny, nz) float32 device arrays.  Writes
+ * out[8] = mean_T, mean_S, mean_T_top, mean_S_top, heat_content_J,
+ * salt_content_kg, total_volume_m3, mean_depth_m.  The sums are float64 with
+ * compensation (Neumaier per thread, double-double across threads) in a fixed
+ * order, so repeated calls agree bit for bit.  Synchronizes the stream. */
+int zm_budgets(zm_solver* s, void* stream, const float* T, const float* S, double rho0, double cp, double* out);
+
 /* Classify a float32 state held in the caller's device arrays (reference
  * layout) without allocating any device memory.  No counterpart in the
  * reference: its classify_state (runtime/monitor.py:20-30) runs inside JAX,

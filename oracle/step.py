@@ -383,6 +383,24 @@ def baroclinic_pressure(T, S, p):
     return out
 
 
+def hydrostatic_pressure(T, S, eta, p, surface_pressure_pa=None):
+    """dynamics/pressure.py:62-74 (reference-plane surface, trapezoid):
+    rho0 g eta (+ the surface load) + the baroclinic integral."""
+    p_bt = RHO_0 * G_EARTH * eta[:, :, None]
+    if surface_pressure_pa is not None:
+        p_bt = p_bt + np.asarray(surface_pressure_pa, dtype=np.float64)[..., None]
+    return p_bt + baroclinic_pressure(T, S, p)
+
+
+def diagnostics(state, p, surface_pressure_pa=None):
+    """The diagnostics closure of factory.py:752-760: full density
+    rho0 + rho', hydrostatic pressure and the dual-face vertical velocity."""
+    rho = RHO_0 + density_anomaly(state["T"], state["S"], p)
+    pres = hydrostatic_pressure(state["T"], state["S"], state["eta"], p, surface_pressure_pa)
+    w = vertical_velocity(state["u"], state["v"], p)
+    return rho, pres, w
+
+
 def pressure_gradient(T, S, eta, p):
     """dynamics/pressure.py:62-97: -grad(rho0 g eta + p_bc)/rho0."""
     pres = RHO_0 * G_EARTH * eta[:, :, None] + baroclinic_pressure(T, S, p)

@@ -204,8 +204,37 @@ def make_operator_case(seed=11):
     print("operators saved", len(results), "arrays")
 
 
+def make_diagnostics_case(seed=5):
+    """The reference's diagnostics closure (factory.py:752-760: rho, hydrostatic
+    pressure, vertical velocity), with and without a surface-pressure load, and
+    its budget snapshot (diagnostics/snapshot.py:67-128) on a moving float32
+    state of the 48x24x10 option-set grid."""
+    from zhenmode.model.diagnostics import snapshot as ref_snapshot
+    grid = workloads.build_grid(48, 24, 10, land_lat=75.0)
+    T, S = workloads.initial_fields(grid, perturb_sigma=0.2)
+    kw = dict(workloads.PLAIN_OPTIONS)
+    kw.update(forcing=workloads.wind_forcing(grid), dt_bt=75.0, dtype="float64")
+    _, _, diagnostics = make_solver_global(grid, _physics(workloads.PLAIN_PHYSICS), 1800.0, **kw)
+    u, v, T0, S0, eta = _moving_state(grid, T, S, seed, amp_u=0.1, amp_eta=0.3)
+    st = JaxStateG(*[_f32(a) for a in (u, v, T0, S0, eta)], np.zeros((48, 24)))
+    rng = np.random.default_rng(seed + 1)
+    sp = _f32(101325.0 + 500.0 * _smooth_noise(rng, (48, 24)))
+    rho, pres, w = diagnostics(st)
+    _, pres_sp, _ = diagnostics(st, surface_pressure_pa=sp)
+    b = ref_snapshot.compute_budget_diagnostics(st, grid)
+    data = dict(_grid_arrays(grid))
+    data.update(in_u=_np(st.u), in_v=_np(st.v), in_T=_np(st.T), in_S=_np(st.S), in_eta=_np(st.eta),
+                surface_pressure_pa=sp, rho=_np(rho), pressure=_np(pres), w=_np(w), pressure_sp=_np(pres_sp),
+                budget_names=np.array(list(b.as_dict().keys())),
+                budget_values=np.array(list(b.as_dict().values()), dtype=np.float64),
+                options=np.array(repr(workloads.PLAIN_OPTIONS)))
+    np.savez_compressed(os.path.join(HERE, "diagnostics_48x24x10.npz"), **data)
+    print("diagnostics saved", dict(zip(b.as_dict().keys(), b.as_dict().values())))
+
+
 def main():
     make_operator_case()
+    make_diagnostics_case()
     # The 0.5 deg production option set, rescaled to a 7.5 deg x 7.5 deg grid
     # whose polar bands are partly wet, from a moving state (2 steps).
     make_step_case("step_plain_48x24x10", 48, 24, 10, 75.0, workloads.PLAIN_PHYSICS,

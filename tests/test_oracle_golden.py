@@ -115,3 +115,40 @@ def test_full_step(name):
                     assert np.max(np.abs(st[k])) < 1e-14
                 else:
                     _check(f"{name} step {n} {k}", st[k], want, tol=1e-10)
+
+
+def _diag_case():
+    from zhenmode_b200 import workloads
+    data = load("diagnostics_48x24x10")
+    grid = grid_from(data)
+    lat = np.radians(np.asarray(grid.lat))
+    tau_x = np.broadcast_to((0.1 * np.sin(2 * lat) * np.cos(lat))[None, :], (grid.nx, grid.ny)).copy()
+    zeros = np.zeros((grid.nx, grid.ny))
+    kw = dict(workloads.PLAIN_OPTIONS)
+    kw.update(forcing=(tau_x, zeros, zeros.copy()), dt_bt=75.0, dtype="float64")
+    p = oparams.build_params(grid, workloads.PLAIN_PHYSICS, 1800.0, **kw)
+    state = {k: data["in_" + k] for k in ("u", "v", "T", "S", "eta")}
+    return data, grid, p, state
+
+
+def test_diagnostics_closure():
+    """rho, hydrostatic pressure (with and without a surface load) and the
+    vertical velocity of the reference's diagnostics closure."""
+    data, grid, p, state = _diag_case()
+    rho, pres, w = ostep.diagnostics(state, p)
+    _check("rho", rho, data["rho"])
+    _check("pressure", pres, data["pressure"])
+    _check("w", w, data["w"])
+    _, pres_sp, _ = ostep.diagnostics(state, p, surface_pressure_pa=data["surface_pressure_pa"])
+    _check("pressure_sp", pres_sp, data["pressure_sp"])
+
+
+def test_budget_diagnostics():
+    from oracle import budgets
+    data, grid, p, state = _diag_case()
+    got = budgets.budget_diagnostics(state["T"], state["S"], grid.dx_2d, grid.dy, grid.z, grid.wet_mask,
+                                     grid.wet_mask_3d)
+    names = [str(n) for n in data["budget_names"]]
+    assert names == list(budgets.FIELDS)
+    for name, want in zip(names, data["budget_values"]):
+        assert abs(got[name] - want) <= 1e-13 * abs(want), (name, got[name], want)

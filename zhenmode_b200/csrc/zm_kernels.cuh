@@ -62,6 +62,13 @@ __global__ void k_bt_vel(Dev d, const double* eta, const double* ubt, const doub
                          const double* Fy, double* ubt_o, double* vbt_o, double dtb, double drag);
 __global__ void k_cap2d(Dev d, double* f0, double* f1, const float* wts, const double* count, int nb_rows);
 __global__ void k_eta_to_float(Dev d, const double* e64, float* e32);
+// diagnostics outside the step (zm_diagnostics.cu)
+#define ZM_BUDGET_SUMS 7
+__global__ void k_diagnostics(Dev d, const float* T, const float* S, const float* eta, const float* Fz,
+                              const float* sp, float* rho, float* pres, float* w);
+__global__ void k_budget_partials(Dev d, const float* T, const float* S, const double* area, const double* width,
+                                  double* partial);
+__global__ void k_budget_final(const double* partial, int nblocks, double* out);
 __global__ void k_barrier_probe(unsigned* bar, unsigned* err, unsigned expected, unsigned max_polls);
 __global__ void k_nu_tb(Dev d, const float* u, const float* v, float* uo, float* vo, float c, int nsub);
 __global__ void k_lin_t(Dev d, const float* usub, const float* vsub, const float* u0, const float* v0, const float* T0,

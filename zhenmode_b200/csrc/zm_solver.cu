@@ -64,6 +64,9 @@ struct zm_solver {
   float *accT = nullptr, *accS = nullptr, *TsA = nullptr, *SsA = nullptr, *TsB = nullptr, *SsB = nullptr;
   float *dT1 = nullptr, *dS1 = nullptr, *Tp = nullptr, *Sp = nullptr, *Pu = nullptr, *Pv = nullptr;
   float *gsx = nullptr, *gsy = nullptr;  // pressure-gradient scratch
+  // budget snapshot: cell areas (reference layout), node thicknesses, partials
+  double *area64 = nullptr, *width64 = nullptr, *bpart = nullptr, *bout = nullptr;
+  int bblocks = 0;
   float *up = nullptr, *vp = nullptr;
   float *frx = nullptr, *fry = nullptr, *means = nullptr, *wts = nullptr;
   double *ubt0 = nullptr, *vbt0 = nullptr, *ubt[2] = {nullptr, nullptr}, *vbt[2] = {nullptr, nullptr};
@@ -740,6 +743,23 @@ void build(zm_solver* s, const zm_grid* g, const zm_params* p) {
   s->ref = Fields4{s->alloc<float>(nref3), s->alloc<float>(nref3), s->alloc<float>(nref3), s->alloc<float>(nref3)};
   s->ref_eta = s->alloc<float>((size_t)nx * ny);
   s->flags = s->alloc<unsigned int>(1);
+  {
+    // budget snapshot (diagnostics/snapshot.py:42-64, 67-128)
+    std::vector<double> area((size_t)nx * ny), width(nz);
+    for (size_t q = 0; q < area.size(); ++q) area[q] = g->dx_2d[q] * g->dy;
+    for (int k = 0; k < nz; ++k) {
+      if (k == 0) width[k] = std::fabs(g->z[1] - g->z[0]);
+      else if (k == nz - 1) width[k] = std::fabs(g->z[nz - 1] - g->z[nz - 2]);
+      else width[k] = 0.5 * (std::fabs(g->z[k] - g->z[k - 1]) + std::fabs(g->z[k + 1] - g->z[k]));
+    }
+    s->area64 = s->upload(area);
+    s->width64 = s->upload(width);
+    int sms = 0;
+    ZM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
+    s->bblocks = std::max(1, std::min(4 * sms, (int)(((long long)nx * ny + 7) / 8)));
+    s->bpart = s->alloc<double>((size_t)s->bblocks * ZM_BUDGET_SUMS * 2);
+    s->bout = s->alloc<double>(ZM_BUDGET_SUMS * 2);
+  }
   ZM_CUDA(cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking));
   ZM_CUDA(cudaDeviceSynchronize());
 }
@@ -951,6 +971,60 @@ int zm_barrier_probe(zm_solver* s, void* stream, int32_t blocks, int32_t expecte
   } catch (const Err& e) {
     return fail(s, e);
   }
+  return ZM_OK;
+}
+
+int zm_diagnostics(zm_solver* s, void* stream, const zm_state* in, const float* surface_pressure_pa, float* rho,
+                   float* pressure, float* w) {
+  if (!s || !in || !in->u || !in->v || !in->T || !in->S || !in->eta || !rho || !pressure || !w)
+    return ZM_ERR_INVALID;
+  cudaStream_t st = (cudaStream_t)stream;
+  try {
+    // the caller's state goes to work buffers that are idle between steps
+    s->load(st, in, s->s2, s->frx);
+    const float* sp = nullptr;
+    const dim3 c(32, 4);
+    if (surface_pressure_pa) {
+      k_ref_to_int2<<<s->grid2(dim3(32, 8)), dim3(32, 8), 0, st>>>(s->d, surface_pressure_pa, s->fry);
+      sp = s->fry;
+    }
+    k_fz<<<s->grid2(c), c, 0, st>>>(s->d, s->s2.u, s->s2.v, s->Fz);
+    k_diagnostics<<<s->grid2(c), c, 0, st>>>(s->d, s->s2.T, s->s2.S, s->frx, s->Fz, sp, s->W1.u, s->W1.v, s->W2.u);
+    s->check_launch();
+    s->to_ref3(st, s->W1.u, rho, 0.f);
+    s->to_ref3(st, s->W1.v, pressure, 0.f);
+    s->to_ref3(st, s->W2.u, w, 0.f);
+    s->check_launch();
+  } catch (const Err& e) {
+    return fail(s, e);
+  }
+  return ZM_OK;
+}
+
+int zm_budgets(zm_solver* s, void* stream, const float* T, const float* S, double rho0, double cp, double* out) {
+  if (!s || !T || !S || !out || !std::isfinite(rho0) || !std::isfinite(cp)) return ZM_ERR_INVALID;
+  cudaStream_t st = (cudaStream_t)stream;
+  double sums[2 * ZM_BUDGET_SUMS];
+  try {
+    k_budget_partials<<<s->bblocks, 256, 0, st>>>(s->d, T, S, s->area64, s->width64, s->bpart);
+    k_budget_final<<<1, 32, 0, st>>>(s->bpart, s->bblocks, s->bout);
+    s->check_launch();
+    ZM_CUDA(cudaMemcpyAsync(sums, s->bout, sizeof(sums), cudaMemcpyDeviceToHost, st));
+    ZM_CUDA(cudaStreamSynchronize(st));
+  } catch (const Err& e) {
+    return fail(s, e);
+  }
+  double v[ZM_BUDGET_SUMS];
+  for (int q = 0; q < ZM_BUDGET_SUMS; ++q) v[q] = sums[2 * q] + sums[2 * q + 1];
+  if (!(v[0] > 0.0)) return fail(s, Err{ZM_ERR_INVALID, "total wet volume is zero; check the grid/mask"});
+  out[0] = v[1] / v[0];          // mean_T
+  out[1] = v[2] / v[0];          // mean_S
+  out[2] = v[4] / v[3];          // mean_T_top
+  out[3] = v[5] / v[3];          // mean_S_top
+  out[4] = rho0 * cp * v[1];     // heat_content_J
+  out[5] = rho0 / 1000.0 * v[2]; // salt_content_kg
+  out[6] = v[0];                 // total_volume_m3
+  out[7] = v[0] / v[6];          // mean_depth_m
   return ZM_OK;
 }
 

@@ -16,13 +16,14 @@ from __future__ import annotations
 
 import collections
 import ctypes
+import dataclasses
 import math
 import numbers
 
 import numpy as np
 
 from . import _native
-from .config import RHO_0
+from .config import C_P, RHO_0
 
 JaxStateG = collections.namedtuple("JaxStateG", ["u", "v", "T", "S", "eta", "ice"])
 JaxStateG.__new__.__defaults__ = (0.0,)
@@ -203,6 +204,49 @@ def _torch_state_ptrs(state, shape):
 
 
 _BT_KERNELS = {'auto': 0, 'resident': 1, 'streaming': 2}
+
+
+@dataclasses.dataclass(frozen=True)
+class BudgetDiagnostics:
+    """Global tracer/volume diagnostics of one snapshot, with the fields of the
+    reference's ``BudgetDiagnostics`` (diagnostics/snapshot.py:16-40)."""
+    mean_T: float
+    mean_S: float
+    mean_T_top: float
+    mean_S_top: float
+    heat_content_J: float
+    salt_content_kg: float
+    total_volume_m3: float
+    mean_depth_m: float
+
+    def as_dict(self):
+        return dataclasses.asdict(self)
+
+
+def _device_fields(state, shape):
+    """(CUDA float32 tensors u, v, T, S, eta; True if the state was on the host)."""
+    import torch
+    if isinstance(state.u, torch.Tensor):
+        return _torch_state_ptrs(state, shape), False
+    dev = torch.device('cuda')
+    fields = [torch.as_tensor(np.ascontiguousarray(getattr(state, k), dtype=np.float32), device=dev)
+              for k in ("u", "v", "T", "S", "eta")]
+    return _torch_state_ptrs(JaxStateG(*fields, None), shape), True
+
+
+def compute_budget_diagnostics(state, grid=None, rho0=RHO_0, cp=None, *, column_geometry="legacy",
+                               thermodynamics="linear", solver):
+    """Heat/salt/volume snapshot (diagnostics/snapshot.py:67-128) on the GPU.
+
+    ``solver`` is a step returned by :func:`make_solver_global` for ``grid``;
+    its grid defines the areas, node thicknesses and wet mask.  The sums are
+    compensated float64 in a fixed order.
+    """
+    if thermodynamics != "linear":
+        raise UnsupportedOption("only the linear snapshot thermodynamics is implemented on the B200 path")
+    if column_geometry != "legacy":
+        raise UnsupportedOption("only the legacy column geometry is implemented on the B200 path")
+    return solver.budget_diagnostics(state, rho0=rho0, cp=cp)
 
 
 def make_solver_global(grid, physics, dt, forcing=None,
@@ -416,10 +460,44 @@ def make_solver_global(grid, physics, dt, forcing=None,
                          torch.zeros(shape[:2], dtype=torch.float32, device=dev))
 
     def diagnostics(state, surface_pressure_pa=None):
-        raise NotImplementedError("diagnostics (rho, pressure, w) are not implemented on the B200 path yet")
+        """(rho, pressure, w) of a state (factory.py:752-760): full density,
+        hydrostatic pressure with an optional (nx, ny) surface load in Pa, and
+        the vertical velocity, each (nx, ny, nz) float32, on the state's side
+        (CUDA tensors for a device state, NumPy arrays for a host state)."""
+        import torch
+        fin, host = _device_fields(state, solver.shape)
+        sp = None
+        if surface_pressure_pa is not None:
+            sp = torch.as_tensor(np.asarray(surface_pressure_pa, dtype=np.float32)
+                                 if not isinstance(surface_pressure_pa, torch.Tensor) else surface_pressure_pa,
+                                 dtype=torch.float32, device=fin[0].device).contiguous()
+            if tuple(sp.shape) != solver.shape[:2]:
+                raise ValueError('surface pressure must be a finite (nx, ny) Pa field')
+        outs = [torch.empty_like(fin[0]) for _ in range(3)]
+        stream = torch.cuda.current_stream(fin[0].device).cuda_stream
+        sin = _native.ZmState(*[t.data_ptr() for t in fin])
+        solver.check(solver.lib.zm_diagnostics(solver.handle, ctypes.c_void_p(stream), ctypes.byref(sin),
+                                               ctypes.c_void_p(sp.data_ptr() if sp is not None else None),
+                                               *[ctypes.c_void_p(t.data_ptr()) for t in outs]), "zm_diagnostics")
+        if host:
+            return tuple(t.cpu().numpy() for t in outs)
+        return tuple(outs)
+
+    def budget_diagnostics(state, rho0=RHO_0, cp=None):
+        """Heat/salt/volume snapshot of a state (diagnostics/snapshot.py:67-128)
+        with compensated float64 sums on the GPU."""
+        import torch
+        fin, _ = _device_fields(state, solver.shape)
+        out = (ctypes.c_double * 8)()
+        stream = torch.cuda.current_stream(fin[0].device).cuda_stream
+        solver.check(solver.lib.zm_budgets(solver.handle, ctypes.c_void_p(stream), ctypes.c_void_p(fin[2].data_ptr()),
+                                           ctypes.c_void_p(fin[3].data_ptr()), float(rho0),
+                                           float(C_P if cp is None else cp), out), "zm_budgets")
+        return BudgetDiagnostics(*[float(x) for x in out])
 
     step.solver = solver
     step.advance = _run
+    step.budget_diagnostics = budget_diagnostics
     result = [step, init_state, diagnostics]
     if return_params:
         params = dict(n_subcyc=solver.n_subcyc, nu_nsub=solver.n_nu, adv_nsub=solver.adv_nsub,
