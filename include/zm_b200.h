@@ -195,6 +195,41 @@ int zm_status(zm_solver* s, int32_t* monitor_code);
 int zm_diagnostics(zm_solver* s, void* stream, const zm_state* in, const float* surface_pressure_pa, float* rho,
                    float* pressure, float* w);
 
+/* ---- learned vertical-mixing closure: the per-column MLP ---------------
+ * New in this library (the reference's closure is the plain kappa_v + coastal
+ * band + convective gate of physics/vertical.py:40-82, which these calls are
+ * trained to stand in for).  256 -> 256 -> 256 -> 64 with GELU after the
+ * hidden layers; parameters are one float32 array of ZM_MLP_NPARAMS values:
+ * W1 [256][256], b1 [256], W2 [256][256], b2 [256], W3 [64][256], b3 [64],
+ * each W[out][in] with the input index contiguous. */
+#define ZM_MLP_IN 256
+#define ZM_MLP_OUT 64
+#define ZM_MLP_NPARAMS 148032
+
+/* Inference on the tensor cores: X [ncol][256] BF16 rows, W1/W2/W3 BF16 as
+ * above, float32 biases; Y [ncol][64] float32 (raw outputs).  *err gets bit 0
+ * set if a wait on the tensor cores ran out of polls.  Stream ordered. */
+int zm_mlp_forward_bf16(void* stream, int32_t ncol, const void* X, const void* W1, const float* b1, const void* W2,
+                        const float* b2, const void* W3, const float* b3, float* Y, uint32_t* err);
+
+/* float32 parameters -> BF16 W1, W2, W3 (device arrays). Stream ordered. */
+int zm_mlp_pack_bf16(void* stream, const float* params, void* W1, void* W2, void* W3);
+
+/* float32 training: a trainer owns the workspaces for batches of up to
+ * batch_max rows.  X [B][256], targets T [B][64], mask M [B][64] (1 where an
+ * output is trained), mask_count = sum of M.  The loss is the masked mean
+ * square error.  zm_mlp_grad writes the gradient of every parameter;
+ * zm_mlp_train_step applies one Adam step (step counts from 1) in place.
+ * *loss, when given, receives the batch loss (synchronizes the stream). */
+typedef struct zm_mlp_trainer zm_mlp_trainer;
+int zm_mlp_trainer_create(int32_t batch_max, zm_mlp_trainer** out);
+void zm_mlp_trainer_destroy(zm_mlp_trainer* tr);
+int zm_mlp_grad(zm_mlp_trainer* tr, void* stream, int32_t batch, const float* X, const float* T, const float* M,
+                double mask_count, const float* params, float* grad_out, double* loss);
+int zm_mlp_train_step(zm_mlp_trainer* tr, void* stream, int32_t batch, const float* X, const float* T, const float* M,
+                      double mask_count, float* params, float* adam_m, float* adam_v, int32_t step, float lr,
+                      float beta1, float beta2, float eps, double* loss);
+
 /* Global heat/salt/volume snapshot of a state (compute_budget_diagnostics,
  * diagnostics/snapshot.py:67-128, legacy node thickness, linear
  * thermodynamics): T and S are (nx, ny, nz) float32 device arrays.  Writes

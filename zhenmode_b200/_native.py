@@ -76,6 +76,17 @@ EXPORTS = {
     "zm_status": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
     "zm_diagnostics": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ZmState), ctypes.c_void_p,
                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "zm_mlp_forward_bf16": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32] + [ctypes.c_void_p] * 8
+                            + [ctypes.c_void_p]),
+    "zm_mlp_pack_bf16": (ctypes.c_int, [ctypes.c_void_p] * 5),
+    "zm_mlp_trainer_create": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
+    "zm_mlp_trainer_destroy": (None, [ctypes.c_void_p]),
+    "zm_mlp_grad": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32] + [ctypes.c_void_p] * 3
+                    + [ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
+    "zm_mlp_train_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32] + [ctypes.c_void_p] * 3
+                          + [ctypes.c_double] + [ctypes.c_void_p] * 3
+                          + [ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                             ctypes.POINTER(ctypes.c_double)]),
     "zm_budgets": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                   ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]),
     "zm_classify_state_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,

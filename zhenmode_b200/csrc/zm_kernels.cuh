@@ -1,6 +1,8 @@
 // Declarations shared by the kernel translation units and the solver.
 #pragma once
 
+#include <cuda_bf16.h>
+
 #include "zm_internal.cuh"
 
 namespace zm {
@@ -62,6 +64,12 @@ __global__ void k_bt_vel(Dev d, const double* eta, const double* ubt, const doub
                          const double* Fy, double* ubt_o, double* vbt_o, double dtb, double drag);
 __global__ void k_cap2d(Dev d, double* f0, double* f1, const float* wts, const double* count, int nb_rows);
 __global__ void k_eta_to_float(Dev d, const double* e64, float* e32);
+// per-column MLP of the learned closure (zm_mlp.cu); BF16 weights [out][in]
+struct MlpBf16 {
+  const __nv_bfloat16 *W1, *W2, *W3;
+  const float *b1, *b2, *b3;
+};
+size_t mlp_tc_smem();
 // diagnostics outside the step (zm_diagnostics.cu)
 #define ZM_BUDGET_SUMS 7
 __global__ void k_diagnostics(Dev d, const float* T, const float* S, const float* eta, const float* Fz,
