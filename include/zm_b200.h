@@ -163,7 +163,8 @@ int zm_run_stage(zm_solver* s, void* stream, int32_t stage, const zm_state* in, 
 #define ZM_K_PGF 9           /* pressure gradient, momentum RK combine, BT forcing */
 #define ZM_K_BAROTROPIC 10   /* barotropic subcycle */
 #define ZM_K_FINAL 11        /* projection, polar cap, land hold */
-#define ZM_K_COUNT 12
+#define ZM_K_CLOSURE 12      /* learned closure: features + tensor-core MLP */
+#define ZM_K_COUNT 13
 
 /* Advance the resident state by one step without the CUDA graph, timing
  * every kernel launch with CUDA events on `stream`; ms[c] and launches[c]
@@ -229,6 +230,33 @@ int zm_mlp_grad(zm_mlp_trainer* tr, void* stream, int32_t batch, const float* X,
 int zm_mlp_train_step(zm_mlp_trainer* tr, void* stream, int32_t batch, const float* X, const float* T, const float* M,
                       double mask_count, float* params, float* adam_m, float* adam_v, int32_t step, float lr,
                       float beta1, float beta2, float eps, double* loss);
+
+/* Turn the learned vertical-mixing closure on for every following step of
+ * the handle (params: ZM_MLP_NPARAMS float32 device values, see zm_mlp_*), or
+ * off (params NULL).  While on, each step first infers a diffusivity per wet
+ * interface from the step's input columns on the tensor cores; T and S then
+ * diffuse vertically with it in the implicit interface-flux solve of the
+ * linear half steps (u and v implicitly with nu_v), and the explicit
+ * convective mixing of the tracer residual is dropped, the network standing
+ * in for kappa_v + coastal + kappa_conv (physics/vertical.py:40-82).  A column
+ * with a feature beyond +-bound (or not finite) takes the plain closure. */
+int zm_set_closure(zm_solver* s, void* stream, const float* params, float bound);
+
+/* Columns of the last step that took the plain closure, and tensor-core
+ * waits that ran out of polls (ZM_ERR_TIMEOUT if any).  Synchronizes. */
+int zm_closure_stats(zm_solver* s, uint32_t* fallback_columns, uint32_t* wait_errors);
+
+/* The closure's diffusivity for a state (reference layout device arrays):
+ * kappa [nx*ny][64] float32 in the row order of zm_closure_features, interface
+ * m in column m (0 at dry interfaces and beyond nz-2).  Requires a closure set
+ * by zm_set_closure.  Stream ordered; uses the handle's work buffers. */
+int zm_closure_kappa(zm_solver* s, void* stream, const zm_state* in, float* kappa);
+
+/* Training rows of a state (reference layout device arrays): per column
+ * (j-major, i fastest; nx*ny rows) the 256 features X, log10 of the plain
+ * closure's diffusivity at interfaces 0..nz-2 in T [.][64] and the wet
+ * interface mask M [.][64].  Stream ordered; uses the handle's work buffers. */
+int zm_closure_features(zm_solver* s, void* stream, const zm_state* in, float* X, float* T, float* M);
 
 /* Global heat/salt/volume snapshot of a state (compute_budget_diagnostics,
  * diagnostics/snapshot.py:67-128, legacy node thickness, linear

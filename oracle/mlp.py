@@ -72,3 +72,36 @@ def forward_bf16(p, X, round_bf16):
     H = r(gelu(H @ r(w["W1"]).T + w["b1"]))
     H = r(gelu(H @ r(w["W2"]).T + w["b2"]))
     return H @ r(w["W3"]).T + w["b3"]
+
+
+def closure_features(state, p):
+    """Float64 training rows of a state (the closure's features and the
+    plain closure's log10 diffusivity per interface, physics/vertical.py:40-82),
+    rows j-major with i fastest, as the GPU kernel writes them."""
+    T = np.asarray(state["T"], np.float64) - p.T_ref
+    S = np.asarray(state["S"], np.float64) - p.S_ref
+    u = np.asarray(state["u"], np.float64)
+    v = np.asarray(state["v"], np.float64)
+    wm = np.asarray(p.wet_mask_z, np.float64)
+    nx, ny, nz = T.shape
+    X = np.zeros((nx, ny, 256))
+    X[..., 0:nz] = T * 0.1 * wm
+    X[..., 50:50 + nz] = S * wm
+    X[..., 100:100 + nz] = u * 2.0 * wm
+    X[..., 150:150 + nz] = v * 2.0 * wm
+    wif = wm[..., :-1] * wm[..., 1:]
+    dz = np.asarray(p.dz_3d, np.float64).reshape(-1)
+    n2 = 9.81 * (-2.0e-4 * (T[..., 1:] - T[..., :-1]) + 7.6e-4 * (S[..., 1:] - S[..., :-1])) / dz
+    X[..., 200:200 + nz - 1] = n2 * 1e4 * wif
+    X[..., 250] = np.hypot(p.tau_x_2d, p.tau_y_2d) * 10.0
+    X[..., 251] = p.Q_heat_2d * 0.01
+    unstable = (7.6e-4 * (S[..., :-1] - S[..., 1:]) > 2.0e-4 * (T[..., :-1] - T[..., 1:])) & (wif > 0.5)
+    col = np.any(unstable, axis=-1, keepdims=True)
+    gate = unstable if p.localize_conv else np.broadcast_to(col, unstable.shape)
+    kap = p.kappa_v + p.coastal_kappa_v_2d[..., None] + (p.kappa_conv if p.kappa_conv > 0 else 0.0) * gate
+    Tt = np.zeros((nx, ny, 64))
+    M = np.zeros((nx, ny, 64))
+    Tt[..., :nz - 1] = np.where(wif > 0.5, np.log10(np.where(wif > 0.5, kap, 1.0)), 0.0)
+    M[..., :nz - 1] = wif
+    rows = lambda a: np.transpose(a, (1, 0, 2)).reshape(nx * ny, -1)
+    return rows(X), rows(Tt), rows(M)

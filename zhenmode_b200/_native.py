@@ -20,7 +20,7 @@ ZM_ERR_TIMEOUT = 4
 ZM_ERR_MONITOR = 5
 
 KERNEL_CLASSES = ("nu_sub", "inner_lap", "lin_finish", "implicit", "fz", "madv", "dealias", "tracer_adv",
-                  "tracer_rest", "pgf", "barotropic", "final")
+                  "tracer_rest", "pgf", "barotropic", "final", "closure")
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _fp = ctypes.POINTER(ctypes.c_float)
@@ -87,6 +87,12 @@ EXPORTS = {
                           + [ctypes.c_double] + [ctypes.c_void_p] * 3
                           + [ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                              ctypes.POINTER(ctypes.c_double)]),
+    "zm_set_closure": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float]),
+    "zm_closure_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32),
+                                        ctypes.POINTER(ctypes.c_uint32)]),
+    "zm_closure_kappa": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ZmState), ctypes.c_void_p]),
+    "zm_closure_features": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ZmState),
+                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "zm_budgets": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                   ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]),
     "zm_classify_state_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,

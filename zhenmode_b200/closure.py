@@ -153,3 +153,43 @@ class ClosureMLP:
         if tr is not None:
             self.lib.zm_mlp_trainer_destroy(tr)
             self._tr = None
+
+
+def collect(step, state, nsteps, every=1, max_rows=2_000_000, seed=0):
+    """Run ``step`` (the plain closure) ``nsteps`` times from ``state`` and take
+    the training rows of the wet columns every ``every`` steps; keep at most
+    ``max_rows`` of them (seeded subsample).  Returns (X, T, M, final state)."""
+    import torch
+    parts = []
+    for n in range(nsteps):
+        state = step(state)
+        if (n + 1) % every == 0:
+            X, T, M = step.closure_features(state)
+            keep = M.sum(1) > 0
+            parts.append((X[keep], T[keep], M[keep]))
+    X = torch.cat([p[0] for p in parts])
+    T = torch.cat([p[1] for p in parts])
+    M = torch.cat([p[2] for p in parts])
+    if X.shape[0] > max_rows:
+        g = torch.Generator(device="cpu").manual_seed(seed)
+        idx = torch.randperm(X.shape[0], generator=g)[:max_rows].to(X.device)
+        X, T, M = X[idx], T[idx], M[idx]
+    return X, T, M, state
+
+
+def fit(net, X, T, M, steps=2000, batch=8192, lr=1e-3, seed=0):
+    """Adam on random batches of the rows (the native float32 training
+    kernels); returns the masked mean-square loss on all rows afterwards."""
+    import torch
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    n = X.shape[0]
+    batch = min(batch, n)
+    for _ in range(steps):
+        idx = torch.randint(0, n, (batch,), generator=g).to(X.device)
+        net.train_step(X[idx], T[idx], M[idx], lr=lr)
+    net.pack()
+    losses = []
+    for a in range(0, n, 65536):
+        sl = slice(a, min(n, a + 65536))
+        losses.append(net.grad(X[sl], T[sl], M[sl])[0] * float(M[sl].sum().item()))
+    return sum(losses) / float(M.sum().item())

@@ -451,11 +451,52 @@ __device__ void implicit_column(const Dev& d, float* __restrict__ f, long long b
   for (int k = 0; k < n; ++k) f[base + (long long)k * d.plane] = x[k] + rhs[k];
 }
 
+// Backward-Euler interface-flux diffusion of one tracer column with a
+// diffusivity per interface, kap[m] between wet levels m and m+1:
+// tend_k = (F_{k-1/2} - F_{k+1/2}) / dz_node_k, F_{m+1/2} = -kap_m (c_{m+1} - c_m) / dz_iface_m,
+// zero flux at the surface and the deepest wet level.  FP32 Thomas plus one
+// refinement step, as implicit_column.
+__device__ void implicit_column_iface(const Dev& d, float* __restrict__ f, long long base, uint64_t bits,
+                                      const float* __restrict__ kap3, float dt) {
+  const int kb = kbot_of(bits);
+  if (kb == 0 || !wetb(bits, 0)) return;
+  const int n = kb + 1;
+  float lo[ZM_MAXZ], up[ZM_MAXZ], rhs[ZM_MAXZ], x[ZM_MAXZ], e[ZM_MAXZ], cp[ZM_MAXZ];
+  for (int k = 0; k < n; ++k) {
+    rhs[k] = f[base + (long long)k * d.plane];
+    lo[k] = k > 0 ? -dt * __ldg(kap3 + base + (long long)(k - 1) * d.plane) * d.vc.inv_dz_iface[k - 1] *
+                        d.vc.inv_dz_node[k]
+                  : 0.f;
+    up[k] = k + 1 < n ? -dt * __ldg(kap3 + base + (long long)k * d.plane) * d.vc.inv_dz_iface[k] * d.vc.inv_dz_node[k]
+                      : 0.f;
+  }
+  auto solve = [&](const float* r, float* y) {
+    float inv = 1.f / (1.f - lo[0] - up[0]);
+    cp[0] = up[0] * inv;
+    y[0] = r[0] * inv;
+    for (int k = 1; k < n; ++k) {
+      inv = 1.f / ((1.f - lo[k] - up[k]) - lo[k] * cp[k - 1]);
+      cp[k] = up[k] * inv;
+      y[k] = (r[k] - lo[k] * y[k - 1]) * inv;
+    }
+    for (int k = n - 2; k >= 0; --k) y[k] -= cp[k] * y[k + 1];
+  };
+  solve(rhs, x);
+  for (int k = 0; k < n; ++k) {
+    float ax = (1.f - lo[k] - up[k]) * x[k];
+    if (k > 0) ax += lo[k] * x[k - 1];
+    if (k + 1 < n) ax += up[k] * x[k + 1];
+    e[k] = rhs[k] - ax;
+  }
+  solve(e, rhs);
+  for (int k = 0; k < n; ++k) f[base + (long long)k * d.plane] = x[k] + rhs[k];
+}
+
 __global__ void __launch_bounds__(128) k_implicit_vdiff(Dev d, float* __restrict__ u, float* __restrict__ v,
                                                         float* __restrict__ T, float* __restrict__ S,
                                                         const float* __restrict__ u0, const float* __restrict__ v0,
                                                         const float* __restrict__ T0, const float* __restrict__ S0,
-                                                        float dth) {
+                                                        float dth, const float* __restrict__ kap3) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= d.nx || j >= d.ny) return;
@@ -463,9 +504,14 @@ __global__ void __launch_bounds__(128) k_implicit_vdiff(Dev d, float* __restrict
   const uint64_t bits = wb(d, j, i);
   implicit_column(d, u, base, bits, d.nu_v * dth);
   implicit_column(d, v, base, bits, d.nu_v * dth);
-  const float kv = __ldg(d.kv2 + base);
-  implicit_column(d, T, base, bits, kv * dth);
-  implicit_column(d, S, base, bits, kv * dth);
+  if (kap3) {  // the learned closure's diffusivity per interface
+    implicit_column_iface(d, T, base, bits, kap3, dth);
+    implicit_column_iface(d, S, base, bits, kap3, dth);
+  } else {
+    const float kv = __ldg(d.kv2 + base);
+    implicit_column(d, T, base, bits, kv * dth);
+    implicit_column(d, S, base, bits, kv * dth);
+  }
   // land/ghost hold, then the exact Coriolis rotation
   const float c = __ldg(d.rot_c + base), s = __ldg(d.rot_s + base);
   for (int k = 0; k < d.nz; ++k) {
@@ -803,7 +849,7 @@ __global__ void __launch_bounds__(128) k_tracer_rest(Dev d, RestArgs a) {
     Su = Sl;
   }
   uint64_t allow = 0ull;
-  if (unstable && d.kappa_conv > 0.f) allow = d.localize_conv ? unstable : wetpair;
+  if (unstable && d.kappa_conv > 0.f && !a.no_conv) allow = d.localize_conv ? unstable : wetpair;
   if (a.nc == 1 || allow == 0ull) {
     const float kc = d.kappa_conv;
     float fT = 0.f, fS = 0.f;

@@ -31,6 +31,7 @@ struct RestArgs {
   float *dT1, *dS1, *To, *So;
   float dt, inv_na;
   int nc, stage;
+  int no_conv;  // convective mixing carried by the learned closure instead
 };
 
 // 2.5-D tracer advection tile
@@ -70,6 +71,18 @@ struct MlpBf16 {
   const float *b1, *b2, *b3;
 };
 size_t mlp_tc_smem();
+// learned closure in the step: features of a column, the plain closure per
+// interface, and the fused tensor-core inference writing kappa per interface
+struct ClosureArgs {
+  const float *T, *S, *u, *v;   // internal layout; T, S as anomalies
+  float* kappa3;                // [nz-1][ny][P] diffusivity per interface (fused kernel)
+  float *X, *Tt, *Mt;           // features [ncol][256], targets and mask [ncol][64] (features kernel)
+  unsigned* fallback;           // columns that took the plain closure
+  float bound;                  // largest |feature| the network is trusted with
+};
+__global__ void k_closure_features(Dev d, ClosureArgs a);
+__global__ void k_mlp_closure(MlpBf16 w, Dev d, ClosureArgs a, unsigned* err);
+__global__ void k_kappa_rows(Dev d, const float* kap3, float* out);
 // diagnostics outside the step (zm_diagnostics.cu)
 #define ZM_BUDGET_SUMS 7
 __global__ void k_diagnostics(Dev d, const float* T, const float* S, const float* eta, const float* Fz,
@@ -85,7 +98,7 @@ __global__ void k_lin_t(Dev d, const float* usub, const float* vsub, const float
 constexpr int LT_TX = 32, LT_TY = 16;
 size_t lin_tile_smem();
 __global__ void k_implicit_vdiff(Dev d, float* u, float* v, float* T, float* S, const float* u0, const float* v0,
-                                 const float* T0, const float* S0, float dth);
+                                 const float* T0, const float* S0, float dth, const float* kap3);
 __global__ void k_fz(Dev d, const float* u, const float* v, float* Fz);
 __global__ void k_madv(Dev d, const float* u, const float* v, const float* Fz, float* Ayu, float* Ayv);
 __global__ void k_dealias_lon(Dev d, FftPlan plan, const float* Ayu, const float* Ayv, float* Au, float* Av,

@@ -231,6 +231,140 @@ __global__ void __launch_bounds__(MT, 1) k_mlp_tc(MlpBf16 w, const __nv_bfloat16
       });
 }
 
+// ---------------------------------------------------------------- the closure in the step
+
+// Feature q of the column at 2-D index base (wet bits `bits`): 0..49 T anomaly
+// / 10, 50..99 S anomaly, 100..149 u / 0.5, 150..199 v / 0.5 (wet levels),
+// 200..248 N^2 / 1e-4 at the wet interfaces, 250 |tau| / 0.1, 251 Q / 100,
+// the rest zero.
+__device__ __forceinline__ float closure_feature(const Dev& d, const ClosureArgs& a, long long base, uint64_t bits,
+                                                 int q) {
+  if (q < 200) {
+    const int g = q / 50, k = q - g * 50;
+    if (k >= d.nz || !wetb(bits, k)) return 0.f;
+    const long long id = base + (long long)k * d.plane;
+    if (g == 0) return ld(a.T, id) * 0.1f;
+    if (g == 1) return ld(a.S, id);
+    if (g == 2) return ld(a.u, id) * 2.f;
+    return ld(a.v, id) * 2.f;
+  }
+  if (q < 250) {
+    const int m = q - 200;
+    if (m + 1 >= d.nz || !wetb(bits, m) || !wetb(bits, m + 1)) return 0.f;
+    const long long id = base + (long long)m * d.plane;
+    const float dT = ld(a.T, id + d.plane) - ld(a.T, id), dS = ld(a.S, id + d.plane) - ld(a.S, id);
+    // N^2 = -(g / rho0) d rho / dz with z up: g (-alpha dT + beta dS) / dz, deeper minus upper
+    return kG * (-kAlpha * dT + kBeta * dS) * d.vc.inv_dz_iface[m] * 1e4f;
+  }
+  if (q == 250) {
+    const float tx = __ldg(d.tau_x + base), ty = __ldg(d.tau_y + base);
+    return sqrtf(tx * tx + ty * ty) * 10.f;
+  }
+  if (q == 251) return __ldg(d.qheat + base) * 0.01f;
+  return 0.f;
+}
+
+// The plain closure at interface m of a wet column (physics/vertical.py:40-82):
+// kappa_v + coastal band, plus kappa_conv where the interface is statically
+// unstable (localized) or the column has an unstable interface.
+__device__ __forceinline__ float plain_kappa(const Dev& d, const ClosureArgs& a, long long base, uint64_t bits, int m,
+                                            bool col_unstable) {
+  float k = __ldg(d.kv2 + base);
+  if (d.kappa_conv > 0.f) {
+    bool gate = col_unstable;
+    if (d.localize_conv) {
+      const long long id = base + (long long)m * d.plane;
+      gate = kBeta * (ld(a.S, id) - ld(a.S, id + d.plane)) > kAlpha * (ld(a.T, id) - ld(a.T, id + d.plane));
+    }
+    if (gate) k += d.kappa_conv;
+  }
+  return k;
+}
+
+__device__ __forceinline__ bool column_unstable(const Dev& d, const ClosureArgs& a, long long base, uint64_t bits) {
+  for (int m = 0; m + 1 < d.nz; ++m) {
+    if (!wetb(bits, m) || !wetb(bits, m + 1)) continue;
+    const long long id = base + (long long)m * d.plane;
+    if (kBeta * (ld(a.S, id) - ld(a.S, id + d.plane)) > kAlpha * (ld(a.T, id) - ld(a.T, id + d.plane))) return true;
+  }
+  return false;
+}
+
+// Training rows: features (float32), log10 of the plain closure at the wet
+// interfaces and the mask of those interfaces, one column per thread.
+__global__ void __launch_bounds__(128) k_closure_features(Dev d, ClosureArgs a) {
+  const long long ncol = (long long)d.nx * d.ny;
+  const long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= ncol) return;
+  const int j = (int)(col / d.nx), i = (int)(col - (long long)j * d.nx);
+  const long long base = idx2(d, j, i);
+  const uint64_t bits = __ldg(d.wbits + base);
+  for (int q = 0; q < MK; ++q) a.X[col * MK + q] = closure_feature(d, a, base, bits, q);
+  const bool cu = column_unstable(d, a, base, bits);
+  for (int m = 0; m < MO; ++m) {
+    const bool wet_if = m + 1 < d.nz && wetb(bits, m) && wetb(bits, m + 1);
+    a.Tt[col * MO + m] = wet_if ? log10f(plain_kappa(d, a, base, bits, m, cu)) : 0.f;
+    a.Mt[col * MO + m] = wet_if ? 1.f : 0.f;
+  }
+}
+
+// The closure inside the step: features staged straight into the A tile of
+// the tensor-core MLP; kappa = 10^y at the wet interfaces, clipped to
+// [1e-7, 1] m^2/s, or the plain closure for a column whose features exceed
+// the trusted bound (or are not finite).
+__global__ void __launch_bounds__(MT, 1) k_mlp_closure(MlpBf16 w, Dev d, ClosureArgs a, unsigned* err) {
+  extern __shared__ __align__(1024) uint8_t msm[];
+  const long long ncol = (long long)d.nx * d.ny;
+  const long long col = (long long)blockIdx.x * MT + threadIdx.x;
+  const bool act = col < ncol;
+  const int j = act ? (int)(col / d.nx) : 0, i = act ? (int)(col - (long long)j * d.nx) : 0;
+  const long long base = idx2(d, j, i);
+  const uint64_t bits = act ? __ldg(d.wbits + base) : 0ull;
+  bool trusted = true;
+  int unstable = -1;  // column gate of the plain closure, formed on first use
+  mlp_tc_body(
+      w, msm, err,
+      [&](int, auto put) {
+        for (int kp = 0; kp < MK / 8; ++kp) {
+          __align__(16) __nv_bfloat16 h[8];
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            const float f = act ? closure_feature(d, a, base, bits, kp * 8 + e) : 0.f;
+            if (!(fabsf(f) <= a.bound)) trusted = false;
+            h[e] = __float2bfloat16(f);
+          }
+          put(kp, *reinterpret_cast<const uint4*>(h));
+        }
+      },
+      [&](int, int c0, const float* y) {
+        if (!act) return;
+        if (!trusted && unstable < 0) {
+          unstable = column_unstable(d, a, base, bits) ? 1 : 0;
+          atomicAdd(a.fallback, 1u);
+        }
+        for (int e = 0; e < 16; ++e) {
+          const int m = c0 + e;
+          if (m + 1 >= d.nz) break;
+          float k = 0.f;
+          if (wetb(bits, m) && wetb(bits, m + 1)) {
+            if (trusted) k = fminf(fmaxf(exp10f(y[e]), 1e-7f), 1.f);
+            else k = plain_kappa(d, a, base, bits, m, unstable == 1);
+          }
+          a.kappa3[(long long)m * d.plane + base] = k;
+        }
+      });
+}
+
+// kappa3 [nz-1][ny][P] -> dense rows [col][64] (zero beyond nz-2)
+__global__ void k_kappa_rows(Dev d, const float* __restrict__ kap3, float* __restrict__ out) {
+  const long long ncol = (long long)d.nx * d.ny;
+  const long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= ncol) return;
+  const int j = (int)(col / d.nx), i = (int)(col - (long long)j * d.nx);
+  const long long base = idx2(d, j, i);
+  for (int m = 0; m < MO; ++m) out[col * MO + m] = m + 1 < d.nz ? kap3[(long long)m * d.plane + base] : 0.f;
+}
+
 // float32 parameters -> BF16 weights (biases stay float32)
 __global__ void k_mlp_pack(const float* __restrict__ params, __nv_bfloat16* __restrict__ W1,
                            __nv_bfloat16* __restrict__ W2, __nv_bfloat16* __restrict__ W3) {

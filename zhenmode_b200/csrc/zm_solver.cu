@@ -67,6 +67,12 @@ struct zm_solver {
   // budget snapshot: cell areas (reference layout), node thicknesses, partials
   double *area64 = nullptr, *width64 = nullptr, *bpart = nullptr, *bout = nullptr;
   int bblocks = 0;
+  // learned vertical-mixing closure (off until zm_set_closure)
+  bool closure_on = false;
+  MlpBf16 cw{};
+  float* kappa3 = nullptr;       // [nz-1][ny][P] diffusivity per interface
+  unsigned* cl_count = nullptr;  // [0] fallback columns of the last step, [1] tensor-core wait errors
+  float cl_bound = 8.f;
   float *up = nullptr, *vp = nullptr;
   float *frx = nullptr, *fry = nullptr, *means = nullptr, *wts = nullptr;
   double *ubt0 = nullptr, *vbt0 = nullptr, *ubt[2] = {nullptr, nullptr}, *vbt[2] = {nullptr, nullptr};
@@ -169,12 +175,13 @@ struct zm_solver {
     }
     pb(ZM_K_LIN_FINISH, s);
     k_lin_t<<<dim3((nx + LT_TX - 1) / LT_TX, (ny + LT_TY - 1) / LT_TY, nz), dim3(LT_TX, LT_TY), lin_tile_smem(), s>>>(
-        d, usub, vsub, src.u, src.v, src.T, src.S, dst.u, dst.v, dst.T, dst.S, dth, vdiff);
+        d, usub, vsub, src.u, src.v, src.T, src.S, dst.u, dst.v, dst.T, dst.S, dth, vdiff || closure_on);
     pe(s);
-    if (vdiff) {
+    if (vdiff || closure_on) {
       const dim3 c(32, 4);
       pb(ZM_K_IMPLICIT, s);
-      k_implicit_vdiff<<<grid2(c), c, 0, s>>>(d, dst.u, dst.v, dst.T, dst.S, src.u, src.v, src.T, src.S, dth);
+      k_implicit_vdiff<<<grid2(c), c, 0, s>>>(d, dst.u, dst.v, dst.T, dst.S, src.u, src.v, src.T, src.S, dth,
+                                              closure_on ? kappa3 : nullptr);
       pe(s);
     }
     check_launch();
@@ -196,7 +203,8 @@ struct zm_solver {
       cT = nT;
       cS = nS;
     }
-    RestArgs a{T, S, accT, accS, Tbase, Sbase, dT1, dS1, To, So, (float)dt, 1.f / (float)adv_nsub, conv_nsub, stage};
+    RestArgs a{T, S, accT, accS, Tbase, Sbase, dT1, dS1, To, So, (float)dt, 1.f / (float)adv_nsub, conv_nsub, stage,
+               closure_on ? 1 : 0};
     const dim3 c(32, 4);
     pb(ZM_K_TRACER_REST, s);
     k_tracer_rest<<<grid2(c), c, 0, s>>>(d, a);
@@ -351,8 +359,21 @@ struct zm_solver {
     check_launch();
   }
 
+  // learned closure: diffusivity per interface from the step's input state
+  void closure(cudaStream_t s, const Fields4& in) {
+    ZM_CUDA(cudaMemsetAsync(cl_count, 0, sizeof(unsigned), s));
+    ClosureArgs a{};
+    a.T = in.T; a.S = in.S; a.u = in.u; a.v = in.v; a.kappa3 = kappa3; a.fallback = cl_count; a.bound = cl_bound;
+    const long long ncol = (long long)nx * ny;
+    pb(ZM_K_CLOSURE, s);
+    k_mlp_closure<<<(unsigned)((ncol + 127) / 128), 128, mlp_tc_smem(), s>>>(cw, d, a, cl_count + 1);
+    pe(s);
+    check_launch();
+  }
+
   void full_step(cudaStream_t s, int from, int to) {
     const Fields4& in = st[from];
+    if (closure_on) closure(s, in);
     linear_half(s, in, s1);
     nonlinear(s, s1, s2);
     linear_half(s, s2, s1);
@@ -1025,6 +1046,99 @@ int zm_budgets(zm_solver* s, void* stream, const float* T, const float* S, doubl
   out[5] = rho0 / 1000.0 * v[2]; // salt_content_kg
   out[6] = v[0];                 // total_volume_m3
   out[7] = v[0] / v[6];          // mean_depth_m
+  return ZM_OK;
+}
+
+int zm_set_closure(zm_solver* s, void* stream, const float* params, float bound) {
+  if (!s || (params && !(bound > 0.f))) return ZM_ERR_INVALID;
+  cudaStream_t st = (cudaStream_t)stream;
+  try {
+    if (params) {
+      if (s->nz > 51) return fail(s, Err{ZM_ERR_UNSUPPORTED, "the learned closure covers at most 50 levels"});
+      if (!s->kappa3) {
+        s->kappa3 = s->alloc<float>((size_t)std::max(1, s->nz - 1) * s->d.plane);
+        s->cl_count = s->alloc<unsigned>(2);
+        __nv_bfloat16* W1 = s->alloc<__nv_bfloat16>((size_t)ZM_MLP_IN * ZM_MLP_IN);
+        __nv_bfloat16* W2 = s->alloc<__nv_bfloat16>((size_t)ZM_MLP_IN * ZM_MLP_IN);
+        __nv_bfloat16* W3 = s->alloc<__nv_bfloat16>((size_t)ZM_MLP_OUT * ZM_MLP_IN);
+        float* b = s->alloc<float>(2 * ZM_MLP_IN + ZM_MLP_OUT);
+        s->cw = MlpBf16{W1, W2, W3, b, b + ZM_MLP_IN, b + 2 * ZM_MLP_IN};
+        ZM_CUDA(cudaFuncSetAttribute(k_mlp_closure, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_tc_smem()));
+      }
+      const int rc = zm_mlp_pack_bf16(stream, params, (void*)s->cw.W1, (void*)s->cw.W2, (void*)s->cw.W3);
+      if (rc != ZM_OK) return fail(s, Err{rc, "packing the closure weights failed"});
+      const long long off_b1 = (long long)ZM_MLP_IN * ZM_MLP_IN, off_b2 = 2 * off_b1 + ZM_MLP_IN,
+                      off_b3 = off_b2 + ZM_MLP_IN + (long long)ZM_MLP_OUT * ZM_MLP_IN;
+      float* b = const_cast<float*>(s->cw.b1);
+      ZM_CUDA(cudaMemcpyAsync(b, params + off_b1, ZM_MLP_IN * sizeof(float), cudaMemcpyDeviceToDevice, st));
+      ZM_CUDA(cudaMemcpyAsync(b + ZM_MLP_IN, params + off_b2, ZM_MLP_IN * sizeof(float), cudaMemcpyDeviceToDevice, st));
+      ZM_CUDA(cudaMemcpyAsync(b + 2 * ZM_MLP_IN, params + off_b3, ZM_MLP_OUT * sizeof(float),
+                              cudaMemcpyDeviceToDevice, st));
+      ZM_CUDA(cudaMemsetAsync(s->cl_count, 0, 2 * sizeof(unsigned), st));
+      s->cl_bound = bound;
+    }
+    const bool on = params != nullptr;
+    if (on != s->closure_on) {  // the captured steps change shape
+      s->closure_on = on;
+      ZM_CUDA(cudaStreamSynchronize(st));
+      for (int g = 0; g < 2; ++g)
+        if (s->graph[g]) {
+          cudaGraphExecDestroy(s->graph[g]);
+          s->graph[g] = nullptr;
+        }
+      s->graphs_ready = false;
+    }
+  } catch (const Err& e) {
+    return fail(s, e);
+  }
+  return ZM_OK;
+}
+
+int zm_closure_stats(zm_solver* s, uint32_t* fallback_columns, uint32_t* wait_errors) {
+  if (!s || !fallback_columns || !wait_errors) return ZM_ERR_INVALID;
+  if (!s->cl_count) {
+    *fallback_columns = 0;
+    *wait_errors = 0;
+    return ZM_OK;
+  }
+  unsigned c[2];
+  const cudaError_t e = cudaMemcpy(c, s->cl_count, sizeof(c), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return fail(s, Err{ZM_ERR_CUDA, std::string("zm_closure_stats: ") + cudaGetErrorString(e)});
+  *fallback_columns = c[0];
+  *wait_errors = c[1];
+  return c[1] ? ZM_ERR_TIMEOUT : ZM_OK;
+}
+
+int zm_closure_kappa(zm_solver* s, void* stream, const zm_state* in, float* kappa) {
+  if (!s || !in || !in->u || !in->v || !in->T || !in->S || !in->eta || !kappa) return ZM_ERR_INVALID;
+  if (!s->closure_on) return fail(s, Err{ZM_ERR_INVALID, "zm_closure_kappa: no closure set"});
+  cudaStream_t st = (cudaStream_t)stream;
+  try {
+    s->load(st, in, s->s2, s->frx);
+    s->closure(st, s->s2);
+    const long long ncol = (long long)s->nx * s->ny;
+    k_kappa_rows<<<(unsigned)((ncol + 127) / 128), 128, 0, st>>>(s->d, s->kappa3, kappa);
+    s->check_launch();
+  } catch (const Err& e) {
+    return fail(s, e);
+  }
+  return ZM_OK;
+}
+
+int zm_closure_features(zm_solver* s, void* stream, const zm_state* in, float* X, float* T, float* M) {
+  if (!s || !in || !in->u || !in->v || !in->T || !in->S || !in->eta || !X || !T || !M) return ZM_ERR_INVALID;
+  if (s->nz > 51) return fail(s, Err{ZM_ERR_UNSUPPORTED, "the learned closure covers at most 50 levels"});
+  cudaStream_t st = (cudaStream_t)stream;
+  try {
+    s->load(st, in, s->s2, s->frx);
+    ClosureArgs a{};
+    a.T = s->s2.T; a.S = s->s2.S; a.u = s->s2.u; a.v = s->s2.v; a.X = X; a.Tt = T; a.Mt = M;
+    const long long ncol = (long long)s->nx * s->ny;
+    k_closure_features<<<(unsigned)((ncol + 127) / 128), 128, 0, st>>>(s->d, a);
+    s->check_launch();
+  } catch (const Err& e) {
+    return fail(s, e);
+  }
   return ZM_OK;
 }
 

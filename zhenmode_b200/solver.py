@@ -495,9 +495,71 @@ def make_solver_global(grid, physics, dt, forcing=None,
                                            float(C_P if cp is None else cp), out), "zm_budgets")
         return BudgetDiagnostics(*[float(x) for x in out])
 
+    def _cur_stream():
+        import torch
+        return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def set_closure(net=None, bound=8.0):
+        """Turn the learned vertical-mixing closure on for the following steps
+        (``net``: a :class:`zhenmode_b200.closure.ClosureMLP` or its float32
+        parameters) or off (``None``).  Columns with a feature beyond
+        ``bound`` take the plain closure."""
+        import torch
+        if net is None:
+            solver.check(solver.lib.zm_set_closure(solver.handle, _cur_stream(), None, float(bound)), "zm_set_closure")
+            step.closure_params = None
+            return
+        params = net.params if hasattr(net, "params") else net
+        if not isinstance(params, torch.Tensor):
+            params = torch.as_tensor(np.asarray(params, dtype=np.float32), device="cuda")
+        params = params.to(device="cuda", dtype=torch.float32).contiguous()
+        if params.numel() != 148032:
+            raise ValueError("the closure takes 148032 float32 parameters")
+        solver.check(solver.lib.zm_set_closure(solver.handle, _cur_stream(), ctypes.c_void_p(params.data_ptr()),
+                                               float(bound)), "zm_set_closure")
+        step.closure_params = params
+
+    def closure_features(state):
+        """Training rows of a state: (X [nx*ny][256], log10 plain kappa [nx*ny][64],
+        wet-interface mask [nx*ny][64]), rows j-major with i fastest."""
+        import torch
+        fin, _ = _device_fields(state, solver.shape)
+        n = solver.shape[0] * solver.shape[1]
+        X = torch.empty((n, 256), dtype=torch.float32, device=fin[0].device)
+        T = torch.empty((n, 64), dtype=torch.float32, device=fin[0].device)
+        M = torch.empty((n, 64), dtype=torch.float32, device=fin[0].device)
+        sin = _native.ZmState(*[t.data_ptr() for t in fin])
+        solver.check(solver.lib.zm_closure_features(solver.handle, _cur_stream(), ctypes.byref(sin),
+                                                    *[ctypes.c_void_p(t.data_ptr()) for t in (X, T, M)]),
+                     "zm_closure_features")
+        return X, T, M
+
+    def closure_kappa(state):
+        """The set closure's diffusivity for a state, [nx*ny][64] (rows as in closure_features)."""
+        import torch
+        fin, _ = _device_fields(state, solver.shape)
+        K = torch.empty((solver.shape[0] * solver.shape[1], 64), dtype=torch.float32, device=fin[0].device)
+        sin = _native.ZmState(*[t.data_ptr() for t in fin])
+        solver.check(solver.lib.zm_closure_kappa(solver.handle, _cur_stream(), ctypes.byref(sin),
+                                                 ctypes.c_void_p(K.data_ptr())), "zm_closure_kappa")
+        return K
+
+    def closure_stats():
+        """(columns of the last step that took the plain closure, tensor-core wait errors)."""
+        fb, er = ctypes.c_uint32(), ctypes.c_uint32()
+        rc = solver.lib.zm_closure_stats(solver.handle, ctypes.byref(fb), ctypes.byref(er))
+        if rc not in (_native.ZM_OK, _native.ZM_ERR_TIMEOUT):
+            solver.check(rc, "zm_closure_stats")
+        return int(fb.value), int(er.value)
+
     step.solver = solver
     step.advance = _run
     step.budget_diagnostics = budget_diagnostics
+    step.set_closure = set_closure
+    step.closure_features = closure_features
+    step.closure_kappa = closure_kappa
+    step.closure_stats = closure_stats
+    step.closure_params = None
     result = [step, init_state, diagnostics]
     if return_params:
         params = dict(n_subcyc=solver.n_subcyc, nu_nsub=solver.n_nu, adv_nsub=solver.adv_nsub,
