@@ -92,7 +92,7 @@ def closure_features(state, p):
     wif = wm[..., :-1] * wm[..., 1:]
     dz = np.asarray(p.dz_3d, np.float64).reshape(-1)
     n2 = 9.81 * (-2.0e-4 * (T[..., 1:] - T[..., :-1]) + 7.6e-4 * (S[..., 1:] - S[..., :-1])) / dz
-    X[..., 200:200 + nz - 1] = n2 * 1e4 * wif
+    X[..., 200:200 + nz - 1] = np.arcsinh(n2 * 1e8) * 0.25 * wif
     X[..., 250] = np.hypot(p.tau_x_2d, p.tau_y_2d) * 10.0
     X[..., 251] = p.Q_heat_2d * 0.01
     unstable = (7.6e-4 * (S[..., :-1] - S[..., 1:]) > 2.0e-4 * (T[..., :-1] - T[..., 1:])) & (wif > 0.5)

@@ -79,3 +79,53 @@ def test_step_with_closure_is_stable():
     step.set_closure(None)
     again = step(st)
     assert all(bool((getattr(plain, k) == getattr(again, k)).all()) for k in ("u", "v", "T", "S", "eta"))
+
+
+def test_trained_closure_tracks_the_plain_run():
+    """Train the network on rows of the plain model itself (1 day, 180x90x50,
+    cold surface patches that convect), then run one day from an unseen
+    state: the daily-mean SST of the learned form stays within 0.05 K RMS of
+    the plain run, and well inside what the same form gives without the
+    network (a constant kappa_v, no convective mixing)."""
+    import torch
+    from zhenmode_b200.closure import ClosureMLP, collect, fit, init_params
+    nx, ny, nz, nsteps = 180, 90, 50, 48
+    grid, physics, dt, kw, T, S = workloads.make_case("plain", nx, ny, nz, dtype="float32")
+    step, init, _ = make_solver_global(grid, physics, dt, **kw)
+    wet3 = torch.as_tensor(np.asarray(grid.wet_mask_3d, np.float32), device="cuda")
+
+    def patched(seed):
+        st = init(T, S)
+        g = torch.Generator(device="cpu").manual_seed(seed)
+        patch = (torch.rand((nx, ny), generator=g) < 0.15).float().to("cuda")
+        cool = torch.zeros_like(st.T)
+        cool[:, :, :4] = 2.5 * patch[:, :, None]
+        return JaxStateG(st.u, st.v, st.T - cool * wet3, st.S, st.eta, st.ice)
+
+    def daily_sst(st):
+        acc = torch.zeros((nx, ny), device="cuda")
+        for _ in range(nsteps):
+            st = step(st)
+            acc += st.T[:, :, 0]
+        return acc / nsteps
+
+    X, Tt, M, _ = collect(step, patched(1), nsteps, every=2)
+    net = ClosureMLP(seed=0)
+    loss = fit(net, X, Tt, M, steps=3000, batch=8192, lr=1e-3)
+    assert loss < 0.1, loss
+    st0 = patched(2)
+    ref = daily_sst(st0)
+    step.set_closure(net)
+    learned = daily_sst(st0)
+    assert step.closure_stats() == (0, 0)
+    plain_kv = init_params(0)
+    plain_kv[:] = 0.0
+    plain_kv[-64:] = np.log10(physics.kappa_v)
+    step.set_closure(plain_kv)
+    without = daily_sst(st0)
+    step.set_closure(None)
+    wet = torch.as_tensor(np.asarray(grid.wet_mask), device="cuda") > 0
+    rmse = lambda a: float(torch.sqrt(((a - ref)[wet] ** 2).mean()))
+    print(f"daily-mean SST RMSE vs plain: learned {rmse(learned):.4f} K, without the network {rmse(without):.4f} K")
+    assert rmse(learned) <= 0.05
+    assert rmse(without) > 4.0 * rmse(learned)

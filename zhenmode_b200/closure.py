@@ -3,8 +3,8 @@
 The network stands in for the plain closure of the reference
 (``_effective_kappa_v`` and ``_convective_mask``, physics/vertical.py:40-82):
 kappa_v + coastal band + kappa_conv on statically unstable interfaces.  It
-maps the 252 column features of ``features`` (T, S, u, v and N^2 over 50
-levels, wind stress magnitude, heat flux; 4 zero pads) to 64 outputs, of which
+maps 252 column features (T, S, u, v over 50 levels, N^2 on a signed log
+scale over 49 interfaces, wind stress magnitude, heat flux; 4 zero pads) to 64 outputs, of which
 outputs 0..nz-2 are log10 of the diffusivity at interfaces 0..nz-2 and the
 rest are unused.
 

@@ -235,8 +235,8 @@ __global__ void __launch_bounds__(MT, 1) k_mlp_tc(MlpBf16 w, const __nv_bfloat16
 
 // Feature q of the column at 2-D index base (wet bits `bits`): 0..49 T anomaly
 // / 10, 50..99 S anomaly, 100..149 u / 0.5, 150..199 v / 0.5 (wet levels),
-// 200..248 N^2 / 1e-4 at the wet interfaces, 250 |tau| / 0.1, 251 Q / 100,
-// the rest zero.
+// 200..248 asinh(N^2 / 1e-8) / 4 at the wet interfaces, 250 |tau| / 0.1,
+// 251 Q / 100, the rest zero.
 __device__ __forceinline__ float closure_feature(const Dev& d, const ClosureArgs& a, long long base, uint64_t bits,
                                                  int q) {
   if (q < 200) {
@@ -253,8 +253,9 @@ __device__ __forceinline__ float closure_feature(const Dev& d, const ClosureArgs
     if (m + 1 >= d.nz || !wetb(bits, m) || !wetb(bits, m + 1)) return 0.f;
     const long long id = base + (long long)m * d.plane;
     const float dT = ld(a.T, id + d.plane) - ld(a.T, id), dS = ld(a.S, id + d.plane) - ld(a.S, id);
-    // N^2 = -(g / rho0) d rho / dz with z up: g (-alpha dT + beta dS) / dz, deeper minus upper
-    return kG * (-kAlpha * dT + kBeta * dS) * d.vc.inv_dz_iface[m] * 1e4f;
+    // N^2 = -(g / rho0) d rho / dz with z up: g (-alpha dT + beta dS) / dz, deeper
+    // minus upper, on a signed log scale so that weak stratification keeps its sign
+    return asinhf(kG * (-kAlpha * dT + kBeta * dS) * d.vc.inv_dz_iface[m] * 1e8f) * 0.25f;
   }
   if (q == 250) {
     const float tx = __ldg(d.tau_x + base), ty = __ldg(d.tau_y + base);
