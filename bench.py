@@ -196,6 +196,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", default=None, help="NXxNYxNZ: same option set on another grid (profiling cases)")
+    ap.add_argument("--form", default="plain", choices=["plain", "learned"],
+                    help="learned: train the closure network on the plain model's own columns (30 days, "
+                         "2M rows) first, then time the step with it")
+    ap.add_argument("--closure-days", type=int, default=30)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -226,6 +230,24 @@ def main():
     step, init_state, _ = make_solver_global(grid, physics, dt, **kw)
     solver = step.solver
     st = init_state(T_init=T, S_init=S)
+    closure_info = None
+    if args.form == "learned":
+        from zhenmode_b200.closure import ClosureMLP, collect, fit
+        steps_per_day = int(round(86400.0 / dt))
+        nsteps_c = args.closure_days * steps_per_day
+        every = max(1, nsteps_c // 60)
+        t0 = time.time()
+        X, Tt, M, _ = collect(step, st, nsteps_c, every=every, max_rows=2_000_000, seed=0)
+        torch.cuda.synchronize()
+        t1 = time.time()
+        net = ClosureMLP(seed=0)
+        loss = fit(net, X, Tt, M, steps=3000, batch=8192, lr=1e-3)
+        torch.cuda.synchronize()
+        closure_info = {"rows": int(X.shape[0]), "collect_days": args.closure_days, "snapshots": nsteps_c // every,
+                        "collect_s": round(t1 - t0, 1), "train_steps": 3000, "batch": 8192,
+                        "train_s": round(time.time() - t1, 1), "loss_log10_kappa_mse": loss}
+        del X, Tt, M
+        step.set_closure(net)
     stream = torch.cuda.current_stream()
     sptr = ctypes.c_void_p(stream.cuda_stream)
     sin = _native.ZmState(*[t.data_ptr() for t in (st.u, st.v, st.T, st.S, st.eta)])
@@ -318,7 +340,7 @@ def main():
                 "config": {"workload": f"{wl.nx}x{wl.ny}x{wl.nz} 0.5-degree plain FP32 option set, dt={wl.dt:.0f} s, "
                                        f"{solver.n_subcyc} barotropic subcycles, {solver.n_nu} nu_h subcycles",
                            "parallelism": f"replicas x{world}", "l2": "per-step working set >> L2 (no flush)",
-                           "monitor_code": int(code.value)},
+                           "monitor_code": int(code.value), "form": args.form},
                 "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
                              "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                              "traffic": traffic, "algorithmic_bytes_per_launch": algo,
@@ -329,6 +351,9 @@ def main():
                 "kernel_ms_unrolled_total": total_prof,
                 "gpu_launches": args.steps * kernels_per_step + 1,
                 "clocks": clk, "e2e": e2e, "cpu_baseline": cpu}
+        if closure_info is not None:
+            closure_info["fallback_columns_last_step"] = step.closure_stats()[0]
+            line["closure"] = closure_info
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()

@@ -158,20 +158,24 @@ class ClosureMLP:
 def collect(step, state, nsteps, every=1, max_rows=2_000_000, seed=0):
     """Run ``step`` (the plain closure) ``nsteps`` times from ``state`` and take
     the training rows of the wet columns every ``every`` steps; keep at most
-    ``max_rows`` of them (seeded subsample).  Returns (X, T, M, final state)."""
+    ``max_rows`` of them, spread evenly over the snapshots (seeded
+    subsample).  Returns (X, T, M, final state)."""
     import torch
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    per_snapshot = -(-max_rows // max(1, nsteps // every))
     parts = []
     for n in range(nsteps):
         state = step(state)
         if (n + 1) % every == 0:
             X, T, M = step.closure_features(state)
-            keep = M.sum(1) > 0
+            keep = torch.nonzero(M.sum(1) > 0).squeeze(1)
+            if keep.numel() > per_snapshot:
+                keep = keep[torch.randperm(keep.numel(), generator=g)[:per_snapshot].to(keep.device)]
             parts.append((X[keep], T[keep], M[keep]))
     X = torch.cat([p[0] for p in parts])
     T = torch.cat([p[1] for p in parts])
     M = torch.cat([p[2] for p in parts])
     if X.shape[0] > max_rows:
-        g = torch.Generator(device="cpu").manual_seed(seed)
         idx = torch.randperm(X.shape[0], generator=g)[:max_rows].to(X.device)
         X, T, M = X[idx], T[idx], M[idx]
     return X, T, M, state
