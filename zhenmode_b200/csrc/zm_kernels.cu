@@ -417,81 +417,72 @@ __device__ __forceinline__ void vcoef(const Dev& d, int k, int kb, float s, floa
   if (k < kb) c = -s * d.vc.d2_hi[k]; else b -= s * d.vc.d2_hi[k];
 }
 
-__device__ void thomas(const Dev& d, int n, int kb, float s, const float* rhs, float* x, float* cp) {
-  float a, b, c;
-  vcoef(d, 0, kb, s, a, b, c);
-  float inv = 1.f / b;
-  cp[0] = c * inv;
-  x[0] = rhs[0] * inv;
+// Backward-Euler vertical diffusion of two fields of one column that share
+// the tridiagonal matrix over the wet levels 0..kbot (lower lo, diagonal dg,
+// upper up): one FP32 factorization, then per field a Thomas solve and one
+// step of iterative refinement with the residual against the original
+// right-hand side.
+__device__ void implicit_pair(const Dev& d, float* __restrict__ fa, float* __restrict__ fb, long long base, int n,
+                              const float* lo, const float* dg, const float* up) {
+  // the two fields' recurrences run interleaved: two independent chains
+  float cp[ZM_MAXZ], inv[ZM_MAXZ], ra[ZM_MAXZ], rb[ZM_MAXZ], xa[ZM_MAXZ], xb[ZM_MAXZ];
+  inv[0] = 1.f / dg[0];
+  cp[0] = up[0] * inv[0];
+  ra[0] = fa[base];
+  rb[0] = fb[base];
+  xa[0] = ra[0] * inv[0];
+  xb[0] = rb[0] * inv[0];
+#pragma unroll 4
   for (int k = 1; k < n; ++k) {
-    vcoef(d, k, kb, s, a, b, c);
-    inv = 1.f / (b - a * cp[k - 1]);
-    cp[k] = c * inv;
-    x[k] = (rhs[k] - a * x[k - 1]) * inv;
+    const long long id = base + (long long)k * d.plane;
+    ra[k] = fa[id];
+    rb[k] = fb[id];
+    inv[k] = 1.f / (dg[k] - lo[k] * cp[k - 1]);
+    cp[k] = up[k] * inv[k];
+    xa[k] = (ra[k] - lo[k] * xa[k - 1]) * inv[k];
+    xb[k] = (rb[k] - lo[k] * xb[k - 1]) * inv[k];
   }
-  for (int k = n - 2; k >= 0; --k) x[k] -= cp[k] * x[k + 1];
-}
-
-__device__ void implicit_column(const Dev& d, float* __restrict__ f, long long base, uint64_t bits, float s) {
-  const int kb = kbot_of(bits);
-  if (kb == 0) return;  // a single wet node: the zero-flux operator vanishes
-  const int n = kb + 1;
-  float rhs[ZM_MAXZ], x[ZM_MAXZ], e[ZM_MAXZ], cp[ZM_MAXZ];
-  for (int k = 0; k < n; ++k) rhs[k] = f[base + (long long)k * d.plane];
-  thomas(d, n, kb, s, rhs, x, cp);
-  for (int k = 0; k < n; ++k) {  // residual of the FP32 solution
-    float a, b, c;
-    vcoef(d, k, kb, s, a, b, c);
-    float ax = b * x[k];
-    if (k > 0) ax += a * x[k - 1];
-    if (k + 1 < n) ax += c * x[k + 1];
-    e[k] = rhs[k] - ax;
+#pragma unroll 4
+  for (int k = n - 2; k >= 0; --k) {
+    xa[k] -= cp[k] * xa[k + 1];
+    xb[k] -= cp[k] * xb[k + 1];
   }
-  thomas(d, n, kb, s, e, rhs, cp);
-  for (int k = 0; k < n; ++k) f[base + (long long)k * d.plane] = x[k] + rhs[k];
-}
-
-// Backward-Euler interface-flux diffusion of one tracer column with a
-// diffusivity per interface, kap[m] between wet levels m and m+1:
-// tend_k = (F_{k-1/2} - F_{k+1/2}) / dz_node_k, F_{m+1/2} = -kap_m (c_{m+1} - c_m) / dz_iface_m,
-// zero flux at the surface and the deepest wet level.  FP32 Thomas plus one
-// refinement step, as implicit_column.
-__device__ void implicit_column_iface(const Dev& d, float* __restrict__ f, long long base, uint64_t bits,
-                                      const float* __restrict__ kap3, float dt) {
-  const int kb = kbot_of(bits);
-  if (kb == 0 || !wetb(bits, 0)) return;
-  const int n = kb + 1;
-  float lo[ZM_MAXZ], up[ZM_MAXZ], rhs[ZM_MAXZ], x[ZM_MAXZ], e[ZM_MAXZ], cp[ZM_MAXZ];
+  // residual of the FP32 solution, solved again with the same factorization
+  float ea = 0.f, eb = 0.f;
+#pragma unroll 4
   for (int k = 0; k < n; ++k) {
-    rhs[k] = f[base + (long long)k * d.plane];
-    lo[k] = k > 0 ? -dt * __ldg(kap3 + base + (long long)(k - 1) * d.plane) * d.vc.inv_dz_iface[k - 1] *
-                        d.vc.inv_dz_node[k]
-                  : 0.f;
-    up[k] = k + 1 < n ? -dt * __ldg(kap3 + base + (long long)k * d.plane) * d.vc.inv_dz_iface[k] * d.vc.inv_dz_node[k]
-                      : 0.f;
-  }
-  auto solve = [&](const float* r, float* y) {
-    float inv = 1.f / (1.f - lo[0] - up[0]);
-    cp[0] = up[0] * inv;
-    y[0] = r[0] * inv;
-    for (int k = 1; k < n; ++k) {
-      inv = 1.f / ((1.f - lo[k] - up[k]) - lo[k] * cp[k - 1]);
-      cp[k] = up[k] * inv;
-      y[k] = (r[k] - lo[k] * y[k - 1]) * inv;
+    float aa = dg[k] * xa[k], ab = dg[k] * xb[k];
+    if (k > 0) {
+      aa += lo[k] * xa[k - 1];
+      ab += lo[k] * xb[k - 1];
     }
-    for (int k = n - 2; k >= 0; --k) y[k] -= cp[k] * y[k + 1];
-  };
-  solve(rhs, x);
-  for (int k = 0; k < n; ++k) {
-    float ax = (1.f - lo[k] - up[k]) * x[k];
-    if (k > 0) ax += lo[k] * x[k - 1];
-    if (k + 1 < n) ax += up[k] * x[k + 1];
-    e[k] = rhs[k] - ax;
+    if (k + 1 < n) {
+      aa += up[k] * xa[k + 1];
+      ab += up[k] * xb[k + 1];
+    }
+    ea = ((ra[k] - aa) - lo[k] * ea) * inv[k];
+    eb = ((rb[k] - ab) - lo[k] * eb) * inv[k];
+    ra[k] = ea;
+    rb[k] = eb;
   }
-  solve(e, rhs);
-  for (int k = 0; k < n; ++k) f[base + (long long)k * d.plane] = x[k] + rhs[k];
+#pragma unroll 4
+  for (int k = n - 2; k >= 0; --k) {
+    ra[k] -= cp[k] * ra[k + 1];
+    rb[k] -= cp[k] * rb[k + 1];
+  }
+#pragma unroll 4
+  for (int k = 0; k < n; ++k) {
+    const long long id = base + (long long)k * d.plane;
+    fa[id] = xa[k] + ra[k];
+    fb[id] = xb[k] + rb[k];
+  }
 }
 
+// One thread per (column, pair): blockIdx.z = 0 solves u and v (nu_v, node
+// form of d2z with the ghost fill) and applies the land hold and the exact
+// Coriolis rotation; blockIdx.z = 1 solves T and S (kappa_v + coastal in the
+// node form, or the learned closure's diffusivity per interface kap3 in the
+// interface-flux form) and applies the land hold.
 __global__ void __launch_bounds__(128) k_implicit_vdiff(Dev d, float* __restrict__ u, float* __restrict__ v,
                                                         float* __restrict__ T, float* __restrict__ S,
                                                         const float* __restrict__ u0, const float* __restrict__ v0,
@@ -502,15 +493,36 @@ __global__ void __launch_bounds__(128) k_implicit_vdiff(Dev d, float* __restrict
   if (i >= d.nx || j >= d.ny) return;
   const long long base = idx2(d, j, i);
   const uint64_t bits = wb(d, j, i);
-  implicit_column(d, u, base, bits, d.nu_v * dth);
-  implicit_column(d, v, base, bits, d.nu_v * dth);
-  if (kap3) {  // the learned closure's diffusivity per interface
-    implicit_column_iface(d, T, base, bits, kap3, dth);
-    implicit_column_iface(d, S, base, bits, kap3, dth);
-  } else {
-    const float kv = __ldg(d.kv2 + base);
-    implicit_column(d, T, base, bits, kv * dth);
-    implicit_column(d, S, base, bits, kv * dth);
+  const bool tracers = blockIdx.z == 1;
+  const int kb = kbot_of(bits);
+  if (kb > 0 && wetb(bits, 0)) {
+    const int n = kb + 1;
+    float lo[ZM_MAXZ], dg[ZM_MAXZ], up[ZM_MAXZ];
+    if (tracers && kap3) {
+      for (int k = 0; k < n; ++k) {
+        lo[k] = k > 0 ? -dth * __ldg(kap3 + base + (long long)(k - 1) * d.plane) * d.vc.inv_dz_iface[k - 1] *
+                            d.vc.inv_dz_node[k]
+                      : 0.f;
+        up[k] = k + 1 < n
+                    ? -dth * __ldg(kap3 + base + (long long)k * d.plane) * d.vc.inv_dz_iface[k] * d.vc.inv_dz_node[k]
+                    : 0.f;
+        dg[k] = 1.f - lo[k] - up[k];
+      }
+    } else {
+      const float sc = tracers ? __ldg(d.kv2 + base) * dth : d.nu_v * dth;
+      for (int k = 0; k < n; ++k) vcoef(d, k, kb, sc, lo[k], dg[k], up[k]);
+    }
+    if (tracers) implicit_pair(d, T, S, base, n, lo, dg, up);
+    else implicit_pair(d, u, v, base, n, lo, dg, up);
+  }
+  if (tracers) {
+    for (int k = 0; k < d.nz; ++k)
+      if (!wetb(bits, k)) {
+        const long long id = base + (long long)k * d.plane;
+        T[id] = ld(T0, id);
+        S[id] = ld(S0, id);
+      }
+    return;
   }
   // land/ghost hold, then the exact Coriolis rotation
   const float c = __ldg(d.rot_c + base), s = __ldg(d.rot_s + base);
@@ -518,8 +530,8 @@ __global__ void __launch_bounds__(128) k_implicit_vdiff(Dev d, float* __restrict
     const long long id = base + (long long)k * d.plane;
     float uu = u[id], vv = v[id];
     if (!wetb(bits, k)) {
-      uu = ld(u0, id); vv = ld(v0, id);
-      T[id] = ld(T0, id); S[id] = ld(S0, id);
+      uu = ld(u0, id);
+      vv = ld(v0, id);
     }
     u[id] = c * uu + s * vv;
     v[id] = -s * uu + c * vv;

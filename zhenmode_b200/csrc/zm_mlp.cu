@@ -115,9 +115,9 @@ __device__ __forceinline__ float gelu_grad(float x) {
 
 size_t mlp_tc_smem() { return TC_SMEM; }
 
-// One MLP pass over BF16 rows staged by `stage` (row r of the CTA's tile,
-// returning 16-byte pieces of the 256 inputs), writing the 64 raw outputs of
-// each row through `emit`.  Shared by the standalone and the fused kernels.
+// One MLP pass over BF16 rows that `stage(t, act)` writes as row t of the
+// activation tile (core_off layout), writing the 64 raw outputs of each row
+// through `emit`.  Shared by the standalone and the fused kernels.
 template <class Stage, class Emit>
 __device__ __forceinline__ void mlp_tc_body(const MlpBf16& w, uint8_t* msm, unsigned* err, Stage stage, Emit emit) {
   uint8_t* act = msm;
@@ -136,7 +136,7 @@ __device__ __forceinline__ void mlp_tc_body(const MlpBf16& w, uint8_t* msm, unsi
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   // the inputs of this thread's column as row t of the A tile
-  stage(t, [&](int kp, uint4 v) { *reinterpret_cast<uint4*>(act + core_off(t, kp * 8, MK)) = v; });
+  stage(t, act);
   fence_async_smem();
   fence_before();
   __syncthreads();
@@ -218,11 +218,11 @@ __global__ void __launch_bounds__(MT, 1) k_mlp_tc(MlpBf16 w, const __nv_bfloat16
   const long long col = (long long)blockIdx.x * MT + threadIdx.x;
   mlp_tc_body(
       w, msm, err,
-      [&](int, auto put) {
+      [&](int t, uint8_t* act) {
         for (int kp = 0; kp < MK / 8; ++kp) {
           uint4 v = make_uint4(0u, 0u, 0u, 0u);
           if (col < ncol) v = *reinterpret_cast<const uint4*>(X + col * MK + kp * 8);
-          put(kp, v);
+          *reinterpret_cast<uint4*>(act + core_off(t, kp * 8, MK)) = v;
         }
       },
       [&](int, int c0, const float* v) {
@@ -325,17 +325,44 @@ __global__ void __launch_bounds__(MT, 1) k_mlp_closure(MlpBf16 w, Dev d, Closure
   int unstable = -1;  // column gate of the plain closure, formed on first use
   mlp_tc_body(
       w, msm, err,
-      [&](int, auto put) {
-        for (int kp = 0; kp < MK / 8; ++kp) {
-          __align__(16) __nv_bfloat16 h[8];
-#pragma unroll
-          for (int e = 0; e < 8; ++e) {
-            const float f = act ? closure_feature(d, a, base, bits, kp * 8 + e) : 0.f;
-            if (!(fabsf(f) <= a.bound)) trusted = false;
-            h[e] = __float2bfloat16(f);
+      [&](int t, uint8_t* tile) {
+        // the row is zero, then the features level by level: four loads per
+        // level, coalesced over the CTA's consecutive columns; N^2 from the
+        // level above kept in registers
+        for (int kp = 0; kp < MK / 8; ++kp)
+          *reinterpret_cast<uint4*>(tile + core_off(t, kp * 8, MK)) = make_uint4(0u, 0u, 0u, 0u);
+        float amax = 0.f;
+        auto put = [&](int q, float f) {
+          amax = fmaxf(amax, fabsf(f));
+          if (!(f == f) || isinf(f)) amax = INFINITY;
+          *reinterpret_cast<__nv_bfloat16*>(tile + core_off(t, q, MK)) = __float2bfloat16(f);
+        };
+        if (act) {
+          float Tu = 0.f, Su = 0.f;
+          bool wu = false;
+#pragma unroll 4
+          for (int k = 0; k < d.nz; ++k) {
+            const long long id = base + (long long)k * d.plane;
+            const float Tk = ld(a.T, id), Sk = ld(a.S, id), uk = ld(a.u, id), vk = ld(a.v, id);
+            const bool wk = wetb(bits, k);
+            if (wk) {
+              put(k, Tk * 0.1f);
+              put(50 + k, Sk);
+              put(100 + k, uk * 2.f);
+              put(150 + k, vk * 2.f);
+              if (k > 0 && wu)
+                put(199 + k, asinhf(kG * (-kAlpha * (Tk - Tu) + kBeta * (Sk - Su)) * d.vc.inv_dz_iface[k - 1] * 1e8f) *
+                                 0.25f);
+            }
+            Tu = Tk;
+            Su = Sk;
+            wu = wk;
           }
-          put(kp, *reinterpret_cast<const uint4*>(h));
+          const float tx = __ldg(d.tau_x + base), ty = __ldg(d.tau_y + base);
+          put(250, sqrtf(tx * tx + ty * ty) * 10.f);
+          put(251, __ldg(d.qheat + base) * 0.01f);
         }
+        trusted = amax <= a.bound;
       },
       [&](int, int c0, const float* y) {
         if (!act) return;

@@ -180,8 +180,10 @@ struct zm_solver {
     if (vdiff || closure_on) {
       const dim3 c(32, 4);
       pb(ZM_K_IMPLICIT, s);
-      k_implicit_vdiff<<<grid2(c), c, 0, s>>>(d, dst.u, dst.v, dst.T, dst.S, src.u, src.v, src.T, src.S, dth,
-                                              closure_on ? kappa3 : nullptr);
+      dim3 g = grid2(c);
+      g.z = 2;
+      k_implicit_vdiff<<<g, c, 0, s>>>(d, dst.u, dst.v, dst.T, dst.S, src.u, src.v, src.T, src.S, dth,
+                                       closure_on ? kappa3 : nullptr);
       pe(s);
     }
     check_launch();
