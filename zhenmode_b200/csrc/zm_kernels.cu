@@ -129,7 +129,9 @@ __device__ __forceinline__ float vdiff_tracer(const Dev& d, const float* __restr
 // metric term -(tan(lat)/R) du/dy), and the mirror ghost of the closed
 // walls folded in: at j = ny-1 the north neighbour equals u0, so aN = 0; at
 // j = 0, aS = 0.  The coefficients, scaled by nu_h dt_sub, are formed once
-// per pass.  Longitude wraps.
+// per pass.  Longitude wraps.  The lane's two columns are held as packed
+// pairs, so the update runs on the paired FP32 instructions (__ffma2_rn,
+// __fadd2_rn; the same roundings as the scalar form).
 __global__ void __launch_bounds__(32 * (NB_W / NB_R), 2)
 k_nu_tb(Dev d, const float* __restrict__ u, const float* __restrict__ v, float* __restrict__ uo,
         float* __restrict__ vo, float c, int nsub) {
@@ -148,21 +150,22 @@ k_nu_tb(Dev d, const float* __restrict__ u, const float* __restrict__ v, float* 
     gi[h] = g < 0 ? g + d.nx : g;
   }
   const long long kb = (long long)k * d.plane;
-  float2 a[NB_R][2];
+  // the lane's two columns as pairs: au[q] = (u[2l], u[2l+1]) of row q, av likewise
+  float2 au[NB_R], av[NB_R];
 #pragma unroll
   for (int q = 0; q < NB_R; ++q) {
     int gj = gy0 + r0 + q;
     gj = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
+    const long long id0 = kb + (long long)gj * d.P + gi[0], id1 = kb + (long long)gj * d.P + gi[1];
+    au[q] = make_float2(ld(u, id0), ld(u, id1));
+    av[q] = make_float2(ld(v, id0), ld(v, id1));
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const long long id = kb + (long long)gj * d.P + gi[h];
-      a[q][h] = make_float2(ld(u, id), ld(v, id));
-      sw[r0 + q][c0 + h] = (unsigned char)wetb(wb(d, gj, gi[h]), k);
-    }
+    for (int h = 0; h < 2; ++h) sw[r0 + q][c0 + h] = (unsigned char)wetb(wb(d, gj, gi[h]), k);
   }
   __syncthreads();
   const float cn = d.nu_h * c;
-  float4 cf[NB_R][2];
+  // face coefficients, paired like the state: (column 2l, column 2l+1)
+  float2 kE[NB_R], kW[NB_R], kN[NB_R], kS[NB_R];
 #pragma unroll
   for (int q = 0; q < NB_R; ++q) {
     const int r = r0 + q;
@@ -171,6 +174,7 @@ k_nu_tb(Dev d, const float* __restrict__ u, const float* __restrict__ v, float* 
     const bool n_in = gj < d.ny - 1;  // north neighbour inside the domain
     const bool s_in = gj > 0;
     const float t = 0.5f * d.inv_dy * __ldg(d.tanR + gjc);
+    float ce[2], cw[2], cnn[2], cs[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int col = c0 + h;
@@ -181,47 +185,52 @@ k_nu_tb(Dev d, const float* __restrict__ u, const float* __restrict__ v, float* 
       const bool ws = s_in && r > 0 && sw[r - 1][col];
       const float ix2 = __ldg(d.inv_dx2 + idx2(d, gjc, gi[h]));
       const float cN = (w0 && wn) ? d.inv_dy2 : 0.f, cS = (w0 && ws) ? d.inv_dy2 : 0.f;
-      cf[q][h].x = (w0 && we) ? ix2 * cn : 0.f;
-      cf[q][h].y = (w0 && ww) ? ix2 * cn : 0.f;
-      cf[q][h].z = n_in ? (cN - t) * cn : 0.f;
-      cf[q][h].w = s_in ? (cS + t) * cn : 0.f;
+      ce[h] = (w0 && we) ? ix2 * cn : 0.f;
+      cw[h] = (w0 && ww) ? ix2 * cn : 0.f;
+      cnn[h] = n_in ? (cN - t) * cn : 0.f;
+      cs[h] = s_in ? (cS + t) * cn : 0.f;
     }
+    kE[q] = make_float2(ce[0], ce[1]);
+    kW[q] = make_float2(cw[0], cw[1]);
+    kN[q] = make_float2(cnn[0], cnn[1]);
+    kS[q] = make_float2(cs[0], cs[1]);
   }
   const unsigned full = 0xffffffffu;
+  const float2 m1 = make_float2(-1.f, -1.f);
   for (int s = 0; s < nsub; ++s) {
     const int p = s & 1;
-    edge[p][wp][0][lane] = make_float4(a[0][0].x, a[0][0].y, a[0][1].x, a[0][1].y);
-    edge[p][wp][1][lane] = make_float4(a[NB_R - 1][0].x, a[NB_R - 1][0].y, a[NB_R - 1][1].x, a[NB_R - 1][1].y);
+    edge[p][wp][0][lane] = make_float4(au[0].x, au[0].y, av[0].x, av[0].y);
+    edge[p][wp][1][lane] = make_float4(au[NB_R - 1].x, au[NB_R - 1].y, av[NB_R - 1].x, av[NB_R - 1].y);
     __syncthreads();
     // rows just outside the strip (the tile edge reuses the strip's own row)
     const float4 nt = edge[p][wp + 1 < NW ? wp + 1 : wp][wp + 1 < NW ? 0 : 1][lane];
     const float4 sb = edge[p][wp > 0 ? wp - 1 : wp][wp > 0 ? 1 : 0][lane];
-    float2 south[2] = {make_float2(sb.x, sb.y), make_float2(sb.z, sb.w)};
+    float2 su = make_float2(sb.x, sb.y), sv = make_float2(sb.z, sb.w);
 #pragma unroll
     for (int q = 0; q < NB_R; ++q) {
-      float2 north[2];
-      if (q + 1 < NB_R) {
-        north[0] = a[q + 1][0];
-        north[1] = a[q + 1][1];
-      } else {
-        north[0] = make_float2(nt.x, nt.y);
-        north[1] = make_float2(nt.z, nt.w);
-      }
-      // west of column 2l is column 2l+1 of lane l-1; east of 2l+1 is 2l of lane l+1
-      // (lanes 0 and 31 get their own values: tile-edge error)
-      const float2 west0 = make_float2(__shfl_up_sync(full, a[q][1].x, 1), __shfl_up_sync(full, a[q][1].y, 1));
-      const float2 east1 = make_float2(__shfl_down_sync(full, a[q][0].x, 1), __shfl_down_sync(full, a[q][0].y, 1));
-      const float2 ew[2][2] = {{a[q][1], west0}, {east1, a[q][0]}};
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const float4 k4 = cf[q][h];
-        const float2 c0v = a[q][h], e = ew[h][0], w = ew[h][1], nn = north[h], ss = south[h];
-        float2 o;
-        o.x = c0v.x + k4.x * (e.x - c0v.x) + k4.y * (w.x - c0v.x) + k4.z * (nn.x - c0v.x) + k4.w * (ss.x - c0v.x);
-        o.y = c0v.y + k4.x * (e.y - c0v.y) + k4.y * (w.y - c0v.y) + k4.z * (nn.y - c0v.y) + k4.w * (ss.y - c0v.y);
-        south[h] = c0v;
-        a[q][h] = o;
-      }
+      const float2 nu = q + 1 < NB_R ? au[q + 1] : make_float2(nt.x, nt.y);
+      const float2 nv = q + 1 < NB_R ? av[q + 1] : make_float2(nt.z, nt.w);
+      // east of (2l, 2l+1) is (2l+1, 2l+2), west is (2l-1, 2l); the outside
+      // columns come from the neighbouring lanes (lanes 0 and 31 get their
+      // own values: tile-edge error)
+      const float2 eu = make_float2(au[q].y, __shfl_down_sync(full, au[q].x, 1));
+      const float2 wu = make_float2(__shfl_up_sync(full, au[q].y, 1), au[q].x);
+      const float2 ev = make_float2(av[q].y, __shfl_down_sync(full, av[q].x, 1));
+      const float2 wv = make_float2(__shfl_up_sync(full, av[q].y, 1), av[q].x);
+      // u0 + aE (uE - u0) + aW (uW - u0) + aN (uN - u0) + aS (uS - u0) on packed pairs
+      const float2 ncu = __fmul2_rn(au[q], m1), ncv = __fmul2_rn(av[q], m1);
+      float2 ou = __ffma2_rn(kE[q], __fadd2_rn(eu, ncu), au[q]);
+      float2 ov = __ffma2_rn(kE[q], __fadd2_rn(ev, ncv), av[q]);
+      ou = __ffma2_rn(kW[q], __fadd2_rn(wu, ncu), ou);
+      ov = __ffma2_rn(kW[q], __fadd2_rn(wv, ncv), ov);
+      ou = __ffma2_rn(kN[q], __fadd2_rn(nu, ncu), ou);
+      ov = __ffma2_rn(kN[q], __fadd2_rn(nv, ncv), ov);
+      ou = __ffma2_rn(kS[q], __fadd2_rn(su, ncu), ou);
+      ov = __ffma2_rn(kS[q], __fadd2_rn(sv, ncv), ov);
+      su = au[q];
+      sv = av[q];
+      au[q] = ou;
+      av[q] = ov;
     }
   }
   // write the exact interior
@@ -236,8 +245,8 @@ k_nu_tb(Dev d, const float* __restrict__ u, const float* __restrict__ v, float* 
       const int ix = gx0 + col;
       if (col < NB_T || col >= NB_W - NB_T || ix >= d.nx) continue;
       const long long id = kb + (long long)gj * d.P + ix;
-      uo[id] = a[q][h].x;
-      vo[id] = a[q][h].y;
+      uo[id] = h == 0 ? au[q].x : au[q].y;
+      vo[id] = h == 0 ? av[q].x : av[q].y;
     }
   }
 }
