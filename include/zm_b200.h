@@ -258,6 +258,21 @@ int zm_closure_kappa(zm_solver* s, void* stream, const zm_state* in, float* kapp
  * interface mask M [.][64].  Stream ordered; uses the handle's work buffers. */
 int zm_closure_features(zm_solver* s, void* stream, const zm_state* in, float* X, float* T, float* M);
 
+/* ---- ensembles -----------------------------------------------------------
+ * Advance several handles (perturbed members, grids of any sizes) together:
+ * each zm_ensemble_advance step is one launch of one CUDA graph holding one
+ * step of every member, the members on parallel branches so that small grids
+ * share the GPU.  The members' cooperative barotropic kernels are chained in
+ * member order inside the graph (they never run at the same time).  States
+ * are loaded and read per member (zm_load_state / zm_store_state); the
+ * ensemble recaptures itself if a member stepped on its own or changed its
+ * closure.  *kernels_per_step (optional) receives the graph's launch count.
+ * New in this library (the reference runs ensemble members one by one). */
+typedef struct zm_ensemble zm_ensemble;
+int zm_ensemble_create(zm_solver* const* members, int32_t n, zm_ensemble** out);
+int zm_ensemble_advance(zm_ensemble* e, void* stream, int32_t nsteps, int32_t* kernels_per_step);
+void zm_ensemble_destroy(zm_ensemble* e);
+
 /* Global heat/salt/volume snapshot of a state (compute_budget_diagnostics,
  * diagnostics/snapshot.py:67-128, legacy node thickness, linear
  * thermodynamics): T and S are (nx, ny, nz) float32 device arrays.  Writes

@@ -89,6 +89,10 @@ struct zm_solver {
   cudaStream_t cap_stream = nullptr;  // graphs are captured here, launched on the caller's stream
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   bool graphs_ready = false;
+  // set while an ensemble captures this member: the cooperative barotropic
+  // kernel waits for bt_wait and records bt_done, so that the members'
+  // grid-barrier kernels never run at the same time
+  cudaEvent_t bt_wait = nullptr, bt_done = nullptr;
   int kernels_per_step = 0;
   std::string last_error;
   // launch accounting: every kernel launch of the step is bracketed by
@@ -312,9 +316,11 @@ struct zm_solver {
       attr[0].val.cooperative = 1;
       cfg.attrs = attr;
       cfg.numAttrs = 1;
+      if (bt_wait) ZM_CUDA(cudaStreamWaitEvent(s, bt_wait, 0));
       pb(ZM_K_BAROTROPIC, s);
       ZM_CUDA(cudaLaunchKernelEx(&cfg, k_bt_loop, d, a2));
       pe(s);
+      if (bt_done) ZM_CUDA(cudaEventRecord(bt_done, s));
       ubt_fin = bt.ubt_out;
       vbt_fin = bt.vbt_out;
     } else {
@@ -856,6 +862,138 @@ int zm_advance(zm_solver* s, void* stream, int32_t nsteps) {
   }
   return ZM_OK;
 }
+
+// ---------------------------------------------------------------- ensembles
+
+struct zm_ensemble {
+  std::vector<zm_solver*> m;
+  std::vector<int> parity;  // members' state index when graph[0] was captured
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  bool ready = false;
+  cudaStream_t cap = nullptr;
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> fork, join, bt;
+  int launches = 0;
+  ~zm_ensemble() {
+    for (int g = 0; g < 2; ++g)
+      if (graph[g]) cudaGraphExecDestroy(graph[g]);
+    for (auto e : fork) cudaEventDestroy(e);
+    for (auto e : join) cudaEventDestroy(e);
+    for (auto e : bt) cudaEventDestroy(e);
+    for (auto st : side) cudaStreamDestroy(st);
+    if (cap) cudaStreamDestroy(cap);
+  }
+  // one graph stepping every member once, members on forked streams
+  void capture() {
+    for (int g = 0; g < 2; ++g) {
+      if (graph[g]) {
+        cudaGraphExecDestroy(graph[g]);
+        graph[g] = nullptr;
+      }
+    }
+    parity.resize(m.size());
+    for (size_t q = 0; q < m.size(); ++q) parity[q] = m[q]->cur;
+    for (int g = 0; g < 2; ++g) {
+      cudaGraph_t def = nullptr;
+      ZM_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+      int count = 0;
+      try {
+        ZM_CUDA(cudaEventRecord(fork[0], cap));
+        for (size_t q = 0; q < m.size(); ++q) {
+          zm_solver* s = m[q];
+          ZM_CUDA(cudaStreamWaitEvent(side[q], fork[0], 0));
+          s->bt_wait = q > 0 ? bt[q - 1] : nullptr;
+          s->bt_done = bt[q];
+          const int from = g == 0 ? parity[q] : 1 - parity[q];
+          const int before = s->launch_count;
+          s->full_step(side[q], from, 1 - from);
+          count += s->launch_count - before;
+          s->bt_wait = s->bt_done = nullptr;
+          ZM_CUDA(cudaEventRecord(join[q], side[q]));
+          ZM_CUDA(cudaStreamWaitEvent(cap, join[q], 0));
+        }
+      } catch (...) {
+        for (auto* s : m) s->bt_wait = s->bt_done = nullptr;
+        cudaStreamEndCapture(cap, &def);
+        if (def) cudaGraphDestroy(def);
+        throw;
+      }
+      ZM_CUDA(cudaStreamEndCapture(cap, &def));
+      ZM_CUDA(cudaGraphInstantiate(&graph[g], def, 0));
+      cudaGraphDestroy(def);
+      launches = count;
+    }
+    ready = true;
+  }
+};
+
+int zm_ensemble_create(zm_solver* const* members, int32_t n, zm_ensemble** out) {
+  if (!members || n < 1 || !out) return ZM_ERR_INVALID;
+  for (int q = 0; q < n; ++q)
+    if (!members[q]) return ZM_ERR_INVALID;
+  for (int q = 0; q < n; ++q)
+    for (int r = q + 1; r < n; ++r)
+      if (members[q] == members[r]) return ZM_ERR_INVALID;
+  auto* e = new zm_ensemble();
+  e->m.assign(members, members + n);
+  bool ok = cudaStreamCreateWithFlags(&e->cap, cudaStreamNonBlocking) == cudaSuccess;
+  e->side.resize(n, nullptr);
+  e->fork.resize(1, nullptr);
+  e->join.resize(n, nullptr);
+  e->bt.resize(n, nullptr);
+  ok = ok && cudaEventCreateWithFlags(&e->fork[0], cudaEventDisableTiming) == cudaSuccess;
+  for (int q = 0; q < n && ok; ++q) {
+    ok = cudaStreamCreateWithFlags(&e->side[q], cudaStreamNonBlocking) == cudaSuccess &&
+         cudaEventCreateWithFlags(&e->join[q], cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&e->bt[q], cudaEventDisableTiming) == cudaSuccess;
+  }
+  if (!ok) {
+    delete e;
+    return ZM_ERR_CUDA;
+  }
+  *out = e;
+  return ZM_OK;
+}
+
+int zm_ensemble_advance(zm_ensemble* e, void* stream, int32_t nsteps, int32_t* kernels_per_step) {
+  if (!e || nsteps < 0) return ZM_ERR_INVALID;
+  cudaStream_t st = (cudaStream_t)stream;
+  try {
+    // a capture exists, every member still has its own graphs (no closure
+    // change), and all members stepped alike since the capture
+    bool stale = !e->ready || e->parity.size() != e->m.size();
+    int rel = 0;
+    if (!stale) {
+      rel = -1;
+      for (size_t q = 0; q < e->m.size(); ++q) {
+        if (!e->m[q]->graphs_ready) stale = true;
+        const int r = e->m[q]->cur == e->parity[q] ? 0 : 1;
+        if (rel < 0) rel = r;
+        else if (r != rel) stale = true;
+      }
+    }
+    if (stale) {
+      for (auto* s : e->m)
+        if (!s->graphs_ready) s->build_graphs();
+      ZM_CUDA(cudaDeviceSynchronize());
+      e->capture();
+      rel = 0;
+    }
+    for (int n = 0; n < nsteps; ++n) {
+      ZM_CUDA(cudaGraphLaunch(e->graph[rel], st));
+      for (auto* s : e->m) s->cur = 1 - s->cur;
+      rel = 1 - rel;
+    }
+    for (auto* s : e->m) s->monitor(st, s->cur);
+    if (kernels_per_step) *kernels_per_step = e->launches;
+  } catch (const Err& err) {
+    std::fprintf(stderr, "zm_ensemble_advance: %s\n", err.msg.c_str());
+    return err.code;
+  }
+  return ZM_OK;
+}
+
+void zm_ensemble_destroy(zm_ensemble* e) { delete e; }
 
 int zm_step(zm_solver* s, void* stream, const zm_state* in, zm_state* out, int32_t nsteps) {
   int rc = zm_load_state(s, stream, in);
