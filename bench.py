@@ -187,6 +187,83 @@ def run_reference(args):
     return 0
 
 
+# the batched ensemble form: (members, nx, ny, nz) groups advanced together
+ENSEMBLE_GROUPS = ((32, 360, 180, 30), (8, 720, 360, 50), (16, 180, 90, 20))
+
+
+def run_ensemble(args):
+    """All members of ENSEMBLE_GROUPS (each T perturbed by its own seed,
+    sigma 0.05 K) advance one simulated day in one CUDA-graph launch per step;
+    the same members advanced one after another (each its own graphs) give the
+    sequential reference.  Value = aggregate simulated years per day."""
+    import numpy as np
+    import torch
+
+    from zhenmode_b200 import make_solver_global, workloads
+    from zhenmode_b200.ensemble import Ensemble
+
+    wl = workloads.WORKLOADS[WORKLOAD]
+    steps, states, sizes = [], [], []
+    seed = 100
+    for count, nx, ny, nz in ENSEMBLE_GROUPS:
+        grid, physics, dt, kw, T, S = workloads.make_case(WORKLOAD, nx, ny, nz, dtype="float32")
+        wet = np.asarray(grid.wet_mask_3d)
+        for _ in range(count):
+            step, init, _ = make_solver_global(grid, physics, dt, **kw)
+            rng = np.random.default_rng(seed)
+            seed += 1
+            steps.append(step)
+            states.append(init(T + 0.05 * rng.standard_normal(T.shape) * wet, S))
+            sizes.append(nx * ny * nz)
+    nday = int(round(86400.0 / wl.dt))
+    ens = Ensemble(steps)
+    ens.load(states)
+    ens.advance(max(args.warmup, 3))
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ens.advance(nday)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms_ens = e0.elapsed_time(e1)
+    codes = ens.monitor_codes()
+    # sequential: each member alone through its own graphs
+    import ctypes
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    for st in steps:
+        st.solver.check(st.solver.lib.zm_advance(st.solver.handle, sp, 3), "zm_advance")
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for st in steps:
+        st.solver.check(st.solver.lib.zm_advance(st.solver.handle, sp, nday), "zm_advance")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_seq = e0.elapsed_time(e1)
+    n = len(steps)
+    years = n * nday * wl.dt / SECONDS_PER_YEAR
+    value = years / (ms_ens * 1e-3) * 86400.0
+    seq_value = years / (ms_seq * 1e-3) * 86400.0
+    line = {"metric": METRIC, "value": value, "unit": "sim-years/day", "n_gpus": 1, "steps": nday,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms_ens / nday, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded bathymetry, "
+            "thermocline, wind stress; per-member seeded T perturbation sigma 0.05 K)",
+            "config": {"workload": "batched ensemble: " + ", ".join(f"{c} x {x}x{y}x{z}" for c, x, y, z in
+                                                                   ENSEMBLE_GROUPS) + ", 1 simulated day each",
+                       "form": "ensemble", "members": n, "points": int(sum(sizes)),
+                       "graph_kernels_per_step": ens.kernels_per_step, "monitor_codes_nonzero": sum(c != 0 for c in codes)},
+            "sequential": {"value": seq_value, "ms_per_step": ms_seq / nday},
+            "ensemble_speedup_vs_sequential": ms_seq / ms_ens,
+            "roofline": None, "gpu_launches": nday * ens.kernels_per_step, "clocks": clk, "e2e": None,
+            "cpu_baseline": None}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -196,7 +273,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", default=None, help="NXxNYxNZ: same option set on another grid (profiling cases)")
-    ap.add_argument("--form", default="plain", choices=["plain", "learned"],
+    ap.add_argument("--form", default="plain", choices=["plain", "learned", "ensemble"],
                     help="learned: train the closure network on the plain model's own columns (30 days, "
                          "2M rows) first, then time the step with it")
     ap.add_argument("--closure-days", type=int, default=30)
@@ -205,6 +282,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.form == "ensemble":
+        return run_ensemble(args)
 
     import ctypes
 

@@ -41,3 +41,15 @@ def test_ensemble_matches_members_alone():
     for a, b in zip(again, got):
         for k in ("u", "v", "T", "S", "eta"):
             assert torch.equal(getattr(a, k), getattr(b, k)), k
+
+
+def test_handles_of_different_widths_coexist():
+    """A narrow grid's handle created after a wide one leaves the wide one's
+    kernels launchable (per-kernel launch limits are process-wide)."""
+    import torch
+    wide_step, wide_st = _member(96, 48, 10, 4)
+    first = wide_step(wide_st)
+    _member(24, 12, 6, 5)
+    again = wide_step(wide_st)
+    for k in ("u", "v", "T", "S", "eta"):
+        assert torch.equal(getattr(first, k), getattr(again, k)), k

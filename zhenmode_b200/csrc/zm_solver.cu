@@ -685,7 +685,14 @@ void build(zm_solver* s, const zm_grid* g, const zm_params* p) {
   s->fft_lines = std::max(1, std::min(4, (int)((200 * 1024 / sizeof(float2)) / (2 * nx))));
   s->fft_smem = (size_t)2 * s->fft_lines * nx * sizeof(float2);
   require(s->fft_smem <= 227 * 1024, ZM_ERR_UNSUPPORTED, "nx too large for the shared-memory FFT filter");
-  ZM_CUDA(cudaFuncSetAttribute(k_dealias_lon, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->fft_smem));
+  {
+    // the attribute belongs to the kernel, not to this handle: allow the
+    // device's opt-in maximum so that handles of every grid width can launch
+    int optin = 0;
+    ZM_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device));
+    require((int)s->fft_smem <= optin, ZM_ERR_UNSUPPORTED, "nx too large for the shared-memory FFT filter");
+    ZM_CUDA(cudaFuncSetAttribute(k_dealias_lon, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  }
   ZM_CUDA(cudaFuncSetAttribute(k_lin_t, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lin_tile_smem()));
   // ---- buffers
   for (int q = 0; q < 2; ++q) {
