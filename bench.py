@@ -209,7 +209,7 @@ def run_ensemble(args):
         grid, physics, dt, kw, T, S = workloads.make_case(WORKLOAD, nx, ny, nz, dtype="float32")
         wet = np.asarray(grid.wet_mask_3d)
         for _ in range(count):
-            step, init, _ = make_solver_global(grid, physics, dt, **kw)
+            step, init, _ = make_solver_global(grid, physics, dt, autotune=True, **kw)
             rng = np.random.default_rng(seed)
             seed += 1
             steps.append(step)
@@ -306,7 +306,7 @@ def main():
         gnx, gny, gnz = (int(x) for x in args.grid.lower().split("x"))
         wl = dataclasses.replace(wl, nx=gnx, ny=gny, nz=gnz)
     grid, physics, dt, kw, T, S = workloads.make_case(WORKLOAD, wl.nx, wl.ny, wl.nz, dtype="float32")
-    step, init_state, _ = make_solver_global(grid, physics, dt, **kw)
+    step, init_state, _ = make_solver_global(grid, physics, dt, autotune=True, **kw)
     solver = step.solver
     st = init_state(T_init=T, S_init=S)
     closure_info = None
@@ -419,7 +419,9 @@ def main():
                 "config": {"workload": f"{wl.nx}x{wl.ny}x{wl.nz} 0.5-degree plain FP32 option set, dt={wl.dt:.0f} s, "
                                        f"{solver.n_subcyc} barotropic subcycles, {solver.n_nu} nu_h subcycles",
                            "parallelism": f"replicas x{world}", "l2": "per-step working set >> L2 (no flush)",
-                           "monitor_code": int(code.value), "form": args.form},
+                           "monitor_code": int(code.value), "form": args.form,
+                           "autotuned": {"nu_h_subcycles_per_pass": solver.tuned_shapes()[0],
+                                         "fft_lines_per_block": solver.tuned_shapes()[1]}},
                 "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
                              "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                              "traffic": traffic, "algorithmic_bytes_per_launch": algo,

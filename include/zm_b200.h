@@ -78,7 +78,7 @@ typedef struct {
   int32_t localize_conv, conservative_kv, freeze_adv_vel;
   int32_t vertical_diffusion; /* ZM_VDIFF_* */
   int32_t bt_kernel;          /* ZM_BT_* barotropic kernel choice */
-  int32_t reserved0;          /* explicit padding to the pointers; set 0 */
+  int32_t autotune;           /* 1: time the result-neutral launch shapes at the first zm_advance */
   /* (nx, ny) float64 fields; NULL means zeros */
   const double* tau_x;
   const double* tau_y;
@@ -112,8 +112,9 @@ int zm_create(const zm_grid* grid, const zm_params* params, zm_solver** out);
  * out[3] conv_nsub, out[4] row pitch, out[5] device MiB held, out[6] kernel
  * launches in one captured step (0 before the first zm_advance), out[7]
  * barotropic blocks of the resident kernel (0: streaming kernels), out[8] 1
- * when the polar cap of the barotropic mode is active (a band row is wet).
- * Writes min(n, 9) values. */
+ * when the polar cap of the barotropic mode is active (a band row is wet),
+ * out[9] nu_h subcycles per temporally blocked pass (the halo width), out[10]
+ * FFT lines per block.  Writes min(n, 11) values. */
 int zm_info(const zm_solver* s, int32_t* out, int32_t n);
 
 /* Copy a device state (reference layout) into the solver's resident state. */
@@ -230,6 +231,14 @@ int zm_mlp_grad(zm_mlp_trainer* tr, void* stream, int32_t batch, const float* X,
 int zm_mlp_train_step(zm_mlp_trainer* tr, void* stream, int32_t batch, const float* X, const float* T, const float* M,
                       double mask_count, float* params, float* adam_m, float* adam_v, int32_t step, float lr,
                       float beta1, float beta2, float eps, double* loss);
+
+/* Autotuner: time, on the resident state and through stages that write only
+ * work buffers, the launch shapes that change no result (the nu_h halo
+ * width 3..6, i.e. subcycles per temporally blocked pass, and the FFT lines
+ * per block 1..8) and keep the fastest; the next zm_advance recaptures its
+ * graphs.  zm_params.autotune = 1 runs it at the first zm_advance.  Writes
+ * the choices when the pointers are given.  Synchronizes. */
+int zm_autotune(zm_solver* s, void* stream, int32_t* nu_halo, int32_t* fft_lines);
 
 /* Turn the learned vertical-mixing closure on for every following step of
  * the handle (params: ZM_MLP_NPARAMS float32 device values, see zm_mlp_*), or

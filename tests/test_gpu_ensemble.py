@@ -53,3 +53,18 @@ def test_handles_of_different_widths_coexist():
     again = wide_step(wide_st)
     for k in ("u", "v", "T", "S", "eta"):
         assert torch.equal(getattr(first, k), getattr(again, k)), k
+
+
+def test_autotuned_shapes_change_no_result():
+    """The autotuner only picks among launch shapes with identical arithmetic."""
+    import torch
+    grid, physics, dt, kw, T, S = workloads.make_case("plain", 96, 48, 10, dtype="float32")
+    plain, init, _ = make_solver_global(grid, physics, dt, **kw)
+    tuned = make_solver_global(grid, physics, dt, autotune=True, **kw)[0]
+    st = init(T, S)
+    a = plain.advance(st, 2)
+    b = tuned.advance(st, 2)
+    halo, lines = tuned.solver.tuned_shapes()
+    assert 3 <= halo <= 6 and lines in (1, 2, 4, 8)
+    for k in ("u", "v", "T", "S", "eta"):
+        assert torch.equal(getattr(a, k), getattr(b, k)), k

@@ -44,7 +44,7 @@ class ZmParams(ctypes.Structure):
                 ("polar_cap_taper", ctypes.c_int32), ("limiter", ctypes.c_int32),
                 ("localize_conv", ctypes.c_int32), ("conservative_kv", ctypes.c_int32),
                 ("freeze_adv_vel", ctypes.c_int32), ("vertical_diffusion", ctypes.c_int32),
-                ("bt_kernel", ctypes.c_int32), ("reserved0", ctypes.c_int32),
+                ("bt_kernel", ctypes.c_int32), ("autotune", ctypes.c_int32),
                 ("tau_x", _dp), ("tau_y", _dp), ("q_heat", _dp), ("t_atm", _dp), ("s_ref", _dp),
                 ("coastal_restore_coef", _dp), ("coastal_restore_t", _dp),
                 ("coastal_bulk_lambda", _dp), ("coastal_kappa_h", _dp), ("coastal_kappa_v", _dp)]
@@ -87,6 +87,8 @@ EXPORTS = {
                           + [ctypes.c_double] + [ctypes.c_void_p] * 3
                           + [ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                              ctypes.POINTER(ctypes.c_double)]),
+    "zm_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32),
+                                   ctypes.POINTER(ctypes.c_int32)]),
     "zm_set_closure": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float]),
     "zm_closure_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32),
                                         ctypes.POINTER(ctypes.c_uint32)]),

@@ -119,8 +119,9 @@ __device__ __forceinline__ float vdiff_tracer(const Dev& d, const float* __restr
 // coefficients.  East/west neighbours move between lanes by shuffles; the
 // rows above and below a warp's strip pass through shared memory, double
 // buffered, so one barrier per subcycle suffices.  Values at the tile edge
-// are wrong, and the error enters one cell per subcycle: after nsub <= NB_T
-// subcycles the inner (NB_W - 2 NB_T)^2 points are exact.
+// are wrong, and the error enters one cell per subcycle: after nsub <= halo
+// subcycles the inner (NB_W - 2 halo)^2 points are exact (halo <= NB_T is a
+// launch parameter chosen by the autotuner).
 //
 // The Laplacian of numerics/horizontal.py:181-215 is rewritten per point as
 //   lap = aE (uE - u0) + aW (uW - u0) + aN (uN - u0) + aS (uS - u0)
@@ -134,14 +135,14 @@ __device__ __forceinline__ float vdiff_tracer(const Dev& d, const float* __restr
 // __fadd2_rn; the same roundings as the scalar form).
 __global__ void __launch_bounds__(32 * (NB_W / NB_R), 2)
 k_nu_tb(Dev d, const float* __restrict__ u, const float* __restrict__ v, float* __restrict__ uo,
-        float* __restrict__ vo, float c, int nsub) {
+        float* __restrict__ vo, float c, int nsub, int halo) {
   constexpr int NW = NB_W / NB_R;                 // warps per block
-  constexpr int TI = NB_W - 2 * NB_T;
+  const int TI = NB_W - 2 * halo;
   __shared__ float4 edge[2][NW][2][32];           // [parity][warp][0 bottom row, 1 top row][lane]
   __shared__ unsigned char sw[NB_W][NB_W + 4];    // wet flags (coefficient setup)
   const int lane = threadIdx.x, wp = threadIdx.y;
   const int k = blockIdx.z;
-  const int gx0 = blockIdx.x * TI - NB_T, gy0 = blockIdx.y * TI - NB_T;
+  const int gx0 = blockIdx.x * TI - halo, gy0 = blockIdx.y * TI - halo;
   const int c0 = 2 * lane, r0 = wp * NB_R;
   int gi[2];
 #pragma unroll
@@ -238,12 +239,12 @@ k_nu_tb(Dev d, const float* __restrict__ u, const float* __restrict__ v, float* 
   for (int q = 0; q < NB_R; ++q) {
     const int r = r0 + q;
     const int gj = gy0 + r;
-    if (r < NB_T || r >= NB_W - NB_T || gj >= d.ny) continue;
+    if (r < halo || r >= NB_W - halo || gj >= d.ny) continue;
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int col = c0 + h;
       const int ix = gx0 + col;
-      if (col < NB_T || col >= NB_W - NB_T || ix >= d.nx) continue;
+      if (col < halo || col >= NB_W - halo || ix >= d.nx) continue;
       const long long id = kb + (long long)gj * d.P + ix;
       uo[id] = h == 0 ? au[q].x : au[q].y;
       vo[id] = h == 0 ? av[q].x : av[q].y;

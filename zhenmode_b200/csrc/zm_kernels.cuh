@@ -91,7 +91,7 @@ __global__ void k_budget_partials(Dev d, const float* T, const float* S, const d
                                   double* partial);
 __global__ void k_budget_final(const double* partial, int nblocks, double* out);
 __global__ void k_barrier_probe(unsigned* bar, unsigned* err, unsigned expected, unsigned max_polls);
-__global__ void k_nu_tb(Dev d, const float* u, const float* v, float* uo, float* vo, float c, int nsub);
+__global__ void k_nu_tb(Dev d, const float* u, const float* v, float* uo, float* vo, float c, int nsub, int halo);
 __global__ void k_lin_t(Dev d, const float* usub, const float* vsub, const float* u0, const float* v0, const float* T0,
                         const float* S0, float* uo, float* vo, float* To, float* So, float dth, int implicit_v);
 // tile of k_lin_t

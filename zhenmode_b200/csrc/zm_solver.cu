@@ -68,6 +68,9 @@ struct zm_solver {
   double *area64 = nullptr, *width64 = nullptr, *bpart = nullptr, *bout = nullptr;
   int bblocks = 0;
   // learned vertical-mixing closure (off until zm_set_closure)
+  int nu_halo = NB_T;            // nu_h subcycles per pass (autotuned)
+  bool want_tune = false;
+  bool tuned = false;
   bool closure_on = false;
   MlpBf16 cw{};
   float* kappa3 = nullptr;       // [nz-1][ny][P] diffusivity per interface
@@ -159,15 +162,15 @@ struct zm_solver {
       const float dts = (float)(dt / 2.0 / n_nu);
       const float* a = src.u;
       const float* c = src.v;
-      constexpr int TI = NB_W - 2 * NB_T;
+      const int TI = NB_W - 2 * nu_halo;
       const dim3 blk(32, NB_W / NB_R);
       const dim3 grd((nx + TI - 1) / TI, (ny + TI - 1) / TI, nz);
       int done = 0, pass = 0;
       while (done < n_nu) {
-        const int nsub = std::min(NB_T, n_nu - done);
+        const int nsub = std::min(nu_halo, n_nu - done);
         const Fields4& o = (pass % 2 == 0) ? W1 : W2;
         pb(ZM_K_NU_SUB, s);
-        k_nu_tb<<<grd, blk, 0, s>>>(d, a, c, o.u, o.v, dts, nsub);
+        k_nu_tb<<<grd, blk, 0, s>>>(d, a, c, o.u, o.v, dts, nsub, nu_halo);
         pe(s);
         a = o.u;
         c = o.v;
@@ -395,6 +398,63 @@ struct zm_solver {
     check_launch();
   }
 
+  // Time the launch shapes that change no result on the resident state,
+  // through stages that only write work buffers, and keep the fastest:
+  // nu_h halo width (3..NB_T) and FFT lines per block (1..8).
+  void autotune(cudaStream_t s) {
+    cudaEvent_t e0, e1;
+    ZM_CUDA(cudaEventCreate(&e0));
+    ZM_CUDA(cudaEventCreate(&e1));
+    auto time_ms = [&](auto&& run) {
+      run();
+      ZM_CUDA(cudaEventRecord(e0, s));
+      for (int r = 0; r < 3; ++r) run();
+      ZM_CUDA(cudaEventRecord(e1, s));
+      ZM_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      ZM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      return ms;
+    };
+    try {
+      const Fields4& in = st[cur];
+      if (d.nu_h != 0.f) {
+        float best = 1e30f;
+        int pick = nu_halo;
+        for (int h = 3; h <= NB_T; ++h) {
+          nu_halo = h;
+          const float ms = time_ms([&] { linear_half(s, in, s1); });
+          if (ms < best) {
+            best = ms;
+            pick = h;
+          }
+        }
+        nu_halo = pick;
+      }
+      float best = 1e30f;
+      int pick = fft_lines;
+      for (int lines = 1; lines <= 8; lines *= 2) {
+        const size_t smem = (size_t)2 * lines * nx * sizeof(float2);
+        if (smem > 200 * 1024) break;
+        fft_lines = lines;
+        fft_smem = smem;
+        const float ms = time_ms([&] { momentum_advection_part(s, in); });
+        if (ms < best) {
+          best = ms;
+          pick = lines;
+        }
+      }
+      fft_lines = pick;
+      fft_smem = (size_t)2 * pick * nx * sizeof(float2);
+    } catch (...) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    tuned = true;
+  }
+
   void build_graphs() {
     cudaStream_t s = cap_stream;
     for (int g = 0; g < 2; ++g) {
@@ -508,6 +568,7 @@ void build(zm_solver* s, const zm_grid* g, const zm_params* p) {
   s->cap_rows = p->polar_cap_rows;
   s->cap_nb = nb;
   s->vdiff = p->vertical_diffusion;
+  s->want_tune = p->autotune != 0;
   s->freeze = p->freeze_adv_vel;
   s->bottom_decay = (float)std::exp(-p->r_bot * p->dt);
   s->bt_drag = 1.0 / (1.0 + p->r_bot * s->dt_bt);
@@ -827,9 +888,9 @@ int zm_create(const zm_grid* grid, const zm_params* params, zm_solver** out) {
 
 int zm_info(const zm_solver* s, int32_t* out, int32_t n) {
   if (!s || !out) return ZM_ERR_INVALID;
-  const int32_t v[9] = {s->n_subcyc, s->n_nu, s->adv_nsub, s->conv_nsub, s->P, (int32_t)(s->bytes >> 20),
-                        s->kernels_per_step, s->bt_blocks, s->bt.cap_active};
-  for (int q = 0; q < n && q < 9; ++q) out[q] = v[q];
+  const int32_t v[11] = {s->n_subcyc, s->n_nu, s->adv_nsub, s->conv_nsub, s->P, (int32_t)(s->bytes >> 20),
+                         s->kernels_per_step, s->bt_blocks, s->bt.cap_active, s->nu_halo, s->fft_lines};
+  for (int q = 0; q < n && q < 11; ++q) out[q] = v[q];
   return ZM_OK;
 }
 
@@ -858,6 +919,7 @@ int zm_advance(zm_solver* s, void* stream, int32_t nsteps) {
   if (!s || nsteps < 0) return ZM_ERR_INVALID;
   cudaStream_t st = (cudaStream_t)stream;
   try {
+    if (s->want_tune && !s->tuned) s->autotune(st);
     if (!s->graphs_ready) s->build_graphs();
     for (int n = 0; n < nsteps; ++n) {
       ZM_CUDA(cudaGraphLaunch(s->graph[s->cur], st));
@@ -980,8 +1042,10 @@ int zm_ensemble_advance(zm_ensemble* e, void* stream, int32_t nsteps, int32_t* k
       }
     }
     if (stale) {
-      for (auto* s : e->m)
+      for (auto* s : e->m) {
+        if (s->want_tune && !s->tuned) s->autotune(st);
         if (!s->graphs_ready) s->build_graphs();
+      }
       ZM_CUDA(cudaDeviceSynchronize());
       e->capture();
       rel = 0;
@@ -1238,6 +1302,25 @@ int zm_set_closure(zm_solver* s, void* stream, const float* params, float bound)
   } catch (const Err& e) {
     return fail(s, e);
   }
+  return ZM_OK;
+}
+
+int zm_autotune(zm_solver* s, void* stream, int32_t* nu_halo, int32_t* fft_lines) {
+  if (!s) return ZM_ERR_INVALID;
+  cudaStream_t st = (cudaStream_t)stream;
+  try {
+    s->autotune(st);
+    for (int g = 0; g < 2; ++g)
+      if (s->graph[g]) {
+        cudaGraphExecDestroy(s->graph[g]);
+        s->graph[g] = nullptr;
+      }
+    s->graphs_ready = false;
+  } catch (const Err& e) {
+    return fail(s, e);
+  }
+  if (nu_halo) *nu_halo = s->nu_halo;
+  if (fft_lines) *fft_lines = s->fft_lines;
   return ZM_OK;
 }
 

@@ -147,6 +147,7 @@ class _Solver:
         p.freeze_adv_vel = int(bool(opts["freeze_adv_vel"]))
         p.vertical_diffusion = 1 if opts["vertical_diffusion"] == "implicit" else 0
         p.bt_kernel = _BT_KERNELS[opts["barotropic_kernel"]]
+        p.autotune = 1 if opts.get("autotune") else 0
         for name in ("tau_x", "tau_y", "q_heat", "t_atm", "s_ref", "coastal_restore_coef",
                      "coastal_restore_t", "coastal_bulk_lambda", "coastal_kappa_h", "coastal_kappa_v"):
             setattr(p, name, _native.dptr(arr(opts["fields"].get(name), (nx, ny))))
@@ -160,10 +161,16 @@ class _Solver:
         if rc != _native.ZM_OK:
             raise RuntimeError(f"zm_create failed with status {rc}")
         self.handle = handle
-        info = (ctypes.c_int32 * 9)()
-        self.lib.zm_info(handle, info, 9)
+        info = (ctypes.c_int32 * 11)()
+        self.lib.zm_info(handle, info, 11)
         (self.n_subcyc, self.n_nu, self.adv_nsub, self.conv_nsub, self.pitch, self.mib, _,
-         self.bt_blocks, self.bt_cap_active) = list(info)
+         self.bt_blocks, self.bt_cap_active, self.nu_halo, self.fft_lines) = list(info)
+
+    def tuned_shapes(self):
+        """(nu_h halo width, FFT lines per block) in use."""
+        info = (ctypes.c_int32 * 11)()
+        self.lib.zm_info(self.handle, info, 11)
+        return int(info[9]), int(info[10])
 
     def kernels_per_step(self):
         info = (ctypes.c_int32 * 7)()
@@ -275,14 +282,16 @@ def make_solver_global(grid, physics, dt, forcing=None,
                        projection_max_refinements=2, column_geometry='legacy',
                        match_barotropic_transport=False, process_time_scheme='legacy',
                        eos_pressure_dbar=None, surface_pressure_pa=None,
-                       vertical_diffusion='explicit', barotropic_kernel='auto', **schemes):
+                       vertical_diffusion='explicit', barotropic_kernel='auto', autotune=False, **schemes):
     """Build the B200 step; the argument list is the reference factory's.
 
     Two options are not the reference's: ``vertical_diffusion='implicit'``
     replaces the explicit L-step vertical diffusion by a per-column
     backward-Euler solve, and ``barotropic_kernel`` ('auto', 'resident',
     'streaming') picks the CUDA kernels of the barotropic subcycle (same
-    arithmetic; 'auto' takes the resident kernel when the grid fits).
+    arithmetic; 'auto' takes the resident kernel when the grid fits), and
+    ``autotune=True`` times the launch shapes that change no result (nu_h halo
+    width, FFT lines per block) at the first step and keeps the fastest.
     """
     # ---- validation, in the reference's order where it matters (factory.py:166-395)
     _finite('dt', dt, positive=True)
@@ -414,7 +423,7 @@ def make_solver_global(grid, physics, dt, forcing=None,
                 polar_cap_rows=polar_cap_rows, polar_cap_taper=polar_cap_taper, fct_adv=fct_adv,
                 monotone_adv=monotone_adv, localize_conv=localize_conv, conservative_kv=conservative_kv,
                 freeze_adv_vel=freeze_adv_vel, vertical_diffusion=vertical_diffusion,
-                barotropic_kernel=barotropic_kernel, fields=fields)
+                barotropic_kernel=barotropic_kernel, autotune=bool(autotune), fields=fields)
     solver = _Solver(grid, physics, dt, opts)
     wet3 = np.asarray(getattr(grid, 'wet_mask_3d', None) if getattr(grid, 'wet_mask_3d', None) is not None
                       else np.broadcast_to(np.asarray(grid.wet_mask)[:, :, None], (nx, ny, nz)), dtype=np.float64)
