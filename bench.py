@@ -277,6 +277,8 @@ def main():
                     help="learned: train the closure network on the plain model's own columns (30 days, "
                          "2M rows) first, then time the step with it")
     ap.add_argument("--closure-days", type=int, default=30)
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default launch shapes (profiling: no autotuner trial launches)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -306,7 +308,7 @@ def main():
         gnx, gny, gnz = (int(x) for x in args.grid.lower().split("x"))
         wl = dataclasses.replace(wl, nx=gnx, ny=gny, nz=gnz)
     grid, physics, dt, kw, T, S = workloads.make_case(WORKLOAD, wl.nx, wl.ny, wl.nz, dtype="float32")
-    step, init_state, _ = make_solver_global(grid, physics, dt, autotune=True, **kw)
+    step, init_state, _ = make_solver_global(grid, physics, dt, autotune=not args.no_autotune, **kw)
     solver = step.solver
     st = init_state(T_init=T, S_init=S)
     closure_info = None
