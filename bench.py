@@ -264,6 +264,103 @@ def run_ensemble(args):
     return 0
 
 
+def run_precision(args):
+    """The precision form: 800x400x50, implicit vertical diffusion (FP32 Thomas
+    plus one refinement step), float64 barotropic mode, a seasonal forcing
+    (wind stress x (1 + 0.25 sin) and a +-100 W/m^2 heat flux over 12 monthly
+    fields, blended on the device before every step) for 10 simulated days,
+    with the compensated float64 heat / salt budgets taken every day."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    from zhenmode_b200 import _native, make_solver_global, workloads
+
+    # the 0.45-degree option set: nu_h, nu_bi, kappa_bi and dt_bt scaled from the
+    # 0.5-degree values by the CFL powers of dx (runtime/cli.py:49-61)
+    grid, physics, dt, kw, T, S = workloads.make_case("precision", dtype="float32")
+    nx, ny, nz = grid.nx, grid.ny, grid.nz
+    kw = dict(kw)
+    kw.update(vertical_diffusion="implicit")
+    step, init_state, _ = make_solver_global(grid, physics, dt, autotune=not args.no_autotune, **kw)
+    solver = step.solver
+    st = init_state(T_init=T, S_init=S)
+    lat = np.radians(np.asarray(grid.lat))
+    tau0 = np.broadcast_to((0.1 * np.sin(2 * lat) * np.cos(lat))[None, :], (nx, ny))
+    phase = np.sin(2 * np.pi * (np.arange(12) + 0.5) / 12.0)
+    taux = torch.as_tensor(np.stack([tau0 * (1 + 0.25 * p) for p in phase]).astype(np.float32), device="cuda")
+    qh = torch.as_tensor(np.stack([np.broadcast_to(100.0 * p * np.cos(lat)[None, :], (nx, ny)) for p in phase])
+                         .astype(np.float32), device="cuda")
+    stream = torch.cuda.current_stream()
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    sin = _native.ZmState(*[t.data_ptr() for t in (st.u, st.v, st.T, st.S, st.eta)])
+    solver.check(solver.lib.zm_load_state(solver.handle, sp, ctypes.byref(sin)), "zm_load_state")
+    out = [torch.empty_like(t) for t in (st.u, st.v, st.T, st.S, st.eta)]
+    sout = _native.ZmState(*[t.data_ptr() for t in out])
+
+    def budgets():
+        solver.check(solver.lib.zm_store_state(solver.handle, sp, ctypes.byref(sout)), "zm_store_state")
+        b = (ctypes.c_double * 8)()
+        solver.check(solver.lib.zm_budgets(solver.handle, sp, ctypes.c_void_p(out[2].data_ptr()),
+                                           ctypes.c_void_p(out[3].data_ptr()), 1025.0, 3992.0, b), "zm_budgets")
+        return list(b)
+
+    per_day = int(round(86400.0 / dt))
+    days = 10
+
+    def one_step(n):
+        step.set_forcing_seasonal(tau_x=taux, q_heat=qh, day=n * dt / 86400.0)
+        solver.check(solver.lib.zm_advance(solver.handle, sp, 1), "zm_advance")
+
+    for n in range(max(args.warmup, 3)):
+        one_step(n)
+    b0 = budgets()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    time.sleep(0.3)
+    total_ms = 0.0
+    daily = [b0]
+    for dday in range(days):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for n in range(per_day):
+            one_step(dday * per_day + n)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        daily.append(budgets())
+    clk = clocks.stop()
+    code = ctypes.c_int32()
+    solver.check(solver.lib.zm_status(solver.handle, ctypes.byref(code)), "zm_status")
+    nsteps = days * per_day
+    ms = total_ms / nsteps
+    heat = [d[4] for d in daily]
+    salt = [d[5] for d in daily]
+    drift = lambda v: max(abs(v[i + 1] - v[i]) / abs(v[i]) for i in range(len(v) - 1))
+    F = 4.0 * nx * ny * nz
+    bstep = step_bytes(nx, ny, nz, solver.n_nu, solver.adv_nsub)
+    peak, peak_kind = measured_peaks()
+    line = {"metric": METRIC, "value": sim_years_per_day(ms, dt), "unit": "sim-years/day", "n_gpus": 1,
+            "steps": nsteps, "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded bathymetry, thermocline; seasonal wind stress and +-100 W/m^2 heat flux)",
+            "config": {"workload": f"{nx}x{ny}x{nz} precision form: implicit vertical diffusion with one refinement "
+                                   f"step, float64 barotropic mode, {solver.n_subcyc} subcycles, seasonal forcing "
+                                   f"blended on the device every step, {days} simulated days",
+                       "form": "precision", "monitor_code": int(code.value)},
+            "budgets": {"heat_content_J": heat, "salt_content_kg": salt,
+                        "max_relative_change_per_day": {"heat": drift(heat), "salt": drift(salt)},
+                        "total_volume_m3": daily[-1][6], "sums": "float64, compensated, fixed order"},
+            "roofline": {"bound": "hbm", "step_stage_bytes": bstep, "step_frac": bstep / (ms * 1e-3) / 1e9 / peak,
+                         "peak": peak, "peak_kind": peak_kind, "unit": "GB/s"},
+            "gpu_launches": nsteps * (solver.kernels_per_step() + 3), "clocks": clk, "e2e": None,
+            "cpu_baseline": None}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -273,7 +370,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", default=None, help="NXxNYxNZ: same option set on another grid (profiling cases)")
-    ap.add_argument("--form", default="plain", choices=["plain", "learned", "ensemble"],
+    ap.add_argument("--form", default="plain", choices=["plain", "learned", "ensemble", "precision"],
                     help="learned: train the closure network on the plain model's own columns (30 days, "
                          "2M rows) first, then time the step with it")
     ap.add_argument("--closure-days", type=int, default=30)
@@ -286,6 +383,8 @@ def main():
         return run_reference(args)
     if args.form == "ensemble":
         return run_ensemble(args)
+    if args.form == "precision":
+        return run_precision(args)
 
     import ctypes
 

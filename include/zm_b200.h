@@ -139,6 +139,15 @@ int zm_step_host(zm_solver* s, void* stream, const zm_state* in, zm_state* out, 
  * `step_dyn` path of factory.py:735-750.  NULL keeps a field. */
 int zm_set_forcing(zm_solver* s, void* stream, const float* tau_x, const float* tau_y, const float* q_heat);
 
+/* Seasonal forcing on the device (inputs/forcing/seasonal.py:86-103): each
+ * given (12, nx, ny) float32 stack of monthly fields (device, reference
+ * layout; NULL keeps the field) is blended for `day` (30-day months: the
+ * current month, with the previous / next month over the first / last
+ * blend_days / 2 days) into the forcing of the following steps.  Stream
+ * ordered; the captured steps read the blended fields, no recapture. */
+int zm_set_forcing_seasonal(zm_solver* s, void* stream, const float* tau_x, const float* tau_y, const float* q_heat,
+                            double day, double blend_days);
+
 /* Run one stage of the step on a device state, for stage-level checks:
  * 1 = linear half step L(dt/2) (step.py:76-187), 2 = nonlinear step N(dt)
  * (step.py:249-320), 3 = one full step, 4 = the velocity-only part of the

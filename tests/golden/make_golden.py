@@ -232,8 +232,21 @@ def make_diagnostics_case(seed=5):
     print("diagnostics saved", dict(zip(b.as_dict().keys(), b.as_dict().values())))
 
 
+def make_seasonal_case(seed=9):
+    """The reference's seasonal blend (inputs/forcing/seasonal.py:86-103) of a
+    random 12-month stack at days around the month boundaries."""
+    from zhenmode.model.inputs.forcing import seasonal as ref_seasonal
+    stack = _f32(np.random.default_rng(seed).standard_normal((12, 8, 6)))
+    days = np.array([0.0, 1.0, 2.4, 14.5, 27.6, 28.7, 29.9, 30.0, 31.2, 359.5, 361.0, 725.3])
+    out = np.stack([_np(ref_seasonal.interp_monthly_field_jit(stack, float(d), 5.0)) for d in days])
+    out0 = np.stack([_np(ref_seasonal.interp_monthly_field_jit(stack, float(d), 0.0)) for d in days])
+    np.savez_compressed(os.path.join(HERE, "seasonal_blend.npz"), stack=stack, days=days, blend5=out, blend0=out0)
+    print("seasonal saved")
+
+
 def main():
     make_operator_case()
+    make_seasonal_case()
     make_diagnostics_case()
     # The 0.5 deg production option set, rescaled to a 7.5 deg x 7.5 deg grid
     # whose polar bands are partly wet, from a moving state (2 steps).

@@ -152,3 +152,11 @@ def test_budget_diagnostics():
     assert names == list(budgets.FIELDS)
     for name, want in zip(names, data["budget_values"]):
         assert abs(got[name] - want) <= 1e-13 * abs(want), (name, got[name], want)
+
+
+def test_seasonal_blend():
+    from oracle import seasonal
+    data = load("seasonal_blend")
+    for n, day in enumerate(data["days"]):
+        _check(f"blend5 day {day}", seasonal.blend(data["stack"], float(day), 5.0), data["blend5"][n], 1e-14)
+        _check(f"blend0 day {day}", seasonal.blend(data["stack"], float(day), 0.0), data["blend0"][n], 1e-14)

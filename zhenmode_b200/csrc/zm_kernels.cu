@@ -1062,6 +1062,20 @@ __global__ void __launch_bounds__(128) k_pgf(Dev d, PgfArgs a) {
   }
 }
 
+// Seasonal forcing blend (inputs/forcing/seasonal.py:86-103): the current
+// month's field blended with the previous and next month's near the month
+// boundaries, weights w_prev, w_cur, w_next from the host; a (12, nx, ny)
+// reference-layout stack into the internal 2-D forcing field.
+__global__ void k_forcing_blend(Dev d, const float* __restrict__ stack, int prev, int cur, int next, float w_prev,
+                                float w_cur, float w_next, float* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= d.nx || j >= d.ny) return;
+  const long long plane = (long long)d.nx * d.ny, r = (long long)i * d.ny + j;
+  out[idx2(d, j, i)] = w_cur * stack[cur * plane + r] + w_next * stack[next * plane + r] +
+                       w_prev * stack[prev * plane + r];
+}
+
 // ------------------------------------------------------------------ barotropic mode (float64)
 // Total barotropic forcing F_rho + tau / (rho0 H) in float64.
 __global__ void k_bt_forcing(Dev d, const float* __restrict__ frx, const float* __restrict__ fry,

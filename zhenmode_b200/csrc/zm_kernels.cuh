@@ -90,6 +90,8 @@ __global__ void k_diagnostics(Dev d, const float* T, const float* S, const float
 __global__ void k_budget_partials(Dev d, const float* T, const float* S, const double* area, const double* width,
                                   double* partial);
 __global__ void k_budget_final(const double* partial, int nblocks, double* out);
+__global__ void k_forcing_blend(Dev d, const float* stack, int prev, int cur, int next, float w_prev, float w_cur,
+                                float w_next, float* out);
 __global__ void k_barrier_probe(unsigned* bar, unsigned* err, unsigned expected, unsigned max_polls);
 __global__ void k_nu_tb(Dev d, const float* u, const float* v, float* uo, float* vo, float c, int nsub, int halo);
 __global__ void k_lin_t(Dev d, const float* usub, const float* vsub, const float* u0, const float* v0, const float* T0,

@@ -1116,6 +1116,36 @@ int zm_set_forcing(zm_solver* s, void* stream, const float* tau_x, const float* 
   return ZM_OK;
 }
 
+int zm_set_forcing_seasonal(zm_solver* s, void* stream, const float* tau_x, const float* tau_y, const float* q_heat,
+                            double day, double blend_days) {
+  if (!s || !std::isfinite(day) || !std::isfinite(blend_days)) return ZM_ERR_INVALID;
+  // weights as inputs/forcing/seasonal.py:86-103 forms them (30-day months)
+  const double month_len = 30.0;
+  const double mpos = std::fmod(day, month_len) + (std::fmod(day, month_len) < 0 ? month_len : 0.0);
+  int mi = (int)std::floor(day / month_len) % 12;
+  if (mi < 0) mi += 12;
+  const int prev = (mi + 11) % 12, next = (mi + 1) % 12;
+  double w_after = 0.0, w_before = 0.0;
+  if (blend_days > 0.0) {
+    const double half = blend_days / 2.0;
+    w_after = std::min(1.0, std::max(0.0, (mpos - (month_len - half)) / blend_days));
+    w_before = std::min(1.0, std::max(0.0, (half - mpos) / blend_days));
+  }
+  const float wc = (float)(1.0 - w_after - w_before), wn = (float)w_after, wp = (float)w_before;
+  cudaStream_t st = (cudaStream_t)stream;
+  try {
+    const dim3 c(32, 8);
+    const float* stacks[3] = {tau_x, tau_y, q_heat};
+    float* outs[3] = {s->tau_x, s->tau_y, s->qheat};
+    for (int q = 0; q < 3; ++q)
+      if (stacks[q]) k_forcing_blend<<<s->grid2(c), c, 0, st>>>(s->d, stacks[q], prev, mi, next, wp, wc, wn, outs[q]);
+    s->check_launch();
+  } catch (const Err& e) {
+    return fail(s, e);
+  }
+  return ZM_OK;
+}
+
 int zm_run_stage(zm_solver* s, void* stream, int32_t stage, const zm_state* in, zm_state* out) {
   if (!s || !in || !out || stage < 1 || stage > 7) return ZM_ERR_INVALID;
   cudaStream_t st = (cudaStream_t)stream;

@@ -561,8 +561,38 @@ def make_solver_global(grid, physics, dt, forcing=None,
             solver.check(rc, "zm_closure_stats")
         return int(fb.value), int(er.value)
 
+    def set_forcing(tau_x=None, tau_y=None, q_heat=None):
+        """Replace the 2-D forcing of the following steps ((nx, ny) fields)."""
+        import torch
+        fs = [None if a is None else torch.as_tensor(np.asarray(a, dtype=np.float32) if not isinstance(a, torch.Tensor)
+                                                    else a, dtype=torch.float32, device='cuda').contiguous()
+              for a in (tau_x, tau_y, q_heat)]
+        solver.check(solver.lib.zm_set_forcing(solver.handle, _cur_stream(),
+                                               *[ctypes.c_void_p(t.data_ptr() if t is not None else None)
+                                                 for t in fs]), "zm_set_forcing")
+        step._forcing_keep = fs
+
+    def set_forcing_seasonal(tau_x=None, tau_y=None, q_heat=None, day=0.0, blend_days=5.0):
+        """Blend (12, nx, ny) monthly stacks on the device for ``day``
+        (inputs/forcing/seasonal.py:86-103) into the forcing of the following
+        steps; stacks left as None keep their field."""
+        import torch
+        fs = [None if a is None else torch.as_tensor(np.asarray(a, dtype=np.float32) if not isinstance(a, torch.Tensor)
+                                                    else a, dtype=torch.float32, device='cuda').contiguous()
+              for a in (tau_x, tau_y, q_heat)]
+        for t in fs:
+            if t is not None and tuple(t.shape) != (12,) + solver.shape[:2]:
+                raise ValueError("monthly stacks are (12, nx, ny)")
+        solver.check(solver.lib.zm_set_forcing_seasonal(solver.handle, _cur_stream(),
+                                                        *[ctypes.c_void_p(t.data_ptr() if t is not None else None)
+                                                          for t in fs], float(day), float(blend_days)),
+                     "zm_set_forcing_seasonal")
+        step._forcing_keep = fs
+
     step.solver = solver
     step.advance = _run
+    step.set_forcing = set_forcing
+    step.set_forcing_seasonal = set_forcing_seasonal
     step.budget_diagnostics = budget_diagnostics
     step.set_closure = set_closure
     step.closure_features = closure_features
