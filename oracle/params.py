@@ -34,7 +34,8 @@ SUPPORTED = ("mode_split", "dt_bt", "nu_nsub", "dtype", "use_scan", "forcing", "
              "T_init", "S_init", "polar_cap_rows", "polar_cap_taper", "eta_relax_days",
              "eta_relax_box", "eta_relax_buffer", "freeze_adv_vel", "conservative_kv",
              "localize_conv", "monotone_adv", "fct_adv", "ice_freeze_temp_c", "ice_salt_flux",
-             "vertical_diffusion")
+             "vertical_diffusion", "project_adv_vel", "projection_niter", "projection_rtol",
+             "projection_preconditioner", "projection_max_refinements")
 
 
 def _coastal(mask, coefficient, shape):
@@ -221,6 +222,23 @@ def build_params(grid, physics, dt, **opts):
     p.fct_adv = bool(opts.get("fct_adv", False))
     p.ice_freeze_temp_c = float(opts.get("ice_freeze_temp_c", -1.8))
     p.ice_salt_flux = float(opts.get("ice_salt_flux", 0.0))
+    # column projection of the stage-2 advective velocity (factory.py:366-386, 650)
+    p.project_adv_vel = bool(opts.get("project_adv_vel", False))
+    niter = opts.get("projection_niter")
+    p.projection_niter = 150 if niter is None else int(niter)
+    if p.projection_niter <= 0:
+        raise ValueError("projection_niter must be a positive integer")
+    rtol = opts.get("projection_rtol")
+    # the tolerance floors follow the dtype the step runs in (float32 / float64)
+    eps = float(np.finfo(np.float32 if opts.get("dtype", "float64") == "float32" else np.float64).eps)
+    p.projection_rtol = max(float(rtol or 1e-12), 32.0 * eps)
+    p.projection_transport_rtol = max(1e-10, 32.0 * eps)
+    p.projection_preconditioner = opts.get("projection_preconditioner", "none")
+    if p.projection_preconditioner not in ("none", "jacobi"):
+        raise ValueError("projection_preconditioner must be none or jacobi")
+    p.projection_max_refinements = int(opts.get("projection_max_refinements", 2))
+    if not 0 <= p.projection_max_refinements <= 2:
+        raise ValueError("projection_max_refinements must be an integer from 0 to 2")
     p.vertical_diffusion = opts.get("vertical_diffusion", "explicit")
     if p.vertical_diffusion not in ("explicit", "implicit"):
         raise ValueError("vertical_diffusion must be 'explicit' or 'implicit'")

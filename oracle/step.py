@@ -631,6 +631,107 @@ def linear_half_step(st, p, dt_half):
 
 
 # ---------------------------------------------------------------- nonlinear full step
+# ---------------------------------------------------------------- column projection
+def column_divergence(u, v, p):
+    """dynamics/transport.py:45-57 (legacy): sum_k div_h[k] dz_node[k] on wet columns."""
+    return np.sum(divergence_h(u, v, p) * p.dz_node, axis=-1) * p.wet_mask
+
+
+def column_projection_diagonal(p):
+    """dynamics/projection.py:10-51 (legacy branch): the exact diagonal of the
+    projection operator."""
+    wet = p.wet_mask_z
+    pos_x = wet * np.roll(wet, -1, axis=0)
+    neg_x = wet * np.roll(wet, 1, axis=0)
+    dxg = 0.25 * p.inv_dx[..., :1] ** 2 * ((pos_x - neg_x) ** 2 + pos_x ** 2 + neg_x ** 2)
+    if p.nx <= 2:
+        dxg = np.zeros_like(wet)
+    c = p.cos_lat[None, :, None]
+    cn = np.roll(c, -1, axis=1)
+    cs = np.roll(c, 1, axis=1)
+    pos_y = wet * np.roll(wet, -1, axis=1)
+    pos_y[:, -1, :] = 0.0
+    neg_y = wet * np.roll(wet, 1, axis=1)
+    neg_y[:, 0, :] = 0.0
+    pos_y = pos_y * 0.5 * (c + cn)
+    neg_y = neg_y * 0.5 * (c + cs)
+    dyg = 0.25 * p.inv_dy ** 2 * ((pos_y - neg_y) ** 2 / c ** 2 + pos_y ** 2 / (c * cn) + neg_y ** 2 / (c * cs))
+    area = p.dx_2d * p.dy * p.wet_mask
+    return area * np.sum((dxg + dyg) * p.dz_node, axis=-1)
+
+
+def conjugate_gradient(A, b, tol, maxiter, M=None, atol=0.0):
+    """Preconditioned CG with the loop of jax.scipy.sparse.linalg.cg (jax 0.11.2,
+    the reference's pinned version; the dependency is absent here): x0 = 0,
+    stop when the squared residual norm (<r, z> without a preconditioner,
+    <r, r> with one) is at most max(tol^2 <b, b>, atol^2) or after maxiter
+    iterations."""
+    identity = M is None
+    prec = (lambda r: r) if identity else M
+    x = np.zeros_like(b)
+    atol2 = max(tol * tol * float(np.vdot(b, b)), atol * atol)
+    r = b - A(x)
+    z = prec(r)
+    pdir = z
+    gamma = float(np.vdot(r, z))
+    k = 0
+    while (gamma if identity else float(np.vdot(r, r))) > atol2 and k < maxiter:
+        Ap = A(pdir)
+        alpha = gamma / float(np.vdot(pdir, Ap))
+        x = x + alpha * pdir
+        r = r - alpha * Ap
+        z = prec(r)
+        gamma_new = float(np.vdot(r, z))
+        pdir = z + (gamma_new / gamma) * pdir
+        gamma = gamma_new
+        k += 1
+    return x
+
+
+def project_column_divergence(u, v, p, dt):
+    """dynamics/projection.py:64-127: remove the column-integrated horizontal
+    divergence by the Euler correction -dt g grad(psi) of the potential that
+    solves the area-weighted problem with the exact column divergence, then up
+    to projection_max_refinements corrective solves while the actual surface
+    transport stays above its threshold."""
+    g = G_EARTH
+    area = p.dx_2d * p.dy * p.wet_mask
+    rhs = -(column_divergence(u, v, p) / (dt * g)) * area
+
+    def matvec(psi):
+        gx, gy = gradient_conservative_3d(psi[:, :, None], p)
+        return -column_divergence(gx, gy, p) * area
+
+    M = None
+    if p.projection_preconditioner == "jacobi":
+        diag = column_projection_diagonal(p)
+        inv = 1.0 / np.where(diag > 0.0, diag, 1.0)
+        M = lambda r: r * inv  # noqa: E731
+
+    def correct(vel, psi):
+        gx, gy = gradient_conservative_3d(psi[..., None], p)
+        return vel[0] - (dt * g) * gx, vel[1] - (dt * g) * gy
+
+    tol = p.projection_rtol
+    psi = conjugate_gradient(matvec, rhs, tol, p.projection_niter, M)
+    corrected = correct((u, v), psi)
+    if p.projection_max_refinements == 0:
+        return corrected
+
+    def transport_norm_squared(vel):
+        top = vertical_transport_iface(vel[0], vel[1], p)[..., 0]
+        return float(np.sum(top ** 2 * p.dx_2d * p.dy * p.wet_mask))
+
+    threshold = p.projection_transport_rtol ** 2 * transport_norm_squared((u, v))
+    floor = tol * float(np.linalg.norm(rhs))
+    for _ in range(p.projection_max_refinements):
+        if transport_norm_squared(corrected) > threshold:
+            residual = -(column_divergence(corrected[0], corrected[1], p) / (dt * g)) * area
+            delta = conjugate_gradient(matvec, residual, tol, p.projection_niter, M, atol=floor)
+            corrected = correct(corrected, delta)
+    return corrected
+
+
 def explicit_full_step(st, p):
     """timestepping/step.py:249-320 ``_explicit_full_step`` (legacy RK2 with
     the exact linear-drag decay of the mode-split path)."""
@@ -646,6 +747,8 @@ def explicit_full_step(st, p):
     if p.freeze_adv_vel:
         dT2, dS2 = tracer_residual(u, v, Tp, Sp, p)
     else:
+        if p.project_adv_vel:   # step.py:292-303
+            up, vp = project_column_divergence(up, vp, p, dt)
         dT2, dS2 = tracer_residual(up, vp, Tp, Sp, p)
     Tn = T + 0.5 * (dT1 + dT2) * dt
     Sn = S + 0.5 * (dS1 + dS2) * dt

@@ -244,14 +244,42 @@ def make_seasonal_case(seed=9):
     print("seasonal saved")
 
 
+def make_projection_case(seed=13):
+    """The reference's column-divergence projection (dynamics/projection.py:64-127)
+    called on a moving float64 state of the 48x24x10 option-set grid, with
+    the preset's settings and with the Jacobi preconditioner."""
+    from zhenmode.model.solver.dynamics import projection as ref_proj
+    grid = workloads.build_grid(48, 24, 10, land_lat=75.0)
+    T, S = workloads.initial_fields(grid, perturb_sigma=0.2)
+    data = dict(_grid_arrays(grid))
+    u, v, T0, S0, eta = _moving_state(grid, T, S, seed, amp_u=0.2)
+    data.update(in_u=_f32(u), in_v=_f32(v))
+    for pre in ("none", "jacobi"):
+        kw = dict(workloads.PLAIN_OPTIONS)
+        kw.update(forcing=workloads.wind_forcing(grid), dt_bt=75.0, dtype="float64", project_adv_vel=True,
+                  projection_preconditioner=pre)
+        _, _, _, params, _ = make_solver_global(grid, _physics(workloads.PLAIN_PHYSICS), 1800.0,
+                                                return_params=True, **kw)
+        ua, va = ref_proj._project_column_divergence(_f32(u), _f32(v), params, 1800.0)
+        data[f"{pre}_u"] = _np(ua)
+        data[f"{pre}_v"] = _np(va)
+    np.savez_compressed(os.path.join(HERE, "projection_48x24x10.npz"), **data)
+    print("projection saved")
+
+
 def main():
     make_operator_case()
+    make_projection_case()
     make_seasonal_case()
     make_diagnostics_case()
     # The 0.5 deg production option set, rescaled to a 7.5 deg x 7.5 deg grid
     # whose polar bands are partly wet, from a moving state (2 steps).
     make_step_case("step_plain_48x24x10", 48, 24, 10, 75.0, workloads.PLAIN_PHYSICS,
                    workloads.PLAIN_OPTIONS, 1800.0, 75.0, 30.0, 2, moving=True)
+    # The 0.5 deg preset proper: column projection of the stage-2 advective
+    # velocity on (dynamics/projection.py, step.py:292-303).
+    make_step_case("step_projected_48x24x10", 48, 24, 10, 75.0, workloads.PLAIN_PHYSICS,
+                   dict(workloads.PLAIN_OPTIONS, project_adv_vel=True), 1800.0, 75.0, 30.0, 2, moving=True)
     # Same physics from rest on an all-land-polar grid (production geometry).
     make_step_case("step_plain_rest_64x32x12", 64, 32, 12, 65.0, workloads.PLAIN_PHYSICS,
                    workloads.PLAIN_OPTIONS, 1800.0, 75.0, 30.0, 1, moving=False)

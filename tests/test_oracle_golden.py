@@ -95,7 +95,7 @@ def test_single_operators(ops):
         _check("nl_" + k, nl[k], ops["nl_" + k])
 
 
-@pytest.mark.parametrize("name", ["step_plain_48x24x10", "step_plain_rest_64x32x12",
+@pytest.mark.parametrize("name", ["step_plain_48x24x10", "step_projected_48x24x10", "step_plain_rest_64x32x12",
                                   "step_smoke_90x45x15"])
 def test_full_step(name):
     data = load(name)
@@ -160,3 +160,17 @@ def test_seasonal_blend():
     for n, day in enumerate(data["days"]):
         _check(f"blend5 day {day}", seasonal.blend(data["stack"], float(day), 5.0), data["blend5"][n], 1e-14)
         _check(f"blend0 day {day}", seasonal.blend(data["stack"], float(day), 0.0), data["blend0"][n], 1e-14)
+
+
+@pytest.mark.parametrize("pre", ["none", "jacobi"])
+def test_column_projection(pre):
+    from zhenmode_b200 import workloads
+    data = load("projection_48x24x10")
+    grid = grid_from(data)
+    kw = dict(workloads.PLAIN_OPTIONS)
+    kw.update(forcing=workloads.wind_forcing(grid), dt_bt=75.0, dtype="float64", project_adv_vel=True,
+              projection_preconditioner=pre)
+    p = oparams.build_params(grid, workloads.PLAIN_PHYSICS, 1800.0, **kw)
+    ua, va = ostep.project_column_divergence(data["in_u"], data["in_v"], p, 1800.0)
+    _check("u", ua, data[f"{pre}_u"], 1e-9)
+    _check("v", va, data[f"{pre}_v"], 1e-9)
