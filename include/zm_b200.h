@@ -64,6 +64,10 @@ typedef struct {
 #define ZM_BT_RESIDENT 1
 #define ZM_BT_STREAMING 2
 
+/* Preconditioner of the column projection's CG (projection_preconditioner). */
+#define ZM_PROJ_NONE 0
+#define ZM_PROJ_JACOBI 1
+
 /* PhysicsConfig coefficients (src/zhenmode/model/config.py:86-140) and the
  * make_solver_global options of the mode-split production path
  * (src/zhenmode/model/solver/factory.py:30-68, 397-695). */
@@ -90,6 +94,13 @@ typedef struct {
   const double* coastal_bulk_lambda;
   const double* coastal_kappa_h;
   const double* coastal_kappa_v;
+  /* column-divergence projection of the stage-2 advective velocity
+   * (project_adv_vel; factory.py:366-386, dynamics/projection.py:64-127) */
+  int32_t project_adv_vel;            /* 1: on */
+  int32_t projection_niter;           /* CG iterations per solve, >= 1 */
+  int32_t projection_preconditioner;  /* ZM_PROJ_NONE / ZM_PROJ_JACOBI */
+  int32_t projection_max_refinements; /* 0..2 */
+  double projection_rtol;             /* > 0, or 0 for the default 1e-12; floored at 32 float32 eps */
 } zm_params;
 
 /* JaxStateG fields u, v, T, S, eta (float32, reference layout); device
@@ -156,8 +167,11 @@ int zm_set_forcing_seasonal(zm_solver* s, void* stream, const float* tau_x, cons
  * density part (baroclinic pressure-gradient force minus its barotropic
  * layer average, wet-masked; pressure.py:86-97, 144-180) into out->u/v,
  * 6 = the advection of stage 4 before its longitude filter (latitude
- * filter applied, no wind, no mask) into out->u/v.
- * out->T/S/eta receive the input fields for stages 4 to 6. */
+ * filter applied, no wind, no mask) into out->u/v, 7 = the longitude FFT
+ * filter alone applied to in->u/v, 8 = the column-divergence projection of
+ * in->u/v with the solver's dt (dynamics/projection.py:64-127; needs
+ * project_adv_vel) into out->u/v.
+ * out->T/S/eta receive the input fields for stages 4 to 8. */
 int zm_run_stage(zm_solver* s, void* stream, int32_t stage, const zm_state* in, zm_state* out);
 
 /* Kernel classes reported by zm_profile. */
@@ -174,7 +188,8 @@ int zm_run_stage(zm_solver* s, void* stream, int32_t stage, const zm_state* in, 
 #define ZM_K_BAROTROPIC 10   /* barotropic subcycle */
 #define ZM_K_FINAL 11        /* projection, polar cap, land hold */
 #define ZM_K_CLOSURE 12      /* learned closure: features + tensor-core MLP */
-#define ZM_K_COUNT 13
+#define ZM_K_PROJECTION 13   /* column-divergence projection (right-hand side, CG, correction) */
+#define ZM_K_COUNT 14
 
 /* Advance the resident state by one step without the CUDA graph, timing
  * every kernel launch with CUDA events on `stream`; ms[c] and launches[c]
@@ -191,9 +206,15 @@ int zm_barrier_probe(zm_solver* s, void* stream, int32_t blocks, int32_t expecte
 
 /* Monitor of the resident state after the last zm_advance (runtime/monitor.py:20-30):
  * 0 accepted, 1 non-finite, 3 velocity above 10 m/s, 4 |eta| above 15 m.
- * Returns ZM_ERR_TIMEOUT if a grid barrier of the barotropic kernel gave up
- * (the state is then not a valid step result).  Synchronizes the device. */
+ * Returns ZM_ERR_TIMEOUT if a grid barrier of the barotropic or the column
+ * projection kernel gave up (the state is then not a valid step result).  Synchronizes the device. */
 int zm_status(zm_solver* s, int32_t* monitor_code);
+
+/* CG iterations of the last column projection (needs project_adv_vel):
+ * out[0] the first solve, out[1] and out[2] the refinement solves (0 when not
+ * run), out[3] the refinement solves run.  Writes min(n, 4) values;
+ * synchronizes the device. */
+int zm_projection_stats(zm_solver* s, int32_t* out, int32_t n);
 
 /* The diagnostics closure of make_solver_global (factory.py:752-760) on a
  * state in the caller's device arrays, reference layout (nx, ny, nz) float32:

@@ -10,10 +10,10 @@ from zhenmode_b200.ensemble import Ensemble
 pytestmark = pytest.mark.gpu
 
 
-def _member(nx, ny, nz, seed):
+def _member(nx, ny, nz, seed, **extra):
     import torch
     grid, physics, dt, kw, T, S = workloads.make_case("plain", nx, ny, nz, dtype="float32")
-    step, init, _ = make_solver_global(grid, physics, dt, **kw)
+    step, init, _ = make_solver_global(grid, physics, dt, **dict(kw, **extra))
     rng = np.random.default_rng(seed)
     wet = np.asarray(grid.wet_mask_3d)
     st = init(T + 0.05 * rng.standard_normal(T.shape) * wet, S)
@@ -41,6 +41,23 @@ def test_ensemble_matches_members_alone():
     for a, b in zip(again, got):
         for k in ("u", "v", "T", "S", "eta"):
             assert torch.equal(getattr(a, k), getattr(b, k)), k
+
+
+def test_ensemble_with_projection_matches_members_alone():
+    """Two cooperative kernels per member (column projection, barotropic
+    subcycle), chained across the members inside the one graph."""
+    import torch
+    members = [_member(48, 24, 10, 1, project_adv_vel=True),
+               _member(64, 32, 12, 3, project_adv_vel=True, projection_preconditioner="jacobi")]
+    ens = Ensemble([m[0] for m in members])
+    ens.load([m[1] for m in members])
+    ens.advance(2)
+    got = ens.store()
+    assert ens.monitor_codes() == [0, 0]
+    for (step, st), g in zip(members, got):
+        want = step.advance(st, 2)
+        for k in ("u", "v", "T", "S", "eta"):
+            assert torch.equal(getattr(g, k), getattr(want, k)), k
 
 
 def test_handles_of_different_widths_coexist():

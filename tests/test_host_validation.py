@@ -47,12 +47,32 @@ def test_invalid_grid(case):
         make_solver_global(bad, physics, dt, **kw)
 
 
-@pytest.mark.parametrize("over", [dict(mode_split=False), dict(dtype="float64"), dict(project_adv_vel=True),
+@pytest.mark.parametrize("over", [dict(mode_split=False), dict(dtype="float64"),
                                   dict(sponge_days=10.0, sponge_cells=3), dict(dynamic_ice=True),
                                   dict(mixed_layer_depth_m=50.0)])
 def test_unsupported_options(case, over):
     with pytest.raises(UnsupportedOption):
         _call(case, **over)
+
+
+@pytest.mark.parametrize("over", [dict(projection_niter=0), dict(projection_niter=True), dict(projection_niter=2.5),
+                                  dict(projection_rtol=0.0), dict(projection_rtol=float("nan")),
+                                  dict(projection_preconditioner="ilu"), dict(projection_max_refinements=3),
+                                  dict(projection_max_refinements=-1)])
+def test_invalid_projection_options(case, over):
+    """factory.py:377-384: the projection options are checked whether or not it is on."""
+    with pytest.raises(ValueError):
+        _call(case, **over)
+
+
+def test_projection_niter_environment(case, monkeypatch):
+    """factory.py:368-376: OCEAN_PAV_NITER stands in for projection_niter=None."""
+    monkeypatch.setenv("OCEAN_PAV_NITER", "many")
+    with pytest.raises(ValueError, match="environment"):
+        _call(case, project_adv_vel=True)
+    monkeypatch.setenv("OCEAN_PAV_NITER", "0")
+    with pytest.raises(ValueError, match="positive"):
+        _call(case, project_adv_vel=True)
 
 
 def test_unknown_scheme_keyword(case):

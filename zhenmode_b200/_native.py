@@ -20,7 +20,7 @@ ZM_ERR_TIMEOUT = 4
 ZM_ERR_MONITOR = 5
 
 KERNEL_CLASSES = ("nu_sub", "inner_lap", "lin_finish", "implicit", "fz", "madv", "dealias", "tracer_adv",
-                  "tracer_rest", "pgf", "barotropic", "final", "closure")
+                  "tracer_rest", "pgf", "barotropic", "final", "closure", "projection")
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _fp = ctypes.POINTER(ctypes.c_float)
@@ -47,7 +47,10 @@ class ZmParams(ctypes.Structure):
                 ("bt_kernel", ctypes.c_int32), ("autotune", ctypes.c_int32),
                 ("tau_x", _dp), ("tau_y", _dp), ("q_heat", _dp), ("t_atm", _dp), ("s_ref", _dp),
                 ("coastal_restore_coef", _dp), ("coastal_restore_t", _dp),
-                ("coastal_bulk_lambda", _dp), ("coastal_kappa_h", _dp), ("coastal_kappa_v", _dp)]
+                ("coastal_bulk_lambda", _dp), ("coastal_kappa_h", _dp), ("coastal_kappa_v", _dp),
+                ("project_adv_vel", ctypes.c_int32), ("projection_niter", ctypes.c_int32),
+                ("projection_preconditioner", ctypes.c_int32), ("projection_max_refinements", ctypes.c_int32),
+                ("projection_rtol", ctypes.c_double)]
 
 
 class ZmState(ctypes.Structure):
@@ -74,6 +77,7 @@ EXPORTS = {
     "zm_barrier_probe": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.c_int32]),
     "zm_status": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
+    "zm_projection_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32]),
     "zm_diagnostics": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ZmState), ctypes.c_void_p,
                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "zm_mlp_forward_bf16": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32] + [ctypes.c_void_p] * 8

@@ -25,49 +25,11 @@
 // Every grid barrier polls with a bounded count; if it runs out the kernel
 // records ZM_BT_ERR_BARRIER in *err and every block returns.
 #include "zm_kernels.cuh"
+#include "zm_sync.cuh"
 
 namespace zm {
 
 namespace {
-
-__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-
-// Grid-wide barrier over co-resident blocks: arrival counter + generation.
-// Returns false (and sets *err) if the wait exceeded its poll limit.
-__device__ bool grid_barrier(unsigned* bar, unsigned* err, unsigned nblocks, unsigned max_polls) {
-  __syncthreads();
-  __shared__ int ok;
-  if (threadIdx.x == 0) {
-    ok = 1;
-    unsigned* count = bar;
-    unsigned* gen = bar + 1;
-    const unsigned my_gen = ld_acquire(gen);
-    __threadfence();
-    const unsigned arrived = atomicAdd(count, 1u);
-    if (arrived == nblocks - 1) {
-      *count = 0u;
-      __threadfence();
-      atomicAdd(gen, 1u);
-    } else {
-      unsigned polls = 0;
-      while (ld_acquire(gen) == my_gen) {
-        if (++polls > max_polls || ld_acquire(err) != 0u) {
-          atomicOr(err, ZM_BT_ERR_BARRIER);
-          ok = 0;
-          break;
-        }
-        __nanosleep(64);
-      }
-    }
-    __threadfence();
-  }
-  __syncthreads();
-  return ok != 0;
-}
 
 // band-row index of row j (0..2nb-1), or -1 outside the cap bands
 __device__ __forceinline__ int band_of(int ny, int nb, int j) {

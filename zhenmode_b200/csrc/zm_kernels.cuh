@@ -117,6 +117,29 @@ __global__ void k_final(Dev d, const float* u3, const float* v3, const float* T3
                         const double* ubt0, const double* vbt, const double* vbt0, const float* u0, const float* v0,
                         const float* T0, const float* S0, const float* means, const float* wts, int nb_rows,
                         float* uo, float* vo, float* To, float* So);
+// column-divergence projection of the stage-2 advective velocity (zm_projection.cu)
+constexpr int PJ_THREADS = 1024;
+#define ZM_PJ_SUMS 4
+struct ProjArgs {
+  const double* cx;     // [3][ny][P] weights of D_{i-1}, D_i, D_{i+1} in the east-face column flux
+  const double* cy;     // [3][ny][P] weights of E_{j-1}, E_j, E_{j+1} in the north-face column flux
+  const double* sxy;    // [2][ny][P] area / dx, area / (dy cos)
+  const double* minv;   // Jacobi inverse diagonal [ny][P], or null (no preconditioner)
+  const double* rarea;  // 1 / area on wet columns, 0 elsewhere
+  const double* b;      // right-hand side -(coldiv / (dt g)) area
+  double *psi, *x, *r, *z, *p0, *p1, *Ap;
+  double* part;         // [blocks][ZM_PJ_SUMS] block partial sums
+  unsigned *bar, *err;
+  int* stats;           // iterations of each solve (3), refinement solves run
+  double tol2, trtol2;  // tol^2, transport rtol^2
+  int niter, refinements;
+};
+__global__ void k_proj_coef(Dev d, const double* dzn, const double* cosd, const double* area, double* cx, double* cy,
+                            double* sxy, double* minv, double* rarea);
+__global__ void k_proj_rhs(Dev d, const float* u, const float* v, const double* dzn, const double* cosd,
+                           const double* area, double dtg, double* b);
+__global__ void k_proj_cg(Dev d, ProjArgs a);
+__global__ void k_proj_correct(Dev d, float* u, float* v, const double* psi, const double* cosd, double dtg);
 __global__ void k_ref_to_int3(Dev d, const float* src, float* dst, float offset);
 __global__ void k_int_to_ref3(Dev d, const float* src, float* dst, float offset);
 __global__ void k_ref_to_int2(Dev d, const float* src, float* dst);

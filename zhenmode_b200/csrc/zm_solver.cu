@@ -76,6 +76,12 @@ struct zm_solver {
   float* kappa3 = nullptr;       // [nz-1][ny][P] diffusivity per interface
   unsigned* cl_count = nullptr;  // [0] fallback columns of the last step, [1] tensor-core wait errors
   float cl_bound = 8.f;
+  // column-divergence projection of the stage-2 advective velocity (off unless project_adv_vel)
+  bool proj_on = false;
+  ProjArgs pj{};
+  int pj_blocks = 0;
+  double pj_dtg = 0.0;
+  double *pj_dzn = nullptr, *pj_cos = nullptr, *pj_area = nullptr;
   float *up = nullptr, *vp = nullptr;
   float *frx = nullptr, *fry = nullptr, *means = nullptr, *wts = nullptr;
   double *ubt0 = nullptr, *vbt0 = nullptr, *ubt[2] = {nullptr, nullptr}, *vbt[2] = {nullptr, nullptr};
@@ -267,6 +273,41 @@ struct zm_solver {
     ZM_CUDA(cudaMemcpyAsync(dst.S, src.S, n3 * sizeof(float), cudaMemcpyDeviceToDevice, s));
   }
 
+  // A cooperative launch.  Inside an ensemble capture it waits for the
+  // previous member's cooperative kernels (bt_wait) and records bt_done, so
+  // that no two grid-barrier kernels are resident at the same time.
+  template <class... A>
+  void coop_launch(cudaStream_t s, int cls, void (*kern)(A...), int blocks, int threads, size_t smem,
+                   A... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (bt_wait) ZM_CUDA(cudaStreamWaitEvent(s, bt_wait, 0));
+    pb(cls, s);
+    ZM_CUDA(cudaLaunchKernelEx(&cfg, kern, args...));
+    pe(s);
+    if (bt_done) ZM_CUDA(cudaEventRecord(bt_done, s));
+  }
+
+  // Column-divergence projection of (u, v) in place (projection.py:64-127).
+  void project(cudaStream_t s, float* u, float* v) {
+    const dim3 c(32, 8);
+    pb(ZM_K_PROJECTION, s);
+    k_proj_rhs<<<grid2(c), c, 0, s>>>(d, u, v, pj_dzn, pj_cos, pj_area, pj_dtg, const_cast<double*>(pj.b));
+    pe(s);
+    coop_launch(s, ZM_K_PROJECTION, k_proj_cg, pj_blocks, PJ_THREADS, 0, d, pj);
+    pb(ZM_K_PROJECTION, s);
+    k_proj_correct<<<grid2(c), c, 0, s>>>(d, u, v, pj.psi, pj_cos, pj_dtg);
+    pe(s);
+  }
+
   // Nonlinear RK2 step N(dt): src -> dst.
   void nonlinear(cudaStream_t s, const Fields4& src, const Fields4& dst) {
     const dim3 c(32, 4);
@@ -281,6 +322,7 @@ struct zm_solver {
     const float* u2 = src.u;
     const float* v2 = src.v;
     if (!freeze) {
+      if (proj_on) project(s, up, vp);  // step.py:292-303
       pb(ZM_K_FZ, s);
       k_fz<<<grid2(c), c, 0, s>>>(d, up, vp, Fz);
       pe(s);
@@ -309,21 +351,7 @@ struct zm_solver {
     if (bt_blocks > 0) {
       BtArgs a2 = bt;
       a2.eta_out = eta_out;
-      cudaLaunchConfig_t cfg = {};
-      cfg.gridDim = dim3(bt_blocks);
-      cfg.blockDim = dim3(BT_THREADS);
-      cfg.dynamicSmemBytes = bt_tile_smem();
-      cfg.stream = s;
-      cudaLaunchAttribute attr[1];
-      attr[0].id = cudaLaunchAttributeCooperative;
-      attr[0].val.cooperative = 1;
-      cfg.attrs = attr;
-      cfg.numAttrs = 1;
-      if (bt_wait) ZM_CUDA(cudaStreamWaitEvent(s, bt_wait, 0));
-      pb(ZM_K_BAROTROPIC, s);
-      ZM_CUDA(cudaLaunchKernelEx(&cfg, k_bt_loop, d, a2));
-      pe(s);
-      if (bt_done) ZM_CUDA(cudaEventRecord(bt_done, s));
+      coop_launch(s, ZM_K_BAROTROPIC, k_bt_loop, bt_blocks, BT_THREADS, bt_tile_smem(), d, a2);
       ubt_fin = bt.ubt_out;
       vbt_fin = bt.vbt_out;
     } else {
@@ -836,6 +864,70 @@ void build(zm_solver* s, const zm_grid* g, const zm_params* p) {
     a.bar = s->bt_sync;
     a.err = s->bt_sync + 2;
   }
+  // projection options are validated whether or not the projection is on (factory.py:368-386)
+  require(p->projection_niter > 0, ZM_ERR_INVALID, "projection_niter must be a positive integer");
+  require(std::isfinite(p->projection_rtol) && p->projection_rtol >= 0.0, ZM_ERR_INVALID,
+          "projection_rtol must be finite and positive");
+  require(p->projection_preconditioner == ZM_PROJ_NONE || p->projection_preconditioner == ZM_PROJ_JACOBI,
+          ZM_ERR_INVALID, "projection_preconditioner must be none or jacobi");
+  require(p->projection_max_refinements >= 0 && p->projection_max_refinements <= 2, ZM_ERR_INVALID,
+          "projection_max_refinements must be an integer from 0 to 2");
+  if (p->project_adv_vel && !p->freeze_adv_vel) {
+    // column projection (projection.py:10-127): tolerances with the float32 floors
+    const double eps32 = 1.1920928955078125e-07;
+    const double tol = std::max(p->projection_rtol > 0.0 ? p->projection_rtol : 1e-12, 32.0 * eps32);
+    const double trtol = std::max(1e-10, 32.0 * eps32);
+    int per_sm = 0, sms = 0, coop = 0;
+    ZM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_proj_cg, PJ_THREADS, 0));
+    ZM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
+    ZM_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, s->device));
+    require(coop && per_sm >= 1, ZM_ERR_UNSUPPORTED, "the column projection needs a cooperative launch");
+    s->pj_blocks = std::max(1, std::min(sms, (int)(((long long)nx * ny + PJ_THREADS - 1) / PJ_THREADS)));
+    std::vector<double> dzn(nz), cosd(ny), area(s->n2, 0.0);
+    for (int k = 0; k < nz; ++k) {
+      if (k == 0) dzn[k] = std::fabs(g->z[1] - g->z[0]);
+      else if (k == nz - 1) dzn[k] = std::fabs(g->z[nz - 1] - g->z[nz - 2]);
+      else dzn[k] = 0.5 * (std::fabs(g->z[k] - g->z[k - 1]) + std::fabs(g->z[k + 1] - g->z[k]));
+    }
+    for (int j = 0; j < ny; ++j) cosd[j] = g->cos_lat[j];
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        const size_t r = (size_t)i * ny + j;
+        area[(size_t)j * P + i] = g->dx_2d[r] * g->dy * g->wet_mask[r];
+      }
+    s->pj_dzn = s->upload(dzn);
+    s->pj_cos = s->upload(cosd);
+    s->pj_area = s->upload(area);
+    ProjArgs& a = s->pj;
+    double* cx = s->alloc<double>(3 * s->n2);
+    double* cy = s->alloc<double>(3 * s->n2);
+    double* sxy = s->alloc<double>(2 * s->n2);
+    double* minv = p->projection_preconditioner == ZM_PROJ_JACOBI ? s->alloc<double>(s->n2) : nullptr;
+    double* rarea = s->alloc<double>(s->n2);
+    const dim3 c(32, 8);
+    k_proj_coef<<<s->grid2(c), c>>>(s->d, s->pj_dzn, s->pj_cos, s->pj_area, cx, cy, sxy, minv, rarea);
+    s->check_launch();
+    a.cx = cx; a.cy = cy; a.sxy = sxy; a.minv = minv; a.rarea = rarea;
+    a.b = s->alloc<double>(s->n2);
+    a.psi = s->alloc<double>(s->n2);
+    a.x = s->alloc<double>(s->n2);
+    a.r = s->alloc<double>(s->n2);
+    a.z = s->alloc<double>(s->n2);
+    a.p0 = s->alloc<double>(s->n2);
+    a.p1 = s->alloc<double>(s->n2);
+    a.Ap = s->alloc<double>(s->n2);
+    a.part = s->alloc<double>((size_t)2 * s->pj_blocks * ZM_PJ_SUMS);
+    unsigned* sync = s->alloc<unsigned>(4);
+    a.bar = sync;
+    a.err = sync + 2;
+    a.stats = s->alloc<int>(4);
+    a.tol2 = tol * tol;
+    a.trtol2 = trtol * trtol;
+    a.niter = p->projection_niter;
+    a.refinements = p->projection_max_refinements;
+    s->pj_dtg = p->dt * 9.81;
+    s->proj_on = true;
+  }
   const size_t nref3 = (size_t)nx * ny * nz;
   s->ref = Fields4{s->alloc<float>(nref3), s->alloc<float>(nref3), s->alloc<float>(nref3), s->alloc<float>(nref3)};
   s->ref_eta = s->alloc<float>((size_t)nx * ny);
@@ -1147,7 +1239,8 @@ int zm_set_forcing_seasonal(zm_solver* s, void* stream, const float* tau_x, cons
 }
 
 int zm_run_stage(zm_solver* s, void* stream, int32_t stage, const zm_state* in, zm_state* out) {
-  if (!s || !in || !out || stage < 1 || stage > 7) return ZM_ERR_INVALID;
+  if (!s || !in || !out || stage < 1 || stage > 8) return ZM_ERR_INVALID;
+  if (stage == 8 && !s->proj_on) return fail(s, Err{ZM_ERR_INVALID, "stage 8 needs project_adv_vel"});
   cudaStream_t st = (cudaStream_t)stream;
   try {
     s->load(st, in, s->st[s->cur], s->eta[s->cur]);
@@ -1167,6 +1260,9 @@ int zm_run_stage(zm_solver* s, void* stream, int32_t stage, const zm_state* in, 
     } else if (stage == 6) {
       s->momentum_advection_part(st, s->st[a]);
       s->copy_uv(st, s->Ayu, s->Ayv, s->st[a], s->st[b]);
+    } else if (stage == 8) {
+      s->project(st, s->st[a].u, s->st[a].v);
+      s->copy_uv(st, s->st[a].u, s->st[a].v, s->st[a], s->st[b]);
     } else {
       const int nlines = s->ny * s->nz;
       k_dealias_lon<<<(nlines + s->fft_lines - 1) / s->fft_lines, 256, s->fft_smem, st>>>(
@@ -1412,6 +1508,21 @@ int zm_status(zm_solver* s, int32_t* monitor_code) {
   e = cudaMemcpy(&berr, s->bt.err, sizeof(berr), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return fail(s, Err{ZM_ERR_CUDA, std::string("zm_status: ") + cudaGetErrorString(e)});
   if (berr) return fail(s, Err{ZM_ERR_TIMEOUT, "barotropic grid barrier timed out"});
+  if (s->proj_on) {
+    e = cudaMemcpy(&berr, s->pj.err, sizeof(berr), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return fail(s, Err{ZM_ERR_CUDA, std::string("zm_status: ") + cudaGetErrorString(e)});
+    if (berr) return fail(s, Err{ZM_ERR_TIMEOUT, "column projection grid barrier timed out"});
+  }
+  return ZM_OK;
+}
+
+int zm_projection_stats(zm_solver* s, int32_t* out, int32_t n) {
+  if (!s || !out || n < 0) return ZM_ERR_INVALID;
+  if (!s->proj_on) return fail(s, Err{ZM_ERR_INVALID, "the column projection is off"});
+  int v[4] = {0, 0, 0, 0};
+  const cudaError_t e = cudaMemcpy(v, s->pj.stats, sizeof(v), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return fail(s, Err{ZM_ERR_CUDA, std::string("zm_projection_stats: ") + cudaGetErrorString(e)});
+  for (int q = 0; q < n && q < 4; ++q) out[q] = v[q];
   return ZM_OK;
 }
 

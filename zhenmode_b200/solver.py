@@ -19,6 +19,7 @@ import ctypes
 import dataclasses
 import math
 import numbers
+import os
 
 import numpy as np
 
@@ -148,6 +149,11 @@ class _Solver:
         p.vertical_diffusion = 1 if opts["vertical_diffusion"] == "implicit" else 0
         p.bt_kernel = _BT_KERNELS[opts["barotropic_kernel"]]
         p.autotune = 1 if opts.get("autotune") else 0
+        p.project_adv_vel = int(bool(opts.get("project_adv_vel", False)))
+        p.projection_niter = int(opts.get("projection_niter", 150))
+        p.projection_preconditioner = 1 if opts.get("projection_preconditioner", "none") == "jacobi" else 0
+        p.projection_max_refinements = int(opts.get("projection_max_refinements", 2))
+        p.projection_rtol = float(opts.get("projection_rtol", 0.0))
         for name in ("tau_x", "tau_y", "q_heat", "t_atm", "s_ref", "coastal_restore_coef",
                      "coastal_restore_t", "coastal_bulk_lambda", "coastal_kappa_h", "coastal_kappa_v"):
             setattr(p, name, _native.dptr(arr(opts["fields"].get(name), (nx, ny))))
@@ -333,9 +339,15 @@ def make_solver_global(grid, physics, dt, forcing=None,
         raise ValueError("reference column geometry requires conservative_kv=True and localize_conv=True")
     if polar_cap_rows > 0 and 2 * (polar_cap_rows + polar_cap_taper) > grid.ny:
         raise ValueError('polar cap bands must not overlap; reduce rows/taper or disable the cap')
-    if projection_niter is not None and (isinstance(projection_niter, (bool, np.bool_))
-                                         or not isinstance(projection_niter, (int, np.integer))
-                                         or projection_niter <= 0):
+    if projection_niter is None:
+        # factory.py:368-376: the legacy environment cap, resolved once here
+        legacy_cap = os.environ.get('OCEAN_PAV_NITER')
+        try:
+            projection_niter = 150 if legacy_cap is None else int(legacy_cap)
+        except ValueError as error:
+            raise ValueError('projection_niter environment value must be an integer') from error
+    if (isinstance(projection_niter, (bool, np.bool_)) or not isinstance(projection_niter, (int, np.integer))
+            or projection_niter <= 0):
         raise ValueError('projection_niter must be a positive integer')
     if projection_rtol is not None and (not np.isfinite(projection_rtol) or projection_rtol <= 0.):
         raise ValueError('projection_rtol must be finite and positive')
@@ -367,8 +379,6 @@ def make_solver_global(grid, physics, dt, forcing=None,
         unsupported.append('non-legacy column geometry or process time scheme')
     if any(schemes.get(k, v) != v for k, v in _DEFAULTS.items() if k in schemes):
         unsupported.append('non-default numerical scheme options')
-    if project_adv_vel:
-        unsupported.append('project_adv_vel (column-divergence projection)')
     if physics.thermodynamics != 'linear':
         unsupported.append('TEOS-10 thermodynamics')
     if physics.kappa_gm > 0 or physics.kappa_redi > 0:
@@ -423,7 +433,11 @@ def make_solver_global(grid, physics, dt, forcing=None,
                 polar_cap_rows=polar_cap_rows, polar_cap_taper=polar_cap_taper, fct_adv=fct_adv,
                 monotone_adv=monotone_adv, localize_conv=localize_conv, conservative_kv=conservative_kv,
                 freeze_adv_vel=freeze_adv_vel, vertical_diffusion=vertical_diffusion,
-                barotropic_kernel=barotropic_kernel, autotune=bool(autotune), fields=fields)
+                barotropic_kernel=barotropic_kernel, autotune=bool(autotune), fields=fields,
+                project_adv_vel=bool(project_adv_vel), projection_niter=int(projection_niter),
+                projection_preconditioner=projection_preconditioner,
+                projection_max_refinements=int(projection_max_refinements),
+                projection_rtol=0.0 if projection_rtol is None else float(projection_rtol))
     solver = _Solver(grid, physics, dt, opts)
     wet3 = np.asarray(getattr(grid, 'wet_mask_3d', None) if getattr(grid, 'wet_mask_3d', None) is not None
                       else np.broadcast_to(np.asarray(grid.wet_mask)[:, :, None], (nx, ny, nz)), dtype=np.float64)
@@ -561,6 +575,13 @@ def make_solver_global(grid, physics, dt, forcing=None,
             solver.check(rc, "zm_closure_stats")
         return int(fb.value), int(er.value)
 
+    def projection_stats():
+        """CG iterations of the last column projection: (first solve, refinement 1,
+        refinement 2, refinement solves run)."""
+        out = (ctypes.c_int32 * 4)()
+        solver.check(solver.lib.zm_projection_stats(solver.handle, out, 4), "zm_projection_stats")
+        return tuple(int(x) for x in out)
+
     def set_forcing(tau_x=None, tau_y=None, q_heat=None):
         """Replace the 2-D forcing of the following steps ((nx, ny) fields)."""
         import torch
@@ -598,6 +619,7 @@ def make_solver_global(grid, physics, dt, forcing=None,
     step.closure_features = closure_features
     step.closure_kappa = closure_kappa
     step.closure_stats = closure_stats
+    step.projection_stats = projection_stats
     step.closure_params = None
     result = [step, init_state, diagnostics]
     if return_params:
