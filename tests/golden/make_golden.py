@@ -267,7 +267,42 @@ def make_projection_case(seed=13):
     print("projection saved")
 
 
+def make_restart_case():
+    """A checkpoint written by the reference's save_restart
+    (model/io/restart.py:153-179) for a plain-dict contract, with the inputs
+    that made it, so the restart module's file format is pinned both ways."""
+    from zhenmode.model.io.restart import make_restart_contract, save_restart
+    from collections import namedtuple
+    grid = workloads.build_grid(8, 6, 4, land_lat=70.0)
+    rng = np.random.default_rng(21)
+    shape = (8, 6, 4)
+    state = dict(u=rng.standard_normal(shape).astype(np.float32), v=rng.standard_normal(shape).astype(np.float32),
+                 T=(10 + rng.standard_normal(shape)).astype(np.float32),
+                 S=(35 + 0.1 * rng.standard_normal(shape)).astype(np.float32),
+                 eta=rng.standard_normal(shape[:2]).astype(np.float32), ice=np.zeros(shape[:2], np.float32))
+    params = namedtuple("Params", ["dt", "nu_h", "polar_cap_rows"])(1800.0, 2.5e4, 2)
+    forcing = {"tau_x": rng.standard_normal(shape[:2]), "heat": np.zeros(shape[:2])}
+    controls = {"calendar": "360_day", "blend_days": 5.0}
+    execution = {"backend": "cpu", "devices": 1}
+    contract = make_restart_contract(grid, params, dtype="float32", forcing=forcing, controls=controls,
+                                     code_paths={}, execution=execution)
+    cumulative = {"heat": np.array([1.5, -2.25]), "salt": np.array([3.0])}
+    history = {"days": np.array([0.0, 1.0, 2.0]), "sst_mean": np.array([15.1, 15.2, 15.3])}
+    path = os.path.join(HERE, "restart_reference.npz")
+    save_restart(path, state, contract, step=96, counters={"n_snaps": 3}, cumulative=cumulative,
+                 history=history, outputs={"out/global.npz": "ab" * 32})
+    inputs = dict(grid_nx=8, grid_ny=6, grid_nz=4, land_lat=70.0, seed=21)
+    np.savez_compressed(os.path.join(HERE, "restart_inputs.npz"),
+                        **{f"state_{k}": v for k, v in state.items()},
+                        **{f"forcing_{k}": v for k, v in forcing.items()},
+                        **{f"cumulative_{k}": v for k, v in cumulative.items()},
+                        **{f"history_{k}": v for k, v in history.items()},
+                        **{k: np.asarray(v) for k, v in inputs.items()})
+    print("restart saved")
+
+
 def main():
+    make_restart_case()
     make_operator_case()
     make_projection_case()
     make_seasonal_case()

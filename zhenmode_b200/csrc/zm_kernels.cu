@@ -1167,8 +1167,14 @@ __global__ void __launch_bounds__(256) k_final(Dev d, const float* __restrict__ 
   }
   uo[id] = u;
   vo[id] = (j == 0 || j == d.ny - 1) ? 0.f : v;
-  To[id] = T;
-  So[id] = S;
+  // The step hands back absolute float32 tracers, T = anomaly + T_ref, and
+  // reads them back as T - T_ref.  Keeping the anomaly that this round trip
+  // gives (a fixed point of it for every float32 anomaly) makes the resident
+  // state after each step exactly the one reloaded from the step's output, so
+  // several steps on the device equal the same steps through the host state
+  // and a restart from a saved state continues bit for bit.
+  To[id] = __fsub_rn(__fadd_rn(T, d.T_ref), d.T_ref);
+  So[id] = __fsub_rn(__fadd_rn(S, d.S_ref), d.S_ref);
 }
 
 // ------------------------------------------------------------------ layout conversion
