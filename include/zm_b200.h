@@ -101,6 +101,14 @@ typedef struct {
   int32_t projection_preconditioner;  /* ZM_PROJ_NONE / ZM_PROJ_JACOBI */
   int32_t projection_max_refinements; /* 0..2 */
   double projection_rtol;             /* > 0, or 0 for the default 1e-12; floored at 32 float32 eps */
+  /* lateral sponge (factory.py:456-491; step.py:142-156; barotropic.py:22-41):
+   * NULL sponge_rate or all zeros is off; when on, T_clim and S_clim are required */
+  const double* sponge_rate;          /* (nx, ny) Rayleigh rate [1/s] */
+  const double* T_clim;               /* (nx, ny, nz) relaxation targets */
+  const double* S_clim;
+  /* semi-enclosed-sea eta relaxation (factory.py:493-521): off when the rate is 0 or the mask NULL */
+  const double* eta_relax_mask;       /* (nx, ny) in [0, 1] */
+  double eta_relax_rate;              /* [1/s] */
 } zm_params;
 
 /* JaxStateG fields u, v, T, S, eta (float32, reference layout); device

@@ -135,6 +135,37 @@ def make_step_case(name, nx, ny, nz, land_lat, physics, options, dt, dt_bt, rest
     print(name, "saved", {k: v.shape for k, v in data.items() if hasattr(v, 'shape') and v.ndim > 1})
 
 
+def make_sponge_case(name="step_sponge_48x24x10", seed=7):
+    """The step with the lateral sponge toward the initial fields and a
+    mass-conserving eta relaxation box (factory.py:456-521, step.py:142-156,
+    barotropic.py:22-41), strong enough to act within two steps."""
+    nx, ny, nz = 48, 24, 10
+    grid = workloads.build_grid(nx, ny, nz, land_lat=75.0)
+    T, S = workloads.initial_fields(grid, perturb_sigma=0.2)
+    lon, lat = np.asarray(grid.lon), np.asarray(grid.lat)
+    extra = dict(sponge_days=0.5, sponge_cells=4, eta_relax_days=0.25,
+                 eta_relax_box=(float(lon[10]), float(lon[20]), float(lat[8]), float(lat[14])), eta_relax_buffer=10.0)
+    options = dict(workloads.PLAIN_OPTIONS, **extra)
+    kw = dict(options, forcing=workloads.wind_forcing(grid), dt_bt=75.0, dtype="float64", T_init=T, S_init=S)
+    step, init, _, params, _ = make_solver_global(grid, _physics(workloads.PLAIN_PHYSICS), 1800.0,
+                                                  return_params=True, **kw)
+    u, v, T0, S0, eta = _moving_state(grid, T, S, seed)
+    st = JaxStateG(*[_f32(a) for a in (u, v, T0, S0, eta)], np.zeros((nx, ny)))
+    outs = _run_steps(step, st, 2)
+    data = dict(_grid_arrays(grid))
+    data.update(in_u=_np(st.u), in_v=_np(st.v), in_T=_np(st.T), in_S=_np(st.S), in_eta=_np(st.eta),
+                clim_T=_np(T), clim_S=_np(S), dt=np.float64(1800.0), dt_bt=np.float64(75.0),
+                restore_days=np.float64(0.0), nsteps=np.int64(2), n_subcyc=np.int64(params.n_subcyc),
+                adv_nsub=np.int64(params.adv_nsub), conv_nsub=np.int64(params.conv_nsub),
+                physics=np.array(repr(dataclasses.asdict(workloads.PLAIN_PHYSICS))),
+                options=np.array(repr(options)))
+    for n, s in enumerate(outs, start=1):
+        for key in ("u", "v", "T", "S", "eta"):
+            data[f"out{n}_{key}"] = _np(getattr(s, key))
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **data)
+    print(name, "saved")
+
+
 def make_operator_case(seed=11):
     """Single-operator goldens on a 24x16x6 grid with land blocks and a wet
     polar band, random fields (reference functions called directly)."""
@@ -302,6 +333,7 @@ def make_restart_case():
 
 
 def main():
+    make_sponge_case()
     make_restart_case()
     make_operator_case()
     make_projection_case()

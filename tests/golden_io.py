@@ -39,6 +39,8 @@ def case_inputs(data):
     if restore > 0:
         options.update(coastal_restore_mask=np.asarray(grid.wet_mask), coastal_restore_days=restore,
                        coastal_restore_T=np.array(data["in_T"][:, :, 0]))
+    if "clim_T" in data:  # the sponge's relaxation targets (factory.py:470-483)
+        options.update(T_init=data["clim_T"], S_init=data["clim_S"])
     state = {k: data["in_" + k] for k in ("u", "v", "T", "S", "eta")}
     return grid, physics, float(data["dt"]), options, state
 

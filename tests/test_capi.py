@@ -32,5 +32,5 @@ def test_struct_layouts():
     assert ctypes.sizeof(_native.ZmState) == 5 * 8
     p = _native.ZmParams
     assert p.tau_x.offset % 8 == 0
-    assert ctypes.sizeof(p) == 16 * 8 + 10 * 4 + 10 * 8 + 4 * 4 + 8
+    assert ctypes.sizeof(p) == 16 * 8 + 10 * 4 + 10 * 8 + 4 * 4 + 8 + 4 * 8 + 8
     assert p.projection_rtol.offset % 8 == 0

@@ -65,7 +65,8 @@ def test_full_step_matches_oracle_on_moving_state(operator_case):
     assert max(errs.values()) < STEP_TOL, errs
 
 
-@pytest.mark.parametrize("name", ["step_plain_48x24x10", "step_plain_rest_64x32x12", "step_smoke_90x45x15"])
+@pytest.mark.parametrize("name", ["step_plain_48x24x10", "step_sponge_48x24x10", "step_plain_rest_64x32x12",
+                                  "step_smoke_90x45x15"])
 def test_steps_match_reference_goldens(name):
     data = load(name)
     grid, physics, dt, options, state = case_inputs(data)
@@ -156,7 +157,7 @@ def test_pressure_part_matches_oracle(shape):
 
 
 
-def _polar_case(nx, ny, nz, land_lat, barotropic_kernel="auto"):
+def _polar_case(nx, ny, nz, land_lat, barotropic_kernel="auto", **extra):
     """The 0.5-degree option set on a grid whose polar cap band rows are all
     land (land_lat = 65: the barotropic polar cap is the identity) or partly
     ocean (land_lat = 87 on a 1.9-degree grid: the cap averages wet band
@@ -168,6 +169,9 @@ def _polar_case(nx, ny, nz, land_lat, barotropic_kernel="auto"):
     kw.update(forcing=workloads.wind_forcing(grid), dt_bt=wl.dt_bt,
               coastal_restore_mask=np.asarray(grid.wet_mask), coastal_restore_days=wl.restore_days,
               coastal_restore_T=np.array(T[:, :, 0]), barotropic_kernel=barotropic_kernel)
+    if extra.pop("sponge_targets", False):
+        kw.update(T_init=T, S_init=S)
+    kw.update(extra)
     gpu, p = gu.build_pair(grid, wl.physics, wl.dt, kw)
     from oracle.params import init_state
     st = init_state(p, T, S)
@@ -190,6 +194,22 @@ def test_barotropic_paths_match_oracle(land_lat, kernel, resident, cap):
     solver = gpu.solver
     assert (solver.bt_blocks > 0) == resident
     assert bool(solver.bt_cap_active) == cap
+    want = ostep.step(dict(st), p)
+    got = gu.run_steps(gpu, st, 1)
+    errs = gu.errors(got, want)
+    assert max(errs.values()) < STEP_TOL, errs
+
+
+@pytest.mark.parametrize("kernel,resident", [("auto", True), ("streaming", False)])
+def test_sponge_and_eta_relaxation_match_oracle(kernel, resident):
+    """Lateral sponge toward the initial fields in the L half steps and on the
+    barotropic mode, and an eta relaxation box, each with the uniform refill
+    of the removed volume (barotropic.py:22-41), on both barotropic paths."""
+    grid_lon = np.linspace(-180.0, 180.0, 192, endpoint=False)
+    gpu, p, st = _polar_case(192, 96, 8, 87.0, kernel, sponge_targets=True, sponge_days=0.5, sponge_cells=6,
+                             eta_relax_days=0.25, eta_relax_box=(float(grid_lon[40]), float(grid_lon[70]), 10.0, 30.0),
+                             eta_relax_buffer=6.0)
+    assert (gpu.solver.bt_blocks > 0) == resident
     want = ostep.step(dict(st), p)
     got = gu.run_steps(gpu, st, 1)
     errs = gu.errors(got, want)

@@ -48,7 +48,7 @@ def test_invalid_grid(case):
 
 
 @pytest.mark.parametrize("over", [dict(mode_split=False), dict(dtype="float64"),
-                                  dict(sponge_days=10.0, sponge_cells=3), dict(dynamic_ice=True),
+                                  dict(dynamic_ice=True),
                                   dict(mixed_layer_depth_m=50.0)])
 def test_unsupported_options(case, over):
     with pytest.raises(UnsupportedOption):

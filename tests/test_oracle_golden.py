@@ -95,8 +95,8 @@ def test_single_operators(ops):
         _check("nl_" + k, nl[k], ops["nl_" + k])
 
 
-@pytest.mark.parametrize("name", ["step_plain_48x24x10", "step_projected_48x24x10", "step_plain_rest_64x32x12",
-                                  "step_smoke_90x45x15"])
+@pytest.mark.parametrize("name", ["step_plain_48x24x10", "step_projected_48x24x10", "step_sponge_48x24x10",
+                                  "step_plain_rest_64x32x12", "step_smoke_90x45x15"])
 def test_full_step(name):
     data = load(name)
     grid, physics, dt, options, state = case_inputs(data)

@@ -50,7 +50,9 @@ class ZmParams(ctypes.Structure):
                 ("coastal_bulk_lambda", _dp), ("coastal_kappa_h", _dp), ("coastal_kappa_v", _dp),
                 ("project_adv_vel", ctypes.c_int32), ("projection_niter", ctypes.c_int32),
                 ("projection_preconditioner", ctypes.c_int32), ("projection_max_refinements", ctypes.c_int32),
-                ("projection_rtol", ctypes.c_double)]
+                ("projection_rtol", ctypes.c_double),
+                ("sponge_rate", _dp), ("T_clim", _dp), ("S_clim", _dp), ("eta_relax_mask", _dp),
+                ("eta_relax_rate", ctypes.c_double)]
 
 
 class ZmState(ctypes.Structure):

@@ -114,6 +114,50 @@ __device__ __forceinline__ double cap_val(const BtArgs& a, const BtTile& t, int 
   return wt * (t.mean[q][b] * w) + (1.0 - wt) * (f * w);
 }
 
+// Decay of eta* by fac on the tile and its ring with the uniform refill of the
+// removed volume (barotropic.py:22-31): the owned cells' sum of
+// area (eta fac - eta) is published per block, and after a grid barrier every
+// block folds the partials in block order.
+__device__ bool refill(const Dev& d, const BtArgs& a, BtTile& t, const double* fac, double* part, unsigned nblocks) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  constexpr int NT = BT_TX * BT_TY;
+  constexpr int NR = (BT_TX + 2) * (BT_TY + 2);
+  double s = 0.0;
+  for (int e = tid; e < NT; e += nt) {
+    const int r = BT_H + e / BT_TX, c = BT_H + e % BT_TX;
+    const int j = t.gj[r];
+    if (j < 0 || !t.own_c[c]) continue;
+    const int g = idx2(d, j, t.gx[c]);
+    const double e0 = t.E[r][c];
+    s += a.area[g] * (e0 * fac[g] - e0);
+  }
+  t.red[tid] = s;
+  __syncthreads();
+  for (int o = nt / 2; o > 0; o >>= 1) {
+    if (tid < o) t.red[tid] += t.red[tid + o];
+    __syncthreads();
+  }
+  if (tid == 0) part[blockIdx.x] = t.red[0];
+  if (!grid_barrier(a.bar, a.err, nblocks, ZM_BT_BARRIER_POLLS)) return false;
+  if (tid < 32) {
+    double x = 0.0;
+    for (unsigned b = tid; b < nblocks; b += 32) x += __ldcg(part + b);
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (tid == 0) t.red[0] = x;
+  }
+  __syncthreads();
+  const double shift = -t.red[0] / a.ocean;
+  for (int e = tid; e < NR; e += nt) {
+    const int r = 1 + e / (BT_TX + 2), c = 1 + e % (BT_TX + 2);
+    const int j = t.gj[r];
+    if (j < 0) continue;
+    const int g = idx2(d, j, t.gx[c]);
+    t.E[r][c] = t.E[r][c] * fac[g] + shift * (double)t.w[r][c];
+  }
+  __syncthreads();
+  return true;
+}
+
 }  // namespace
 
 size_t bt_tile_smem() { return sizeof(BtTile); }
@@ -218,6 +262,9 @@ __global__ void __launch_bounds__(BT_THREADS, 4) k_bt_loop(Dev d, BtArgs a) {
       }
     }
     __syncthreads();
+    // 2b: lateral sponge, then eta relaxation, each with its volume refill
+    if (a.sponge && !refill(d, a, t, a.es, a.part_s[pout], nblocks)) return;
+    if (a.relax && !refill(d, a, t, a.er, a.part_r[pout], nblocks)) return;
     // 3: polar cap of eta*
     if (cap) {
       band_partials(d, a, t, t.E, a.part_e[pout], xt);
@@ -248,8 +295,12 @@ __global__ void __launch_bounds__(BT_THREADS, 4) k_bt_loop(Dev d, BtArgs a) {
       const double vs = t.V[r][c] + a.dtb * (-g9 * gy + a.Fy[g]);
       const double fd = __ldg(d.fcor_d + g) * a.dtb;
       const double den = 1.0 + fd * fd;
-      const double un = (us + fd * vs) / den * a.drag * w0;
-      const double vn = (vs - fd * us) / den * a.drag * w0;
+      double un = (us + fd * vs) / den * a.drag * w0;
+      double vn = (vs - fd * us) / den * a.drag * w0;
+      if (a.sponge) {
+        un *= a.es[g];
+        vn *= a.es[g];
+      }
       t.U[r][c] = un;
       t.V[r][c] = vn;
       a.pub_u[pout][g] = un;
@@ -320,7 +371,8 @@ __global__ void __launch_bounds__(256) k_bt_eta(Dev d, const double* __restrict_
 __global__ void __launch_bounds__(256) k_bt_vel(Dev d, const double* __restrict__ eta, const double* __restrict__ ubt,
                                                 const double* __restrict__ vbt, const double* __restrict__ Fx,
                                                 const double* __restrict__ Fy, double* __restrict__ ubt_o,
-                                                double* __restrict__ vbt_o, double dtb, double drag) {
+                                                double* __restrict__ vbt_o, double dtb, double drag,
+                                                const double* __restrict__ sv) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= d.nx || j >= d.ny) return;
@@ -342,8 +394,60 @@ __global__ void __launch_bounds__(256) k_bt_vel(Dev d, const double* __restrict_
   const double vs = vbt[c] + dtb * (-9.81 * gy + Fy[c]);
   const double fd = __ldg(d.fcor_d + c) * dtb;
   const double den = 1.0 + fd * fd;
-  ubt_o[c] = (us + fd * vs) / den * drag * w0;
-  vbt_o[c] = (vs - fd * us) / den * drag * w0;
+  double un = (us + fd * vs) / den * drag * w0;
+  double vn = (vs - fd * us) / den * drag * w0;
+  if (sv) {
+    un *= sv[c];
+    vn *= sv[c];
+  }
+  ubt_o[c] = un;
+  vbt_o[c] = vn;
+}
+
+// Uniform refill of the volume a decay removes (barotropic.py:22-31), streaming
+// path: per-block partial sums of area (eta f - eta) ...
+__global__ void __launch_bounds__(256) k_refill_part(Dev d, const double* __restrict__ eta,
+                                                     const double* __restrict__ fac,
+                                                     const double* __restrict__ area, double* __restrict__ part) {
+  __shared__ double red[256];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int t = threadIdx.y * blockDim.x + threadIdx.x;
+  double s = 0.0;
+  if (i < d.nx && j < d.ny) {
+    const int c = idx2(d, j, i);
+    const double e0 = eta[c];
+    s = area[c] * (e0 * fac[c] - e0);
+  }
+  red[t] = s;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (t < o) red[t] += red[t + o];
+    __syncthreads();
+  }
+  if (t == 0) part[blockIdx.y * gridDim.x + blockIdx.x] = red[0];
+}
+
+// ... then every block folds the partials in the same order and applies
+// eta f + (-dV / ocean_area) wet.
+__global__ void __launch_bounds__(256) k_refill_apply(Dev d, double* __restrict__ eta, const double* __restrict__ fac,
+                                                      const double* __restrict__ part, int nparts, double ocean) {
+  __shared__ double red[256];
+  const int t = threadIdx.y * blockDim.x + threadIdx.x;
+  double s = 0.0;
+  for (int b = t; b < nparts; b += 256) s += part[b];
+  red[t] = s;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (t < o) red[t] += red[t + o];
+    __syncthreads();
+  }
+  const double shift = -red[0] / ocean;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= d.nx || j >= d.ny) return;
+  const int c = idx2(d, j, i);
+  eta[c] = eta[c] * fac[c] + shift * (double)__ldg(d.wet2 + c);
 }
 
 // Polar cap of up to two 2-D float64 fields in place: one block per band row,

@@ -1127,6 +1127,22 @@ __global__ void __launch_bounds__(256) k_cap3_means(Dev d, const float* __restri
   }
 }
 
+// Lateral sponge of the linear half step (timestepping/step.py:142-156):
+// u, v *= decay and C = C_clim + (C - C_clim) decay, decay = exp(-rate dt/2)
+// per column; tracers and their targets as anomalies.
+__global__ void __launch_bounds__(256) k_sponge(Dev d, float* __restrict__ u, float* __restrict__ v,
+                                                float* __restrict__ T, float* __restrict__ S,
+                                                const float* __restrict__ dec, const float* __restrict__ Tc,
+                                                const float* __restrict__ Sc) {
+  ZM_POINT_IDX
+  const float q = ld(dec, idx2(d, j, i));
+  u[id] = u[id] * q;
+  v[id] = v[id] * q;
+  const float tc = ld(Tc, id), sc = ld(Sc, id);
+  T[id] = tc + (T[id] - tc) * q;
+  S[id] = sc + (S[id] - sc) * q;
+}
+
 // Uniform barotropic projection, polar cap, land/ghost hold and the no-flux
 // wall on v (timestepping/step.py:419-450).
 __global__ void __launch_bounds__(256) k_final(Dev d, const float* __restrict__ u3, const float* __restrict__ v3,

@@ -57,12 +57,22 @@ struct BtArgs {
   unsigned *bar, *err;
   int ntx, nb, nsub, cap_active;
   double dtH, dtb, drag;
+  // lateral sponge and eta relaxation (barotropic.py:22-41); off when the flags are 0
+  int sponge, relax;
+  const double *es, *er;     // exp(-sponge_rate dt_bt), exp(-eta_relax_rate dt_bt mask)
+  const double* area;        // dx dy
+  double ocean;              // max(sum area wet, 1)
+  double *part_s[2], *part_r[2];  // per-block refill partials by subcycle parity
 };
 size_t bt_tile_smem();
 __global__ void k_bt_loop(Dev d, BtArgs a);
 __global__ void k_bt_eta(Dev d, const double* eta, const double* ubt, const double* vbt, double* eta_o, double dtH);
 __global__ void k_bt_vel(Dev d, const double* eta, const double* ubt, const double* vbt, const double* Fx,
-                         const double* Fy, double* ubt_o, double* vbt_o, double dtb, double drag);
+                         const double* Fy, double* ubt_o, double* vbt_o, double dtb, double drag, const double* sv);
+__global__ void k_refill_part(Dev d, const double* eta, const double* fac, const double* area, double* part);
+__global__ void k_refill_apply(Dev d, double* eta, const double* fac, const double* part, int nparts, double ocean);
+__global__ void k_sponge(Dev d, float* u, float* v, float* T, float* S, const float* dec, const float* Tc,
+                         const float* Sc);
 __global__ void k_cap2d(Dev d, double* f0, double* f1, const float* wts, const double* count, int nb_rows);
 __global__ void k_eta_to_float(Dev d, const double* e64, float* e32);
 // per-column MLP of the learned closure (zm_mlp.cu); BF16 weights [out][in]

@@ -76,6 +76,8 @@ struct zm_solver {
   float* kappa3 = nullptr;       // [nz-1][ny][P] diffusivity per interface
   unsigned* cl_count = nullptr;  // [0] fallback columns of the last step, [1] tensor-core wait errors
   float cl_bound = 8.f;
+  // lateral sponge of the linear half step (null when off): decay per column, targets as anomalies
+  float *sp_dec = nullptr, *sp_Tc = nullptr, *sp_Sc = nullptr;
   // column-divergence projection of the stage-2 advective velocity (off unless project_adv_vel)
   bool proj_on = false;
   ProjArgs pj{};
@@ -197,6 +199,12 @@ struct zm_solver {
       g.z = 2;
       k_implicit_vdiff<<<g, c, 0, s>>>(d, dst.u, dst.v, dst.T, dst.S, src.u, src.v, src.T, src.S, dth,
                                        closure_on ? kappa3 : nullptr);
+      pe(s);
+    }
+    if (sp_dec) {  // lateral sponge after the diffusion (step.py:142-156)
+      const dim3 c(32, 8);
+      pb(ZM_K_LIN_FINISH, s);
+      k_sponge<<<grid3(c), c, 0, s>>>(d, dst.u, dst.v, dst.T, dst.S, sp_dec, sp_Tc, sp_Sc);
       pe(s);
     }
     check_launch();
@@ -363,13 +371,25 @@ struct zm_solver {
         pb(ZM_K_BAROTROPIC, s);
         k_bt_eta<<<grid2(c), c, 0, s>>>(d, eta64[a0], ubt[a0], vbt[a0], eta64[a1], bt.dtH);
         pe(s);
+        for (int f = 0; f < 2; ++f) {  // sponge, then eta relaxation (barotropic.py:33-40)
+          if (!(f == 0 ? bt.sponge : bt.relax)) continue;
+          const double* fac = f == 0 ? bt.es : bt.er;
+          const dim3 g2 = grid2(c);
+          pb(ZM_K_BAROTROPIC, s);
+          k_refill_part<<<g2, c, 0, s>>>(d, eta64[a1], fac, bt.area, bt.part_s[0]);
+          pe(s);
+          pb(ZM_K_BAROTROPIC, s);
+          k_refill_apply<<<g2, c, 0, s>>>(d, eta64[a1], fac, bt.part_s[0], (int)(g2.x * g2.y), bt.ocean);
+          pe(s);
+        }
         if (cap) {
           pb(ZM_K_BAROTROPIC, s);
           k_cap2d<<<dim3(2 * cap_nb, 1), 256, 0, s>>>(d, eta64[a1], nullptr, wts, bt.count, cap_nb);
           pe(s);
         }
         pb(ZM_K_BAROTROPIC, s);
-        k_bt_vel<<<grid2(c), c, 0, s>>>(d, eta64[a1], ubt[a0], vbt[a0], Fx, Fy, ubt[a1], vbt[a1], dt_bt, bt_drag);
+        k_bt_vel<<<grid2(c), c, 0, s>>>(d, eta64[a1], ubt[a0], vbt[a0], Fx, Fy, ubt[a1], vbt[a1], dt_bt, bt_drag,
+                                        bt.sponge ? bt.es : nullptr);
         pe(s);
         if (cap) {
           pb(ZM_K_BAROTROPIC, s);
@@ -863,6 +883,69 @@ void build(zm_solver* s, const zm_grid* g, const zm_params* p) {
     s->bt_sync = s->alloc<unsigned>(4);
     a.bar = s->bt_sync;
     a.err = s->bt_sync + 2;
+  }
+  {
+    // lateral sponge and eta relaxation (factory.py:456-521)
+    BtArgs& a = s->bt;
+    bool sponge = false, relax = false;
+    if (p->sponge_rate) {
+      for (size_t q = 0; q < (size_t)nx * ny; ++q) {
+        require(std::isfinite(p->sponge_rate[q]) && p->sponge_rate[q] >= 0.0, ZM_ERR_INVALID,
+                "sponge_rate must be finite and nonnegative");
+        if (p->sponge_rate[q] > 0.0) sponge = true;
+      }
+    }
+    require(std::isfinite(p->eta_relax_rate) && p->eta_relax_rate >= 0.0, ZM_ERR_INVALID,
+            "eta_relax_rate must be finite and nonnegative");
+    if (p->eta_relax_mask && p->eta_relax_rate > 0.0) {
+      for (size_t q = 0; q < (size_t)nx * ny; ++q) {
+        require(std::isfinite(p->eta_relax_mask[q]), ZM_ERR_INVALID, "eta_relax_mask must be finite");
+        if (p->eta_relax_mask[q] != 0.0) relax = true;
+      }
+    }
+    if (sponge || relax) {
+      std::vector<double> area(s->n2, 0.0), es(s->n2, 1.0), er(s->n2, 1.0);
+      double ocean = 0.0;
+      for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j) {
+          const size_t r = (size_t)i * ny + j, c = (size_t)j * P + i;
+          area[c] = g->dx_2d[r] * g->dy;
+          ocean += area[c] * g->wet_mask[r];
+          if (sponge) es[c] = std::exp(-p->sponge_rate[r] * s->dt_bt);
+          if (relax) er[c] = std::exp(-p->eta_relax_rate * s->dt_bt * p->eta_relax_mask[r]);
+        }
+      a.area = s->upload(area);
+      a.ocean = std::max(ocean, 1.0);
+      a.sponge = sponge ? 1 : 0;
+      a.relax = relax ? 1 : 0;
+      a.es = s->upload(es);
+      a.er = s->upload(er);
+      const size_t np = std::max<size_t>((size_t)std::max(s->bt_blocks, 1),
+                                         (size_t)((nx + 31) / 32) * ((ny + 7) / 8));
+      for (int q = 0; q < 2; ++q) {
+        a.part_s[q] = s->alloc<double>(np);
+        a.part_r[q] = s->alloc<double>(np);
+      }
+    }
+    if (sponge) {
+      require(p->T_clim && p->S_clim, ZM_ERR_INVALID, "the sponge needs T_clim and S_clim");
+      std::vector<float> dec(s->n2, 1.f), tc(s->n3, 0.f), sc(s->n3, 0.f);
+      for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j) {
+          const size_t r = (size_t)i * ny + j;
+          dec[(size_t)j * P + i] = (float)std::exp(-p->sponge_rate[r] * (p->dt / 2.0));
+          for (int k = 0; k < nz; ++k) {
+            const double tv = p->T_clim[r * nz + k], sv = p->S_clim[r * nz + k];
+            require(std::isfinite(tv) && std::isfinite(sv), ZM_ERR_INVALID, "T_clim and S_clim must be finite");
+            const size_t id = (size_t)k * s->n2 + (size_t)j * P + i;
+            tc[id] = (float)(tv - p->T_ref);
+            sc[id] = (float)(sv - p->S_ref);
+          }
+        }
+      s->sp_dec = s->upload(dec);
+      s->sp_Tc = s->upload(tc);
+      s->sp_Sc = s->upload(sc);
+    }
   }
   // projection options are validated whether or not the projection is on (factory.py:368-386)
   require(p->projection_niter > 0, ZM_ERR_INVALID, "projection_niter must be a positive integer");

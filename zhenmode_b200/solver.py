@@ -154,6 +154,10 @@ class _Solver:
         p.projection_preconditioner = 1 if opts.get("projection_preconditioner", "none") == "jacobi" else 0
         p.projection_max_refinements = int(opts.get("projection_max_refinements", 2))
         p.projection_rtol = float(opts.get("projection_rtol", 0.0))
+        p.eta_relax_rate = float(opts.get("eta_relax_rate", 0.0))
+        sizes = {"sponge_rate": (nx, ny), "T_clim": (nx, ny, nz), "S_clim": (nx, ny, nz), "eta_relax_mask": (nx, ny)}
+        for name, shape in sizes.items():
+            setattr(p, name, _native.dptr(arr(opts["fields"].get(name), shape)))
         for name in ("tau_x", "tau_y", "q_heat", "t_atm", "s_ref", "coastal_restore_coef",
                      "coastal_restore_t", "coastal_bulk_lambda", "coastal_kappa_h", "coastal_kappa_v"):
             setattr(p, name, _native.dptr(arr(opts["fields"].get(name), (nx, ny))))
@@ -389,10 +393,6 @@ def make_solver_global(grid, physics, dt, forcing=None,
         unsupported.append('dynamic ice')
     if (mixed_layer_depth_m or 0.0) > 0.0 or mixed_layer_depth_2d is not None:
         unsupported.append('mixed-layer heat deposition')
-    if sponge_days > 0.0 and sponge_cells > 0:
-        unsupported.append('lateral sponge')
-    if eta_relax_days > 0.0 and eta_relax_box is not None:
-        unsupported.append('eta relaxation box')
     if surface_pressure_pa is not None:
         unsupported.append('surface pressure load')
     if nz > 64:
@@ -425,6 +425,38 @@ def make_solver_global(grid, physics, dt, forcing=None,
     if coastal_restore_mask is not None and coastal_restore_days > 0.0 and coastal_restore_T is not None:
         fields['coastal_restore_coef'] = _f64(coastal_restore_mask, shape2) / (coastal_restore_days * 86400.0)
         fields['coastal_restore_t'] = _f64(coastal_restore_T, shape2)
+    # lateral sponge: cosine taper from the polar edge rows (factory.py:456-491)
+    if sponge_days > 0.0 and sponge_cells > 0:
+        edge = np.minimum(np.arange(ny), ny - 1 - np.arange(ny))
+        band = edge < int(sponge_cells)
+        taper = np.where(band, 0.5 * (1.0 + np.cos(np.pi * edge / int(sponge_cells))), 0.0)
+        fields['sponge_rate'] = np.ascontiguousarray(
+            np.broadcast_to(taper[None, :] / (sponge_days * 86400.0), (nx, ny)))
+        wm3 = np.asarray(getattr(grid, 'wet_mask_3d', None) if getattr(grid, 'wet_mask_3d', None) is not None
+                         else np.broadcast_to(np.asarray(grid.wet_mask)[:, :, None], (nx, ny, nz)), dtype=np.float64)
+        if T_init is not None:
+            T_clim = np.asarray(T_init, dtype=np.float64) * wm3 + (1.0 - wm3) * physics.T_ref
+            S_clim = (np.asarray(S_init, dtype=np.float64) if S_init is not None
+                      else np.full((nx, ny, nz), float(physics.S_ref)))
+            S_clim = S_clim * wm3 + (1.0 - wm3) * physics.S_ref
+        else:  # init_state fills T_ref / S_ref: the target that leaves the sponge a no-op
+            T_clim = np.full((nx, ny, nz), float(physics.T_ref))
+            S_clim = np.full((nx, ny, nz), float(physics.S_ref))
+        fields['T_clim'] = np.ascontiguousarray(T_clim)
+        fields['S_clim'] = np.ascontiguousarray(S_clim)
+    # semi-enclosed-sea eta relaxation box with a cosine buffer (factory.py:493-521)
+    eta_relax_rate = 0.0
+    if eta_relax_days > 0.0 and eta_relax_box is not None:
+        lon0, lon1, lat0, lat1 = eta_relax_box
+        lon2d, lat2d = np.meshgrid(np.asarray(grid.lon, dtype=np.float64), np.asarray(grid.lat, dtype=np.float64),
+                                   indexing='ij')
+        core = (lon2d >= lon0) & (lon2d <= lon1) & (lat2d >= lat0) & (lat2d <= lat1)
+        d_out = np.maximum(np.maximum(np.maximum(lon0 - lon2d, lon2d - lon1), 0.0),
+                           np.maximum(np.maximum(lat0 - lat2d, lat2d - lat1), 0.0))
+        buf = float(eta_relax_buffer)
+        mask = np.where(core, 1.0, np.where(d_out < buf, 0.5 * (1.0 + np.cos(np.pi * d_out / buf)), 0.0))
+        fields['eta_relax_mask'] = mask * np.asarray(grid.wet_mask, dtype=np.float64)
+        eta_relax_rate = 1.0 / (eta_relax_days * 86400.0)
     if nu_nsub == 'cfl':
         inv_dx2_max = float(np.max(np.asarray(grid.dx_2d, dtype=np.float64) ** -2))
         nu_nsub = max(1, int(np.ceil(physics.nu_h * (dt / 2.0) * (inv_dx2_max + 1.0 / float(grid.dy) ** 2) / 0.25)))
@@ -437,7 +469,8 @@ def make_solver_global(grid, physics, dt, forcing=None,
                 project_adv_vel=bool(project_adv_vel), projection_niter=int(projection_niter),
                 projection_preconditioner=projection_preconditioner,
                 projection_max_refinements=int(projection_max_refinements),
-                projection_rtol=0.0 if projection_rtol is None else float(projection_rtol))
+                projection_rtol=0.0 if projection_rtol is None else float(projection_rtol),
+                eta_relax_rate=eta_relax_rate)
     solver = _Solver(grid, physics, dt, opts)
     wet3 = np.asarray(getattr(grid, 'wet_mask_3d', None) if getattr(grid, 'wet_mask_3d', None) is not None
                       else np.broadcast_to(np.asarray(grid.wet_mask)[:, :, None], (nx, ny, nz)), dtype=np.float64)
