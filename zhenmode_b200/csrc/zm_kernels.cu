@@ -351,9 +351,12 @@ __global__ void __launch_bounds__(LT_X * LT_Y) k_lin_t(Dev d, const float* __res
   __syncthreads();
   const bool do_uv = d.nu_bi > 0.f, do_ts = d.kappa_bi > 0.f;
   if (do_uv || do_ts) {
-    constexpr int RX = LT_X + 2, RY = LT_Y + 2;   // the one-cell ring around the interior
-    for (int e = tid; e < RX * RY; e += nt) {
-      const int r = 1 + e / RX, cc = 1 + e % RX;
+    // the one-cell ring around the interior, walked over whole padded rows so
+    // that a warp's shared-memory addresses are consecutive (no bank conflicts)
+    constexpr int RY = LT_Y + 2;
+    for (int e = tid; e < LT_PX * RY; e += nt) {
+      const int r = 1 + e / LT_PX, cc = e % LT_PX;
+      if (cc == 0 || cc == LT_PX - 1) continue;
       if (do_uv) {
         t.Lu[r][cc] = lap_s(d, t, t.u, r, cc, false);
         t.Lv[r][cc] = lap_s(d, t, t.v, r, cc, false);
