@@ -448,26 +448,33 @@ def _surface_heat_factor(p):
     return p.surface_mask * p.wet_mask_z / p.dz_surface / (RHO_0 * C_P)
 
 
-def tracer_tendency(u, v, T, S, p):
+def tracer_tendency(u, v, T, S, p, rec=None):
     """dynamics/tendencies.py:94-219 ``_compute_tracer_tendency`` (no GM/Redi,
-    no dynamic ice, default mixed layer)."""
+    no dynamic ice, default mixed layer); with a ledger recorder ``rec`` the
+    hooks of tendencies.py:211-214 (the surface flux Fz[0] c[0] of the
+    advection, transport.py:459-475, averaged over the substeps like the rate)."""
     Fz = vertical_transport_iface(u, v, p)
     na = int(p.adv_nsub)
     if na > 1:
         dts = p.dt / na
         tT, tS = T, S
-        aT_list, aS_list = [], []
+        aT_list, aS_list, tops_T, tops_S = [], [], [], []
         for _ in range(na):
             aT = tracer_advection(tT, u, v, Fz, p)
             aS = tracer_advection(tS, u, v, Fz, p)
             aT_list.append(aT)
             aS_list.append(aS)
+            tops_T.append(Fz[..., 0] * tT[..., 0])
+            tops_S.append(Fz[..., 0] * tS[..., 0])
             tT, tS = tT + aT * dts, tS + aS * dts
         adv_T = np.mean(np.stack(aT_list), axis=0)
         adv_S = np.mean(np.stack(aS_list), axis=0)
+        top_T = sum(tops_T) / na
+        top_S = sum(tops_S) / na
     else:
         adv_T = tracer_advection(T, u, v, Fz, p)
         adv_S = tracer_advection(S, u, v, Fz, p)
+        top_T, top_S = Fz[..., 0] * T[..., 0], Fz[..., 0] * S[..., 0]
     dh_T = horizontal_tracer_diffusion(T, p)
     dh_S = horizontal_tracer_diffusion(S, p)
     dv_T = vertical_tracer_diffusion(T, p)
@@ -501,12 +508,17 @@ def tracer_tendency(u, v, T, S, p):
     rest_T = p.coastal_restore_coef_2d[:, :, None] * (p.coastal_restore_T_2d[:, :, None] - sst) * p.surface_mask
     dT = adv_T + dh_T + dv_T + heat_T + bulk_T + cbulk_T + conv_T + rest_T
     dS = adv_S + dh_S + dv_S + conv_S + rest_S + ice_salt
+    if rec is not None:
+        zero = np.zeros_like(adv_T)
+        rec.surface_sources((heat_T, bulk_T, cbulk_T, rest_T, rest_S, ice_salt))
+        rec.nonlinear_terms(((adv_T, adv_S), (conv_T, conv_S), (zero, zero), (zero, zero)))
+        rec.advection_boundary_fluxes(top_T, top_S)
     return dT * p.wet_mask_z, dS * p.wet_mask_z
 
 
-def tracer_residual(u, v, T, S, p):
+def tracer_residual(u, v, T, S, p, rec=None):
     """dynamics/tendencies.py:227-245: tendency minus the L-step linear terms."""
-    dT, dS = tracer_tendency(u, v, T, S, p)
+    dT, dS = tracer_tendency(u, v, T, S, p, rec)
     dT = dT - horizontal_tracer_diffusion(T, p)
     dS = dS - horizontal_tracer_diffusion(S, p)
     dT = dT - vertical_tracer_diffusion(T, p)
@@ -589,8 +601,9 @@ def implicit_vertical_solve(rhs, kappa, dt, p):
 
 
 # ---------------------------------------------------------------- linear half step
-def linear_half_step(st, p, dt_half):
-    """timestepping/step.py:76-187 ``_linear_half_step`` (legacy, mode split)."""
+def linear_half_step(st, p, dt_half, rec=None):
+    """timestepping/step.py:76-187 ``_linear_half_step`` (legacy, mode split);
+    ledger hooks of step.py:138-161."""
     u0, v0, T0, S0 = st["u"], st["v"], st["T"], st["S"]
     wm = p.wet_mask_z
     n_nu = max(1, int(p.n_subcyc if p.nu_nsub is None else p.nu_nsub))
@@ -620,11 +633,17 @@ def linear_half_step(st, p, dt_half):
     v = v * wm + v0 * (1.0 - wm)
     T = T * wm + T0 * (1.0 - wm)
     S = S * wm + S0 * (1.0 - wm)
+    diffused = dict(u=u, v=v, T=T, S=S, eta=st["eta"])
+    if rec is not None:
+        rec.stage("linear_diffusion", st, diffused)
     decay = np.exp(-p.sponge_rate * dt_half)
     u = u * decay
     v = v * decay
     T = p.T_clim_3d + (T - p.T_clim_3d) * decay
     S = p.S_clim_3d + (S - p.S_clim_3d) * decay
+    if rec is not None:
+        rec.stage("sponge", diffused, dict(u=u, v=v, T=T, S=S, eta=st["eta"]))
+        rec.sponge_sources(diffused, decay)
     angle = p.f[:, :, None] * dt_half
     ca, sa = np.cos(angle), np.sin(angle)
     return dict(u=ca * u + sa * v, v=-sa * u + ca * v, T=T, S=S, eta=st["eta"])
@@ -732,12 +751,12 @@ def project_column_divergence(u, v, p, dt):
     return corrected
 
 
-def explicit_full_step(st, p):
+def explicit_full_step(st, p, rec=None):
     """timestepping/step.py:249-320 ``_explicit_full_step`` (legacy RK2 with
     the exact linear-drag decay of the mode-split path)."""
     u, v, T, S, eta = st["u"], st["v"], st["T"], st["S"], st["eta"]
     dt = p.dt
-    dT1, dS1 = tracer_residual(u, v, T, S, p)
+    dT1, dS1 = tracer_residual(u, v, T, S, p, rec)
     Tp, Sp = T + dT1 * dt, S + dS1 * dt
     du1, dv1 = momentum_residual(u, v, Tp, Sp, eta, p)
     bm = p.bottom_mask * p.wet_mask_z
@@ -745,11 +764,15 @@ def explicit_full_step(st, p):
     dv1 = dv1 + p.r_bot * v * bm
     up, vp = u + du1 * dt, v + dv1 * dt
     if p.freeze_adv_vel:
-        dT2, dS2 = tracer_residual(u, v, Tp, Sp, p)
+        dT2, dS2 = tracer_residual(u, v, Tp, Sp, p, rec)
     else:
         if p.project_adv_vel:   # step.py:292-303
-            up, vp = project_column_divergence(up, vp, p, dt)
-        dT2, dS2 = tracer_residual(up, vp, Tp, Sp, p)
+            ua, va = project_column_divergence(up, vp, p, dt)
+            if rec is not None:
+                rec.column_projection(vertical_transport_iface(up, vp, p)[..., 0],
+                                      vertical_transport_iface(ua, va, p)[..., 0])
+            up, vp = ua, va
+        dT2, dS2 = tracer_residual(up, vp, Tp, Sp, p, rec)
     Tn = T + 0.5 * (dT1 + dT2) * dt
     Sn = S + 0.5 * (dS1 + dS2) * dt
     du2, dv2 = momentum_residual(u, v, Tn, Sn, eta, p)
@@ -800,15 +823,19 @@ def free_surface_step(eta, ubt, vbt, p, F_rho_x, F_rho_y, dt_bt):
 
 
 # ---------------------------------------------------------------- full step
-def step(st, p):
+def step(st, p, rec=None):
     """timestepping/step.py:341-458 ``_step_impl``: L(dt/2) N(dt) L(dt/2), the
     barotropic subcycle and its uniform projection, polar cap, land hold and
-    the no-flux wall on v."""
+    the no-flux wall on v; with a ledger recorder the stage hooks of
+    step.py:366-368, 425-427 and 452-455."""
     dt_half = p.dt / 2.0
     held = {k: st[k] for k in ("u", "v", "T", "S")}
-    s = linear_half_step(st, p, dt_half)
-    s = explicit_full_step(s, p)
-    s = linear_half_step(s, p, dt_half)
+    s = linear_half_step(st, p, dt_half, rec)
+    n_start = s
+    s = explicit_full_step(s, p, rec)
+    if rec is not None:
+        rec.stage("nonlinear", n_start, s)
+    s = linear_half_step(s, p, dt_half, rec)
     fx, fy = bt_rho_pgf(s["T"], s["S"], p)
     ubt0, vbt0 = barotropic_velocity(s["u"], s["v"], p)
     eta, ubt, vbt = s["eta"], ubt0, vbt0
@@ -816,6 +843,9 @@ def step(st, p):
         eta, ubt, vbt = free_surface_step(eta, ubt, vbt, p, fx, fy, p.dt_bt)
     u = s["u"] + (ubt - ubt0)[:, :, None]
     v = s["v"] + (vbt - vbt0)[:, :, None]
+    after_bt = dict(u=u, v=v, T=s["T"], S=s["S"], eta=eta)
+    if rec is not None:
+        rec.stage("free_surface", s, after_bt)
     wm = p.wet_mask_z
     out = {}
     for key, field in (("u", u), ("v", v), ("T", s["T"]), ("S", s["S"])):
@@ -823,6 +853,9 @@ def step(st, p):
         out[key] = capped * wm + held[key] * (1.0 - wm)
     out["v"] = out["v"] * p.interior_mask_z
     out["eta"] = eta
+    if rec is not None:
+        rec.stage("polar_cap_and_masks", after_bt, out)
+        rec.stage("dynamic_ice", out, out)
     return out
 
 

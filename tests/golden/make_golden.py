@@ -166,6 +166,51 @@ def make_sponge_case(name="step_sponge_48x24x10", seed=7):
     print(name, "saved")
 
 
+def make_ledger_case(seed=9):
+    """The reference's FP64 stage/source ledger (diagnostics/budgets.py:264-288
+    ``make_budget_step``) over two steps with every source of the legacy path
+    switched on: lateral sponge and eta relaxation, the column projection,
+    bulk and coastal-bulk heat flux toward an air temperature, SSS restoring,
+    coastal SST restoring and brine rejection below a raised freezing point."""
+    from zhenmode.model.diagnostics.budgets import make_budget_step
+    nx, ny, nz = 48, 24, 10
+    grid = workloads.build_grid(nx, ny, nz, land_lat=75.0)
+    T, S = workloads.initial_fields(grid, perturb_sigma=0.2)
+    lon, lat = np.asarray(grid.lon), np.asarray(grid.lat)
+    wm = np.asarray(grid.wet_mask)
+    rng = np.random.default_rng(seed)
+    coast = (wm * (rng.random((nx, ny)) < 0.3)).astype(np.float64)
+    arrays = dict(T_atm=T[:, :, 0] - 2.0 + 0.5 * rng.standard_normal((nx, ny)),
+                  S_ref_surf=S[:, :, 0] + 0.1 * rng.standard_normal((nx, ny)),
+                  coastal_bulk_mask=coast, coastal_restore_mask=coast, coastal_restore_T=T[:, :, 0] + 1.0)
+    scalars = dict(sponge_days=0.5, sponge_cells=4, eta_relax_days=0.25,
+                   eta_relax_box=(float(lon[10]), float(lon[20]), float(lat[8]), float(lat[14])),
+                   eta_relax_buffer=10.0, project_adv_vel=True, lambda_bulk=40.0, sss_restore_days=30.0,
+                   coastal_bulk_lambda=20.0, coastal_restore_days=10.0, ice_salt_flux=2e-6, ice_freeze_temp_c=4.0)
+    options = dict(workloads.PLAIN_OPTIONS, **scalars)
+    kw = dict(options, **arrays, forcing=workloads.wind_forcing(grid), dt_bt=75.0, dtype="float64",
+              T_init=T, S_init=S)
+    step, init, _, params, _ = make_solver_global(grid, _physics(workloads.PLAIN_PHYSICS), 1800.0,
+                                                  return_params=True, **kw)
+    advance = make_budget_step(params)
+    u, v, T0, S0, eta = _moving_state(grid, T, S, seed)
+    st = JaxStateG(*[_f32(a) for a in (u, v, T0, S0, eta)], np.zeros((nx, ny)))
+    data = dict(_grid_arrays(grid))
+    data.update(in_u=_np(st.u), in_v=_np(st.v), in_T=_np(st.T), in_S=_np(st.S), in_eta=_np(st.eta),
+                clim_T=_np(T), clim_S=_np(S), dt=np.float64(1800.0), dt_bt=np.float64(75.0),
+                restore_days=np.float64(0.0), nsteps=np.int64(2),
+                physics=np.array(repr(dataclasses.asdict(workloads.PLAIN_PHYSICS))),
+                options=np.array(repr(options)), **{f"arr_{k}": np.asarray(v) for k, v in arrays.items()})
+    for n in (1, 2):
+        st, ledger = advance(st)
+        for key in ("u", "v", "T", "S", "eta"):
+            data[f"out{n}_{key}"] = _np(getattr(st, key))
+        for key, value in ledger.items():
+            data[f"ledger{n}_{key}"] = _np(value)
+    np.savez_compressed(os.path.join(HERE, "ledger_48x24x10.npz"), **data)
+    print("ledger saved")
+
+
 def make_operator_case(seed=11):
     """Single-operator goldens on a 24x16x6 grid with land blocks and a wet
     polar band, random fields (reference functions called directly)."""
@@ -333,6 +378,7 @@ def make_restart_case():
 
 
 def main():
+    make_ledger_case()
     make_sponge_case()
     make_restart_case()
     make_operator_case()

@@ -41,6 +41,9 @@ def case_inputs(data):
                        coastal_restore_T=np.array(data["in_T"][:, :, 0]))
     if "clim_T" in data:  # the sponge's relaxation targets (factory.py:470-483)
         options.update(T_init=data["clim_T"], S_init=data["clim_S"])
+    for key in data:  # array-valued options of the fixture (forcing targets, masks)
+        if key.startswith("arr_"):
+            options[key[4:]] = data[key]
     state = {k: data["in_" + k] for k in ("u", "v", "T", "S", "eta")}
     return grid, physics, float(data["dt"]), options, state
 

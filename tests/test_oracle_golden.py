@@ -174,3 +174,35 @@ def test_column_projection(pre):
     ua, va = ostep.project_column_divergence(data["in_u"], data["in_v"], p, 1800.0)
     _check("u", ua, data[f"{pre}_u"], 1e-9)
     _check("v", va, data[f"{pre}_v"], 1e-9)
+
+
+def test_ledger_matches_reference_budget_step():
+    """The FP64 stage/source ledger (diagnostics/budgets.py:264-288) of two
+    steps with every legacy source on, against the reference's own
+    make_budget_step."""
+    from oracle import ledger
+    data = load("ledger_48x24x10")
+    grid, physics, dt, options, state = case_inputs(data)
+    p = oparams.build_params(grid, physics, dt, **options)
+    st = {k: np.array(v) for k, v in state.items()}
+    for n in (1, 2):
+        st, led = ledger.ledger_step(st, p)
+        for k in ("u", "v", "T", "S", "eta"):
+            _check(f"step {n} {k}", st[k], data[f"out{n}_{k}"], tol=1e-10)
+        for key, value in led.items():
+            want = data[f"ledger{n}_{key}"]
+            got = np.asarray(value, dtype=np.float64)
+            assert got.shape == want.shape, key
+            scale = max(float(np.max(np.abs(want))), 1e-300)
+            err = float(np.max(np.abs(got - want))) if got.size else 0.0
+            # residual identities are differences of large sums: judged against the sums they close
+            if "residual" in key:
+                ref = {"decomposition_residual": "change_scale", "absolute_decomposition_residual": "change_scale",
+                       "budget_residual": "change_scale", "absolute_budget_residual": "change_scale",
+                       "advection_boundary_residual": "nonlinear_process_scale",
+                       "absolute_advection_boundary_residual": "nonlinear_process_scale",
+                       "nonlinear_accounting_residual": "nonlinear_process_scale",
+                       "absolute_nonlinear_accounting_residual": "nonlinear_process_scale"}.get(key)
+                if ref is not None:
+                    scale = max(scale, float(np.max(np.abs(data[f"ledger{n}_{ref}"]))))
+            assert err <= 1e-9 * scale, (n, key, err, scale)
