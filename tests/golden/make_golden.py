@@ -186,9 +186,11 @@ def make_ledger_case(seed=9):
     scalars = dict(sponge_days=0.5, sponge_cells=4, eta_relax_days=0.25,
                    eta_relax_box=(float(lon[10]), float(lon[20]), float(lat[8]), float(lat[14])),
                    eta_relax_buffer=10.0, project_adv_vel=True, lambda_bulk=40.0, sss_restore_days=30.0,
-                   coastal_bulk_lambda=20.0, coastal_restore_days=10.0, ice_salt_flux=2e-6, ice_freeze_temp_c=4.0)
+                   coastal_bulk_lambda=20.0, coastal_restore_days=10.0, ice_salt_flux=2e-6, ice_freeze_temp_c=12.0)
     options = dict(workloads.PLAIN_OPTIONS, **scalars)
-    kw = dict(options, **arrays, forcing=workloads.wind_forcing(grid), dt_bt=75.0, dtype="float64",
+    tau_x, tau_y, _ = workloads.wind_forcing(grid)
+    q_heat = np.broadcast_to((60.0 * np.cos(2.0 * np.radians(lat)))[None, :], (nx, ny)).copy()
+    kw = dict(options, **arrays, forcing=(tau_x, tau_y, q_heat), dt_bt=75.0, dtype="float64",
               T_init=T, S_init=S)
     step, init, _, params, _ = make_solver_global(grid, _physics(workloads.PLAIN_PHYSICS), 1800.0,
                                                   return_params=True, **kw)
@@ -200,7 +202,8 @@ def make_ledger_case(seed=9):
                 clim_T=_np(T), clim_S=_np(S), dt=np.float64(1800.0), dt_bt=np.float64(75.0),
                 restore_days=np.float64(0.0), nsteps=np.int64(2),
                 physics=np.array(repr(dataclasses.asdict(workloads.PLAIN_PHYSICS))),
-                options=np.array(repr(options)), **{f"arr_{k}": np.asarray(v) for k, v in arrays.items()})
+                options=np.array(repr(options)), forcing_q=q_heat,
+                **{f"arr_{k}": np.asarray(v) for k, v in arrays.items()})
     for n in (1, 2):
         st, ledger = advance(st)
         for key in ("u", "v", "T", "S", "eta"):

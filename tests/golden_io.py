@@ -34,7 +34,8 @@ def case_inputs(data):
     lat = np.radians(np.asarray(grid.lat))
     tau_x = np.broadcast_to((0.1 * np.sin(2 * lat) * np.cos(lat))[None, :], (grid.nx, grid.ny)).copy()
     zeros = np.zeros((grid.nx, grid.ny))
-    options.update(forcing=(tau_x, zeros, zeros.copy()), dt_bt=float(data["dt_bt"]))
+    q_heat = np.array(data["forcing_q"]) if "forcing_q" in data else zeros.copy()
+    options.update(forcing=(tau_x, zeros, q_heat), dt_bt=float(data["dt_bt"]))
     restore = float(data["restore_days"])
     if restore > 0:
         options.update(coastal_restore_mask=np.asarray(grid.wet_mask), coastal_restore_days=restore,
