@@ -218,6 +218,27 @@ int zm_barrier_probe(zm_solver* s, void* stream, int32_t blocks, int32_t expecte
  * projection kernel gave up (the state is then not a valid step result).  Synchronizes the device. */
 int zm_status(zm_solver* s, int32_t* monitor_code);
 
+/* One step with the FP64 stage/source ledger of the reference's budget audit
+ * (make_budget_step, diagnostics/budgets.py:62-288): device state in -> out,
+ * like zm_step with nsteps = 1 but without the CUDA graph, and the raw sums
+ * into raw[0..ZM_LED_COUNT) (host memory; synchronizes):
+ *   [0, 18)  stage changes [6][3]: linear_diffusion, sponge, nonlinear,
+ *            free_surface, polar_cap_and_masks, dynamic_ice x (heat J, salt kg,
+ *            volume m^3)
+ *   [18, 21) summed magnitudes of the stage changes
+ *   [21, 48) source inputs [9][3]: prescribed_heat, bulk_heat,
+ *            coastal_bulk_heat, temperature_restore, salinity_restore,
+ *            prescribed_brine, sponge, ice_atmosphere_heat, ice_brine
+ *   [48, 60) nonlinear process changes [4][3]: advection, convection, gm, redi
+ *   [60, 63) their summed magnitudes      [63, 66) advective surface flux
+ *   [66, 69) squared surface-transport norms before / after the column
+ *            projection and the worst ratio sqrt(after / before)
+ *   [69, 72) observed change over the step  [72, 75) eta times the surface
+ *            tracers, after minus before
+ * The residual identities of the reference's ledger follow from these. */
+#define ZM_LED_COUNT 75
+int zm_ledger_step(zm_solver* s, void* stream, const zm_state* in, zm_state* out, double* raw, int32_t n);
+
 /* CG iterations of the last column projection (needs project_adv_vel):
  * out[0] the first solve, out[1] and out[2] the refinement solves (0 when not
  * run), out[3] the refinement solves run.  Writes min(n, 4) values;

@@ -80,6 +80,8 @@ EXPORTS = {
                                         ctypes.c_int32]),
     "zm_status": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
     "zm_projection_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32]),
+    "zm_ledger_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ZmState), ctypes.POINTER(ZmState),
+                                      ctypes.POINTER(ctypes.c_double), ctypes.c_int32]),
     "zm_diagnostics": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ZmState), ctypes.c_void_p,
                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "zm_mlp_forward_bf16": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32] + [ctypes.c_void_p] * 8

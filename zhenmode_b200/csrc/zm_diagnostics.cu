@@ -13,6 +13,7 @@
 // elements; lanes, warps and blocks are combined as double-double values
 // (TwoSum), and the per-block partials are folded by one block in block
 // order, so the result is the same on every run.
+#include "zm_dd.cuh"
 #include "zm_kernels.cuh"
 
 namespace zm {
@@ -42,38 +43,6 @@ __global__ void __launch_bounds__(128) k_diagnostics(Dev d, const float* __restr
   }
 }
 
-namespace {
-
-struct DD {
-  double hi, lo;
-};
-
-__device__ __forceinline__ DD two_sum(double a, double b) {
-  const double s = a + b;
-  const double bb = s - a;
-  return DD{s, (a - (s - bb)) + (b - bb)};
-}
-
-__device__ __forceinline__ DD dd_add(DD x, DD y) {
-  DD s = two_sum(x.hi, y.hi);
-  const double e = s.lo + (x.lo + y.lo);
-  const double hi = s.hi + e;
-  return DD{hi, e - (hi - s.hi)};
-}
-
-// Neumaier step: running sum x.hi, compensation x.lo
-__device__ __forceinline__ void neumaier(DD& x, double v) {
-  const double t = x.hi + v;
-  if (fabs(x.hi) >= fabs(v)) x.lo += (x.hi - t) + v;
-  else x.lo += (v - t) + x.hi;
-  x.hi = t;
-}
-
-__device__ __forceinline__ DD shfl_dd(DD x, int o) {
-  return DD{__shfl_down_sync(0xffffffffu, x.hi, o), __shfl_down_sync(0xffffffffu, x.lo, o)};
-}
-
-}  // namespace
 
 // sums: 0 wet volume, 1 T volume, 2 S volume, 3 wet surface area,
 // 4 T_top surface area, 5 S_top surface area, 6 total cell area.

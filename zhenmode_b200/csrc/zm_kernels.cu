@@ -750,7 +750,9 @@ __global__ void __launch_bounds__(TA_X * TA_Y, 4) k_tracer_adv_t(Dev d, const fl
                                                                  const float* __restrict__ Fz,
                                                                  float* __restrict__ accT, float* __restrict__ accS,
                                                                  float* __restrict__ Tn, float* __restrict__ Sn,
-                                                                 float dts, int first, int last) {
+                                                                 float dts, int first, int last,
+                                                                 float* __restrict__ topT,
+                                                                 float* __restrict__ topS) {
   __shared__ TaTile t;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = ty * TA_X + tx, nt = TA_X * TA_Y;
@@ -779,6 +781,11 @@ __global__ void __launch_bounds__(TA_X * TA_Y, 4) k_tracer_adv_t(Dev d, const fl
   const long long id = kb + base;
   const float w0 = t.w[r][cc];
   const float ck = t.T[r][cc], sk = t.S[r][cc];
+  if (topT && k == 0) {  // ledger mode: the rigid-lid surface flux Fz[0] c[0] of the substep, summed
+    const float fz0 = ld(Fz, id);
+    topT[base] = (first ? 0.f : topT[base]) + fz0 * ck;
+    topS[base] = (first ? 0.f : topS[base]) + fz0 * sk;
+  }
   float aT = 0.f, aS = 0.f;
   if (w0 != 0.f) {
     const uint64_t bits = __ldg(d.wbits + base);
@@ -894,6 +901,10 @@ __global__ void __launch_bounds__(128) k_tracer_rest(Dev d, RestArgs a) {
       const float w = wetf(bits, k);
       const float convT = (fT - gT) * d.vc.inv_dz_node[k] * w;
       const float convS = (fS - gS) * d.vc.inv_dz_node[k] * w;
+      if (a.convT) {
+        a.convT[id] = convT;
+        a.convS[id] = convS;
+      }
       rest_store(d, a, id, base, k, w, ld(a.accT, id) * a.inv_na + convT, ld(a.accS, id) * a.inv_na + convS);
       fT = gT; fS = gS; cT = nT; cS = nS;
     }
@@ -933,6 +944,10 @@ __global__ void __launch_bounds__(128) k_tracer_rest(Dev d, RestArgs a) {
   const float inv_nc = 1.f / (float)a.nc;
   for (int k = 0; k < nz; ++k) {
     const long long id = base + (long long)k * d.plane;
+    if (a.convT) {
+      a.convT[id] = sT[k] * inv_nc;
+      a.convS[id] = sS[k] * inv_nc;
+    }
     rest_store(d, a, id, base, k, wetf(bits, k), ld(a.accT, id) * a.inv_na + sT[k] * inv_nc,
                ld(a.accS, id) * a.inv_na + sS[k] * inv_nc);
   }

@@ -32,6 +32,7 @@ struct RestArgs {
   float dt, inv_na;
   int nc, stage;
   int no_conv;  // convective mixing carried by the learned closure instead
+  float *convT, *convS;  // ledger mode: the convective tendency per point (null otherwise)
 };
 
 // 2.5-D tracer advection tile
@@ -116,7 +117,8 @@ __global__ void k_madv(Dev d, const float* u, const float* v, const float* Fz, f
 __global__ void k_dealias_lon(Dev d, FftPlan plan, const float* Ayu, const float* Ayv, float* Au, float* Av,
                               int lines_per_block);
 __global__ void k_tracer_adv_t(Dev d, const float* T, const float* S, const float* u, const float* v, const float* Fz,
-                               float* accT, float* accS, float* Tn, float* Sn, float dts, int first, int last);
+                               float* accT, float* accS, float* Tn, float* Sn, float dts, int first, int last,
+                               float* topT, float* topS);
 __global__ void k_tracer_rest(Dev d, RestArgs a);
 __global__ void k_pgf(Dev d, PgfArgs a);
 __global__ void k_bt_forcing(Dev d, const float* frx, const float* fry, double* Fx, double* Fy, const float* eta32,
@@ -141,7 +143,9 @@ struct ProjArgs {
   double* part;         // [blocks][ZM_PJ_SUMS] block partial sums
   unsigned *bar, *err;
   int* stats;           // iterations of each solve (3), refinement solves run
+  double* norms;        // ledger mode: squared surface-transport norms before / after (null otherwise)
   double tol2, trtol2;  // tol^2, transport rtol^2
+  double dtg;           // dt g
   int niter, refinements;
 };
 __global__ void k_proj_coef(Dev d, const double* dzn, const double* cosd, const double* area, double* cx, double* cy,
@@ -150,6 +154,36 @@ __global__ void k_proj_rhs(Dev d, const float* u, const float* v, const double* 
                            const double* area, double dtg, double* b);
 __global__ void k_proj_cg(Dev d, ProjArgs a);
 __global__ void k_proj_correct(Dev d, float* u, float* v, const double* psi, const double* cosd, double dtg);
+// FP64 stage/source ledger of one step (diagnostics/budgets.py:62-288), zm_ledger.cu.
+// Accumulator layout (doubles) of zm_ledger_step, documented in zm_b200.h.
+#define ZM_LED_STAGE 0      // [6][3] stage changes (heat J, salt kg, volume m^3)
+#define ZM_LED_SCALE 18     // [3] summed magnitudes of the stage changes
+#define ZM_LED_SOURCE 21    // [9][3] source inputs
+#define ZM_LED_PROC 48      // [4][3] nonlinear process changes
+#define ZM_LED_PSCALE 60    // [3] their summed magnitudes
+#define ZM_LED_ADVB 63      // [3] advective flux through the surface
+#define ZM_LED_PROJ 66      // squared transport norms before/after the projection, worst ratio
+#define ZM_LED_OBS 69       // [3] observed change over the step
+#define ZM_LED_DISP 72      // [3] eta * surface tracer change
+#ifndef ZM_LED_COUNT
+#define ZM_LED_COUNT 75
+#endif
+constexpr int LED_Q = 16;   // sums per reduction at most
+struct LedFold {
+  int dst[LED_Q];           // accumulator index of each sum, -1 to drop it
+  double scale[LED_Q];      // factor applied to the sum before it is added
+};
+__global__ void k_led_diff(Dev d, const float* Tb, const float* Sb, const float* eb, const float* Ta, const float* Sa,
+                           const float* ea, const double* area, const double* dzn, double* part);
+__global__ void k_led_rk(Dev d, const float* Tev, const float* Sev, const float* accT, const float* accS,
+                         const float* topT, const float* topS, const float* convT, const float* convS, const float* Fz,
+                         float inv_na, const double* area, const double* dzn, double* part);
+__global__ void k_led_sponge(Dev d, const float* Tb, const float* Sb, const float* dec, const float* Tc,
+                             const float* Sc, const double* area, const double* dzn, double* part);
+__global__ void k_led_disp(Dev d, const float* eb, const float* Tb, const float* Sb, const float* ea, const float* Ta,
+                           const float* Sa, const double* area, double* part);
+__global__ void k_led_fold(const double* part, int nblocks, int nq, LedFold f, double* acc);
+__global__ void k_led_proj(const double* norms, double* acc);
 __global__ void k_ref_to_int3(Dev d, const float* src, float* dst, float offset);
 __global__ void k_int_to_ref3(Dev d, const float* src, float* dst, float offset);
 __global__ void k_ref_to_int2(Dev d, const float* src, float* dst);

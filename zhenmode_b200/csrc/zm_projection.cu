@@ -351,7 +351,28 @@ __global__ void __launch_bounds__(PJ_THREADS, 1) k_proj_cg(Dev d, ProjArgs a) {
       const int g = idx2(d, j, i);
       a.psi[g] = __ldcg(a.psi + g) + __ldcg(a.x + g);
     }
-    if (q + 1 < a.refinements && !grid_barrier(a.bar, a.err, gridDim.x, ZM_BT_BARRIER_POLLS)) return;
+    // the next residual reads the neighbours' psi
+    if (q + 1 < a.refinements || a.norms)
+      if (!grid_barrier(a.bar, a.err, gridDim.x, ZM_BT_BARRIER_POLLS)) return;
+  }
+  if (a.norms) {
+    // ledger mode: squared surface-transport norms of the input and of the
+    // corrected velocity, (dt g)^2 sum b^2 / area and (dt g)^2 sum res^2 / area
+    // (diagnostics/budgets.py:175-183)
+    double s4[1] = {0.0};
+    for (int c = t0; c < ncell; c += stride) {
+      const int j = c / d.nx, i = c - j * d.nx;
+      const int g = idx2(d, j, i);
+      double pc;
+      const double res = __ldcg(a.b + g) - apply_a(d, a, j, i, [&](int h) { return __ldcg(a.psi + h); }, pc);
+      s4[0] += res * res * __ldg(a.rarea + g);
+    }
+    double t4[1];
+    if (!reduce(a, red, s4, t4)) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      a.norms[0] = a.dtg * a.dtg * t[2];
+      a.norms[1] = a.dtg * a.dtg * t4[0];
+    }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     a.stats[0] = it[0];

@@ -76,6 +76,10 @@ struct zm_solver {
   float* kappa3 = nullptr;       // [nz-1][ny][P] diffusivity per interface
   unsigned* cl_count = nullptr;  // [0] fallback columns of the last step, [1] tensor-core wait errors
   float cl_bound = 8.f;
+  // FP64 stage/source ledger (zm_ledger_step): buffers allocated on first use
+  bool ledger_on = false;
+  double *led_acc = nullptr, *led_part = nullptr, *led_area = nullptr, *led_dzn = nullptr, *led_norms = nullptr;
+  float *led_convT = nullptr, *led_convS = nullptr, *led_topT = nullptr, *led_topS = nullptr;
   // lateral sponge of the linear half step (null when off): decay per column, targets as anomalies
   float *sp_dec = nullptr, *sp_Tc = nullptr, *sp_Sc = nullptr;
   // column-divergence projection of the stage-2 advective velocity (off unless project_adv_vel)
@@ -201,6 +205,14 @@ struct zm_solver {
                                        closure_on ? kappa3 : nullptr);
       pe(s);
     }
+    if (ledger_on) led_stage(s, 0, src.T, src.S, nullptr, dst.T, dst.S, nullptr);  // step.py:138-140
+    if (sp_dec && ledger_on) {  // step.py:158-161, from the diffused state
+      k_led_sponge<<<led_grid(), dim3(32, 8), 0, s>>>(d, dst.T, dst.S, sp_dec, sp_Tc, sp_Sc, led_area, led_dzn,
+                                                      led_part);
+      const int b = ZM_LED_STAGE + 3;
+      led_fold(s, 6, {{ZM_LED_SOURCE + 18, kHeat}, {ZM_LED_SOURCE + 19, kSalt}, {b, kHeat}, {b + 1, kSalt},
+                      {ZM_LED_SCALE, kHeat}, {ZM_LED_SCALE + 1, kSalt}});
+    }
     if (sp_dec) {  // lateral sponge after the diffusion (step.py:142-156)
       const dim3 c(32, 8);
       pb(ZM_K_LIN_FINISH, s);
@@ -221,18 +233,20 @@ struct zm_solver {
       float* nS = (n % 2 == 0) ? SsA : SsB;
       pb(ZM_K_TRACER_ADV, s);
       k_tracer_adv_t<<<dim3((nx + TA_X - 1) / TA_X, (ny + TA_Y - 1) / TA_Y, nz), dim3(TA_X, TA_Y), 0, s>>>(
-          d, cT, cS, u, v, Fz, accT, accS, nT, nS, dts, n == 0, n == adv_nsub - 1);
+          d, cT, cS, u, v, Fz, accT, accS, nT, nS, dts, n == 0, n == adv_nsub - 1, ledger_on ? led_topT : nullptr,
+          ledger_on ? led_topS : nullptr);
       pe(s);
       cT = nT;
       cS = nS;
     }
     RestArgs a{T, S, accT, accS, Tbase, Sbase, dT1, dS1, To, So, (float)dt, 1.f / (float)adv_nsub, conv_nsub, stage,
-               closure_on ? 1 : 0};
+               closure_on ? 1 : 0, ledger_on ? led_convT : nullptr, ledger_on ? led_convS : nullptr};
     const dim3 c(32, 4);
     pb(ZM_K_TRACER_REST, s);
     k_tracer_rest<<<grid2(c), c, 0, s>>>(d, a);
     pe(s);
     check_launch();
+    if (ledger_on) led_rk(s, T, S);  // tendencies.py:211-214
   }
 
   void pgf(cudaStream_t s, PgfArgs a) {
@@ -304,13 +318,66 @@ struct zm_solver {
     if (bt_done) ZM_CUDA(cudaEventRecord(bt_done, s));
   }
 
+  // ---- ledger reductions (each: one partial-sum kernel, then the in-order fold)
+  static constexpr double kHeat = 1025.0 * 3992.0, kSalt = 1025.0 / 1000.0;
+  dim3 led_grid() const { return grid2(dim3(32, 8)); }
+  void led_fold(cudaStream_t s, int nq, std::initializer_list<std::pair<int, double>> dst) {
+    LedFold f{};
+    int q = 0;
+    for (auto& e : dst) {
+      f.dst[q] = e.first;
+      f.scale[q] = e.second;
+      ++q;
+    }
+    for (; q < LED_Q; ++q) f.dst[q] = -1;
+    const dim3 g = led_grid();
+    k_led_fold<<<1, 32, 0, s>>>(led_part, (int)(g.x * g.y), nq, f, led_acc);
+    check_launch();
+  }
+  // stage change between two states into stage `st_idx` (and the change scale)
+  void led_stage(cudaStream_t s, int st_idx, const float* Tb, const float* Sb, const float* eb, const float* Ta,
+                 const float* Sa, const float* ea) {
+    k_led_diff<<<led_grid(), dim3(32, 8), 0, s>>>(d, Tb, Sb, eb, Ta, Sa, ea, led_area, led_dzn, led_part);
+    const int b = ZM_LED_STAGE + 3 * st_idx;
+    led_fold(s, 6, {{b, kHeat}, {b + 1, kSalt}, {b + 2, 1.0}, {ZM_LED_SCALE, kHeat}, {ZM_LED_SCALE + 1, kSalt},
+                    {ZM_LED_SCALE + 2, 1.0}});
+  }
+  // one tracer residual's sources, processes and surface flux over dt/2
+  void led_rk(cudaStream_t s, const float* Tev, const float* Sev) {
+    k_led_rk<<<led_grid(), dim3(32, 8), 0, s>>>(d, Tev, Sev, accT, accS, led_topT, led_topS, led_convT, led_convS,
+                                                Fz, 1.f / (float)adv_nsub, led_area, led_dzn, led_part);
+    const double h = kHeat * dt / 2.0, sl = kSalt * dt / 2.0;
+    const int P0 = ZM_LED_PROC, P1 = ZM_LED_PROC + 3, S0 = ZM_LED_SOURCE;
+    led_fold(s, 16, {{P0, h}, {ZM_LED_PSCALE, h}, {P0 + 1, sl}, {ZM_LED_PSCALE + 1, sl},
+                     {P1, h}, {ZM_LED_PSCALE, h}, {P1 + 1, sl}, {ZM_LED_PSCALE + 1, sl},
+                     {S0, h}, {S0 + 3, h}, {S0 + 6, h}, {S0 + 9, h}, {S0 + 12 + 1, sl}, {S0 + 15 + 1, sl},
+                     {ZM_LED_ADVB, h}, {ZM_LED_ADVB + 1, sl}});
+  }
+  void ensure_ledger() {
+    if (led_acc) return;
+    const dim3 g = led_grid();
+    led_acc = alloc<double>(ZM_LED_COUNT);
+    led_part = alloc<double>((size_t)g.x * g.y * LED_Q * 2);
+    led_norms = alloc<double>(2);
+    led_convT = f3();
+    led_convS = f3();
+    led_topT = f2();
+    led_topS = f2();
+  }
+
   // Column-divergence projection of (u, v) in place (projection.py:64-127).
   void project(cudaStream_t s, float* u, float* v) {
     const dim3 c(32, 8);
     pb(ZM_K_PROJECTION, s);
     k_proj_rhs<<<grid2(c), c, 0, s>>>(d, u, v, pj_dzn, pj_cos, pj_area, pj_dtg, const_cast<double*>(pj.b));
     pe(s);
-    coop_launch(s, ZM_K_PROJECTION, k_proj_cg, pj_blocks, PJ_THREADS, 0, d, pj);
+    ProjArgs pa = pj;
+    pa.norms = ledger_on ? led_norms : nullptr;
+    coop_launch(s, ZM_K_PROJECTION, k_proj_cg, pj_blocks, PJ_THREADS, 0, d, pa);
+    if (ledger_on) {
+      k_led_proj<<<1, 32, 0, s>>>(led_norms, led_acc);
+      check_launch();
+    }
     pb(ZM_K_PROJECTION, s);
     k_proj_correct<<<grid2(c), c, 0, s>>>(d, u, v, pj.psi, pj_cos, pj_dtg);
     pe(s);
@@ -435,8 +502,22 @@ struct zm_solver {
     if (closure_on) closure(s, in);
     linear_half(s, in, s1);
     nonlinear(s, s1, s2);
+    if (ledger_on) led_stage(s, 2, s1.T, s1.S, nullptr, s2.T, s2.S, nullptr);  // step.py:366-368
     linear_half(s, s2, s1);
     barotropic_and_final(s, s1, eta[from], in, st[to], eta[to]);
+    if (ledger_on) {
+      // free surface (step.py:425-427): only eta changes; then the polar cap and
+      // the land hold (step.py:452-453); dynamic ice is absent (no change)
+      led_stage(s, 3, s1.T, s1.S, eta[from], s1.T, s1.S, eta[to]);
+      led_stage(s, 4, s1.T, s1.S, nullptr, st[to].T, st[to].S, nullptr);
+      // observed change (budgets.py:230-231) and eta times the surface tracers
+      k_led_diff<<<led_grid(), dim3(32, 8), 0, s>>>(d, in.T, in.S, eta[from], st[to].T, st[to].S, eta[to], led_area,
+                                                    led_dzn, led_part);
+      led_fold(s, 6, {{ZM_LED_OBS, kHeat}, {ZM_LED_OBS + 1, kSalt}, {ZM_LED_OBS + 2, 1.0}});
+      k_led_disp<<<led_grid(), dim3(32, 8), 0, s>>>(d, eta[from], in.T, in.S, eta[to], st[to].T, st[to].S, led_area,
+                                                    led_part);
+      led_fold(s, 2, {{ZM_LED_DISP, kHeat}, {ZM_LED_DISP + 1, kSalt}});
+    }
   }
 
   void monitor(cudaStream_t s, int which) {
@@ -1009,6 +1090,7 @@ void build(zm_solver* s, const zm_grid* g, const zm_params* p) {
     a.niter = p->projection_niter;
     a.refinements = p->projection_max_refinements;
     s->pj_dtg = p->dt * 9.81;
+    a.dtg = s->pj_dtg;
     s->proj_on = true;
   }
   const size_t nref3 = (size_t)nx * ny * nz;
@@ -1026,6 +1108,12 @@ void build(zm_solver* s, const zm_grid* g, const zm_params* p) {
     }
     s->area64 = s->upload(area);
     s->width64 = s->upload(width);
+    // the ledger's cell areas in the internal layout and node thicknesses
+    std::vector<double> area_int(s->n2, 0.0);
+    for (int i = 0; i < nx; ++i)
+      for (int j = 0; j < ny; ++j) area_int[(size_t)j * P + i] = g->dx_2d[(size_t)i * ny + j] * g->dy;
+    s->led_area = s->upload(area_int);
+    s->led_dzn = s->upload(width);
     int sms = 0;
     ZM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
     s->bblocks = std::max(1, std::min(4 * sms, (int)(((long long)nx * ny + 7) / 8)));
@@ -1595,6 +1683,32 @@ int zm_status(zm_solver* s, int32_t* monitor_code) {
     e = cudaMemcpy(&berr, s->pj.err, sizeof(berr), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return fail(s, Err{ZM_ERR_CUDA, std::string("zm_status: ") + cudaGetErrorString(e)});
     if (berr) return fail(s, Err{ZM_ERR_TIMEOUT, "column projection grid barrier timed out"});
+  }
+  return ZM_OK;
+}
+
+int zm_ledger_step(zm_solver* s, void* stream, const zm_state* in, zm_state* out, double* raw, int32_t n) {
+  if (!s || !in || !out || !raw || n < ZM_LED_COUNT) return ZM_ERR_INVALID;
+  cudaStream_t st = (cudaStream_t)stream;
+  try {
+    s->ensure_ledger();
+    ZM_CUDA(cudaMemsetAsync(s->led_acc, 0, ZM_LED_COUNT * sizeof(double), st));
+    s->load(st, in, s->st[s->cur], s->eta[s->cur]);
+    const int a = s->cur, b = 1 - s->cur;
+    s->ledger_on = true;
+    try {
+      s->full_step(st, a, b);
+    } catch (...) {
+      s->ledger_on = false;
+      throw;
+    }
+    s->ledger_on = false;
+    s->cur = b;
+    s->store(st, s->st[b], s->eta[b], out);
+    ZM_CUDA(cudaMemcpyAsync(raw, s->led_acc, ZM_LED_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st));
+    ZM_CUDA(cudaStreamSynchronize(st));
+  } catch (const Err& e) {
+    return fail(s, e);
   }
   return ZM_OK;
 }

@@ -645,6 +645,7 @@ def make_solver_global(grid, physics, dt, forcing=None,
 
     step.solver = solver
     step.advance = _run
+    step.factory_forcing = (tau_x, tau_y, q_heat)
     step.set_forcing = set_forcing
     step.set_forcing_seasonal = set_forcing_seasonal
     step.budget_diagnostics = budget_diagnostics
@@ -658,7 +659,7 @@ def make_solver_global(grid, physics, dt, forcing=None,
     if return_params:
         params = dict(n_subcyc=solver.n_subcyc, nu_nsub=solver.n_nu, adv_nsub=solver.adv_nsub,
                       conv_nsub=solver.conv_nsub, dt_bt=float(dt) / solver.n_subcyc, H_sw=float(np.sum(grid.dz)),
-                      rho0=RHO_0)
+                      rho0=RHO_0, dt=float(dt), step=step)
 
         def terms_fn(state):
             raise NotImplementedError("tracer term decomposition is not implemented on the B200 path")
