@@ -588,7 +588,8 @@ __global__ void __launch_bounds__(128) k_fz(Dev d, const float* __restrict__ u, 
 // of the dealias filter, [1,4,6,4,1]/16 on edge-held rows
 // (numerics/horizontal.py:283-305).  The longitude 2/3-rule half runs in the
 // FFT kernel; the two filters act on different axes and commute.
-constexpr int MADV_TY = 8;
+// MADV_TY (60) rows per tile: the 8 warps take 8 of the 64 rows (tile + 2-row
+// halo each side) per pass, so the halo adds 7 % of work instead of 50 % at 8 rows
 __device__ __forceinline__ void adv_point(const Dev& d, const float* __restrict__ u, const float* __restrict__ v,
                                           const float* __restrict__ Fz, int k, int j, int i, float& au, float& av) {
   const Nb n = nb(d, j, i);
@@ -648,19 +649,21 @@ __global__ void __launch_bounds__(256) k_madv(Dev d, const float* __restrict__ u
     sv[r][threadIdx.x] = av;
   }
   __syncthreads();
-  const int j = j0 + threadIdx.y;
-  if (i >= d.nx || j >= d.ny) return;
   // rows j-2..j+2 clamped to the domain: with the tile loaded on clamped rows
   // the clamp is already applied at the tile edges except inside the tile.
   auto row = [&](int jj) { jj = jj < 0 ? 0 : (jj >= d.ny ? d.ny - 1 : jj); return jj - (j0 - 2); };
   const int t = threadIdx.x;
-  const float fu = (su[row(j - 2)][t] + 4.f * su[row(j - 1)][t] + 6.f * su[row(j)][t] + 4.f * su[row(j + 1)][t] +
-                    su[row(j + 2)][t]) / 16.f;
-  const float fv = (sv[row(j - 2)][t] + 4.f * sv[row(j - 1)][t] + 6.f * sv[row(j)][t] + 4.f * sv[row(j + 1)][t] +
-                    sv[row(j + 2)][t]) / 16.f;
-  const long long id = idx3(d, k, j, i);
-  Ayu[id] = fu;
-  Ayv[id] = fv;
+  for (int jr = threadIdx.y; jr < MADV_TY; jr += blockDim.y) {
+    const int j = j0 + jr;
+    if (i >= d.nx || j >= d.ny) continue;
+    const float fu = (su[row(j - 2)][t] + 4.f * su[row(j - 1)][t] + 6.f * su[row(j)][t] + 4.f * su[row(j + 1)][t] +
+                      su[row(j + 2)][t]) / 16.f;
+    const float fv = (sv[row(j - 2)][t] + 4.f * sv[row(j - 1)][t] + 6.f * sv[row(j)][t] + 4.f * sv[row(j + 1)][t] +
+                      sv[row(j + 2)][t]) / 16.f;
+    const long long id = idx3(d, k, j, i);
+    Ayu[id] = fu;
+    Ayv[id] = fv;
+  }
 }
 
 // Minmod slope over wet neighbours (dynamics/transport.py:199-213).

@@ -35,6 +35,8 @@ struct RestArgs {
   float *convT, *convS;  // ledger mode: the convective tendency per point (null otherwise)
 };
 
+// momentum-advection tile rows (k_madv)
+constexpr int MADV_TY = 60;
 // 2.5-D tracer advection tile
 constexpr int TA_X = 32, TA_Y = 16;
 // temporally blocked nu_h subcycles: tile width, rows per thread, subcycles per pass

@@ -268,7 +268,7 @@ struct zm_solver {
     pe(s);
     const dim3 m(32, 8);
     pb(ZM_K_MADV, s);
-    k_madv<<<dim3((nx + 31) / 32, (ny + 7) / 8, nz), m, 0, s>>>(d, src.u, src.v, Fz, Ayu, Ayv);
+    k_madv<<<dim3((nx + 31) / 32, (ny + MADV_TY - 1) / MADV_TY, nz), m, 0, s>>>(d, src.u, src.v, Fz, Ayu, Ayv);
     pe(s);
     const int nlines = ny * nz;
     pb(ZM_K_DEALIAS, s);
