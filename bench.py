@@ -59,6 +59,19 @@ def algo_fields_per_launch(cls, launches_per_step, n_nu):
     return float(ALGO_FIELDS[cls])
 
 
+def max_over_ranks(value, device="cuda"):
+    """The largest of one float over all ranks of the process group (every
+    rank's step time: the job is as fast as its slowest replica); the value
+    itself without a group."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def sim_years_per_day(ms_per_step, dt):
     return (86400.0 / (ms_per_step * 1e-3)) * dt / SECONDS_PER_YEAR
 
@@ -480,10 +493,7 @@ def main():
     ms = e0.elapsed_time(e1) / args.steps
     code = ctypes.c_int32()
     solver.check(solver.lib.zm_status(solver.handle, ctypes.byref(code)), "zm_status")
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms)
     kernels_per_step = solver.kernels_per_step()
 
     # per-kernel-class breakdown of one step (CUDA events around every launch)
@@ -524,11 +534,7 @@ def main():
                          "zm_step_host")
         e3.record(stream)
         torch.cuda.synchronize()
-        ems = e2.elapsed_time(e3) / args.e2e_steps
-        if world > 1:
-            t = torch.tensor([ems], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+        ems = max_over_ranks(e2.elapsed_time(e3) / args.e2e_steps)
         nbytes = sum(h.numel() * h.element_size() for h in host)
         e2e = {"value": world * sim_years_per_day(ems, wl.dt), "unit": "sim-years/day", "ms_per_step": ems,
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes}
