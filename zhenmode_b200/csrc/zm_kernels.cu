@@ -588,8 +588,6 @@ __global__ void __launch_bounds__(128) k_fz(Dev d, const float* __restrict__ u, 
 // of the dealias filter, [1,4,6,4,1]/16 on edge-held rows
 // (numerics/horizontal.py:283-305).  The longitude 2/3-rule half runs in the
 // FFT kernel; the two filters act on different axes and commute.
-// MADV_TY (60) rows per tile: the 8 warps take 8 of the 64 rows (tile + 2-row
-// halo each side) per pass, so the halo adds 7 % of work instead of 50 % at 8 rows
 __device__ __forceinline__ void adv_point(const Dev& d, const float* __restrict__ u, const float* __restrict__ v,
                                           const float* __restrict__ Fz, int k, int j, int i, float& au, float& av) {
   const Nb n = nb(d, j, i);
@@ -632,6 +630,9 @@ __device__ __forceinline__ void adv_point(const Dev& d, const float* __restrict_
   av = -(uc * dvdx + vc * dvdy + w * dvdz);
 }
 
+// One block: 32 columns x MADV_TY (60) rows of one level.  The 8 warps take 8
+// of the 64 rows (tile and a 2-row halo on each side) per pass, so the halo
+// adds 7 % of the point work (50 % with 8-row tiles).
 __global__ void __launch_bounds__(256) k_madv(Dev d, const float* __restrict__ u, const float* __restrict__ v,
                                               const float* __restrict__ Fz, float* __restrict__ Ayu,
                                               float* __restrict__ Ayv) {
