@@ -890,13 +890,28 @@ __global__ void __launch_bounds__(128) k_tracer_rest(Dev d, RestArgs a) {
     const float kc = d.kappa_conv;
     float fT = 0.f, fS = 0.f;
     float cT = ld(a.Tev, base), cS = ld(a.Sev, base);
-#pragma unroll 4
+    // the next level's inputs are loaded before this level's stores: the
+    // argument pointers may alias, so loads issued after a store would wait
+    const bool st2 = a.stage != 1;
+    float qaT = ld(a.accT, base), qaS = ld(a.accS, base), qbT = ld(a.Tbase, base), qbS = ld(a.Sbase, base);
+    float qdT = st2 ? ld(a.dT1, base) : 0.f, qdS = st2 ? ld(a.dS1, base) : 0.f;
+#pragma unroll 2
     for (int k = 0; k < nz; ++k) {
       const long long id = base + (long long)k * d.plane;
       float nT = 0.f, nS = 0.f, gT = 0.f, gS = 0.f;
+      float naT = 0.f, naS = 0.f, nbT = 0.f, nbS = 0.f, ndT = 0.f, ndS = 0.f;
       if (k + 1 < nz) {
-        nT = ld(a.Tev, id + d.plane);
-        nS = ld(a.Sev, id + d.plane);
+        const long long nid = id + d.plane;
+        nT = ld(a.Tev, nid);
+        nS = ld(a.Sev, nid);
+        naT = ld(a.accT, nid);
+        naS = ld(a.accS, nid);
+        nbT = ld(a.Tbase, nid);
+        nbS = ld(a.Sbase, nid);
+        if (st2) {
+          ndT = ld(a.dT1, nid);
+          ndS = ld(a.dS1, nid);
+        }
         if ((allow >> k) & 1ull) {
           gT = -kc * (nT - cT) * d.vc.inv_dz_iface[k];
           gS = -kc * (nS - cS) * d.vc.inv_dz_iface[k];
@@ -909,8 +924,29 @@ __global__ void __launch_bounds__(128) k_tracer_rest(Dev d, RestArgs a) {
         a.convT[id] = convT;
         a.convS[id] = convS;
       }
-      rest_store(d, a, id, base, k, w, ld(a.accT, id) * a.inv_na + convT, ld(a.accS, id) * a.inv_na + convS);
+      // rest_store's arithmetic, on the prefetched values
+      float rT = qaT * a.inv_na + convT, rS = qaS * a.inv_na + convS;
+      if (k == 0) {
+        const float sst = cT, sss = cS;
+        const float hf = w / (d.dz_surface * kRho0 * kCp);
+        const float tatm = __ldg(d.tatm + base);
+        rT += __ldg(d.qheat + base) * hf + d.lambda_bulk * (tatm - sst) * hf + __ldg(d.cbulk + base) * (tatm - sst) * hf +
+              __ldg(d.rest_c + base) * (__ldg(d.rest_T + base) - sst);
+        rS += d.restore_S * (__ldg(d.sref + base) - sss) + (sst <= d.ice_freeze ? d.ice_salt : 0.f);
+      }
+      rT *= w;
+      rS *= w;
+      if (!st2) {
+        a.dT1[id] = rT;
+        a.dS1[id] = rS;
+        a.To[id] = qbT + rT * a.dt;
+        a.So[id] = qbS + rS * a.dt;
+      } else {
+        a.To[id] = qbT + 0.5f * (qdT + rT) * a.dt;
+        a.So[id] = qbS + 0.5f * (qdS + rS) * a.dt;
+      }
       fT = gT; fS = gS; cT = nT; cS = nS;
+      qaT = naT; qaS = naS; qbT = nbT; qbS = nbS; qdT = ndT; qdS = ndS;
     }
     return;
   }
@@ -1064,13 +1100,32 @@ __global__ void __launch_bounds__(128) k_pgf(Dev d, PgfArgs a) {
     a.vbt0[cc] = sv;
     return;
   }
+  // second pass; the next level's inputs are loaded before this level's
+  // stores (the argument pointers may alias, so later loads would wait)
+  const bool m2 = a.mode == 2;
+  float qx = a.gsx[cc], qy = a.gsy[cc], qAu = ld(a.Au, cc), qAv = ld(a.Av, cc), qu = ld(a.u1, cc), qv = ld(a.v1, cc);
+  float qpu = m2 ? ld(a.Ppu, cc) : 0.f, qpv = m2 ? ld(a.Ppv, cc) : 0.f;
+#pragma unroll 1
   for (int k = 0; k < d.nz; ++k) {
     const long long id = (long long)k * d.plane + cc;
+    float nx_ = 0.f, ny_ = 0.f, nAu = 0.f, nAv = 0.f, nu = 0.f, nv = 0.f, npu = 0.f, npv = 0.f;
+    if (k + 1 < d.nz) {
+      const long long nid = id + d.plane;
+      nx_ = a.gsx[nid];
+      ny_ = a.gsy[nid];
+      nAu = ld(a.Au, nid);
+      nAv = ld(a.Av, nid);
+      nu = ld(a.u1, nid);
+      nv = ld(a.v1, nid);
+      if (m2) {
+        npu = ld(a.Ppu, nid);
+        npv = ld(a.Ppv, nid);
+      }
+    }
     const float w = wetf(m0, k);
-    const float Pu = (a.gsx[id] - Fx) * w;
-    const float Pv = (a.gsy[id] - Fy) * w;
-    const float Au = ld(a.Au, id), Av = ld(a.Av, id);
-    const float u1 = ld(a.u1, id), v1 = ld(a.v1, id);
+    const float Pu = (qx - Fx) * w;
+    const float Pv = (qy - Fy) * w;
+    const float Au = qAu, Av = qAv, u1 = qu, v1 = qv;
     if (a.mode == 1) {
       a.Pu[id] = Pu;
       a.Pv[id] = Pv;
@@ -1078,9 +1133,10 @@ __global__ void __launch_bounds__(128) k_pgf(Dev d, PgfArgs a) {
       a.vo[id] = v1 + (Av + Pv) * a.dt;
     } else {
       const float dec = (k == d.nz - 1 && w != 0.f) ? a.bottom_decay : 1.f;
-      a.uo[id] = (u1 + 0.5f * ((Au + ld(a.Ppu, id)) + (Au + Pu)) * a.dt) * dec;
-      a.vo[id] = (v1 + 0.5f * ((Av + ld(a.Ppv, id)) + (Av + Pv)) * a.dt) * dec;
+      a.uo[id] = (u1 + 0.5f * ((Au + qpu) + (Au + Pu)) * a.dt) * dec;
+      a.vo[id] = (v1 + 0.5f * ((Av + qpv) + (Av + Pv)) * a.dt) * dec;
     }
+    qx = nx_; qy = ny_; qAu = nAu; qAv = nAv; qu = nu; qv = nv; qpu = npu; qpv = npv;
   }
 }
 
