@@ -226,3 +226,31 @@ def test_barotropic_kernel_choice_follows_grid_size():
     assert step.solver.bt_blocks == 0
     with pytest.raises(UnsupportedOption):
         make_solver_global(grid, wl.physics, wl.dt, barotropic_kernel="resident", **kw)
+
+
+def test_deepest_grid_matches_oracle():
+    """nz = 64, the limit of the one-word-per-column wet mask (bit 63 wet at
+    the deep columns), one step of the 0.5-degree option set on a moving state."""
+    grid, physics, dt, kw, T, S = workloads.make_case("plain", 24, 16, 64, dtype="float32")
+    kw = {k: v for k, v in kw.items() if k != "dtype"}
+    gpu, p = gu.build_pair(grid, physics, dt, kw)
+    assert int(np.asarray(grid.wet_mask_3d)[:, :, 63].sum()) > 0
+    from oracle.params import init_state
+    st = init_state(p, T, S)
+    wet3 = np.asarray(grid.wet_mask_3d)
+    lat = np.radians(np.asarray(grid.lat))[None, :, None]
+    st["u"] = 0.1 * np.cos(lat) * wet3
+    st["v"] = 0.02 * np.sin(2 * lat) * wet3
+    st = gu.f32(st)
+    want = ostep.step(dict(st), p)
+    got = gu.run_steps(gpu, st, 1)
+    errs = gu.errors(got, want)
+    assert max(errs.values()) < STEP_TOL, errs
+
+
+def test_longitude_sizes_outside_2_3_5_are_refused():
+    """The longitude filter's FFT takes nx = 2^a 3^b 5^c (zm_create: ZM_ERR_UNSUPPORTED)."""
+    from zhenmode_b200 import UnsupportedOption, make_solver_global
+    grid, physics, dt, kw, _, _ = workloads.make_case("plain", 28, 16, 8, dtype="float32")
+    with pytest.raises(UnsupportedOption):
+        make_solver_global(grid, physics, dt, **kw)

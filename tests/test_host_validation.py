@@ -80,3 +80,10 @@ def test_unknown_scheme_keyword(case):
         _call(case, not_an_option=1)
     with pytest.raises(ValueError):
         _call(case, vertical_tracer_scheme="bogus")
+
+
+def test_more_than_64_levels_is_unsupported():
+    """The 3-D wet mask is one 64-bit word per column: nz <= 64."""
+    grid, physics, dt, kw, _, _ = workloads.make_case("plain", 24, 12, 65, dtype="float32")
+    with pytest.raises(UnsupportedOption):
+        make_solver_global(grid, physics, dt, **kw)
