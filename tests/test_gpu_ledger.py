@@ -13,7 +13,7 @@ from zhenmode_b200 import JaxStateG, ledger, make_solver_global
 pytestmark = pytest.mark.gpu
 
 # Stage changes and sources are sums of per-cell float32 tracer increments:
-# they are judged against the summed magnitudes of the changes they belong to.
+# they are compared with the summed magnitudes of the changes they belong to.
 # The magnitude sums themselves collect the float32 rounding of every
 # increment without cancellation, hence their looser bound.
 REL = 5e-4

@@ -195,7 +195,7 @@ def test_ledger_matches_reference_budget_step():
             assert got.shape == want.shape, key
             scale = max(float(np.max(np.abs(want))), 1e-300)
             err = float(np.max(np.abs(got - want))) if got.size else 0.0
-            # residual identities are differences of large sums: judged against the sums they close
+            # residual identities are differences of large sums: compared with the sums they close
             if "residual" in key:
                 ref = {"decomposition_residual": "change_scale", "absolute_decomposition_residual": "change_scale",
                        "budget_residual": "change_scale", "absolute_budget_residual": "change_scale",
