@@ -49,6 +49,7 @@ struct BtTile {
   double cosl[BT_PY], cfp[BT_PY], cfm[BT_PY];
   double mean[3][2 * ZM_BT_MAX_NB];         // band-row means: eta*, u, v
   double red[BT_THREADS];
+  double fx[BT_TY][BT_TX], fy[BT_TY][BT_TX], fc[BT_TY][BT_TX];  // forcing and f of the owned cells
   int gj[BT_PY];                            // global row, -1 beyond the walls
   int gx[BT_PX];                            // global column (periodic wrap)
   unsigned char own_c[BT_PX];               // column owned by this block
@@ -203,6 +204,18 @@ __global__ void __launch_bounds__(BT_THREADS, 4) k_bt_loop(Dev d, BtArgs a) {
     t.w[r][c] = __ldg(d.wet2 + g);
     t.ix[r][c] = __ldg(d.inv_dx_d + g);
   }
+  for (int e = tid; e < NT; e += nt) {
+    const int r = e / BT_TX, c = e - r * BT_TX;
+    const int gj = t.gj[r + BT_H];
+    if (gj < 0 || !t.own_c[c + BT_H]) {
+      t.fx[r][c] = t.fy[r][c] = t.fc[r][c] = 0.0;
+      continue;
+    }
+    const int g = idx2(d, gj, t.gx[c + BT_H]);
+    t.fx[r][c] = a.Fx[g];
+    t.fy[r][c] = a.Fy[g];
+    t.fc[r][c] = __ldg(d.fcor_d + g);
+  }
   __syncthreads();
   const double g9 = 9.81;
   for (int n = 0; n < a.nsub; ++n) {
@@ -291,9 +304,9 @@ __global__ void __launch_bounds__(BT_THREADS, 4) k_bt_loop(Dev d, BtArgs a) {
       if (j < d.ny - 1) dyp = (t.E[r + 1][c] - e0) * (w0 * t.w[r + 1][c]) * t.cfp[r];
       if (j > 0) dym = (e0 - t.E[r - 1][c]) * (w0 * t.w[r - 1][c]) * t.cfm[r];
       const double gy = (d.inv_dy_d / t.cosl[r]) * 0.5 * (dyp + dym);
-      const double us = t.U[r][c] + a.dtb * (-g9 * gx + a.Fx[g]);
-      const double vs = t.V[r][c] + a.dtb * (-g9 * gy + a.Fy[g]);
-      const double fd = __ldg(d.fcor_d + g) * a.dtb;
+      const double us = t.U[r][c] + a.dtb * (-g9 * gx + t.fx[r - BT_H][c - BT_H]);
+      const double vs = t.V[r][c] + a.dtb * (-g9 * gy + t.fy[r - BT_H][c - BT_H]);
+      const double fd = t.fc[r - BT_H][c - BT_H] * a.dtb;
       const double den = 1.0 + fd * fd;
       double un = (us + fd * vs) / den * a.drag * w0;
       double vn = (vs - fd * us) / den * a.drag * w0;
