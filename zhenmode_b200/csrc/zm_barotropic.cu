@@ -4,7 +4,8 @@
 // Resident path (k_bt_loop): one cooperative kernel runs all subcycles.  Each
 // block owns one BT_TX x BT_TY tile and keeps its float64 state (eta, ubt,
 // vbt) plus the static fields it stencils over (wet mask, 1/dx) in shared
-// memory, with a two-cell halo, for the whole loop.  Per subcycle:
+// memory, with a two-cell halo, and the forcing and Coriolis parameter of its
+// owned cells, for the whole loop.  Per subcycle:
 //   1  refresh the halo from the neighbours' published values of the previous
 //      subcycle (and apply the polar cap to the velocities);
 //   2  continuity eta* = (eta - dt H div(ubt wm, vbt wm)) wm on the tile and,
