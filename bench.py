@@ -410,9 +410,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", default=None, help="NXxNYxNZ: same option set on another grid (profiling cases)")
-    ap.add_argument("--form", default="plain", choices=["plain", "learned", "ensemble", "precision"],
+    ap.add_argument("--form", default="plain", choices=["plain", "learned", "ensemble", "precision", "projected"],
                     help="learned: train the closure network on the plain model's own columns (30 days, "
-                         "2M rows) first, then time the step with it")
+                         "2M rows) first, then time the step with it; projected: the plain step with the "
+                         "column-divergence projection of the stage-2 advective velocity on")
     ap.add_argument("--closure-days", type=int, default=30)
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default launch shapes (profiling: no autotuner trial launches)")
@@ -447,6 +448,8 @@ def main():
         gnx, gny, gnz = (int(x) for x in args.grid.lower().split("x"))
         wl = dataclasses.replace(wl, nx=gnx, ny=gny, nz=gnz)
     grid, physics, dt, kw, T, S = workloads.make_case(WORKLOAD, wl.nx, wl.ny, wl.nz, dtype="float32")
+    if args.form == "projected":
+        kw = dict(kw, project_adv_vel=True)
     step, init_state, _ = make_solver_global(grid, physics, dt, autotune=not args.no_autotune, **kw)
     solver = step.solver
     st = init_state(T_init=T, S_init=S)
@@ -569,6 +572,10 @@ def main():
         if closure_info is not None:
             closure_info["fallback_columns_last_step"] = step.closure_stats()[0]
             line["closure"] = closure_info
+        if args.form == "projected":
+            it = step.projection_stats()
+            line["projection"] = {"cg_iterations": list(it[:3]), "refinement_solves": it[3],
+                                  "ms_per_step": round(prof.get("projection", (0.0, 0))[0], 4)}
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
