@@ -415,12 +415,12 @@ __global__ void __launch_bounds__(LT_X * LT_Y) k_lin_t(Dev d, const float* __res
   vo[id] = -sn * u + c * v;
 }
 
-// Backward-Euler vertical diffusion, one column per thread (extension: the
-// implicit replacement of the explicit L-step vertical diffusion).  The
-// matrix is (I - s D2) with D2 the node-form operator of d2z on the wet
-// levels 0..kbot (ghost fill below); Thomas algorithm in FP32 plus one step of
-// iterative refinement, residual formed in FP32 against the original
-// right-hand side.  Rows below the deepest wet level are untouched.
+// Backward-Euler vertical diffusion (extension: the implicit replacement of
+// the explicit L-step vertical diffusion).  The matrix is (I - s D2) with D2
+// the node-form operator of d2z on the wet levels 0..kbot (ghost fill below);
+// Thomas algorithm in FP32 plus one step of iterative refinement, residual
+// formed in FP32 against the original right-hand side.  Rows below the
+// deepest wet level are untouched.
 __device__ __forceinline__ void vcoef(const Dev& d, int k, int kb, float s, float& a, float& b, float& c) {
   a = 0.f; c = 0.f; b = 1.f;
   if (k == 0) { b += s * d.vc.d2_top; c = -s * d.vc.d2_top; return; }
@@ -430,125 +430,127 @@ __device__ __forceinline__ void vcoef(const Dev& d, int k, int kb, float s, floa
   if (k < kb) c = -s * d.vc.d2_hi[k]; else b -= s * d.vc.d2_hi[k];
 }
 
-// Backward-Euler vertical diffusion of two fields of one column that share
-// the tridiagonal matrix over the wet levels 0..kbot (lower lo, diagonal dg,
-// upper up): one FP32 factorization, then per field a Thomas solve and one
-// step of iterative refinement with the residual against the original
-// right-hand side.
-__device__ void implicit_pair(const Dev& d, float* __restrict__ fa, float* __restrict__ fb, long long base, int n,
-                              const float* lo, const float* dg, const float* up) {
-  // the two fields' recurrences run interleaved: two independent chains
-  float cp[ZM_MAXZ], inv[ZM_MAXZ], ra[ZM_MAXZ], rb[ZM_MAXZ], xa[ZM_MAXZ], xb[ZM_MAXZ];
-  inv[0] = 1.f / dg[0];
-  cp[0] = up[0] * inv[0];
-  ra[0] = fa[base];
-  rb[0] = fb[base];
-  xa[0] = ra[0] * inv[0];
-  xb[0] = rb[0] * inv[0];
-#pragma unroll 4
-  for (int k = 1; k < n; ++k) {
-    const long long id = base + (long long)k * d.plane;
-    ra[k] = fa[id];
-    rb[k] = fb[id];
-    inv[k] = 1.f / (dg[k] - lo[k] * cp[k - 1]);
-    cp[k] = up[k] * inv[k];
-    xa[k] = (ra[k] - lo[k] * xa[k - 1]) * inv[k];
-    xb[k] = (rb[k] - lo[k] * xb[k - 1]) * inv[k];
-  }
-#pragma unroll 4
-  for (int k = n - 2; k >= 0; --k) {
-    xa[k] -= cp[k] * xa[k + 1];
-    xb[k] -= cp[k] * xb[k + 1];
-  }
-  // residual of the FP32 solution, solved again with the same factorization
-  float ea = 0.f, eb = 0.f;
-#pragma unroll 4
-  for (int k = 0; k < n; ++k) {
-    float aa = dg[k] * xa[k], ab = dg[k] * xb[k];
-    if (k > 0) {
-      aa += lo[k] * xa[k - 1];
-      ab += lo[k] * xb[k - 1];
-    }
-    if (k + 1 < n) {
-      aa += up[k] * xa[k + 1];
-      ab += up[k] * xb[k + 1];
-    }
-    ea = ((ra[k] - aa) - lo[k] * ea) * inv[k];
-    eb = ((rb[k] - ab) - lo[k] * eb) * inv[k];
-    ra[k] = ea;
-    rb[k] = eb;
-  }
-#pragma unroll 4
-  for (int k = n - 2; k >= 0; --k) {
-    ra[k] -= cp[k] * ra[k + 1];
-    rb[k] -= cp[k] * rb[k + 1];
-  }
-#pragma unroll 4
-  for (int k = 0; k < n; ++k) {
-    const long long id = base + (long long)k * d.plane;
-    fa[id] = xa[k] + ra[k];
-    fb[id] = xb[k] + rb[k];
-  }
-}
-
-// One thread per (column, pair): blockIdx.z = 0 solves u and v (nu_v, node
-// form of d2z with the ghost fill) and applies the land hold and the exact
-// Coriolis rotation; blockIdx.z = 1 solves T and S (kappa_v + coastal in the
-// node form, or the learned closure's diffusivity per interface kap3 in the
-// interface-flux form) and applies the land hold.
-__global__ void __launch_bounds__(128) k_implicit_vdiff(Dev d, float* __restrict__ u, float* __restrict__ v,
+// One thread per (column, field); lanes 2c and 2c+1 hold u and v (blockIdx.z
+// = 0: nu_v, node form of d2z with the ghost fill, then the land hold and the
+// exact Coriolis rotation, which swaps values within the lane pair) or T and S
+// (blockIdx.z = 1: kappa_v + coastal in the node form, or the learned
+// closure's diffusivity per interface kap3 in the interface-flux form, then
+// the land hold).  Each thread runs its own sequential Thomas sweeps (the two
+// fields of a pair repeat the same pivots).  The sweeps are latency-bound, so
+// the kernel is held to 32 registers for full occupancy: more independent
+// column chains in flight per SM outweigh a few spilled scalars and the
+// per-thread level arrays in local memory.  Passes over the n = kbot + 1 wet
+// levels:
+//   1. forward elimination, keeping 1 / pivot;
+//   2. back substitution: the FP32 solution x;
+//   3. the residual r - A x (r read again) and its forward elimination;
+//   4. back substitution of the correction e; x + e, hold, rotation, store.
+// The factor up / pivot is formed again where it is needed.
+template <bool KAP>
+__global__ void __launch_bounds__(IV_T, 32) k_implicit_vdiff(Dev d, float* __restrict__ u, float* __restrict__ v,
                                                         float* __restrict__ T, float* __restrict__ S,
                                                         const float* __restrict__ u0, const float* __restrict__ v0,
                                                         const float* __restrict__ T0, const float* __restrict__ S0,
                                                         float dth, const float* __restrict__ kap3) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= d.nx || j >= d.ny) return;
-  const long long base = idx2(d, j, i);
-  const uint64_t bits = wb(d, j, i);
+  const int f = threadIdx.x & 1;
+  const int i = blockIdx.x * (IV_T / 2) + (threadIdx.x >> 1);
+  const int j = blockIdx.y;
   const bool tracers = blockIdx.z == 1;
+  const bool in = i < d.nx;  // lanes past the last column run along (the pair exchange needs every lane) unstored
+  const long long base = idx2(d, j, in ? i : d.nx - 1);
+  float* __restrict__ fld = tracers ? (f ? S : T) : (f ? v : u);
+  const float* __restrict__ hold = tracers ? (f ? S0 : T0) : (f ? v0 : u0);
+  const bool kap = KAP && tracers;  // the u, v blocks of a closure launch keep nu_v
+  const uint64_t bits = wb(d, j, in ? i : d.nx - 1);
   const int kb = kbot_of(bits);
-  if (kb > 0 && wetb(bits, 0)) {
-    const int n = kb + 1;
-    float lo[ZM_MAXZ], dg[ZM_MAXZ], up[ZM_MAXZ];
-    if (tracers && kap3) {
-      for (int k = 0; k < n; ++k) {
-        lo[k] = k > 0 ? -dth * __ldg(kap3 + base + (long long)(k - 1) * d.plane) * d.vc.inv_dz_iface[k - 1] *
-                            d.vc.inv_dz_node[k]
-                      : 0.f;
-        up[k] = k + 1 < n
-                    ? -dth * __ldg(kap3 + base + (long long)k * d.plane) * d.vc.inv_dz_iface[k] * d.vc.inv_dz_node[k]
-                    : 0.f;
-        dg[k] = 1.f - lo[k] - up[k];
-      }
+  const int n = kb > 0 && wetb(bits, 0) ? kb + 1 : 0;
+  const float sc = tracers ? __ldg(d.kv2 + base) * dth : d.nu_v * dth;
+  const long long pl = d.plane;
+  float x[ZM_MAXZ], inv[ZM_MAXZ], e[ZM_MAXZ], kq[KAP ? ZM_MAXZ : 1];
+  for (int k = 0; k < n; ++k) {
+    x[k] = fld[base + k * pl];
+    if (KAP && kap && k + 1 < n) kq[k] = __ldg(kap3 + base + k * pl);
+  }
+  // tridiagonal row k: lower lo, diagonal dg, upper up
+  auto row = [&](int k, float& lo, float& dg, float& up) {
+    if (KAP && kap) {
+      lo = k > 0 ? -dth * kq[k - 1] * d.vc.inv_dz_iface[k - 1] * d.vc.inv_dz_node[k] : 0.f;
+      up = k + 1 < n ? -dth * kq[k] * d.vc.inv_dz_iface[k] * d.vc.inv_dz_node[k] : 0.f;
+      dg = 1.f - lo - up;
     } else {
-      const float sc = tracers ? __ldg(d.kv2 + base) * dth : d.nu_v * dth;
-      for (int k = 0; k < n; ++k) vcoef(d, k, kb, sc, lo[k], dg[k], up[k]);
+      vcoef(d, k, kb, sc, lo, dg, up);
     }
-    if (tracers) implicit_pair(d, T, S, base, n, lo, dg, up);
-    else implicit_pair(d, u, v, base, n, lo, dg, up);
+  };
+  // 1. forward elimination (lo = 0 in row 0, so its pivot is dg)
+  {
+    float cpp = 0.f, y = 0.f;
+    for (int k = 0; k < n; ++k) {
+      float lo, dg, up;
+      row(k, lo, dg, up);
+      const float iv = 1.f / (dg - lo * cpp);
+      cpp = up * iv;
+      y = (x[k] - lo * y) * iv;
+      x[k] = y;
+      inv[k] = iv;
+    }
   }
-  if (tracers) {
-    for (int k = 0; k < d.nz; ++k)
-      if (!wetb(bits, k)) {
-        const long long id = base + (long long)k * d.plane;
-        T[id] = ld(T0, id);
-        S[id] = ld(S0, id);
+  // 2. back substitution
+  for (int k = n - 2; k >= 0; --k) {
+    float lo, dg, up;
+    row(k, lo, dg, up);
+    x[k] -= (up * inv[k]) * x[k + 1];
+  }
+  // 3. residual of the FP32 solution, eliminated with the same factorization
+  {
+    float ep = 0.f, xm = 0.f, x0 = n > 0 ? x[0] : 0.f;
+    for (int k = 0; k < n; ++k) {
+      float lo, dg, up;
+      row(k, lo, dg, up);
+      const float xp = k + 1 < n ? x[k + 1] : 0.f;
+      float a = dg * x0;
+      if (k > 0) a += lo * xm;
+      if (k + 1 < n) a += up * xp;
+      ep = ((fld[base + k * pl] - a) - lo * ep) * inv[k];
+      e[k] = ep;
+      xm = x0;
+      x0 = xp;
+    }
+  }
+  // 4. back substitution of the correction; x + e, land hold, rotation
+  const float rc = tracers ? 0.f : __ldg(d.rot_c + base), rs = tracers ? 0.f : __ldg(d.rot_s + base);
+  float en = 0.f;
+  for (int k = d.nz - 1; k >= 0; --k) {
+    const long long id = base + k * pl;
+    const bool wet = wetb(bits, k);
+    float val = 0.f;
+    if (k < n) {
+      float ek = e[k];
+      if (k + 1 < n) {
+        float lo, dg, up;
+        row(k, lo, dg, up);
+        ek -= (up * inv[k]) * en;
       }
-    return;
-  }
-  // land/ghost hold, then the exact Coriolis rotation
-  const float c = __ldg(d.rot_c + base), s = __ldg(d.rot_s + base);
-  for (int k = 0; k < d.nz; ++k) {
-    const long long id = base + (long long)k * d.plane;
-    float uu = u[id], vv = v[id];
-    if (!wetb(bits, k)) {
-      uu = ld(u0, id);
-      vv = ld(v0, id);
+      en = ek;
+      val = x[k] + ek;
+    } else if (!tracers && wet) {
+      val = fld[id];
     }
-    u[id] = c * uu + s * vv;
-    v[id] = -s * uu + c * vv;
+    if (!wet) val = ld(hold, id);
+    if (tracers) {
+      if (in && (k < n || !wet)) fld[id] = val;
+    } else {
+      const float other = __shfl_xor_sync(0xffffffffu, val, 1);
+      const float uu = f ? other : val, vv = f ? val : other;
+      if (in) fld[id] = f ? -rs * uu + rc * vv : rc * uu + rs * vv;
+    }
   }
+}
+
+void launch_implicit_vdiff(cudaStream_t s, const Dev& d, float* u, float* v, float* T, float* S, const float* u0,
+                           const float* v0, const float* T0, const float* S0, float dth, const float* kap3) {
+  const dim3 g((d.nx + IV_T / 2 - 1) / (IV_T / 2), d.ny, 2);
+  if (kap3) k_implicit_vdiff<true><<<g, IV_T, 0, s>>>(d, u, v, T, S, u0, v0, T0, S0, dth, kap3);
+  else k_implicit_vdiff<false><<<g, IV_T, 0, s>>>(d, u, v, T, S, u0, v0, T0, S0, dth, kap3);
 }
 
 // ------------------------------------------------------------------ transport

@@ -112,8 +112,10 @@ __global__ void k_lin_t(Dev d, const float* usub, const float* vsub, const float
 // tile of k_lin_t
 constexpr int LT_TX = 32, LT_TY = 16;
 size_t lin_tile_smem();
-__global__ void k_implicit_vdiff(Dev d, float* u, float* v, float* T, float* S, const float* u0, const float* v0,
-                                 const float* T0, const float* S0, float dth, const float* kap3);
+// threads per block of k_implicit_vdiff (two per column) and its launch
+constexpr int IV_T = 64;
+void launch_implicit_vdiff(cudaStream_t s, const Dev& d, float* u, float* v, float* T, float* S, const float* u0,
+                           const float* v0, const float* T0, const float* S0, float dth, const float* kap3);
 __global__ void k_fz(Dev d, const float* u, const float* v, float* Fz);
 __global__ void k_madv(Dev d, const float* u, const float* v, const float* Fz, float* Ayu, float* Ayv);
 __global__ void k_dealias_lon(Dev d, FftPlan plan, const float* Ayu, const float* Ayv, float* Au, float* Av,

@@ -197,12 +197,9 @@ struct zm_solver {
         d, usub, vsub, src.u, src.v, src.T, src.S, dst.u, dst.v, dst.T, dst.S, dth, vdiff || closure_on);
     pe(s);
     if (vdiff || closure_on) {
-      const dim3 c(32, 4);
       pb(ZM_K_IMPLICIT, s);
-      dim3 g = grid2(c);
-      g.z = 2;
-      k_implicit_vdiff<<<g, c, 0, s>>>(d, dst.u, dst.v, dst.T, dst.S, src.u, src.v, src.T, src.S, dth,
-                                       closure_on ? kappa3 : nullptr);
+      launch_implicit_vdiff(s, d, dst.u, dst.v, dst.T, dst.S, src.u, src.v, src.T, src.S, dth,
+                            closure_on ? kappa3 : nullptr);
       pe(s);
     }
     if (ledger_on) led_stage(s, 0, src.T, src.S, nullptr, dst.T, dst.S, nullptr);  // step.py:138-140
