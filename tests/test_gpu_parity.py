@@ -57,6 +57,19 @@ def test_nonlinear_step_matches_oracle(operator_case):
     assert max(errs.values()) < STAGE_TOL, errs
 
 
+@pytest.mark.parametrize("limiter", ["monotone", "centered"])
+def test_nonlinear_step_with_other_tracer_limiters(limiter):
+    """The donor-cell (monotone_adv) and centred tracer face values
+    (transport.py:199-290) in the N stage, against the oracle."""
+    grid, physics, dt, kw, state = _operator_case()
+    kw = dict(kw, fct_adv=False, monotone_adv=(limiter == "monotone"))
+    gpu, p = gu.build_pair(grid, physics, dt, kw)
+    got = gu.run_stage(gpu, 2, state)
+    want = ostep.explicit_full_step(dict(state), p)
+    errs = gu.errors(got, want, ("u", "v", "T", "S"))
+    assert max(errs.values()) < STAGE_TOL, errs
+
+
 def test_full_step_matches_oracle_on_moving_state(operator_case):
     gpu, p, state = operator_case
     got = gu.run_stage(gpu, 3, state)

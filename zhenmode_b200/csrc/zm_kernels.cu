@@ -701,27 +701,30 @@ struct TaTile {
 // triple (a, b, c) = (c-, c0, c1) for a flow towards +, (c+, c1, c0) towards -,
 // the minmod face state is b + 0.5 minmod(a, b, c): for the negative
 // direction minmod(c+, c1, c0) = -minmod(c0, c1, c+) exactly, so this is
-// c1 - 0.5 minmod(c0, c1, c+) without a divergent branch.
-__device__ __forceinline__ float ta_face_value(int limiter, bool pos, float cm, float c0, float c1, float cp, float wm,
+// c1 - 0.5 minmod(c0, c1, c+) without a divergent branch.  LIM: 2 minmod
+// (fct_adv), 1 donor cell (monotone_adv), 0 centred.
+template <int LIM>
+__device__ __forceinline__ float ta_face_value(bool pos, float cm, float c0, float c1, float cp, float wm,
                                                float w0, float w1, float wp) {
-  if (limiter == 2) {
+  if (LIM == 2) {
     const float a = pos ? cm : cp, b = pos ? c0 : c1, c = pos ? c1 : c0;
     const float wa = pos ? wm : wp, wb = pos ? w0 : w1, wc = pos ? w1 : w0;
     return b + 0.5f * minmod_slope(a, b, c, wa, wb, wc);
   }
-  if (limiter == 1) return pos ? c0 : c1;
+  if (LIM == 1) return pos ? c0 : c1;
   return 0.5f * (c0 + c1);
 }
 
 // T and S fluxes through the x face between tile columns cc and cc+1 of row r
-__device__ __forceinline__ void ta_faces_x(int limiter, const TaTile& t, int r, int cc, float& fT, float& fS) {
+template <int LIM>
+__device__ __forceinline__ void ta_faces_x(const TaTile& t, int r, int cc, float& fT, float& fS) {
   const float w0 = t.w[r][cc], we = t.w[r][cc + 1];
   const float ux = 0.5f * (t.u[r][cc] + t.u[r][cc + 1]);
   const bool pos = ux >= 0.f;
   const float wm = t.w[r][cc - 1], wp = t.w[r][cc + 2];
-  const float cT = ta_face_value(limiter, pos, t.T[r][cc - 1], t.T[r][cc], t.T[r][cc + 1], t.T[r][cc + 2], wm, w0,
+  const float cT = ta_face_value<LIM>(pos, t.T[r][cc - 1], t.T[r][cc], t.T[r][cc + 1], t.T[r][cc + 2], wm, w0,
                                  we, wp);
-  const float cS = ta_face_value(limiter, pos, t.S[r][cc - 1], t.S[r][cc], t.S[r][cc + 1], t.S[r][cc + 2], wm, w0,
+  const float cS = ta_face_value<LIM>(pos, t.S[r][cc - 1], t.S[r][cc], t.S[r][cc + 1], t.S[r][cc + 2], wm, w0,
                                  we, wp);
   const float g = w0 * we;
   fT = ux * cT * g;
@@ -730,6 +733,7 @@ __device__ __forceinline__ void ta_faces_x(int limiter, const TaTile& t, int r, 
 
 // T and S fluxes through the y face between tile rows r and r+1 (global rows
 // gj, gj+1); zero through the closed walls
+template <int LIM>
 __device__ __forceinline__ void ta_faces_y(const Dev& d, const TaTile& t, int r, int cc, int gj, float& fT,
                                            float& fS) {
   if (gj < 0 || gj >= d.ny - 1) {
@@ -740,15 +744,16 @@ __device__ __forceinline__ void ta_faces_y(const Dev& d, const TaTile& t, int r,
   const float vy = 0.5f * (t.v[r][cc] + t.v[r + 1][cc]);
   const bool pos = vy >= 0.f;
   const float wm = t.w[r - 1][cc], wp = t.w[r + 2][cc];
-  const float cT = ta_face_value(d.limiter, pos, t.T[r - 1][cc], t.T[r][cc], t.T[r + 1][cc], t.T[r + 2][cc], wm, w0,
+  const float cT = ta_face_value<LIM>(pos, t.T[r - 1][cc], t.T[r][cc], t.T[r + 1][cc], t.T[r + 2][cc], wm, w0,
                                  wn, wp);
-  const float cS = ta_face_value(d.limiter, pos, t.S[r - 1][cc], t.S[r][cc], t.S[r + 1][cc], t.S[r + 2][cc], wm, w0,
+  const float cS = ta_face_value<LIM>(pos, t.S[r - 1][cc], t.S[r][cc], t.S[r + 1][cc], t.S[r + 2][cc], wm, w0,
                                  wn, wp);
   const float g = w0 * wn, cf = __ldg(d.cfp + gj);
   fT = vy * cT * g * cf;
   fS = vy * cS * g * cf;
 }
 
+template <int LIM>
 __global__ void __launch_bounds__(TA_X * TA_Y, 4) k_tracer_adv_t(Dev d, const float* __restrict__ T,
                                                                  const float* __restrict__ S,
                                                                  const float* __restrict__ u,
@@ -796,10 +801,10 @@ __global__ void __launch_bounds__(TA_X * TA_Y, 4) k_tracer_adv_t(Dev d, const fl
   if (w0 != 0.f) {
     const uint64_t bits = __ldg(d.wbits + base);
     float fxeT, fxeS, fxwT, fxwS, fynT, fynS, fysT, fysS;
-    ta_faces_x(d.limiter, t, r, cc, fxeT, fxeS);
-    ta_faces_x(d.limiter, t, r, cc - 1, fxwT, fxwS);
-    ta_faces_y(d, t, r, cc, j, fynT, fynS);
-    ta_faces_y(d, t, r - 1, cc, j - 1, fysT, fysS);
+    ta_faces_x<LIM>(t, r, cc, fxeT, fxeS);
+    ta_faces_x<LIM>(t, r, cc - 1, fxwT, fxwS);
+    ta_faces_y<LIM>(d, t, r, cc, j, fynT, fynS);
+    ta_faces_y<LIM>(d, t, r - 1, cc, j - 1, fysT, fysS);
     const float ix = __ldg(d.inv_dx + base), ysc = d.inv_dy * __ldg(d.inv_cos + j);
     const float hT = (fxeT - fxwT) * ix + (fynT - fysT) * ysc;
     const float hS = (fxeS - fxwS) * ix + (fynS - fysS) * ysc;
@@ -831,6 +836,19 @@ __global__ void __launch_bounds__(TA_X * TA_Y, 4) k_tracer_adv_t(Dev d, const fl
     Tn[id] = ck + aT * dts;
     Sn[id] = sk + aS * dts;
   }
+}
+
+// The face limiter is a template argument: the face arithmetic is specialised
+// instead of branching on it at every face.
+void launch_tracer_adv(dim3 g, dim3 b, cudaStream_t s, const Dev& d, const float* T, const float* S,
+                       const float* u, const float* v, const float* Fz, float* accT, float* accS, float* Tn,
+                       float* Sn, float dts, int first, int last, float* topT, float* topS) {
+  if (d.limiter == 2)
+    k_tracer_adv_t<2><<<g, b, 0, s>>>(d, T, S, u, v, Fz, accT, accS, Tn, Sn, dts, first, last, topT, topS);
+  else if (d.limiter == 1)
+    k_tracer_adv_t<1><<<g, b, 0, s>>>(d, T, S, u, v, Fz, accT, accS, Tn, Sn, dts, first, last, topT, topS);
+  else
+    k_tracer_adv_t<0><<<g, b, 0, s>>>(d, T, S, u, v, Fz, accT, accS, Tn, Sn, dts, first, last, topT, topS);
 }
 
 // Tracer residual of the N step (dynamics/tendencies.py:94-245) without the

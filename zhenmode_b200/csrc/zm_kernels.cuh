@@ -120,9 +120,9 @@ __global__ void k_fz(Dev d, const float* u, const float* v, float* Fz);
 __global__ void k_madv(Dev d, const float* u, const float* v, const float* Fz, float* Ayu, float* Ayv);
 __global__ void k_dealias_lon(Dev d, FftPlan plan, const float* Ayu, const float* Ayv, float* Au, float* Av,
                               int lines_per_block);
-__global__ void k_tracer_adv_t(Dev d, const float* T, const float* S, const float* u, const float* v, const float* Fz,
-                               float* accT, float* accS, float* Tn, float* Sn, float dts, int first, int last,
-                               float* topT, float* topS);
+void launch_tracer_adv(dim3 g, dim3 b, cudaStream_t s, const Dev& d, const float* T, const float* S,
+                       const float* u, const float* v, const float* Fz, float* accT, float* accS,
+                       float* Tn, float* Sn, float dts, int first, int last, float* topT, float* topS);
 __global__ void k_tracer_rest(Dev d, RestArgs a);
 __global__ void k_pgf(Dev d, PgfArgs a);
 __global__ void k_bt_forcing(Dev d, const float* frx, const float* fry, double* Fx, double* Fy, const float* eta32,
