@@ -308,14 +308,13 @@ __device__ __forceinline__ float hdiff_s(const Dev& d, const LtTile& t, const fl
   return (fe - fw) * t.ix[r][c] + (fn - fs) * d.inv_dy * t.icos[r];
 }
 
-size_t lin_tile_smem() { return sizeof(LtTile); }
-
+template <bool UV, bool TS, bool IMPL>
 __global__ void __launch_bounds__(LT_X * LT_Y) k_lin_t(Dev d, const float* __restrict__ usub,
                                                       const float* __restrict__ vsub, const float* __restrict__ u0,
                                                       const float* __restrict__ v0, const float* __restrict__ T0,
                                                       const float* __restrict__ S0, float* __restrict__ uo,
                                                       float* __restrict__ vo, float* __restrict__ To,
-                                                      float* __restrict__ So, float dth, int implicit_v) {
+                                                      float* __restrict__ So, float dth) {
   extern __shared__ float lt_smem[];
   LtTile& t = *reinterpret_cast<LtTile*>(lt_smem);
   const int tx = threadIdx.x, ty = threadIdx.y;
@@ -349,7 +348,7 @@ __global__ void __launch_bounds__(LT_X * LT_Y) k_lin_t(Dev d, const float* __res
     t.icos[tid] = __ldg(d.inv_cos + gj);
   }
   __syncthreads();
-  const bool do_uv = d.nu_bi > 0.f, do_ts = d.kappa_bi > 0.f;
+  constexpr bool do_uv = UV, do_ts = TS;
   if (do_uv || do_ts) {
     // the one-cell ring around the interior, walked over whole padded rows so
     // that a warp's shared-memory addresses are consecutive (no bank conflicts)
@@ -394,7 +393,7 @@ __global__ void __launch_bounds__(LT_X * LT_Y) k_lin_t(Dev d, const float* __res
       u = u - d.nu_bi * lap_s(d, t, t.Lu, r, cc, true) * dth;
       v = v - d.nu_bi * lap_s(d, t, t.Lv, r, cc, true) * dth;
     }
-    if (!implicit_v) {
+    if (!IMPL) {
       const int kbt = kbot_of(bits);
       const float kv = __ldg(d.kv2 + base);
       u = u + d.nu_v * d2z(d, u0, base, k, kbt) * dth;
@@ -405,7 +404,7 @@ __global__ void __launch_bounds__(LT_X * LT_Y) k_lin_t(Dev d, const float* __res
   }
   To[id] = T;
   So[id] = S;
-  if (implicit_v) {  // the column solve and the rotation follow
+  if (IMPL) {  // the column solve and the rotation follow
     uo[id] = u;
     vo[id] = v;
     return;
@@ -413,6 +412,31 @@ __global__ void __launch_bounds__(LT_X * LT_Y) k_lin_t(Dev d, const float* __res
   const float c = __ldg(d.rot_c + base), sn = __ldg(d.rot_s + base);
   uo[id] = c * u + sn * v;
   vo[id] = -sn * u + c * v;
+}
+
+// The biharmonic and implicit-diffusion options are template arguments: a
+// launch carries only the operators its option set uses.
+static_assert(sizeof(LtTile) <= 48 * 1024, "k_lin_t tile within the default dynamic shared memory");
+void launch_lin_t(dim3 g, dim3 b, cudaStream_t s, const Dev& d, const float* usub, const float* vsub,
+                  const float* u0, const float* v0, const float* T0, const float* S0, float* uo, float* vo,
+                  float* To, float* So, float dth, int implicit_v) {
+  const int key = (d.nu_bi > 0.f ? 4 : 0) | (d.kappa_bi > 0.f ? 2 : 0) | (implicit_v ? 1 : 0);
+  const size_t sm = sizeof(LtTile);
+#define ZM_LIN(K, UV, TS, IM)                                                                       \
+  case K:                                                                                           \
+    k_lin_t<UV, TS, IM><<<g, b, sm, s>>>(d, usub, vsub, u0, v0, T0, S0, uo, vo, To, So, dth);       \
+    break;
+  switch (key) {
+    ZM_LIN(0, false, false, false)
+    ZM_LIN(1, false, false, true)
+    ZM_LIN(2, false, true, false)
+    ZM_LIN(3, false, true, true)
+    ZM_LIN(4, true, false, false)
+    ZM_LIN(5, true, false, true)
+    ZM_LIN(6, true, true, false)
+    ZM_LIN(7, true, true, true)
+  }
+#undef ZM_LIN
 }
 
 // Backward-Euler vertical diffusion (extension: the implicit replacement of
@@ -1054,6 +1078,7 @@ __device__ __forceinline__ PgLevel pg_load(const float* __restrict__ T, const fl
   return L;
 }
 
+template <int MODE>
 __global__ void __launch_bounds__(128) k_pgf(Dev d, PgfArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -1096,7 +1121,7 @@ __global__ void __launch_bounds__(128) k_pgf(Dev d, PgfArgs a) {
     }
     gx_prev = gx;
     gy_prev = gy;
-    if (a.mode != 0) {
+    if (MODE != 0) {
       const long long id = (long long)k * d.plane + cc;
       a.gsx[id] = -gx / kRho0;
       a.gsy[id] = -gy / kRho0;
@@ -1104,7 +1129,7 @@ __global__ void __launch_bounds__(128) k_pgf(Dev d, PgfArgs a) {
   }
   const float Fx = -fx / (kRho0 * d.H_sw);
   const float Fy = -fy / (kRho0 * d.H_sw);
-  if (a.mode == 0) {
+  if (MODE == 0) {
     a.frx[cc] = Fx;
     a.fry[cc] = Fy;
     double su = 0.0, sv = 0.0;
@@ -1122,7 +1147,7 @@ __global__ void __launch_bounds__(128) k_pgf(Dev d, PgfArgs a) {
   }
   // second pass; the next level's inputs are loaded before this level's
   // stores (the argument pointers may alias, so later loads would wait)
-  const bool m2 = a.mode == 2;
+  constexpr bool m2 = MODE == 2;
   float qx = a.gsx[cc], qy = a.gsy[cc], qAu = ld(a.Au, cc), qAv = ld(a.Av, cc), qu = ld(a.u1, cc), qv = ld(a.v1, cc);
   float qpu = m2 ? ld(a.Ppu, cc) : 0.f, qpv = m2 ? ld(a.Ppv, cc) : 0.f;
 #pragma unroll 1
@@ -1146,7 +1171,7 @@ __global__ void __launch_bounds__(128) k_pgf(Dev d, PgfArgs a) {
     const float Pu = (qx - Fx) * w;
     const float Pv = (qy - Fy) * w;
     const float Au = qAu, Av = qAv, u1 = qu, v1 = qv;
-    if (a.mode == 1) {
+    if (MODE == 1) {
       a.Pu[id] = Pu;
       a.Pv[id] = Pv;
       a.uo[id] = u1 + (Au + Pu) * a.dt;
@@ -1158,6 +1183,13 @@ __global__ void __launch_bounds__(128) k_pgf(Dev d, PgfArgs a) {
     }
     qx = nx_; qy = ny_; qAu = nAu; qAv = nAv; qu = nu; qv = nv; qpu = npu; qpv = npv;
   }
+}
+
+// The mode is a template argument: each launch runs only its own passes.
+void launch_pgf(dim3 g, dim3 b, cudaStream_t s, const Dev& d, const PgfArgs& a) {
+  if (a.mode == 0) k_pgf<0><<<g, b, 0, s>>>(d, a);
+  else if (a.mode == 1) k_pgf<1><<<g, b, 0, s>>>(d, a);
+  else k_pgf<2><<<g, b, 0, s>>>(d, a);
 }
 
 // Seasonal forcing blend (inputs/forcing/seasonal.py:86-103): the current

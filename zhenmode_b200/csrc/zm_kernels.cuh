@@ -107,11 +107,11 @@ __global__ void k_forcing_blend(Dev d, const float* stack, int prev, int cur, in
                                 float w_next, float* out);
 __global__ void k_barrier_probe(unsigned* bar, unsigned* err, unsigned expected, unsigned max_polls);
 __global__ void k_nu_tb(Dev d, const float* u, const float* v, float* uo, float* vo, float c, int nsub, int halo);
-__global__ void k_lin_t(Dev d, const float* usub, const float* vsub, const float* u0, const float* v0, const float* T0,
-                        const float* S0, float* uo, float* vo, float* To, float* So, float dth, int implicit_v);
+void launch_lin_t(dim3 g, dim3 b, cudaStream_t s, const Dev& d, const float* usub, const float* vsub,
+                  const float* u0, const float* v0, const float* T0, const float* S0, float* uo, float* vo,
+                  float* To, float* So, float dth, int implicit_v);
 // tile of k_lin_t
 constexpr int LT_TX = 32, LT_TY = 16;
-size_t lin_tile_smem();
 // threads per block of k_implicit_vdiff (two per column) and its launch
 constexpr int IV_T = 64;
 void launch_implicit_vdiff(cudaStream_t s, const Dev& d, float* u, float* v, float* T, float* S, const float* u0,
@@ -124,7 +124,7 @@ void launch_tracer_adv(dim3 g, dim3 b, cudaStream_t s, const Dev& d, const float
                        const float* u, const float* v, const float* Fz, float* accT, float* accS,
                        float* Tn, float* Sn, float dts, int first, int last, float* topT, float* topS);
 __global__ void k_tracer_rest(Dev d, RestArgs a);
-__global__ void k_pgf(Dev d, PgfArgs a);
+void launch_pgf(dim3 g, dim3 b, cudaStream_t s, const Dev& d, const PgfArgs& a);
 __global__ void k_bt_forcing(Dev d, const float* frx, const float* fry, double* Fx, double* Fy, const float* eta32,
                              double* eta64);
 __global__ void k_cap3_means(Dev d, const float* u, const float* v, const float* T, const float* S, const double* ubt,

@@ -193,7 +193,7 @@ struct zm_solver {
       vsub = c;
     }
     pb(ZM_K_LIN_FINISH, s);
-    k_lin_t<<<dim3((nx + LT_TX - 1) / LT_TX, (ny + LT_TY - 1) / LT_TY, nz), dim3(LT_TX, LT_TY), lin_tile_smem(), s>>>(
+    launch_lin_t(dim3((nx + LT_TX - 1) / LT_TX, (ny + LT_TY - 1) / LT_TY, nz), dim3(LT_TX, LT_TY), s,
         d, usub, vsub, src.u, src.v, src.T, src.S, dst.u, dst.v, dst.T, dst.S, dth, vdiff || closure_on);
     pe(s);
     if (vdiff || closure_on) {
@@ -251,7 +251,7 @@ struct zm_solver {
     a.gsx = gsx;
     a.gsy = gsy;
     pb(ZM_K_PGF, s);
-    k_pgf<<<grid2(c), c, 0, s>>>(d, a);
+    launch_pgf(grid2(c), c, s, d, a);
     pe(s);
     check_launch();
   }
@@ -880,7 +880,6 @@ void build(zm_solver* s, const zm_grid* g, const zm_params* p) {
     require((int)s->fft_smem <= optin, ZM_ERR_UNSUPPORTED, "nx too large for the shared-memory FFT filter");
     ZM_CUDA(cudaFuncSetAttribute(k_dealias_lon, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
   }
-  ZM_CUDA(cudaFuncSetAttribute(k_lin_t, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lin_tile_smem()));
   // ---- buffers
   for (int q = 0; q < 2; ++q) {
     s->st[q] = s->four();
