@@ -906,6 +906,7 @@ __device__ __forceinline__ void rest_store(const Dev& d, const RestArgs& a, long
   }
 }
 
+template <bool ST2>
 __global__ void __launch_bounds__(128) k_tracer_rest(Dev d, RestArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -936,7 +937,7 @@ __global__ void __launch_bounds__(128) k_tracer_rest(Dev d, RestArgs a) {
     float cT = ld(a.Tev, base), cS = ld(a.Sev, base);
     // the next level's inputs are loaded before this level's stores: the
     // argument pointers may alias, so loads issued after a store would wait
-    const bool st2 = a.stage != 1;
+    constexpr bool st2 = ST2;  // stage 2 reads the stage-1 tendency
     float qaT = ld(a.accT, base), qaS = ld(a.accS, base), qbT = ld(a.Tbase, base), qbS = ld(a.Sbase, base);
     float qdT = st2 ? ld(a.dT1, base) : 0.f, qdS = st2 ? ld(a.dS1, base) : 0.f;
 #pragma unroll 2
@@ -1035,6 +1036,12 @@ __global__ void __launch_bounds__(128) k_tracer_rest(Dev d, RestArgs a) {
     rest_store(d, a, id, base, k, wetf(bits, k), ld(a.accT, id) * a.inv_na + sT[k] * inv_nc,
                ld(a.accS, id) * a.inv_na + sS[k] * inv_nc);
   }
+}
+
+// The RK stage is a template argument (stage 2 also reads dT1, dS1).
+void launch_tracer_rest(dim3 g, dim3 b, cudaStream_t s, const Dev& d, const RestArgs& a) {
+  if (a.stage == 1) k_tracer_rest<false><<<g, b, 0, s>>>(d, a);
+  else k_tracer_rest<true><<<g, b, 0, s>>>(d, a);
 }
 
 // ------------------------------------------------------------------ pressure

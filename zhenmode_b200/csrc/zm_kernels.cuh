@@ -123,7 +123,7 @@ __global__ void k_dealias_lon(Dev d, FftPlan plan, const float* Ayu, const float
 void launch_tracer_adv(dim3 g, dim3 b, cudaStream_t s, const Dev& d, const float* T, const float* S,
                        const float* u, const float* v, const float* Fz, float* accT, float* accS,
                        float* Tn, float* Sn, float dts, int first, int last, float* topT, float* topS);
-__global__ void k_tracer_rest(Dev d, RestArgs a);
+void launch_tracer_rest(dim3 g, dim3 b, cudaStream_t s, const Dev& d, const RestArgs& a);
 void launch_pgf(dim3 g, dim3 b, cudaStream_t s, const Dev& d, const PgfArgs& a);
 __global__ void k_bt_forcing(Dev d, const float* frx, const float* fry, double* Fx, double* Fy, const float* eta32,
                              double* eta64);

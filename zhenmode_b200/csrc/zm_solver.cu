@@ -240,7 +240,7 @@ struct zm_solver {
                closure_on ? 1 : 0, ledger_on ? led_convT : nullptr, ledger_on ? led_convS : nullptr};
     const dim3 c(32, 4);
     pb(ZM_K_TRACER_REST, s);
-    k_tracer_rest<<<grid2(c), c, 0, s>>>(d, a);
+    launch_tracer_rest(grid2(c), c, s, d, a);
     pe(s);
     check_launch();
     if (ledger_on) led_rk(s, T, S);  // tendencies.py:211-214
