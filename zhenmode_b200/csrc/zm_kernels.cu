@@ -1064,53 +1064,95 @@ __device__ __forceinline__ float drho(const Dev& d, float Ta, float Sa, float wa
 // Pressure-gradient kernel (physics/pressure.py:32-97, legacy trapezoid form,
 // in differences), one column per thread.  Modes: 0 the barotropic forcing
 // F_rho and the depth-mean velocity; 1 and 2 the P part of the momentum
-// residual with the RK combination of the first and second stage.  The march
-// down the column keeps the density differences to the four neighbours and
-// their downward accumulation in registers, with the next level's ten T/S
-// values loaded while the current level computes.  Modes 1 and 2 need the
-// depth integral before the first output level, so the per-level gradient
-// goes to a scratch field (read back by the same thread, normally from L2).
-struct PgLevel {
-  float Tc, Sc, Te, Se, Tw, Sw, Tn, Sn, Ts, Ss;
-};
+// residual with the RK combination of the first and second stage.  A block
+// owns a PG_X x PG_Y tile of columns and marches down the levels together:
+// each level's T and S on the tile and a one-cell halo (rows clamped at the
+// closed walls like north()/south(), longitude wrapped like east()/west())
+// arrive in shared memory by cp.async, PG_NB - 1 levels ahead of the one being
+// used, so every value is fetched once and the loads of later levels overlap
+// the arithmetic.  Each thread keeps its column's density differences to the
+// four neighbours and their downward accumulation in registers.  Modes 1 and
+// 2 need the depth integral before the first output level, so the per-level
+// gradient goes to a scratch field (read back by the same thread, normally
+// from L2).
+constexpr int PG_X = 32, PG_Y = 8, PG_NB = 4;  // tile columns, tile rows, level buffers
+constexpr int PG_PX = PG_X + 2, PG_PY = PG_Y + 2;
+constexpr int PG_CELLS = PG_PX * PG_PY;
+static_assert(PG_CELLS <= 2 * PG_X * PG_Y, "two tile cells per thread at most");
 
-__device__ __forceinline__ PgLevel pg_load(const float* __restrict__ T, const float* __restrict__ S, long long b,
-                                           long long cc, long long ce, long long cw, long long cn, long long cs) {
-  PgLevel L;
-  L.Tc = ld(T, b + cc); L.Sc = ld(S, b + cc);
-  L.Te = ld(T, b + ce); L.Se = ld(S, b + ce);
-  L.Tw = ld(T, b + cw); L.Sw = ld(S, b + cw);
-  L.Tn = ld(T, b + cn); L.Sn = ld(S, b + cn);
-  L.Ts = ld(T, b + cs); L.Ss = ld(S, b + cs);
-  return L;
+// 4-byte global -> shared copy that completes asynchronously, and the commit
+// and wait of such copies in groups (cp.async)
+__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// plane offset of padded-tile cell e of the tile at (i0, j0)
+__device__ __forceinline__ int pg_cell(const Dev& d, int e, int i0, int j0) {
+  const int rr = e / PG_PX, cc = e - rr * PG_PX;
+  const int gj = min(max(j0 - 1 + rr, 0), d.ny - 1);
+  int gi = (i0 - 1 + cc) % d.nx;
+  if (gi < 0) gi += d.nx;
+  return idx2(d, gj, gi);
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(128) k_pgf(Dev d, PgfArgs a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= d.nx || j >= d.ny) return;
-  const Nb n = nb(d, j, i);
-  const uint64_t m0 = wb(d, j, i), me = wb(d, j, n.ie), mw = wb(d, j, n.iw), mn = wb(d, n.jn, i),
-                 ms = wb(d, n.js, i);
-  const long long cc = idx2(d, j, i), ce = idx2(d, j, n.ie), cw = idx2(d, j, n.iw), cn = idx2(d, n.jn, i),
-                  cs = idx2(d, n.js, i);
+__global__ void __launch_bounds__(PG_X * PG_Y) k_pgf(Dev d, PgfArgs a) {
+  __shared__ float sT[PG_NB][PG_PY][PG_PX], sS[PG_NB][PG_PY][PG_PX];
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * PG_X + tx;
+  const int i0 = blockIdx.x * PG_X, j0 = blockIdx.y * PG_Y;
+  const int i = i0 + tx, j = j0 + ty;
+  // threads outside the grid copy their tile cells and meet the barriers, nothing else
+  const bool in = i < d.nx && j < d.ny;
+  const int e0 = tid, e1 = tid + PG_X * PG_Y;
+  const bool has1 = e1 < PG_CELLS;
+  const int s0 = pg_cell(d, e0, i0, j0), s1 = has1 ? pg_cell(d, e1, i0, j0) : 0;
+  auto issue = [&](int k) {  // level k into buffer k % PG_NB; one commit group per call
+    if (k < d.nz) {
+      const long long off = (long long)k * d.plane;
+      float* bt = &sT[k % PG_NB][0][0];
+      float* bs = &sS[k % PG_NB][0][0];
+      cp_async4(bt + e0, a.T + off + s0);
+      cp_async4(bs + e0, a.S + off + s0);
+      if (has1) {
+        cp_async4(bt + e1, a.T + off + s1);
+        cp_async4(bs + e1, a.S + off + s1);
+      }
+    }
+    cp_async_commit();
+  };
+  const int ic = in ? i : 0, jc = in ? j : 0;
+  const Nb n = nb(d, jc, ic);
+  const uint64_t m0 = wb(d, jc, ic), me = wb(d, jc, n.ie), mw = wb(d, jc, n.iw), mn = wb(d, n.jn, ic),
+                 ms = wb(d, n.js, ic);
+  const long long cc = idx2(d, jc, ic);
   const float hx = __ldg(d.inv_dx + cc) * 0.5f;
-  const float hy = d.inv_dy * __ldg(d.inv_cos + j) * 0.5f;
-  const float cfp = __ldg(d.cfp + j), cfm = __ldg(d.cfm + j);
-  const bool has_n = j < d.ny - 1, has_s = j > 0;
+  const float hy = d.inv_dy * __ldg(d.inv_cos + jc) * 0.5f;
+  const float cfp = __ldg(d.cfp + jc), cfm = __ldg(d.cfm + jc);
+  const bool has_n = jc < d.ny - 1, has_s = jc > 0;
   float pe = 0.f, pw = 0.f, pn = 0.f, ps = 0.f;       // p[e]-p[c], p[c]-p[w], p[n]-p[c], p[c]-p[s]
   float de0 = 0.f, dw0 = 0.f, dn0 = 0.f, ds0 = 0.f;   // density differences at the level above
   float gx_prev = 0.f, gy_prev = 0.f, fx = 0.f, fy = 0.f;
-  PgLevel nxt = pg_load(a.T, a.S, 0, cc, ce, cw, cn, cs);
+#pragma unroll
+  for (int q = 0; q < PG_NB - 1; ++q) issue(q);
+  const int r = ty + 1, c = tx + 1;
   for (int k = 0; k < d.nz; ++k) {
-    const PgLevel L = nxt;
-    if (k + 1 < d.nz) nxt = pg_load(a.T, a.S, (long long)(k + 1) * d.plane, cc, ce, cw, cn, cs);
+    cp_async_wait<PG_NB - 2>();  // this thread's copies of level k are done
+    __syncthreads();             // everyone's are, and level k - 1's buffer is free
+    issue(k + PG_NB - 1);
+    if (!in) continue;
+    const int b = k % PG_NB;
+    const float Tc = sT[b][r][c], Sc = sS[b][r][c];
     const float w0 = wetf(m0, k), we = wetf(me, k), ww = wetf(mw, k), wn = wetf(mn, k), ws = wetf(ms, k);
-    const float de = drho(d, L.Te, L.Se, we, L.Tc, L.Sc, w0);
-    const float dw = drho(d, L.Tc, L.Sc, w0, L.Tw, L.Sw, ww);
-    const float dn = drho(d, L.Tn, L.Sn, wn, L.Tc, L.Sc, w0);
-    const float ds = drho(d, L.Tc, L.Sc, w0, L.Ts, L.Ss, ws);
+    const float de = drho(d, sT[b][r][c + 1], sS[b][r][c + 1], we, Tc, Sc, w0);
+    const float dw = drho(d, Tc, Sc, w0, sT[b][r][c - 1], sS[b][r][c - 1], ww);
+    const float dn = drho(d, sT[b][r + 1][c], sS[b][r + 1][c], wn, Tc, Sc, w0);
+    const float ds = drho(d, Tc, Sc, w0, sT[b][r - 1][c], sS[b][r - 1][c], ws);
     if (k > 0) {
       const float h = kG * 0.5f * d.vc.dz3d[k - 1];
       pe += (de0 + de) * h;
@@ -1134,6 +1176,7 @@ __global__ void __launch_bounds__(128) k_pgf(Dev d, PgfArgs a) {
       a.gsy[id] = -gy / kRho0;
     }
   }
+  if (!in) return;
   const float Fx = -fx / (kRho0 * d.H_sw);
   const float Fy = -fy / (kRho0 * d.H_sw);
   if (MODE == 0) {
@@ -1193,7 +1236,8 @@ __global__ void __launch_bounds__(128) k_pgf(Dev d, PgfArgs a) {
 }
 
 // The mode is a template argument: each launch runs only its own passes.
-void launch_pgf(dim3 g, dim3 b, cudaStream_t s, const Dev& d, const PgfArgs& a) {
+void launch_pgf(cudaStream_t s, const Dev& d, const PgfArgs& a) {
+  const dim3 g((d.nx + PG_X - 1) / PG_X, (d.ny + PG_Y - 1) / PG_Y), b(PG_X, PG_Y);
   if (a.mode == 0) k_pgf<0><<<g, b, 0, s>>>(d, a);
   else if (a.mode == 1) k_pgf<1><<<g, b, 0, s>>>(d, a);
   else k_pgf<2><<<g, b, 0, s>>>(d, a);

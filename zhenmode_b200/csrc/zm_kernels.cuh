@@ -124,7 +124,7 @@ void launch_tracer_adv(dim3 g, dim3 b, cudaStream_t s, const Dev& d, const float
                        const float* u, const float* v, const float* Fz, float* accT, float* accS,
                        float* Tn, float* Sn, float dts, int first, int last, float* topT, float* topS);
 void launch_tracer_rest(dim3 g, dim3 b, cudaStream_t s, const Dev& d, const RestArgs& a);
-void launch_pgf(dim3 g, dim3 b, cudaStream_t s, const Dev& d, const PgfArgs& a);
+void launch_pgf(cudaStream_t s, const Dev& d, const PgfArgs& a);
 __global__ void k_bt_forcing(Dev d, const float* frx, const float* fry, double* Fx, double* Fy, const float* eta32,
                              double* eta64);
 __global__ void k_cap3_means(Dev d, const float* u, const float* v, const float* T, const float* S, const double* ubt,

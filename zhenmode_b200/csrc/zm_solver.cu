@@ -247,11 +247,10 @@ struct zm_solver {
   }
 
   void pgf(cudaStream_t s, PgfArgs a) {
-    const dim3 c(32, 4);
     a.gsx = gsx;
     a.gsy = gsy;
     pb(ZM_K_PGF, s);
-    launch_pgf(grid2(c), c, s, d, a);
+    launch_pgf(s, d, a);
     pe(s);
     check_launch();
   }
