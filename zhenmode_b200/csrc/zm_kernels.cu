@@ -1075,7 +1075,7 @@ __device__ __forceinline__ float drho(const Dev& d, float Ta, float Sa, float wa
 // 2 need the depth integral before the first output level, so the per-level
 // gradient goes to a scratch field (read back by the same thread, normally
 // from L2).
-constexpr int PG_X = 32, PG_Y = 8, PG_NB = 4;  // tile columns, tile rows, level buffers
+constexpr int PG_X = 32, PG_Y = 4, PG_NB = 4;  // tile columns, tile rows, level buffers
 constexpr int PG_PX = PG_X + 2, PG_PY = PG_Y + 2;
 constexpr int PG_CELLS = PG_PX * PG_PY;
 static_assert(PG_CELLS <= 2 * PG_X * PG_Y, "two tile cells per thread at most");
