@@ -14,6 +14,30 @@ __device__ __forceinline__ Nb nb(const Dev& d, int j, int i) {
   return Nb{i, j, east(d, i), west(d, i), north(d, j), south(j)};
 }
 
+// 4-byte global -> shared copy that completes asynchronously, and the commit
+// and wait of such copies in groups (cp.async)
+__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Plane offset of cell e of a padded column tile PX cells wide whose interior
+// starts at (i0, j0), with a one-cell halo: rows clamped at the closed walls
+// like north()/south(), longitude wrapped like east()/west().
+template <int PX>
+__device__ __forceinline__ int tile_cell(const Dev& d, int e, int i0, int j0) {
+  const int rr = e / PX, cc = e - rr * PX;
+  const int gj = min(max(j0 - 1 + rr, 0), d.ny - 1);
+  int gi = (i0 - 1 + cc) % d.nx;
+  if (gi < 0) gi += d.nx;
+  return idx2(d, gj, gi);
+}
+
 // Horizontal Laplacian on the sphere, legacy branch
 // (numerics/horizontal.py:181-215): face-gated d2/dx2, mirror-ghost face-gated
 // d2/dy2, metric term -(tan(lat)/R) d/dy on the unmasked centred difference.
@@ -580,33 +604,75 @@ void launch_implicit_vdiff(cudaStream_t s, const Dev& d, float* u, float* v, flo
 // ------------------------------------------------------------------ transport
 // Interface volume transport Fz[k] = sum_{m>=k} div_h[m] dz_node[m]
 // (dynamics/transport.py:110-133 with the face-flux divergence of
-// numerics/horizontal.py:255-281); Fz[nz] = 0 is implicit.
-__global__ void __launch_bounds__(128) k_fz(Dev d, const float* __restrict__ u, const float* __restrict__ v,
-                                            float* __restrict__ Fz) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= d.nx || j >= d.ny) return;
-  const Nb n = nb(d, j, i);
-  const uint64_t m0 = wb(d, j, i), me = wb(d, j, n.ie), mw = wb(d, j, n.iw);
-  const uint64_t mn = wb(d, n.jn, i), ms = wb(d, n.js, i);
-  const float idx_c = __ldg(d.inv_dx + idx2(d, j, i));
-  const float cf_n = __ldg(d.cfp + j), cf_s = j > 0 ? __ldg(d.cfp + j - 1) : 0.f;
-  const float yscale = d.inv_dy * __ldg(d.inv_cos + j);
+// numerics/horizontal.py:255-281); Fz[nz] = 0 is implicit.  A block owns a
+// FZ_X x FZ_Y tile of columns and marches up from the bottom level: each
+// level's u and v on the tile and a one-cell halo arrive in shared memory by
+// cp.async, FZ_NB - 1 levels ahead, so each value is fetched once; one column
+// per thread accumulates the sum.
+constexpr int FZ_X = 32, FZ_Y = 4, FZ_NB = 4;  // tile columns, tile rows, level buffers
+constexpr int FZ_PX = FZ_X + 2, FZ_PY = FZ_Y + 2;
+constexpr int FZ_CELLS = FZ_PX * FZ_PY;
+static_assert(FZ_CELLS <= 2 * FZ_X * FZ_Y, "two tile cells per thread at most");
+
+__global__ void __launch_bounds__(FZ_X * FZ_Y) k_fz(Dev d, const float* __restrict__ u, const float* __restrict__ v,
+                                                    float* __restrict__ Fz) {
+  __shared__ float su[FZ_NB][FZ_PY][FZ_PX], sv[FZ_NB][FZ_PY][FZ_PX];
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * FZ_X + tx;
+  const int i0 = blockIdx.x * FZ_X, j0 = blockIdx.y * FZ_Y;
+  const int i = i0 + tx, j = j0 + ty;
+  // threads outside the grid copy their tile cells and meet the barriers, nothing else
+  const bool in = i < d.nx && j < d.ny;
+  const int e0 = tid, e1 = tid + FZ_X * FZ_Y;
+  const bool has1 = e1 < FZ_CELLS;
+  const int s0 = tile_cell<FZ_PX>(d, e0, i0, j0), s1 = has1 ? tile_cell<FZ_PX>(d, e1, i0, j0) : 0;
+  auto issue = [&](int q) {  // the q-th level from the bottom into buffer q % FZ_NB; one commit group per call
+    if (q < d.nz) {
+      const long long off = (long long)(d.nz - 1 - q) * d.plane;
+      float* bu = &su[q % FZ_NB][0][0];
+      float* bv = &sv[q % FZ_NB][0][0];
+      cp_async4(bu + e0, u + off + s0);
+      cp_async4(bv + e0, v + off + s0);
+      if (has1) {
+        cp_async4(bu + e1, u + off + s1);
+        cp_async4(bv + e1, v + off + s1);
+      }
+    }
+    cp_async_commit();
+  };
+  const int ic = in ? i : 0, jc = in ? j : 0;
+  const Nb n = nb(d, jc, ic);
+  const uint64_t m0 = wb(d, jc, ic), me = wb(d, jc, n.ie), mw = wb(d, jc, n.iw);
+  const uint64_t mn = wb(d, n.jn, ic), ms = wb(d, n.js, ic);
+  const long long cc = idx2(d, jc, ic);
+  const float idx_c = __ldg(d.inv_dx + cc);
+  const float cf_n = __ldg(d.cfp + jc), cf_s = jc > 0 ? __ldg(d.cfp + jc - 1) : 0.f;
+  const float yscale = d.inv_dy * __ldg(d.inv_cos + jc);
   float acc = 0.f;
-  for (int k = d.nz - 1; k >= 0; --k) {
-    const long long b = (long long)k * d.plane;
-    const float uc = ld(u, b + idx2(d, j, i)), ue = ld(u, b + idx2(d, j, n.ie)), uw = ld(u, b + idx2(d, j, n.iw));
+#pragma unroll
+  for (int q = 0; q < FZ_NB - 1; ++q) issue(q);
+  const int r = ty + 1, c = tx + 1;
+  for (int q = 0; q < d.nz; ++q) {
+    cp_async_wait<FZ_NB - 2>();  // this thread's copies of level q are done
+    __syncthreads();             // everyone's are, and level q - 1's buffer is free
+    issue(q + FZ_NB - 1);
+    if (!in) continue;
+    const int k = d.nz - 1 - q, bq = q % FZ_NB;
+    const float uc = su[bq][r][c], ue = su[bq][r][c + 1], uw = su[bq][r][c - 1];
     const float w0 = wetf(m0, k);
     const float fxe = 0.5f * (uc + ue) * w0 * wetf(me, k);
     const float fxw = 0.5f * (uw + uc) * wetf(mw, k) * w0;
     float fyn = 0.f, fys = 0.f;
-    const float vc = ld(v, b + idx2(d, j, i));
-    if (j < d.ny - 1) fyn = 0.5f * (vc + ld(v, b + idx2(d, n.jn, i))) * w0 * wetf(mn, k) * cf_n;
-    if (j > 0) fys = 0.5f * (ld(v, b + idx2(d, n.js, i)) + vc) * wetf(ms, k) * w0 * cf_s;
+    const float vc = sv[bq][r][c];
+    if (jc < d.ny - 1) fyn = 0.5f * (vc + sv[bq][r + 1][c]) * w0 * wetf(mn, k) * cf_n;
+    if (jc > 0) fys = 0.5f * (sv[bq][r - 1][c] + vc) * wetf(ms, k) * w0 * cf_s;
     const float div = (fxe - fxw) * idx_c + (fyn - fys) * yscale;
     acc += div * d.vc.dz_node[k];
-    Fz[b + idx2(d, j, i)] = acc;
+    Fz[(long long)k * d.plane + cc] = acc;
   }
+}
+
+void launch_fz(cudaStream_t s, const Dev& d, const float* u, const float* v, float* Fz) {
+  k_fz<<<dim3((d.nx + FZ_X - 1) / FZ_X, (d.ny + FZ_Y - 1) / FZ_Y), dim3(FZ_X, FZ_Y), 0, s>>>(d, u, v, Fz);
 }
 
 // Raw advective-form momentum advection -(u d/dx + v d/dy + w d/dz) of u and
@@ -1080,27 +1146,6 @@ constexpr int PG_PX = PG_X + 2, PG_PY = PG_Y + 2;
 constexpr int PG_CELLS = PG_PX * PG_PY;
 static_assert(PG_CELLS <= 2 * PG_X * PG_Y, "two tile cells per thread at most");
 
-// 4-byte global -> shared copy that completes asynchronously, and the commit
-// and wait of such copies in groups (cp.async)
-__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
-// plane offset of padded-tile cell e of the tile at (i0, j0)
-__device__ __forceinline__ int pg_cell(const Dev& d, int e, int i0, int j0) {
-  const int rr = e / PG_PX, cc = e - rr * PG_PX;
-  const int gj = min(max(j0 - 1 + rr, 0), d.ny - 1);
-  int gi = (i0 - 1 + cc) % d.nx;
-  if (gi < 0) gi += d.nx;
-  return idx2(d, gj, gi);
-}
-
 template <int MODE>
 __global__ void __launch_bounds__(PG_X * PG_Y) k_pgf(Dev d, PgfArgs a) {
   __shared__ float sT[PG_NB][PG_PY][PG_PX], sS[PG_NB][PG_PY][PG_PX];
@@ -1111,7 +1156,7 @@ __global__ void __launch_bounds__(PG_X * PG_Y) k_pgf(Dev d, PgfArgs a) {
   const bool in = i < d.nx && j < d.ny;
   const int e0 = tid, e1 = tid + PG_X * PG_Y;
   const bool has1 = e1 < PG_CELLS;
-  const int s0 = pg_cell(d, e0, i0, j0), s1 = has1 ? pg_cell(d, e1, i0, j0) : 0;
+  const int s0 = tile_cell<PG_PX>(d, e0, i0, j0), s1 = has1 ? tile_cell<PG_PX>(d, e1, i0, j0) : 0;
   auto issue = [&](int k) {  // level k into buffer k % PG_NB; one commit group per call
     if (k < d.nz) {
       const long long off = (long long)k * d.plane;

@@ -116,7 +116,7 @@ constexpr int LT_TX = 32, LT_TY = 16;
 constexpr int IV_T = 64;
 void launch_implicit_vdiff(cudaStream_t s, const Dev& d, float* u, float* v, float* T, float* S, const float* u0,
                            const float* v0, const float* T0, const float* S0, float dth, const float* kap3);
-__global__ void k_fz(Dev d, const float* u, const float* v, float* Fz);
+void launch_fz(cudaStream_t s, const Dev& d, const float* u, const float* v, float* Fz);
 __global__ void k_madv(Dev d, const float* u, const float* v, const float* Fz, float* Ayu, float* Ayv);
 __global__ void k_dealias_lon(Dev d, FftPlan plan, const float* Ayu, const float* Ayv, float* Au, float* Av,
                               int lines_per_block);

@@ -258,9 +258,8 @@ struct zm_solver {
   // T/S-independent part of the momentum residual, A = wm (dealiased
   // advection + surface wind - barotropic wind), into Au/Av.
   void momentum_advection_part(cudaStream_t s, const Fields4& src) {
-    const dim3 c(32, 4);
     pb(ZM_K_FZ, s);
-    k_fz<<<grid2(c), c, 0, s>>>(d, src.u, src.v, Fz);
+    launch_fz(s, d, src.u, src.v, Fz);
     pe(s);
     const dim3 m(32, 8);
     pb(ZM_K_MADV, s);
@@ -381,7 +380,6 @@ struct zm_solver {
 
   // Nonlinear RK2 step N(dt): src -> dst.
   void nonlinear(cudaStream_t s, const Fields4& src, const Fields4& dst) {
-    const dim3 c(32, 4);
     momentum_advection_part(s, src);
     // stage 1: tracers at the old velocity, momentum with the predicted tracers
     tracer_residual(s, 1, src.u, src.v, src.T, src.S, src.T, src.S, Tp, Sp);
@@ -395,7 +393,7 @@ struct zm_solver {
     if (!freeze) {
       if (proj_on) project(s, up, vp);  // step.py:292-303
       pb(ZM_K_FZ, s);
-      k_fz<<<grid2(c), c, 0, s>>>(d, up, vp, Fz);
+      launch_fz(s, d, up, vp, Fz);
       pe(s);
       u2 = up;
       v2 = vp;
@@ -1512,7 +1510,7 @@ int zm_diagnostics(zm_solver* s, void* stream, const zm_state* in, const float* 
       k_ref_to_int2<<<s->grid2(dim3(32, 8)), dim3(32, 8), 0, st>>>(s->d, surface_pressure_pa, s->fry);
       sp = s->fry;
     }
-    k_fz<<<s->grid2(c), c, 0, st>>>(s->d, s->s2.u, s->s2.v, s->Fz);
+    launch_fz(st, s->d, s->s2.u, s->s2.v, s->Fz);
     k_diagnostics<<<s->grid2(c), c, 0, st>>>(s->d, s->s2.T, s->s2.S, s->frx, s->Fz, sp, s->W1.u, s->W1.v, s->W2.u);
     s->check_launch();
     s->to_ref3(st, s->W1.u, rho, 0.f);
