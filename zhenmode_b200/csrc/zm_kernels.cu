@@ -27,13 +27,13 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 
 // Plane offset of cell e of a padded column tile PX cells wide whose interior
-// starts at (i0, j0), with a one-cell halo: rows clamped at the closed walls
+// starts at (i0, j0), with an H-cell halo: rows clamped at the closed walls
 // like north()/south(), longitude wrapped like east()/west().
-template <int PX>
+template <int PX, int H = 1>
 __device__ __forceinline__ int tile_cell(const Dev& d, int e, int i0, int j0) {
   const int rr = e / PX, cc = e - rr * PX;
-  const int gj = min(max(j0 - 1 + rr, 0), d.ny - 1);
-  int gi = (i0 - 1 + cc) % d.nx;
+  const int gj = min(max(j0 - H + rr, 0), d.ny - 1);
+  int gi = (i0 - H + cc) % d.nx;
   if (gi < 0) gi += d.nx;
   return idx2(d, gj, gi);
 }
@@ -769,22 +769,29 @@ __device__ __forceinline__ float minmod_slope(float cm, float c0, float cp, floa
 }
 
 // Tracer advection substep (dynamics/tendencies.py:111-140 with
-// _advection_scalar, dynamics/transport.py:365-475) on one level tile: each
-// block owns a TA_X x TA_Y tile of one level; T, S, u, v of that level with a
-// two-cell halo (for the minmod slopes of the face states) and the level's wet
-// flags sit in shared memory.  Each thread forms the four faces of its point,
-// T and S together.  Rows beyond the closed walls are loaded from the clamped
-// row, which is the edge padding of transport.py:199-290; longitude wraps.
-// The vertical donor-cell flux reads the column neighbours directly.
-constexpr int TA_H = 2;
+// _advection_scalar, dynamics/transport.py:365-475).  A block owns a
+// TA_X x TA_Y tile of columns and marches down TA_KC levels of them (the
+// chunks of a column are separate blocks, so the grid fills the GPU in even
+// waves): T, S, u, v of each
+// level on the tile with a two-cell halo (for the minmod slopes of the face
+// states) arrive in shared memory by cp.async one level ahead, in TA_NB
+// rotating buffers; the level's wet flags are formed one level ahead from the
+// cells' bitmasks, held in registers.  Each thread forms the four faces of its
+// point, T and S together; the vertical donor-cell flux takes the level above
+// from registers and the level below from the next buffer.  Rows beyond the
+// closed walls are loaded from the clamped row, which is the edge padding of
+// transport.py:199-290; longitude wraps.
+constexpr int TA_H = 2, TA_NB = 3, TA_KC = 10;
 constexpr int TA_PX = TA_X + 2 * TA_H, TA_PY = TA_Y + 2 * TA_H;
+constexpr int TA_CELLS = TA_PX * TA_PY;
+static_assert(TA_CELLS <= 2 * TA_X * TA_Y, "two tile cells per thread at most");
 
 struct TaTile {
-  float T[TA_PY][TA_PX];
-  float S[TA_PY][TA_PX];
-  float u[TA_PY][TA_PX];
-  float v[TA_PY][TA_PX];
-  float w[TA_PY][TA_PX];
+  float T[TA_NB][TA_PY][TA_PX];
+  float S[TA_NB][TA_PY][TA_PX];
+  float u[TA_NB][TA_PY][TA_PX];
+  float v[TA_NB][TA_PY][TA_PX];
+  float w[2][TA_PY][TA_PX];
 };
 
 // Limited face value of one tracer (transport.py:199-290).  With the upwind
@@ -806,16 +813,17 @@ __device__ __forceinline__ float ta_face_value(bool pos, float cm, float c0, flo
 }
 
 // T and S fluxes through the x face between tile columns cc and cc+1 of row r
+// of level buffer q (wet flags in buffer wq)
 template <int LIM>
-__device__ __forceinline__ void ta_faces_x(const TaTile& t, int r, int cc, float& fT, float& fS) {
-  const float w0 = t.w[r][cc], we = t.w[r][cc + 1];
-  const float ux = 0.5f * (t.u[r][cc] + t.u[r][cc + 1]);
+__device__ __forceinline__ void ta_faces_x(const TaTile& t, int q, int wq, int r, int cc, float& fT, float& fS) {
+  const float w0 = t.w[wq][r][cc], we = t.w[wq][r][cc + 1];
+  const float ux = 0.5f * (t.u[q][r][cc] + t.u[q][r][cc + 1]);
   const bool pos = ux >= 0.f;
-  const float wm = t.w[r][cc - 1], wp = t.w[r][cc + 2];
-  const float cT = ta_face_value<LIM>(pos, t.T[r][cc - 1], t.T[r][cc], t.T[r][cc + 1], t.T[r][cc + 2], wm, w0,
-                                 we, wp);
-  const float cS = ta_face_value<LIM>(pos, t.S[r][cc - 1], t.S[r][cc], t.S[r][cc + 1], t.S[r][cc + 2], wm, w0,
-                                 we, wp);
+  const float wm = t.w[wq][r][cc - 1], wp = t.w[wq][r][cc + 2];
+  const float cT = ta_face_value<LIM>(pos, t.T[q][r][cc - 1], t.T[q][r][cc], t.T[q][r][cc + 1], t.T[q][r][cc + 2],
+                                      wm, w0, we, wp);
+  const float cS = ta_face_value<LIM>(pos, t.S[q][r][cc - 1], t.S[q][r][cc], t.S[q][r][cc + 1], t.S[q][r][cc + 2],
+                                      wm, w0, we, wp);
   const float g = w0 * we;
   fT = ux * cT * g;
   fS = ux * cS * g;
@@ -824,27 +832,27 @@ __device__ __forceinline__ void ta_faces_x(const TaTile& t, int r, int cc, float
 // T and S fluxes through the y face between tile rows r and r+1 (global rows
 // gj, gj+1); zero through the closed walls
 template <int LIM>
-__device__ __forceinline__ void ta_faces_y(const Dev& d, const TaTile& t, int r, int cc, int gj, float& fT,
-                                           float& fS) {
+__device__ __forceinline__ void ta_faces_y(const Dev& d, const TaTile& t, int q, int wq, int r, int cc, int gj,
+                                           float& fT, float& fS) {
   if (gj < 0 || gj >= d.ny - 1) {
     fT = fS = 0.f;
     return;
   }
-  const float w0 = t.w[r][cc], wn = t.w[r + 1][cc];
-  const float vy = 0.5f * (t.v[r][cc] + t.v[r + 1][cc]);
+  const float w0 = t.w[wq][r][cc], wn = t.w[wq][r + 1][cc];
+  const float vy = 0.5f * (t.v[q][r][cc] + t.v[q][r + 1][cc]);
   const bool pos = vy >= 0.f;
-  const float wm = t.w[r - 1][cc], wp = t.w[r + 2][cc];
-  const float cT = ta_face_value<LIM>(pos, t.T[r - 1][cc], t.T[r][cc], t.T[r + 1][cc], t.T[r + 2][cc], wm, w0,
-                                 wn, wp);
-  const float cS = ta_face_value<LIM>(pos, t.S[r - 1][cc], t.S[r][cc], t.S[r + 1][cc], t.S[r + 2][cc], wm, w0,
-                                 wn, wp);
+  const float wm = t.w[wq][r - 1][cc], wp = t.w[wq][r + 2][cc];
+  const float cT = ta_face_value<LIM>(pos, t.T[q][r - 1][cc], t.T[q][r][cc], t.T[q][r + 1][cc], t.T[q][r + 2][cc],
+                                      wm, w0, wn, wp);
+  const float cS = ta_face_value<LIM>(pos, t.S[q][r - 1][cc], t.S[q][r][cc], t.S[q][r + 1][cc], t.S[q][r + 2][cc],
+                                      wm, w0, wn, wp);
   const float g = w0 * wn, cf = __ldg(d.cfp + gj);
   fT = vy * cT * g * cf;
   fS = vy * cS * g * cf;
 }
 
 template <int LIM>
-__global__ void __launch_bounds__(TA_X * TA_Y, 4) k_tracer_adv_t(Dev d, const float* __restrict__ T,
+__global__ void __launch_bounds__(TA_X * TA_Y, 5) k_tracer_adv_t(Dev d, const float* __restrict__ T,
                                                                  const float* __restrict__ S,
                                                                  const float* __restrict__ u,
                                                                  const float* __restrict__ v,
@@ -855,84 +863,118 @@ __global__ void __launch_bounds__(TA_X * TA_Y, 4) k_tracer_adv_t(Dev d, const fl
                                                                  float* __restrict__ topT,
                                                                  float* __restrict__ topS) {
   __shared__ TaTile t;
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int tid = ty * TA_X + tx, nt = TA_X * TA_Y;
-  const int i0 = blockIdx.x * TA_X, j0 = blockIdx.y * TA_Y, k = blockIdx.z;
-  const long long kb = (long long)k * d.plane;
-  constexpr int NCELL = TA_PX * TA_PY;
-  for (int e = tid; e < NCELL; e += nt) {
-    const int r = e / TA_PX, cc = e - r * TA_PX;
-    int gj = j0 - TA_H + r;
-    gj = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
-    int gi = i0 - TA_H + cc;
-    if (gi < 0 || gi >= d.nx) gi = ((gi % d.nx) + d.nx) % d.nx;
-    const int c2 = idx2(d, gj, gi);
-    const long long g = kb + c2;
-    t.T[r][cc] = ld(T, g);
-    t.S[r][cc] = ld(S, g);
-    t.u[r][cc] = ld(u, g);
-    t.v[r][cc] = ld(v, g);
-    t.w[r][cc] = wetf(__ldg(d.wbits + c2), k);
-  }
-  __syncthreads();
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TA_X + tx;
+  const int i0 = blockIdx.x * TA_X, j0 = blockIdx.y * TA_Y;
   const int i = i0 + tx, j = j0 + ty;
-  if (i >= d.nx || j >= d.ny) return;
+  // threads outside the grid copy their tile cells, form their wet flags and
+  // meet the barriers, nothing else
+  const bool in = i < d.nx && j < d.ny;
+  const int e0 = tid, e1 = tid + TA_X * TA_Y;
+  const bool has1 = e1 < TA_CELLS;
+  const int s0 = tile_cell<TA_PX, TA_H>(d, e0, i0, j0), s1 = has1 ? tile_cell<TA_PX, TA_H>(d, e1, i0, j0) : 0;
+  const uint64_t b0 = __ldg(d.wbits + s0), b1 = has1 ? __ldg(d.wbits + s1) : 0ull;
+  const int k0 = blockIdx.z * TA_KC, k1 = min(d.nz, k0 + TA_KC);  // this block's levels
+  auto issue = [&](int k) {  // level k into buffer k % TA_NB; one commit group per call
+    if (k < d.nz && k <= k1) {  // level k1 only for the column neighbour below the chunk
+      const long long off = (long long)k * d.plane;
+      const int q = k % TA_NB;
+      cp_async4(&t.T[q][0][0] + e0, T + off + s0);
+      cp_async4(&t.S[q][0][0] + e0, S + off + s0);
+      cp_async4(&t.u[q][0][0] + e0, u + off + s0);
+      cp_async4(&t.v[q][0][0] + e0, v + off + s0);
+      if (has1) {
+        cp_async4(&t.T[q][0][0] + e1, T + off + s1);
+        cp_async4(&t.S[q][0][0] + e1, S + off + s1);
+        cp_async4(&t.u[q][0][0] + e1, u + off + s1);
+        cp_async4(&t.v[q][0][0] + e1, v + off + s1);
+      }
+    }
+    cp_async_commit();
+  };
+  auto wet_level = [&](int k) {  // wet flags of level k into w[k % 2]
+    if (k < d.nz) {
+      float* pw = &t.w[k & 1][0][0];
+      pw[e0] = wetf(b0, k);
+      if (has1) pw[e1] = wetf(b1, k);
+    }
+  };
+  issue(k0);
+  issue(k0 + 1);
+  wet_level(k0);
+  const int ic = in ? i : 0, jc = in ? j : 0;
+  const long long base = idx2(d, jc, ic);
+  const uint64_t bits = __ldg(d.wbits + base);
+  const int kbt = kbot_of(bits);
+  const float ix = __ldg(d.inv_dx + base), ysc = d.inv_dy * __ldg(d.inv_cos + jc);
   const int r = ty + TA_H, cc = tx + TA_H;
-  const long long base = idx2(d, j, i);
-  const long long id = kb + base;
-  const float w0 = t.w[r][cc];
-  const float ck = t.T[r][cc], sk = t.S[r][cc];
-  if (topT && k == 0) {  // ledger mode: the rigid-lid surface flux Fz[0] c[0] of the substep, summed
-    const float fz0 = ld(Fz, id);
-    topT[base] = (first ? 0.f : topT[base]) + fz0 * ck;
-    topS[base] = (first ? 0.f : topS[base]) + fz0 * sk;
-  }
-  float aT = 0.f, aS = 0.f;
-  if (w0 != 0.f) {
-    const uint64_t bits = __ldg(d.wbits + base);
-    float fxeT, fxeS, fxwT, fxwS, fynT, fynS, fysT, fysS;
-    ta_faces_x<LIM>(t, r, cc, fxeT, fxeS);
-    ta_faces_x<LIM>(t, r, cc - 1, fxwT, fxwS);
-    ta_faces_y<LIM>(d, t, r, cc, j, fynT, fynS);
-    ta_faces_y<LIM>(d, t, r - 1, cc, j - 1, fysT, fysS);
-    const float ix = __ldg(d.inv_dx + base), ysc = d.inv_dy * __ldg(d.inv_cos + j);
-    const float hT = (fxeT - fxwT) * ix + (fynT - fysT) * ysc;
-    const float hS = (fxeS - fxwS) * ix + (fynS - fysS) * ysc;
-    const float fz_k = ld(Fz, id);
-    float upT, upS, dnT = 0.f, dnS = 0.f;
-    if (k == 0) {
-      upT = fz_k * ck;
-      upS = fz_k * sk;
-    } else {
-      const float g = wetf(bits, k - 1) * w0;
-      upT = fz_k * (fz_k > 0.f ? ld(T, id - d.plane) : ck) * g;
-      upS = fz_k * (fz_k > 0.f ? ld(S, id - d.plane) : sk) * g;
+  // T, S of the level above and Fz of the current level
+  float ckm = k0 > 0 ? ld(T, base + (long long)(k0 - 1) * d.plane) : 0.f;
+  float skm = k0 > 0 ? ld(S, base + (long long)(k0 - 1) * d.plane) : 0.f;
+  float fzk = ld(Fz, base + (long long)k0 * d.plane);
+  for (int k = k0; k < k1; ++k) {
+    cp_async_wait<0>();  // this thread's copies of levels k and k + 1 are done
+    __syncthreads();     // everyone's are, w[k % 2] is formed, level k - 1's buffers are free
+    issue(k + 2);
+    wet_level(k + 1);
+    const long long id = (long long)k * d.plane + base;
+    const float fzn = k + 1 < d.nz ? ld(Fz, id + d.plane) : 0.f;
+    if (!in) continue;
+    const int q = k % TA_NB, qn = (k + 1) % TA_NB, wq = k & 1;
+    const float w0 = t.w[wq][r][cc];
+    const float ck = t.T[q][r][cc], sk = t.S[q][r][cc];
+    if (topT && k == 0) {  // ledger mode: the rigid-lid surface flux Fz[0] c[0] of the substep, summed
+      topT[base] = (first ? 0.f : topT[base]) + fzk * ck;
+      topS[base] = (first ? 0.f : topS[base]) + fzk * sk;
     }
-    if (k + 1 < d.nz) {
-      const float g = w0 * wetf(bits, k + 1);
-      const float fz_n = ld(Fz, id + d.plane);
-      // ghost fill below the deepest wet level: node k+1 carries node k's value
-      const bool below = k + 1 <= kbot_of(bits);
-      const float tn = below ? ld(T, id + d.plane) : ck, sn = below ? ld(S, id + d.plane) : sk;
-      dnT = fz_n * (fz_n > 0.f ? ck : tn) * g;
-      dnS = fz_n * (fz_n > 0.f ? sk : sn) * g;
+    float aT = 0.f, aS = 0.f;
+    if (w0 != 0.f) {
+      float fxeT, fxeS, fxwT, fxwS, fynT, fynS, fysT, fysS;
+      ta_faces_x<LIM>(t, q, wq, r, cc, fxeT, fxeS);
+      ta_faces_x<LIM>(t, q, wq, r, cc - 1, fxwT, fxwS);
+      ta_faces_y<LIM>(d, t, q, wq, r, cc, jc, fynT, fynS);
+      ta_faces_y<LIM>(d, t, q, wq, r - 1, cc, jc - 1, fysT, fysS);
+      const float hT = (fxeT - fxwT) * ix + (fynT - fysT) * ysc;
+      const float hS = (fxeS - fxwS) * ix + (fynS - fysS) * ysc;
+      const float fz_k = fzk;
+      float upT, upS, dnT = 0.f, dnS = 0.f;
+      if (k == 0) {
+        upT = fz_k * ck;
+        upS = fz_k * sk;
+      } else {
+        const float g = wetf(bits, k - 1) * w0;
+        upT = fz_k * (fz_k > 0.f ? ckm : ck) * g;
+        upS = fz_k * (fz_k > 0.f ? skm : sk) * g;
+      }
+      if (k + 1 < d.nz) {
+        const float g = w0 * wetf(bits, k + 1);
+        const float fz_n = fzn;
+        // ghost fill below the deepest wet level: node k+1 carries node k's value
+        const bool below = k + 1 <= kbt;
+        const float tn = below ? t.T[qn][r][cc] : ck, sn = below ? t.S[qn][r][cc] : sk;
+        dnT = fz_n * (fz_n > 0.f ? ck : tn) * g;
+        dnS = fz_n * (fz_n > 0.f ? sk : sn) * g;
+      }
+      aT = -(hT + (dnT - upT) * d.vc.inv_dz_node[k]) * w0;
+      aS = -(hS + (dnS - upS) * d.vc.inv_dz_node[k]) * w0;
     }
-    aT = -(hT + (dnT - upT) * d.vc.inv_dz_node[k]) * w0;
-    aS = -(hS + (dnS - upS) * d.vc.inv_dz_node[k]) * w0;
-  }
-  accT[id] = first ? aT : accT[id] + aT;
-  accS[id] = first ? aS : accS[id] + aS;
-  if (!last) {
-    Tn[id] = ck + aT * dts;
-    Sn[id] = sk + aS * dts;
+    accT[id] = first ? aT : accT[id] + aT;
+    accS[id] = first ? aS : accS[id] + aS;
+    if (!last) {
+      Tn[id] = ck + aT * dts;
+      Sn[id] = sk + aS * dts;
+    }
+    ckm = ck;
+    skm = sk;
+    fzk = fzn;
   }
 }
 
 // The face limiter is a template argument: the face arithmetic is specialised
 // instead of branching on it at every face.
-void launch_tracer_adv(dim3 g, dim3 b, cudaStream_t s, const Dev& d, const float* T, const float* S,
-                       const float* u, const float* v, const float* Fz, float* accT, float* accS, float* Tn,
-                       float* Sn, float dts, int first, int last, float* topT, float* topS) {
+void launch_tracer_adv(cudaStream_t s, const Dev& d, const float* T, const float* S, const float* u, const float* v,
+                       const float* Fz, float* accT, float* accS, float* Tn, float* Sn, float dts, int first, int last,
+                       float* topT, float* topS) {
+  const dim3 g((d.nx + TA_X - 1) / TA_X, (d.ny + TA_Y - 1) / TA_Y, (d.nz + TA_KC - 1) / TA_KC), b(TA_X, TA_Y);
   if (d.limiter == 2)
     k_tracer_adv_t<2><<<g, b, 0, s>>>(d, T, S, u, v, Fz, accT, accS, Tn, Sn, dts, first, last, topT, topS);
   else if (d.limiter == 1)

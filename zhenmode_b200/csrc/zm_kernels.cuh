@@ -37,8 +37,8 @@ struct RestArgs {
 
 // momentum-advection tile rows (k_madv)
 constexpr int MADV_TY = 60;
-// 2.5-D tracer advection tile
-constexpr int TA_X = 32, TA_Y = 16;
+// tracer advection column tile (k_tracer_adv_t marches it down the levels)
+constexpr int TA_X = 32, TA_Y = 8;
 // temporally blocked nu_h subcycles: tile width, rows per thread, subcycles per pass
 constexpr int NB_W = 64;
 constexpr int NB_R = 8;
@@ -120,9 +120,9 @@ void launch_fz(cudaStream_t s, const Dev& d, const float* u, const float* v, flo
 __global__ void k_madv(Dev d, const float* u, const float* v, const float* Fz, float* Ayu, float* Ayv);
 __global__ void k_dealias_lon(Dev d, FftPlan plan, const float* Ayu, const float* Ayv, float* Au, float* Av,
                               int lines_per_block);
-void launch_tracer_adv(dim3 g, dim3 b, cudaStream_t s, const Dev& d, const float* T, const float* S,
-                       const float* u, const float* v, const float* Fz, float* accT, float* accS,
-                       float* Tn, float* Sn, float dts, int first, int last, float* topT, float* topS);
+void launch_tracer_adv(cudaStream_t s, const Dev& d, const float* T, const float* S, const float* u, const float* v,
+                       const float* Fz, float* accT, float* accS, float* Tn, float* Sn, float dts, int first, int last,
+                       float* topT, float* topS);
 void launch_tracer_rest(dim3 g, dim3 b, cudaStream_t s, const Dev& d, const RestArgs& a);
 void launch_pgf(cudaStream_t s, const Dev& d, const PgfArgs& a);
 __global__ void k_bt_forcing(Dev d, const float* frx, const float* fry, double* Fx, double* Fy, const float* eta32,

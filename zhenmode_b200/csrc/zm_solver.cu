@@ -229,9 +229,8 @@ struct zm_solver {
       float* nT = (n % 2 == 0) ? TsA : TsB;
       float* nS = (n % 2 == 0) ? SsA : SsB;
       pb(ZM_K_TRACER_ADV, s);
-      launch_tracer_adv(dim3((nx + TA_X - 1) / TA_X, (ny + TA_Y - 1) / TA_Y, nz), dim3(TA_X, TA_Y), s,
-          d, cT, cS, u, v, Fz, accT, accS, nT, nS, dts, n == 0, n == adv_nsub - 1, ledger_on ? led_topT : nullptr,
-          ledger_on ? led_topS : nullptr);
+      launch_tracer_adv(s, d, cT, cS, u, v, Fz, accT, accS, nT, nS, dts, n == 0, n == adv_nsub - 1,
+                        ledger_on ? led_topT : nullptr, ledger_on ? led_topS : nullptr);
       pe(s);
       cT = nT;
       cS = nS;
