@@ -95,39 +95,6 @@ __device__ __forceinline__ float colv(const float* __restrict__ a, long long bas
   return ld(a, base + (long long)(k < kb ? k : kb) * plane);
 }
 
-// Node-form d2/dz2 with zero-flux ends on the ghost-filled column
-// (numerics/vertical.py:275-293).
-__device__ __forceinline__ float d2z(const Dev& d, const float* __restrict__ a, long long base, int k, int kb) {
-  if (k == 0) {
-    if (d.nz < 2) return 0.f;
-    return d.vc.d2_top * (colv(a, base, d.plane, 1, kb) - colv(a, base, d.plane, 0, kb));
-  }
-  if (k == d.nz - 1)
-    return d.vc.d2_bot * (colv(a, base, d.plane, k - 1, kb) - colv(a, base, d.plane, k, kb));
-  const float a0 = colv(a, base, d.plane, k, kb);
-  return d.vc.d2_hi[k] * (colv(a, base, d.plane, k + 1, kb) - a0) +
-         d.vc.d2_lo[k] * (colv(a, base, d.plane, k - 1, kb) - a0);
-}
-
-// Interface-flux vertical diffusion (numerics/vertical.py:317-332), the
-// conservative_kv form.
-__device__ __forceinline__ float d2z_flux(const Dev& d, const float* __restrict__ a, long long base, int k,
-                                          uint64_t bits, float kappa) {
-  const int kb = kbot_of(bits);
-  float up = 0.f, dn = 0.f;
-  if (k > 0 && wetb(bits, k - 1) && wetb(bits, k))
-    up = -kappa * (colv(a, base, d.plane, k, kb) - colv(a, base, d.plane, k - 1, kb)) * d.vc.inv_dz_iface[k - 1];
-  if (k < d.nz - 1 && wetb(bits, k) && wetb(bits, k + 1))
-    dn = -kappa * (colv(a, base, d.plane, k + 1, kb) - colv(a, base, d.plane, k, kb)) * d.vc.inv_dz_iface[k];
-  return (up - dn) * d.vc.inv_dz_node[k] * wetf(bits, k);
-}
-
-__device__ __forceinline__ float vdiff_tracer(const Dev& d, const float* __restrict__ a, long long base, int k,
-                                              uint64_t bits, float kv) {
-  if (d.conservative_kv) return d2z_flux(d, a, base, k, bits, kv);
-  return kv * d2z(d, a, base, k, kbot_of(bits));
-}
-
 #define ZM_POINT_IDX                                   \
   const int i = blockIdx.x * blockDim.x + threadIdx.x; \
   const int j = blockIdx.y * blockDim.y + threadIdx.y; \
@@ -276,174 +243,257 @@ k_nu_tb(Dev d, const float* __restrict__ u, const float* __restrict__ v, float* 
   }
 }
 
-// Whole linear half step except the nu_h subcycles, on one level tile
-// (timestepping/step.py:108-173, legacy, mode split).  u0, v0, T0, S0 of the
-// level with a two-cell halo sit in shared memory; the inner Laplacians of
+// Whole linear half step except the nu_h subcycles (timestepping/step.py:108-173,
+// legacy, mode split).  A block owns an LT_X x LT_Y tile of columns and marches
+// down LT_KC levels of them (the chunks of a column are separate blocks): u0,
+// v0, T0, S0 of each level on the tile with a two-cell halo arrive in shared
+// memory by cp.async one level ahead, in LT_NB rotating buffers; the wet flags
+// are formed one level ahead from the cells' bitmasks, held in registers; the
+// 2-D metric and diffusivity fields are loaded once.  The inner Laplacians of
 // the biharmonic operators (numerics/horizontal.py:245-253) are formed on the
 // one-cell ring, the outer ones at the tile interior.  Rows beyond the closed
 // walls load the clamped row (the edge padding of horizontal.py:14-25); the
-// outer biharmonic applies the mirror to the inner Laplacian field, whose
-// edge row is padded by itself in the reference.  Vertical diffusion reads
-// the column neighbours directly; then land/ghost hold and the exact
-// Coriolis rotation by f dt/2.
-constexpr int LT_X = LT_TX, LT_Y = LT_TY, LT_H = 2;
+// outer biharmonic applies the mirror to the inner Laplacian field, whose edge
+// row is padded by itself in the reference.  Vertical diffusion takes the level
+// above from registers and the level below from the next buffer; then
+// land/ghost hold and the exact Coriolis rotation by f dt/2.
+constexpr int LT_X = 32, LT_Y = 8, LT_H = 2, LT_NB = 3, LT_KC = 10;
 constexpr int LT_PX = LT_X + 2 * LT_H, LT_PY = LT_Y + 2 * LT_H;
+constexpr int LT_CELLS = LT_PX * LT_PY;
+static_assert(LT_CELLS <= 2 * LT_X * LT_Y, "two tile cells per thread at most");
 
 struct LtTile {
-  float u[LT_PY][LT_PX], v[LT_PY][LT_PX], T[LT_PY][LT_PX], S[LT_PY][LT_PX];
+  float u[LT_NB][LT_PY][LT_PX], v[LT_NB][LT_PY][LT_PX], T[LT_NB][LT_PY][LT_PX], S[LT_NB][LT_PY][LT_PX];
   float Lu[LT_PY][LT_PX], Lv[LT_PY][LT_PX], LT[LT_PY][LT_PX], LS[LT_PY][LT_PX];
-  float w[LT_PY][LT_PX], kh[LT_PY][LT_PX], ix[LT_PY][LT_PX], ix2[LT_PY][LT_PX];
+  float w[2][LT_PY][LT_PX], kh[LT_PY][LT_PX], ix[LT_PY][LT_PX], ix2[LT_PY][LT_PX];
   float tanR[LT_PY], cfp[LT_PY], icos[LT_PY];
   int gj[LT_PY];
 };
 
-// Laplacian of a tile field at (r, c) (horizontal.py:181-215); `mirror`
-// replaces the outer neighbour at a wall row by the row itself.
-__device__ __forceinline__ float lap_s(const Dev& d, const LtTile& t, const float (*a)[LT_PX], int r, int c,
-                                      bool mirror) {
+// Laplacian of a tile field at (r, c) (horizontal.py:181-215) with the wet
+// flags w of its level; `mirror` replaces the outer neighbour at a wall row by
+// the row itself.
+__device__ __forceinline__ float lap_s(const Dev& d, const LtTile& t, const float (*w)[LT_PX],
+                                      const float (*a)[LT_PX], int r, int c, bool mirror) {
   const float a0 = a[r][c], ae = a[r][c + 1], aw = a[r][c - 1];
   float an = a[r + 1][c], as = a[r - 1][c];
   if (mirror) {
     if (t.gj[r] == d.ny - 1) an = a0;
     if (t.gj[r] == 0) as = a0;
   }
-  const float w0 = t.w[r][c];
-  const float d2x = ((ae - a0) * w0 * t.w[r][c + 1] - (a0 - aw) * w0 * t.w[r][c - 1]) * t.ix2[r][c];
-  const float d2y = ((an - a0) * t.w[r + 1][c] * w0 - (a0 - as) * w0 * t.w[r - 1][c]) * d.inv_dy2;
+  const float w0 = w[r][c];
+  const float d2x = ((ae - a0) * w0 * w[r][c + 1] - (a0 - aw) * w0 * w[r][c - 1]) * t.ix2[r][c];
+  const float d2y = ((an - a0) * w[r + 1][c] * w0 - (a0 - as) * w0 * w[r - 1][c]) * d.inv_dy2;
   const float ddy = (an - as) * (0.5f * d.inv_dy);
   return d2x + d2y + (-ddy * t.tanR[r]);
 }
 
-// Wet-face flux diffusion of a tile field at (r, c) (horizontal.py:217-243);
-// unit diffusivity when `unit`.  The wall faces are closed explicitly.
-__device__ __forceinline__ float hdiff_s(const Dev& d, const LtTile& t, const float (*a)[LT_PX], int r, int c,
-                                        bool unit) {
+// Wet-face flux diffusion of a tile field at (r, c) (horizontal.py:217-243)
+// with the wet flags w of its level; unit diffusivity when `unit`.  The wall
+// faces are closed explicitly.
+__device__ __forceinline__ float hdiff_s(const Dev& d, const LtTile& t, const float (*w)[LT_PX],
+                                        const float (*a)[LT_PX], int r, int c, bool unit) {
   const float a0 = a[r][c];
   const float k0 = unit ? 1.f : t.kh[r][c];
   const float ke = unit ? 1.f : t.kh[r][c + 1], kw = unit ? 1.f : t.kh[r][c - 1];
   const float kn = unit ? 1.f : t.kh[r + 1][c], ks = unit ? 1.f : t.kh[r - 1][c];
-  const float w0 = t.w[r][c];
-  const float fe = 0.5f * (k0 + ke) * (a[r][c + 1] - a0) * t.ix[r][c] * w0 * t.w[r][c + 1];
-  const float fw = 0.5f * (kw + k0) * (a0 - a[r][c - 1]) * t.ix[r][c - 1] * t.w[r][c - 1] * w0;
+  const float w0 = w[r][c];
+  const float fe = 0.5f * (k0 + ke) * (a[r][c + 1] - a0) * t.ix[r][c] * w0 * w[r][c + 1];
+  const float fw = 0.5f * (kw + k0) * (a0 - a[r][c - 1]) * t.ix[r][c - 1] * w[r][c - 1] * w0;
   const int gj = t.gj[r];
   float fn = 0.f, fs = 0.f;
-  if (gj < d.ny - 1) fn = 0.5f * (k0 + kn) * (a[r + 1][c] - a0) * d.inv_dy * w0 * t.w[r + 1][c] * t.cfp[r];
-  if (gj > 0) fs = 0.5f * (ks + k0) * (a0 - a[r - 1][c]) * d.inv_dy * t.w[r - 1][c] * w0 * t.cfp[r - 1];
+  if (gj < d.ny - 1) fn = 0.5f * (k0 + kn) * (a[r + 1][c] - a0) * d.inv_dy * w0 * w[r + 1][c] * t.cfp[r];
+  if (gj > 0) fs = 0.5f * (ks + k0) * (a0 - a[r - 1][c]) * d.inv_dy * w[r - 1][c] * w0 * t.cfp[r - 1];
   return (fe - fw) * t.ix[r][c] + (fn - fs) * d.inv_dy * t.icos[r];
 }
 
+// Node-form d2/dz2 with zero-flux ends (numerics/vertical.py:275-293) and the
+// tracer vertical diffusion at a wet level k of a column, from its values at
+// k - 1 (am), k (a0) and k + 1 (ap): the column is ghost-filled below kbot
+// with its value at kbot (numerics/vertical.py:122-135), so the level below
+// reads a0 at k = kbot.
+__device__ __forceinline__ float d2z_c(const Dev& d, int k, int kb, float am, float a0, float ap) {
+  const float dn = k < kb ? ap : a0;
+  if (k == 0) {
+    if (d.nz < 2) return 0.f;
+    return d.vc.d2_top * (dn - a0);
+  }
+  if (k == d.nz - 1) return d.vc.d2_bot * (am - a0);
+  return d.vc.d2_hi[k] * (dn - a0) + d.vc.d2_lo[k] * (am - a0);
+}
+
+__device__ __forceinline__ float vdiff_c(const Dev& d, int k, uint64_t bits, float kappa, float am, float a0,
+                                         float ap) {
+  if (d.conservative_kv) {  // interface-flux form (numerics/vertical.py:317-332)
+    float up = 0.f, dn = 0.f;
+    if (k > 0 && wetb(bits, k - 1) && wetb(bits, k)) up = -kappa * (a0 - am) * d.vc.inv_dz_iface[k - 1];
+    if (k < d.nz - 1 && wetb(bits, k) && wetb(bits, k + 1)) dn = -kappa * (ap - a0) * d.vc.inv_dz_iface[k];
+    return (up - dn) * d.vc.inv_dz_node[k] * wetf(bits, k);
+  }
+  return kappa * d2z_c(d, k, kbot_of(bits), am, a0, ap);
+}
+
 template <bool UV, bool TS, bool IMPL>
-__global__ void __launch_bounds__(LT_X * LT_Y) k_lin_t(Dev d, const float* __restrict__ usub,
-                                                      const float* __restrict__ vsub, const float* __restrict__ u0,
-                                                      const float* __restrict__ v0, const float* __restrict__ T0,
-                                                      const float* __restrict__ S0, float* __restrict__ uo,
-                                                      float* __restrict__ vo, float* __restrict__ To,
-                                                      float* __restrict__ So, float dth) {
+__global__ void __launch_bounds__(LT_X * LT_Y, 4) k_lin_t(Dev d, const float* __restrict__ usub,
+                                                         const float* __restrict__ vsub, const float* __restrict__ u0,
+                                                         const float* __restrict__ v0, const float* __restrict__ T0,
+                                                         const float* __restrict__ S0, float* __restrict__ uo,
+                                                         float* __restrict__ vo, float* __restrict__ To,
+                                                         float* __restrict__ So, float dth) {
   extern __shared__ float lt_smem[];
   LtTile& t = *reinterpret_cast<LtTile*>(lt_smem);
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = ty * LT_X + tx, nt = LT_X * LT_Y;
-  const int i0 = blockIdx.x * LT_X, j0 = blockIdx.y * LT_Y, k = blockIdx.z;
-  const long long kb = (long long)k * d.plane;
-  constexpr int NCELL = LT_PX * LT_PY;
-  for (int e = tid; e < NCELL; e += nt) {
-    const int r = e / LT_PX, cc = e - r * LT_PX;
-    int gj = j0 - LT_H + r;
-    gj = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
-    int gi = i0 - LT_H + cc;
-    if (gi < 0 || gi >= d.nx) gi = ((gi % d.nx) + d.nx) % d.nx;
-    const int c2 = idx2(d, gj, gi);
-    const long long g = kb + c2;
-    t.u[r][cc] = ld(u0, g);
-    t.v[r][cc] = ld(v0, g);
-    t.T[r][cc] = ld(T0, g);
-    t.S[r][cc] = ld(S0, g);
-    t.w[r][cc] = wetf(__ldg(d.wbits + c2), k);
-    t.kh[r][cc] = __ldg(d.kh2 + c2);
-    t.ix[r][cc] = __ldg(d.inv_dx + c2);
-    t.ix2[r][cc] = __ldg(d.inv_dx2 + c2);
+  const int i0 = blockIdx.x * LT_X, j0 = blockIdx.y * LT_Y;
+  const int k0 = blockIdx.z * LT_KC, k1 = min(d.nz, k0 + LT_KC);  // this block's levels
+  const int i = i0 + tx, j = j0 + ty;
+  // threads outside the grid copy their tile cells, form their wet flags and
+  // meet the barriers, nothing else
+  const bool in = i < d.nx && j < d.ny;
+  const int e0 = tid, e1 = tid + nt;
+  const bool has1 = e1 < LT_CELLS;
+  const int s0 = tile_cell<LT_PX, LT_H>(d, e0, i0, j0), s1 = has1 ? tile_cell<LT_PX, LT_H>(d, e1, i0, j0) : 0;
+  const uint64_t b0 = __ldg(d.wbits + s0), b1 = has1 ? __ldg(d.wbits + s1) : 0ull;
+  (&t.kh[0][0])[e0] = __ldg(d.kh2 + s0);
+  (&t.ix[0][0])[e0] = __ldg(d.inv_dx + s0);
+  (&t.ix2[0][0])[e0] = __ldg(d.inv_dx2 + s0);
+  if (has1) {
+    (&t.kh[0][0])[e1] = __ldg(d.kh2 + s1);
+    (&t.ix[0][0])[e1] = __ldg(d.inv_dx + s1);
+    (&t.ix2[0][0])[e1] = __ldg(d.inv_dx2 + s1);
   }
   if (tid < LT_PY) {
-    int gj = j0 - LT_H + tid;
-    gj = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
+    const int gj = min(max(j0 - LT_H + tid, 0), d.ny - 1);
     t.gj[tid] = gj;
     t.tanR[tid] = __ldg(d.tanR + gj);
     t.cfp[tid] = __ldg(d.cfp + gj);
     t.icos[tid] = __ldg(d.inv_cos + gj);
   }
-  __syncthreads();
-  constexpr bool do_uv = UV, do_ts = TS;
-  if (do_uv || do_ts) {
-    // the one-cell ring around the interior, walked over whole padded rows so
-    // that a warp's shared-memory addresses are consecutive (no bank conflicts)
-    constexpr int RY = LT_Y + 2;
-    for (int e = tid; e < LT_PX * RY; e += nt) {
-      const int r = 1 + e / LT_PX, cc = e % LT_PX;
-      if (cc == 0 || cc == LT_PX - 1) continue;
-      if (do_uv) {
-        t.Lu[r][cc] = lap_s(d, t, t.u, r, cc, false);
-        t.Lv[r][cc] = lap_s(d, t, t.v, r, cc, false);
-      }
-      if (do_ts) {
-        t.LT[r][cc] = hdiff_s(d, t, t.T, r, cc, true);
-        t.LS[r][cc] = hdiff_s(d, t, t.S, r, cc, true);
+  auto issue = [&](int k) {  // level k into buffer k % LT_NB; one commit group per call
+    if (k < d.nz && k <= k1) {  // level k1 only for the column neighbour below the chunk
+      const long long off = (long long)k * d.plane;
+      const int q = k % LT_NB;
+      cp_async4(&t.u[q][0][0] + e0, u0 + off + s0);
+      cp_async4(&t.v[q][0][0] + e0, v0 + off + s0);
+      cp_async4(&t.T[q][0][0] + e0, T0 + off + s0);
+      cp_async4(&t.S[q][0][0] + e0, S0 + off + s0);
+      if (has1) {
+        cp_async4(&t.u[q][0][0] + e1, u0 + off + s1);
+        cp_async4(&t.v[q][0][0] + e1, v0 + off + s1);
+        cp_async4(&t.T[q][0][0] + e1, T0 + off + s1);
+        cp_async4(&t.S[q][0][0] + e1, S0 + off + s1);
       }
     }
-    __syncthreads();
-  }
-  const int i = i0 + tx, j = j0 + ty;
-  if (i >= d.nx || j >= d.ny) return;
-  const int r = ty + LT_H, cc = tx + LT_H;
-  const long long base = idx2(d, j, i);
-  const long long id = kb + base;
+    cp_async_commit();
+  };
+  auto wet_level = [&](int k) {  // wet flags of level k into w[k % 2]
+    if (k < d.nz) {
+      float* pw = &t.w[k & 1][0][0];
+      pw[e0] = wetf(b0, k);
+      if (has1) pw[e1] = wetf(b1, k);
+    }
+  };
+  issue(k0);
+  issue(k0 + 1);
+  wet_level(k0);
+  const int ic = in ? i : 0, jc = in ? j : 0;
+  const long long base = idx2(d, jc, ic);
   const uint64_t bits = __ldg(d.wbits + base);
-  const bool wet = wetb(bits, k);
-  float u, v, T, S;
-  if (!wet) {
-    u = t.u[r][cc];
-    v = t.v[r][cc];
-    T = t.T[r][cc];
-    S = t.S[r][cc];
-  } else {
-    T = t.T[r][cc] + hdiff_s(d, t, t.T, r, cc, false) * dth;
-    S = t.S[r][cc] + hdiff_s(d, t, t.S, r, cc, false) * dth;
-    if (do_ts) {
-      T = T - d.kappa_bi * hdiff_s(d, t, t.LT, r, cc, true) * dth;
-      S = S - d.kappa_bi * hdiff_s(d, t, t.LS, r, cc, true) * dth;
-    }
-    u = ld(usub, id);
-    v = ld(vsub, id);
-    if (do_uv) {
-      u = u - d.nu_bi * lap_s(d, t, t.Lu, r, cc, true) * dth;
-      v = v - d.nu_bi * lap_s(d, t, t.Lv, r, cc, true) * dth;
-    }
-    if (!IMPL) {
-      const int kbt = kbot_of(bits);
-      const float kv = __ldg(d.kv2 + base);
-      u = u + d.nu_v * d2z(d, u0, base, k, kbt) * dth;
-      v = v + d.nu_v * d2z(d, v0, base, k, kbt) * dth;
-      T = T + vdiff_tracer(d, T0, base, k, bits, kv) * dth;
-      S = S + vdiff_tracer(d, S0, base, k, bits, kv) * dth;
-    }
+  const int kbt = kbot_of(bits);
+  const float kv = __ldg(d.kv2 + base);
+  const float rc = IMPL ? 0.f : __ldg(d.rot_c + base), rs = IMPL ? 0.f : __ldg(d.rot_s + base);
+  // u0, v0, T0, S0 of the level above
+  float um = 0.f, vm = 0.f, Tm = 0.f, Sm = 0.f;
+  if (k0 > 0) {
+    const long long pid = base + (long long)(k0 - 1) * d.plane;
+    um = ld(u0, pid);
+    vm = ld(v0, pid);
+    Tm = ld(T0, pid);
+    Sm = ld(S0, pid);
   }
-  To[id] = T;
-  So[id] = S;
-  if (IMPL) {  // the column solve and the rotation follow
-    uo[id] = u;
-    vo[id] = v;
-    return;
+  const int r = ty + LT_H, cc = tx + LT_H;
+  constexpr bool do_uv = UV, do_ts = TS;
+  for (int k = k0; k < k1; ++k) {
+    cp_async_wait<0>();  // this thread's copies of levels k and k + 1 are done
+    __syncthreads();     // everyone's are, w[k % 2] is formed, the ring fields and level k - 1's buffers are free
+    issue(k + 2);
+    wet_level(k + 1);
+    const int q = k % LT_NB, qn = (k + 1) % LT_NB;
+    const float(*w)[LT_PX] = t.w[k & 1];
+    if (do_uv || do_ts) {
+      // the one-cell ring around the interior, walked over whole padded rows so
+      // that a warp's shared-memory addresses are consecutive (no bank conflicts)
+      constexpr int RY = LT_Y + 2;
+      for (int e = tid; e < LT_PX * RY; e += nt) {
+        const int rr = 1 + e / LT_PX, c2 = e % LT_PX;
+        if (c2 == 0 || c2 == LT_PX - 1) continue;
+        if (do_uv) {
+          t.Lu[rr][c2] = lap_s(d, t, w, t.u[q], rr, c2, false);
+          t.Lv[rr][c2] = lap_s(d, t, w, t.v[q], rr, c2, false);
+        }
+        if (do_ts) {
+          t.LT[rr][c2] = hdiff_s(d, t, w, t.T[q], rr, c2, true);
+          t.LS[rr][c2] = hdiff_s(d, t, w, t.S[q], rr, c2, true);
+        }
+      }
+      __syncthreads();
+    }
+    if (!in) continue;
+    const long long id = (long long)k * d.plane + base;
+    const bool wet = wetb(bits, k);
+    const float uc = t.u[q][r][cc], vc = t.v[q][r][cc], Tc = t.T[q][r][cc], Sc = t.S[q][r][cc];
+    float u, v, T, S;
+    if (!wet) {
+      u = uc;
+      v = vc;
+      T = Tc;
+      S = Sc;
+    } else {
+      T = Tc + hdiff_s(d, t, w, t.T[q], r, cc, false) * dth;
+      S = Sc + hdiff_s(d, t, w, t.S[q], r, cc, false) * dth;
+      if (do_ts) {
+        T = T - d.kappa_bi * hdiff_s(d, t, w, t.LT, r, cc, true) * dth;
+        S = S - d.kappa_bi * hdiff_s(d, t, w, t.LS, r, cc, true) * dth;
+      }
+      u = ld(usub, id);
+      v = ld(vsub, id);
+      if (do_uv) {
+        u = u - d.nu_bi * lap_s(d, t, w, t.Lu, r, cc, true) * dth;
+        v = v - d.nu_bi * lap_s(d, t, w, t.Lv, r, cc, true) * dth;
+      }
+      if (!IMPL) {
+        const bool below = k + 1 < d.nz;  // level k + 1 sits in buffer qn
+        const float up = below ? t.u[qn][r][cc] : uc, vp = below ? t.v[qn][r][cc] : vc;
+        const float Tp = below ? t.T[qn][r][cc] : Tc, Sp = below ? t.S[qn][r][cc] : Sc;
+        u = u + d.nu_v * d2z_c(d, k, kbt, um, uc, up) * dth;
+        v = v + d.nu_v * d2z_c(d, k, kbt, vm, vc, vp) * dth;
+        T = T + vdiff_c(d, k, bits, kv, Tm, Tc, Tp) * dth;
+        S = S + vdiff_c(d, k, bits, kv, Sm, Sc, Sp) * dth;
+      }
+    }
+    To[id] = T;
+    So[id] = S;
+    if (IMPL) {  // the column solve and the rotation follow
+      uo[id] = u;
+      vo[id] = v;
+    } else {
+      uo[id] = rc * u + rs * v;
+      vo[id] = -rs * u + rc * v;
+    }
+    um = uc;
+    vm = vc;
+    Tm = Tc;
+    Sm = Sc;
   }
-  const float c = __ldg(d.rot_c + base), sn = __ldg(d.rot_s + base);
-  uo[id] = c * u + sn * v;
-  vo[id] = -sn * u + c * v;
 }
 
 // The biharmonic and implicit-diffusion options are template arguments: a
 // launch carries only the operators its option set uses.
 static_assert(sizeof(LtTile) <= 48 * 1024, "k_lin_t tile within the default dynamic shared memory");
-void launch_lin_t(dim3 g, dim3 b, cudaStream_t s, const Dev& d, const float* usub, const float* vsub,
-                  const float* u0, const float* v0, const float* T0, const float* S0, float* uo, float* vo,
-                  float* To, float* So, float dth, int implicit_v) {
+void launch_lin_t(cudaStream_t s, const Dev& d, const float* usub, const float* vsub, const float* u0,
+                  const float* v0, const float* T0, const float* S0, float* uo, float* vo, float* To, float* So,
+                  float dth, int implicit_v) {
+  const dim3 g((d.nx + LT_X - 1) / LT_X, (d.ny + LT_Y - 1) / LT_Y, (d.nz + LT_KC - 1) / LT_KC), b(LT_X, LT_Y);
   const int key = (d.nu_bi > 0.f ? 4 : 0) | (d.kappa_bi > 0.f ? 2 : 0) | (implicit_v ? 1 : 0);
   const size_t sm = sizeof(LtTile);
 #define ZM_LIN(K, UV, TS, IM)                                                                       \

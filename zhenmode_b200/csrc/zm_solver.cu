@@ -193,8 +193,8 @@ struct zm_solver {
       vsub = c;
     }
     pb(ZM_K_LIN_FINISH, s);
-    launch_lin_t(dim3((nx + LT_TX - 1) / LT_TX, (ny + LT_TY - 1) / LT_TY, nz), dim3(LT_TX, LT_TY), s,
-        d, usub, vsub, src.u, src.v, src.T, src.S, dst.u, dst.v, dst.T, dst.S, dth, vdiff || closure_on);
+    launch_lin_t(s, d, usub, vsub, src.u, src.v, src.T, src.S, dst.u, dst.v, dst.T, dst.S, dth,
+                 vdiff || closure_on);
     pe(s);
     if (vdiff || closure_on) {
       pb(ZM_K_IMPLICIT, s);
