@@ -123,14 +123,19 @@ __device__ __forceinline__ float colv(const float* __restrict__ a, long long bas
 // j = 0, aS = 0.  The coefficients, scaled by nu_h dt_sub, are formed once
 // per pass.  Longitude wraps.  The lane's two columns are held as packed
 // pairs, so the update runs on the paired FP32 instructions (__ffma2_rn,
-// __fadd2_rn; the same roundings as the scalar form).
+// __fadd2_rn; the same roundings as the scalar form).  The wet flags of the
+// lane's cells are bits of a register; the neighbouring lanes' flags arrive by
+// shuffle and the neighbouring warps' through shared memory.  The state is
+// loaded after the coefficients are formed, so the two sets are not live
+// together during the set-up.
 __global__ void __launch_bounds__(32 * (NB_W / NB_R), 2)
 k_nu_tb(Dev d, const float* __restrict__ u, const float* __restrict__ v, float* __restrict__ uo,
         float* __restrict__ vo, float c, int nsub, int halo) {
   constexpr int NW = NB_W / NB_R;                 // warps per block
+  static_assert(2 * NB_R <= 32, "a lane's wet flags fit one register");
   const int TI = NB_W - 2 * halo;
   __shared__ float4 edge[2][NW][2][32];           // [parity][warp][0 bottom row, 1 top row][lane]
-  __shared__ unsigned char sw[NB_W][NB_W + 4];    // wet flags (coefficient setup)
+  __shared__ unsigned swm[NW][32];                // each lane's wet-flag bits (coefficient setup)
   const int lane = threadIdx.x, wp = threadIdx.y;
   const int k = blockIdx.z;
   const int gx0 = blockIdx.x * TI - halo, gy0 = blockIdx.y * TI - halo;
@@ -142,22 +147,29 @@ k_nu_tb(Dev d, const float* __restrict__ u, const float* __restrict__ v, float* 
     gi[h] = g < 0 ? g + d.nx : g;
   }
   const long long kb = (long long)k * d.plane;
-  // the lane's two columns as pairs: au[q] = (u[2l], u[2l+1]) of row q, av likewise
-  float2 au[NB_R], av[NB_R];
+  // bit 2q + h of wm: cell (row r0 + q, column c0 + h) is wet at level k
+  unsigned wm = 0u;
 #pragma unroll
   for (int q = 0; q < NB_R; ++q) {
     int gj = gy0 + r0 + q;
     gj = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
-    const long long id0 = kb + (long long)gj * d.P + gi[0], id1 = kb + (long long)gj * d.P + gi[1];
-    au[q] = make_float2(ld(u, id0), ld(u, id1));
-    av[q] = make_float2(ld(v, id0), ld(v, id1));
 #pragma unroll
-    for (int h = 0; h < 2; ++h) sw[r0 + q][c0 + h] = (unsigned char)wetb(wb(d, gj, gi[h]), k);
+    for (int h = 0; h < 2; ++h) wm |= (wetb(wb(d, gj, gi[h]), k) ? 1u : 0u) << (2 * q + h);
   }
+  const unsigned full = 0xffffffffu;
+  swm[wp][lane] = wm;
+  const unsigned wm_e = __shfl_down_sync(full, wm, 1);  // lane l + 1 (lane 31: its own, unused)
+  const unsigned wm_w = __shfl_up_sync(full, wm, 1);    // lane l - 1 (lane 0: its own, unused)
   __syncthreads();
+  // flags of the rows just outside the strip; none beyond the tile's top and bottom rows
+  const unsigned wm_n = wp + 1 < NW ? swm[wp + 1][lane] : 0u;  // bits 0, 1: row r0 + NB_R
+  const unsigned wm_s = wp > 0 ? swm[wp - 1][lane] : 0u;       // bits 2 NB_R - 2, - 1: row r0 - 1
   const float cn = d.nu_h * c;
-  // face coefficients, paired like the state: (column 2l, column 2l+1)
-  float2 kE[NB_R], kW[NB_R], kN[NB_R], kS[NB_R];
+  // face coefficients, paired like the state: (column 2l, column 2l+1).  The
+  // west and south ones are held negated (nW = -aW, nS = -aS) and negated back
+  // in the update, an exact round trip: with ptxas 12.9 this form spills 20
+  // bytes per thread where holding aW, aS spills 40, and it ran 4 % faster.
+  float2 kE[NB_R], nW[NB_R], kN[NB_R], nS[NB_R];
 #pragma unroll
   for (int q = 0; q < NB_R; ++q) {
     const int r = r0 + q;
@@ -169,12 +181,13 @@ k_nu_tb(Dev d, const float* __restrict__ u, const float* __restrict__ v, float* 
     float ce[2], cw[2], cnn[2], cs[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      const int col = c0 + h;
-      const bool w0 = sw[r][col];
-      const bool we = col + 1 < NB_W && sw[r][col + 1];
-      const bool ww = col > 0 && sw[r][col - 1];
-      const bool wn = n_in && r + 1 < NB_W && sw[r + 1][col];
-      const bool ws = s_in && r > 0 && sw[r - 1][col];
+      const int b = 2 * q + h;
+      const bool w0 = (wm >> b) & 1u;
+      // neighbours outside the tile count as dry, as at the tile's own edge
+      const bool we = h == 0 ? ((wm >> (b + 1)) & 1u) : (lane < 31 && ((wm_e >> (2 * q)) & 1u));
+      const bool ww = h == 1 ? ((wm >> (b - 1)) & 1u) : (lane > 0 && ((wm_w >> (2 * q + 1)) & 1u));
+      const bool wn = n_in && (q + 1 < NB_R ? ((wm >> (b + 2)) & 1u) : ((wm_n >> h) & 1u));
+      const bool ws = s_in && (q > 0 ? ((wm >> (b - 2)) & 1u) : ((wm_s >> (2 * NB_R - 2 + h)) & 1u));
       const float ix2 = __ldg(d.inv_dx2 + idx2(d, gjc, gi[h]));
       const float cN = (w0 && wn) ? d.inv_dy2 : 0.f, cS = (w0 && ws) ? d.inv_dy2 : 0.f;
       ce[h] = (w0 && we) ? ix2 * cn : 0.f;
@@ -183,11 +196,20 @@ k_nu_tb(Dev d, const float* __restrict__ u, const float* __restrict__ v, float* 
       cs[h] = s_in ? (cS + t) * cn : 0.f;
     }
     kE[q] = make_float2(ce[0], ce[1]);
-    kW[q] = make_float2(cw[0], cw[1]);
+    nW[q] = make_float2(-cw[0], -cw[1]);
     kN[q] = make_float2(cnn[0], cnn[1]);
-    kS[q] = make_float2(cs[0], cs[1]);
+    nS[q] = make_float2(-cs[0], -cs[1]);
   }
-  const unsigned full = 0xffffffffu;
+  // the lane's two columns as pairs: au[q] = (u[2l], u[2l+1]) of row q, av likewise
+  float2 au[NB_R], av[NB_R];
+#pragma unroll
+  for (int q = 0; q < NB_R; ++q) {
+    int gj = gy0 + r0 + q;
+    gj = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
+    const long long id0 = kb + (long long)gj * d.P + gi[0], id1 = kb + (long long)gj * d.P + gi[1];
+    au[q] = make_float2(ld(u, id0), ld(u, id1));
+    av[q] = make_float2(ld(v, id0), ld(v, id1));
+  }
   const float2 m1 = make_float2(-1.f, -1.f);
   for (int s = 0; s < nsub; ++s) {
     const int p = s & 1;
@@ -213,12 +235,12 @@ k_nu_tb(Dev d, const float* __restrict__ u, const float* __restrict__ v, float* 
       const float2 ncu = __fmul2_rn(au[q], m1), ncv = __fmul2_rn(av[q], m1);
       float2 ou = __ffma2_rn(kE[q], __fadd2_rn(eu, ncu), au[q]);
       float2 ov = __ffma2_rn(kE[q], __fadd2_rn(ev, ncv), av[q]);
-      ou = __ffma2_rn(kW[q], __fadd2_rn(wu, ncu), ou);
-      ov = __ffma2_rn(kW[q], __fadd2_rn(wv, ncv), ov);
+      ou = __ffma2_rn(make_float2(-nW[q].x, -nW[q].y), __fadd2_rn(wu, ncu), ou);
+      ov = __ffma2_rn(make_float2(-nW[q].x, -nW[q].y), __fadd2_rn(wv, ncv), ov);
       ou = __ffma2_rn(kN[q], __fadd2_rn(nu, ncu), ou);
       ov = __ffma2_rn(kN[q], __fadd2_rn(nv, ncv), ov);
-      ou = __ffma2_rn(kS[q], __fadd2_rn(su, ncu), ou);
-      ov = __ffma2_rn(kS[q], __fadd2_rn(sv, ncv), ov);
+      ou = __ffma2_rn(make_float2(-nS[q].x, -nS[q].y), __fadd2_rn(su, ncu), ou);
+      ov = __ffma2_rn(make_float2(-nS[q].x, -nS[q].y), __fadd2_rn(sv, ncv), ov);
       su = au[q];
       sv = av[q];
       au[q] = ou;
