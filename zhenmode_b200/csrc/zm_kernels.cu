@@ -147,14 +147,29 @@ k_nu_tb(Dev d, const float* __restrict__ u, const float* __restrict__ v, float* 
     gi[h] = g < 0 ? g + d.nx : g;
   }
   const long long kb = (long long)k * d.plane;
-  // bit 2q + h of wm: cell (row r0 + q, column c0 + h) is wet at level k
+  // metric terms of the lane's cells, loaded first so that their latency
+  // overlaps the wet-flag loads
+  float ix2v[NB_R][2], tv[NB_R];
+#pragma unroll
+  for (int q = 0; q < NB_R; ++q) {
+    const int gj = gy0 + r0 + q;
+    const int gjc = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
+    tv[q] = __ldg(d.tanR + gjc);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) ix2v[q][h] = __ldg(d.inv_dx2 + idx2(d, gjc, gi[h]));
+  }
+  // bit 2q + h of wm: cell (row r0 + q, column c0 + h) is wet at level k, read
+  // from the 32-bit half of the column's 64-bit wet word that holds bit k
+  // (little-endian: levels 0-31 in the first half)
   unsigned wm = 0u;
 #pragma unroll
   for (int q = 0; q < NB_R; ++q) {
     int gj = gy0 + r0 + q;
     gj = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
 #pragma unroll
-    for (int h = 0; h < 2; ++h) wm |= (wetb(wb(d, gj, gi[h]), k) ? 1u : 0u) << (2 * q + h);
+    for (int h = 0; h < 2; ++h)
+      wm |= ((__ldg(reinterpret_cast<const unsigned*>(d.wbits) + 2 * idx2(d, gj, gi[h]) + (k >> 5)) >> (k & 31)) & 1u)
+            << (2 * q + h);
   }
   const unsigned full = 0xffffffffu;
   swm[wp][lane] = wm;
@@ -167,17 +182,17 @@ k_nu_tb(Dev d, const float* __restrict__ u, const float* __restrict__ v, float* 
   const float cn = d.nu_h * c;
   // face coefficients, paired like the state: (column 2l, column 2l+1).  The
   // west and south ones are held negated (nW = -aW, nS = -aS) and negated back
-  // in the update, an exact round trip: with ptxas 12.9 this form spills 20
-  // bytes per thread where holding aW, aS spills 40, and it ran 4 % faster.
+  // in the update, an exact round trip: ptxas 12.9 allocates this form's
+  // registers differently, and it ran 4 % faster than holding aW, aS (timed
+  // before the metric terms were loaded ahead of the wet flags).
   float2 kE[NB_R], nW[NB_R], kN[NB_R], nS[NB_R];
 #pragma unroll
   for (int q = 0; q < NB_R; ++q) {
     const int r = r0 + q;
     const int gj = gy0 + r;
-    const int gjc = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
     const bool n_in = gj < d.ny - 1;  // north neighbour inside the domain
     const bool s_in = gj > 0;
-    const float t = 0.5f * d.inv_dy * __ldg(d.tanR + gjc);
+    const float t = 0.5f * d.inv_dy * tv[q];
     float ce[2], cw[2], cnn[2], cs[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
@@ -188,7 +203,7 @@ k_nu_tb(Dev d, const float* __restrict__ u, const float* __restrict__ v, float* 
       const bool ww = h == 1 ? ((wm >> (b - 1)) & 1u) : (lane > 0 && ((wm_w >> (2 * q + 1)) & 1u));
       const bool wn = n_in && (q + 1 < NB_R ? ((wm >> (b + 2)) & 1u) : ((wm_n >> h) & 1u));
       const bool ws = s_in && (q > 0 ? ((wm >> (b - 2)) & 1u) : ((wm_s >> (2 * NB_R - 2 + h)) & 1u));
-      const float ix2 = __ldg(d.inv_dx2 + idx2(d, gjc, gi[h]));
+      const float ix2 = ix2v[q][h];
       const float cN = (w0 && wn) ? d.inv_dy2 : 0.f, cS = (w0 && ws) ? d.inv_dy2 : 0.f;
       ce[h] = (w0 && we) ? ix2 * cn : 0.f;
       cw[h] = (w0 && ww) ? ix2 * cn : 0.f;
