@@ -50,7 +50,8 @@ ALGO_FIELDS = {"nu_sub": None, "lin_finish": 10, "fz": 3, "madv": 5, "dealias": 
 PROFILE_STEPS = 5
 # DRAM bytes per launch measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum)
 # for a kernel class on a grid, as summarised under profiles/; null for others.
-NCU_TRAFFIC_BYTES = {((720, 360, 50), "nu_sub"): 106850560 + 60880384}   # k_nu_tb_720x360x50.md
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of one full-size k_nu_tb launch (6 subcycles)
+NCU_TRAFFIC_BYTES = {((720, 360, 50), "nu_sub"): 106823424 + 63360256}
 
 
 def algo_fields_per_launch(cls, launches_per_step, n_nu):
