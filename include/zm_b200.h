@@ -6,7 +6,7 @@
  * (src/zhenmode/model/solver/factory.py:30-68, 721-799), whose `step` is a
  * jax.jit closure over `_step_impl` (src/zhenmode/model/solver/timestepping/step.py:341-458).
  * The reference has no C or FFI layer; these entry points are what a jax.ffi
- * custom call or a ctypes/cffi binding of that factory binds (see INTEGRATION.md).
+ * custom call or a ctypes/cffi binding of that factory binds.
  *
  * Conventions
  *  - Every array crossing this ABI uses the reference layout: 2-D fields are
@@ -358,22 +358,26 @@ int zm_budgets(zm_solver* s, void* stream, const float* T, const float* S, doubl
  * preallocates most of it), a check made after a blow-up exhausted that pool,
  * or a coupler working within a fixed memory budget.
  *
- * metrics (host, 4 floats): max |u|, max(|u|, |v|), max |eta| (over finite
- * values) and 1 if every value is finite else 0; *code: 0 accepted,
+ * ice is the (nx, ny) ice field or NULL (the reference's scalar default).
+ * metrics (host, 4 floats): max |u|, max(|u|, |v|), max |eta|, like jnp.max:
+ * NaN when the field holds a NaN, +-inf counted as inf; then 1 if every value
+ * of u, v, T, S, eta and ice is finite, else 0.  *code: 0 accepted,
  * 1 non-finite, 3 velocity above velocity_limit, 4 |eta| above eta_limit
- * (>= with inclusive != 0).  Synchronizes `stream`.
+ * (>= with inclusive != 0).  The call waits for its result on the host, so a
+ * stream that is capturing is refused with ZM_ERR_INVALID.
  *
  * Its only scratch is a fixed ZM_NOALLOC_SCRATCH_BYTES array inside the
- * library, held by every GPU that loads it until exit.  Fields of more than
- * ZM_NOALLOC_MAX_POINTS points are rejected with ZM_ERR_INVALID.  The first
- * call on a device looks up the array's device address; make that first call
- * before any stream capture.  All calls on a device share the array: calls
- * whose work overlaps on the GPU race, so order them. */
+ * library, held by every GPU that loads it until exit; each call looks up the
+ * array's device address for the current device.  Fields of more than
+ * ZM_NOALLOC_MAX_POINTS points are rejected with ZM_ERR_INVALID.  All calls on
+ * a device share the array: calls whose work overlaps on the GPU race, so
+ * order them. */
 #define ZM_NOALLOC_SCRATCH_BYTES 33024
 #define ZM_NOALLOC_MAX_POINTS 134217728LL
 int zm_classify_state_noalloc(void* stream, int32_t nx, int32_t ny, int32_t nz, const float* u, const float* v,
-                              const float* T, const float* S, const float* eta, float velocity_limit,
-                              float eta_limit, int32_t inclusive, float* metrics, int32_t* code);
+                              const float* T, const float* S, const float* eta, const float* ice,
+                              float velocity_limit, float eta_limit, int32_t inclusive, float* metrics,
+                              int32_t* code);
 
 /* Message of the last failure on this handle ("" if none). */
 const char* zm_last_error(const zm_solver* s);

@@ -1,9 +1,10 @@
 """Generate golden vectors by running ZhenMode's own solver code.
 
-Run in a container that holds the ZhenMode source tree (default
-``/root/reference/src``; override with ``ZHENMODE_SRC``)::
+Run in a container that holds the ZhenMode source tree, giving the path of
+its ``src`` directory (the one that holds the ``zhenmode`` package) as the
+argument or in ``ZHENMODE_SRC``::
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py --src <zhenmode-checkout>/src
 
 JAX is not installed here, so the unmodified reference modules are imported
 with the NumPy-backed stand-in under ``tests/golden/_jaxshim`` on
@@ -23,7 +24,17 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF_SRC = os.environ.get("ZHENMODE_SRC", "/root/reference/src")
+
+
+def _ref_src():
+    if "--src" in sys.argv:
+        return sys.argv[sys.argv.index("--src") + 1]
+    if os.environ.get("ZHENMODE_SRC"):
+        return os.environ["ZHENMODE_SRC"]
+    raise SystemExit("make_golden.py: give the ZhenMode source tree with --src <path>/src or ZHENMODE_SRC")
+
+
+REF_SRC = _ref_src()
 sys.path[:0] = [os.path.join(HERE, "_jaxshim"), REF_SRC, ROOT]
 
 import zhenmode.model.config as ref_config  # noqa: E402
@@ -346,44 +357,9 @@ def make_projection_case(seed=13):
     print("projection saved")
 
 
-def make_restart_case():
-    """A checkpoint written by the reference's save_restart
-    (model/io/restart.py:153-179) for a plain-dict contract, with the inputs
-    that made it, so the restart module's file format is pinned both ways."""
-    from zhenmode.model.io.restart import make_restart_contract, save_restart
-    from collections import namedtuple
-    grid = workloads.build_grid(8, 6, 4, land_lat=70.0)
-    rng = np.random.default_rng(21)
-    shape = (8, 6, 4)
-    state = dict(u=rng.standard_normal(shape).astype(np.float32), v=rng.standard_normal(shape).astype(np.float32),
-                 T=(10 + rng.standard_normal(shape)).astype(np.float32),
-                 S=(35 + 0.1 * rng.standard_normal(shape)).astype(np.float32),
-                 eta=rng.standard_normal(shape[:2]).astype(np.float32), ice=np.zeros(shape[:2], np.float32))
-    params = namedtuple("Params", ["dt", "nu_h", "polar_cap_rows"])(1800.0, 2.5e4, 2)
-    forcing = {"tau_x": rng.standard_normal(shape[:2]), "heat": np.zeros(shape[:2])}
-    controls = {"calendar": "360_day", "blend_days": 5.0}
-    execution = {"backend": "cpu", "devices": 1}
-    contract = make_restart_contract(grid, params, dtype="float32", forcing=forcing, controls=controls,
-                                     code_paths={}, execution=execution)
-    cumulative = {"heat": np.array([1.5, -2.25]), "salt": np.array([3.0])}
-    history = {"days": np.array([0.0, 1.0, 2.0]), "sst_mean": np.array([15.1, 15.2, 15.3])}
-    path = os.path.join(HERE, "restart_reference.npz")
-    save_restart(path, state, contract, step=96, counters={"n_snaps": 3}, cumulative=cumulative,
-                 history=history, outputs={"out/global.npz": "ab" * 32})
-    inputs = dict(grid_nx=8, grid_ny=6, grid_nz=4, land_lat=70.0, seed=21)
-    np.savez_compressed(os.path.join(HERE, "restart_inputs.npz"),
-                        **{f"state_{k}": v for k, v in state.items()},
-                        **{f"forcing_{k}": v for k, v in forcing.items()},
-                        **{f"cumulative_{k}": v for k, v in cumulative.items()},
-                        **{f"history_{k}": v for k, v in history.items()},
-                        **{k: np.asarray(v) for k, v in inputs.items()})
-    print("restart saved")
-
-
 def main():
     make_ledger_case()
     make_sponge_case()
-    make_restart_case()
     make_operator_case()
     make_projection_case()
     make_seasonal_case()

@@ -113,7 +113,8 @@ EXPORTS = {
                                   ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]),
     "zm_classify_state_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
-                                                 ctypes.c_void_p, ctypes.c_float, ctypes.c_float, ctypes.c_int32,
+                                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float, ctypes.c_float,
+                                                 ctypes.c_int32,
                                                  ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_int32)]),
     "zm_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "zm_destroy": (None, [ctypes.c_void_p]),

@@ -17,7 +17,6 @@
 
 #include <cmath>
 #include <cstdio>
-#include <mutex>
 
 #include "../../include/zm_b200.h"
 
@@ -38,23 +37,22 @@ static_assert(sizeof(Scratch) <= ZM_NOALLOC_SCRATCH_BYTES, "scratch larger than 
 
 static __device__ __align__(256) unsigned char zm_noalloc_scratch[ZM_NOALLOC_SCRATCH_BYTES];
 
-// Host-side stand-in handling: `zm_noalloc_scratch` named in host code is not
-// a device address, so the address is looked up once per device.
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mutex;
-Scratch* g_scratch[kMaxDevices] = {nullptr};
+// Maximum that keeps a NaN once one is seen, like jnp.max: the reference's
+// metrics are NaN when a field holds a NaN, and +-inf enters as inf.
+__device__ __forceinline__ float nan_max(float m, float a) { return (a != a || a > m) ? a : m; }
 
 __device__ __forceinline__ float warp_max(float v) {
-  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  for (int o = 16; o > 0; o >>= 1) v = nan_max(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
 }
 
 // One pass over the caller's state: each block reduces its chunk into its
 // slot; the last block to finish folds all slots into `result` and rezeroes
-// the counter.  No block waits on another.
+// the counter.  No block waits on another.  `ice` (2-D) may be null.
 __global__ void __launch_bounds__(kThreads) k_classify_noalloc(const float* __restrict__ u, const float* __restrict__ v,
                                                                 const float* __restrict__ T, const float* __restrict__ S,
-                                                                const float* __restrict__ eta, long long n3,
+                                                                const float* __restrict__ eta,
+                                                                const float* __restrict__ ice, long long n3,
                                                                 long long n2, int nblocks, Scratch* sc) {
   __shared__ float red[kSlot][kThreads / 32];
   __shared__ bool last;
@@ -67,13 +65,13 @@ __global__ void __launch_bounds__(kThreads) k_classify_noalloc(const float* __re
   for (long long t = lo3 + threadIdx.x; t < hi3; t += blockDim.x) {
     const float a = u[t], b = v[t], c = T[t], e = S[t];
     if (!(isfinite(a) && isfinite(b) && isfinite(c) && isfinite(e))) bad = 1.f;
-    mu = fmaxf(mu, fabsf(a));
-    mv = fmaxf(mv, fabsf(b));
+    mu = nan_max(mu, fabsf(a));
+    mv = nan_max(mv, fabsf(b));
   }
   for (long long t = lo2 + threadIdx.x; t < hi2; t += blockDim.x) {
     const float h = eta[t];
-    if (!isfinite(h)) bad = 1.f;
-    me = fmaxf(me, fabsf(h));
+    if (!isfinite(h) || (ice && !isfinite(ice[t]))) bad = 1.f;
+    me = nan_max(me, fabsf(h));
   }
   mu = warp_max(mu);
   mv = warp_max(mv);
@@ -89,7 +87,7 @@ __global__ void __launch_bounds__(kThreads) k_classify_noalloc(const float* __re
   __syncthreads();
   if (threadIdx.x < kSlot) {
     float m = 0.f;
-    for (int q = 0; q < kThreads / 32; ++q) m = fmaxf(m, red[threadIdx.x][q]);
+    for (int q = 0; q < kThreads / 32; ++q) m = nan_max(m, red[threadIdx.x][q]);
     sc->partial[blockIdx.x * kSlot + threadIdx.x] = m;
   }
   __threadfence();
@@ -100,7 +98,7 @@ __global__ void __launch_bounds__(kThreads) k_classify_noalloc(const float* __re
   __threadfence();
   if (threadIdx.x < kSlot) {
     float m = 0.f;
-    for (int b = 0; b < nblocks; ++b) m = fmaxf(m, ((volatile float*)sc->partial)[b * kSlot + threadIdx.x]);
+    for (int b = 0; b < nblocks; ++b) m = nan_max(m, ((volatile float*)sc->partial)[b * kSlot + threadIdx.x]);
     sc->result[threadIdx.x] = m;
   }
   if (threadIdx.x == 0) sc->counter = 0u;
@@ -110,8 +108,8 @@ __global__ void __launch_bounds__(kThreads) k_classify_noalloc(const float* __re
 
 extern "C" int zm_classify_state_noalloc(void* stream, int32_t nx, int32_t ny, int32_t nz, const float* u,
                                          const float* v, const float* T, const float* S, const float* eta,
-                                         float velocity_limit, float eta_limit, int32_t inclusive, float* metrics,
-                                         int32_t* code) {
+                                         const float* ice, float velocity_limit, float eta_limit, int32_t inclusive,
+                                         float* metrics, int32_t* code) {
   if (nx < 1 || ny < 1 || nz < 1 || !u || !v || !T || !S || !eta || !metrics || !code) {
     std::fprintf(stderr, "zm_classify_state_noalloc: invalid argument\n");
     return ZM_ERR_INVALID;
@@ -124,35 +122,39 @@ extern "C" int zm_classify_state_noalloc(void* stream, int32_t nx, int32_t ny, i
                  n3, (long long)ZM_NOALLOC_MAX_POINTS, (int)ZM_NOALLOC_SCRATCH_BYTES);
     return ZM_ERR_INVALID;
   }
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return ZM_ERR_CUDA;
-  Scratch* sc;
-  {
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch[dev]) {
-      void* ptr = nullptr;
-      const cudaError_t e = cudaGetSymbolAddress(&ptr, zm_noalloc_scratch);
-      if (e != cudaSuccess) {
-        std::fprintf(stderr, "zm_classify_state_noalloc: cudaGetSymbolAddress: %s\n", cudaGetErrorString(e));
-        return ZM_ERR_CUDA;
-      }
-      g_scratch[dev] = static_cast<Scratch*>(ptr);
-    }
-    sc = g_scratch[dev];
-  }
   cudaStream_t st = (cudaStream_t)stream;
+  // the call waits for its result on the host, which a capturing stream
+  // cannot do: refuse before touching the stream
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) return ZM_ERR_CUDA;
+  if (cap != cudaStreamCaptureStatusNone) {
+    std::fprintf(stderr, "zm_classify_state_noalloc: the stream is capturing; call it outside a capture\n");
+    return ZM_ERR_INVALID;
+  }
+  // `zm_noalloc_scratch` named in host code is a host-side stand-in, not a
+  // device address: look the address up for the current device on every call
+  // (cheap, and never stale after the context is recreated)
+  void* ptr = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&ptr, zm_noalloc_scratch);
+  if (e != cudaSuccess) {
+    std::fprintf(stderr, "zm_classify_state_noalloc: cudaGetSymbolAddress: %s\n", cudaGetErrorString(e));
+    return ZM_ERR_CUDA;
+  }
+  Scratch* sc = static_cast<Scratch*>(ptr);
   const int nblocks = (int)((n3 + kChunk - 1) / kChunk);
   // the completion counter must start at zero (the previous call left it zero
   // unless it was interrupted)
   if (cudaMemsetAsync(&sc->counter, 0, sizeof(unsigned int), st) != cudaSuccess) return ZM_ERR_CUDA;
-  k_classify_noalloc<<<nblocks, kThreads, 0, st>>>(u, v, T, S, eta, n3, n2, nblocks, sc);
+  k_classify_noalloc<<<nblocks, kThreads, 0, st>>>(u, v, T, S, eta, ice, n3, n2, nblocks, sc);
   if (cudaGetLastError() != cudaSuccess) return ZM_ERR_CUDA;
   float res[kSlot];
   if (cudaMemcpyAsync(res, sc->result, sizeof(res), cudaMemcpyDeviceToHost, st) != cudaSuccess) return ZM_ERR_CUDA;
   if (cudaStreamSynchronize(st) != cudaSuccess) return ZM_ERR_CUDA;
-  const float max_u = res[0], max_vel = std::fmax(res[0], res[1]), max_eta = res[2];
+  const float mu = res[0], mv = res[1], max_eta = res[2];
+  // jnp.maximum: NaN if either is NaN
+  const float max_vel = (mu != mu || mv != mv) ? NAN : std::fmax(mu, mv);
   const bool finite = res[3] == 0.f;
-  metrics[0] = max_u;
+  metrics[0] = mu;
   metrics[1] = max_vel;
   metrics[2] = max_eta;
   metrics[3] = finite ? 1.f : 0.f;

@@ -2,8 +2,10 @@
 reference (src/zhenmode/model/diagnostics/budgets.py).
 
 ``make_budget_step(params)`` (budgets.py:264-288) takes the ``params`` that
-``make_solver_global(..., return_params=True)`` returns (or the ``step``
-callable itself) and gives ``advance(state, forcing=None, atmosphere=None,
+``make_solver_global(..., return_params=True)`` returns (a ``B200Params``
+carrying its step; the reference runtime passes it at runtime/run.py:113 when
+``RunServices.make_budget_step`` is this function) or the ``step`` callable
+itself and gives ``advance(state, forcing=None, atmosphere=None,
 surface_pressure_pa=None) -> (new state, ledger)``.  The step is the ordinary
 B200 step run once without the CUDA graph, with compensated float64
 reductions at the reference's hook points (``zm_ledger_step``); the ledger
@@ -92,7 +94,10 @@ def make_budget_step(params):
 
     from .solver import JaxStateG, UnsupportedOption, _torch_state_ptrs
 
-    step = params["step"] if isinstance(params, dict) else params
+    if isinstance(params, dict):
+        step = params["step"]
+    else:
+        step = getattr(params, "step", params)  # the params of make_solver_global, or the step itself
     solver = step.solver
     changed = [False]
 

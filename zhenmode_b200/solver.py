@@ -34,6 +34,30 @@ class UnsupportedOption(ValueError):
     """A reference option the B200 path does not implement (C-ABI status 2)."""
 
 
+# Effective settings of a built step under the reference's FDPhysParams field
+# names (src/zhenmode/model/solver/state.py), for the callers of
+# ``make_solver_global(..., return_params=True)``: the run reporting
+# (runtime/reporting.py:22-25), the output provenance (io/output.py:89-96,
+# projection_config of dynamics/projection.py:53-62), the restart contract's
+# fingerprint (io/restart.py:34-51, 56-75) and the budget audit
+# (zhenmode_b200.ledger.make_budget_step).  Every field is a number, string,
+# flag, None or host array, so the reference's fingerprint() takes it as it
+# is; the step itself is attached as the attribute ``step``, outside the
+# fields.
+_PARAM_FIELDS = (
+    "nx", "ny", "nz", "dt", "dt_bt", "mode_split", "n_subcyc", "nu_nsub", "adv_nsub", "conv_nsub", "use_scan",
+    "H_sw", "nu_h", "nu_v", "kappa_h", "kappa_v", "kappa_conv", "nu_bi", "kappa_bi", "T_ref", "S_ref",
+    "r_bot", "cd", "bottom_friction", "lambda_bulk", "restore_coef_S", "polar_cap_rows", "polar_cap_taper",
+    "eta_relax_rate", "freeze_adv_vel", "conservative_kv", "localize_conv", "monotone_adv", "fct_adv",
+    "project_adv_vel", "projection_niter", "projection_niter_source", "projection_rtol",
+    "projection_preconditioner", "projection_max_refinements", "column_geometry", "process_time_scheme",
+    "thermodynamics", "vertical_diffusion", "dtype", "wet_mask", "wet_mask_z")
+
+
+class B200Params(collections.namedtuple("B200Params", _PARAM_FIELDS)):
+    """Effective parameters of one B200 step (see _PARAM_FIELDS)."""
+
+
 def _finite(name, value, *, positive=False, nonnegative=False):
     """config.py finite_number: a finite real scalar with an optional sign."""
     if isinstance(value, bool) or not isinstance(value, numbers.Real) or not math.isfinite(float(value)):
@@ -343,6 +367,7 @@ def make_solver_global(grid, physics, dt, forcing=None,
         raise ValueError("reference column geometry requires conservative_kv=True and localize_conv=True")
     if polar_cap_rows > 0 and 2 * (polar_cap_rows + polar_cap_taper) > grid.ny:
         raise ValueError('polar cap bands must not overlap; reduce rows/taper or disable the cap')
+    projection_niter_source = 'explicit'
     if projection_niter is None:
         # factory.py:368-376: the legacy environment cap, resolved once here
         legacy_cap = os.environ.get('OCEAN_PAV_NITER')
@@ -350,6 +375,7 @@ def make_solver_global(grid, physics, dt, forcing=None,
             projection_niter = 150 if legacy_cap is None else int(legacy_cap)
         except ValueError as error:
             raise ValueError('projection_niter environment value must be an integer') from error
+        projection_niter_source = 'default' if legacy_cap is None else 'environment:OCEAN_PAV_NITER'
     if (isinstance(projection_niter, (bool, np.bool_)) or not isinstance(projection_niter, (int, np.integer))
             or projection_niter <= 0):
         raise ValueError('projection_niter must be a positive integer')
@@ -657,9 +683,26 @@ def make_solver_global(grid, physics, dt, forcing=None,
     step.closure_params = None
     result = [step, init_state, diagnostics]
     if return_params:
-        params = dict(n_subcyc=solver.n_subcyc, nu_nsub=solver.n_nu, adv_nsub=solver.adv_nsub,
-                      conv_nsub=solver.conv_nsub, dt_bt=float(dt) / solver.n_subcyc, H_sw=float(np.sum(grid.dz)),
-                      rho0=RHO_0, dt=float(dt), step=step)
+        params = B200Params(
+            nx=nx, ny=ny, nz=nz, dt=float(dt), dt_bt=float(dt) / solver.n_subcyc, mode_split=True,
+            n_subcyc=solver.n_subcyc, nu_nsub=solver.n_nu, adv_nsub=solver.adv_nsub, conv_nsub=solver.conv_nsub,
+            use_scan=bool(use_scan), H_sw=float(np.sum(grid.dz)), nu_h=float(physics.nu_h),
+            nu_v=float(physics.nu_v), kappa_h=float(physics.kappa_h), kappa_v=float(physics.kappa_v),
+            kappa_conv=float(physics.kappa_conv), nu_bi=float(physics.nu_bi), kappa_bi=float(physics.kappa_bi),
+            T_ref=float(physics.T_ref), S_ref=float(physics.S_ref), r_bot=float(physics.r_bot),
+            cd=float(physics.cd), bottom_friction=str(physics.bottom_friction), lambda_bulk=float(lambda_bulk),
+            restore_coef_S=float(restore_coef_S), polar_cap_rows=int(polar_cap_rows),
+            polar_cap_taper=int(polar_cap_taper), eta_relax_rate=float(eta_relax_rate),
+            freeze_adv_vel=bool(freeze_adv_vel), conservative_kv=bool(conservative_kv),
+            localize_conv=bool(localize_conv), monotone_adv=bool(monotone_adv), fct_adv=bool(fct_adv),
+            project_adv_vel=bool(project_adv_vel), projection_niter=int(projection_niter),
+            projection_niter_source=projection_niter_source, projection_rtol=projection_rtol,
+            projection_preconditioner=projection_preconditioner,
+            projection_max_refinements=int(projection_max_refinements), column_geometry=column_geometry,
+            process_time_scheme=process_time_scheme, thermodynamics=str(physics.thermodynamics),
+            vertical_diffusion=vertical_diffusion, dtype='float32',
+            wet_mask=np.asarray(grid.wet_mask, dtype=np.float32), wet_mask_z=wet3.astype(np.float32))
+        params.step = step
 
         def terms_fn(state):
             raise NotImplementedError("tracer term decomposition is not implemented on the B200 path")
