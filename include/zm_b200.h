@@ -341,6 +341,17 @@ int zm_ensemble_create(zm_solver* const* members, int32_t n, zm_ensemble** out);
 int zm_ensemble_advance(zm_ensemble* e, void* stream, int32_t nsteps, int32_t* kernels_per_step);
 void zm_ensemble_destroy(zm_ensemble* e);
 
+/* Temperature-term decomposition of a state, the terms_fn of
+ * make_solver_global (factory.py:762-764, dynamics/tendencies.py:74-92): terms
+ * is a (6, nx, ny, nz) float32 device array receiving the land-masked
+ * [advection, horizontal diffusion, vertical diffusion, convection, GM, Redi]
+ * tendencies of T at the state (one advection evaluation with the step's face
+ * limiter, kappa_h / kappa_v with their coastal parts, kappa_conv with the
+ * step's convective gates; GM and Redi are zero on this path).  Stream
+ * ordered, no host sync; uses the handle's work buffers, so it must not
+ * overlap a step of the same handle. */
+int zm_tracer_terms(zm_solver* s, void* stream, const zm_state* in, float* terms);
+
 /* Global heat/salt/volume snapshot of a state (compute_budget_diagnostics,
  * diagnostics/snapshot.py:67-128, legacy node thickness, linear
  * thermodynamics): T and S are (nx, ny, nz) float32 device arrays.  Writes

@@ -516,6 +516,23 @@ def tracer_tendency(u, v, T, S, p, rec=None):
     return dT * p.wet_mask_z, dS * p.wet_mask_z
 
 
+def tracer_terms(st, p):
+    """dynamics/tendencies.py:74-92 ``_tracer_terms`` (what ``terms_fn`` of
+    factory.py:762-764 returns): the (6, nx, ny, nz) stack [adv, diff_h,
+    diff_v, conv, gm, redi] of land-masked temperature terms at the state,
+    one advection evaluation (no substeps) and one convective evaluation
+    with kappa_conv; GM and Redi are zero (kappa_gm = kappa_redi = 0)."""
+    T, S, u, v = st["T"], st["S"], st["u"], st["v"]
+    Fz = vertical_transport_iface(u, v, p)
+    adv = tracer_advection(T, u, v, Fz, p)
+    dh = horizontal_tracer_diffusion(T, p)
+    dv = vertical_tracer_diffusion(T, p)
+    column, unstable = convective_gates(T, S, p)
+    conv = convective_tendency(T, column, p.kappa_conv, p, unstable if p.localize_conv else None)
+    zero = np.zeros_like(T)
+    return np.stack([t * p.wet_mask_z for t in (adv, dh, dv, conv, zero, zero)], axis=0)
+
+
 def tracer_residual(u, v, T, S, p, rec=None):
     """dynamics/tendencies.py:227-245: tendency minus the L-step linear terms."""
     dT, dS = tracer_tendency(u, v, T, S, p, rec)
@@ -561,42 +578,54 @@ def momentum_residual(u, v, T, S, eta, p):
 def implicit_vertical_solve(rhs, kappa, dt, p):
     """Extension (not a reference option): backward-Euler ``(I - dt K D2) x =
     rhs`` per column with the node-form operator of ``d2_dz2`` on the wet
-    levels 0..kbot (rows below kbot pass ``rhs`` through)."""
+    levels 0..kbot (rows below kbot pass ``rhs`` through).  Each column's
+    tridiagonal matrix is assembled in full and solved directly
+    (numpy.linalg.solve, LU in float64), columns in batches."""
     z = p.z
     nz = p.nz
     kbot = bottom_index(p)
     kap = np.broadcast_to(np.asarray(kappa, dtype=np.float64), rhs.shape[:2] + (1,))[..., 0]
     out = np.array(rhs, dtype=np.float64, copy=True)
     hm = np.abs(np.diff(z))            # hm[k-1] = |z[k-1]-z[k]|
-    for i in range(rhs.shape[0]):
-        for j in range(rhs.shape[1]):
-            kb = int(kbot[i, j])
-            if kb == 0:
-                continue
-            n = kb + 1
-            a = np.zeros(n)
-            b = np.ones(n)
-            c = np.zeros(n)
-            s = dt * kap[i, j]
-            h0 = hm[0]
-            b[0] += s * 2.0 / h0 ** 2
-            c[0] -= s * 2.0 / h0 ** 2
-            for k in range(1, n):
-                if k == nz - 1:
-                    hb = hm[-1]
-                    a[k] -= s * 2.0 / hb ** 2
-                    b[k] += s * 2.0 / hb ** 2
-                    continue
-                up, dn = hm[k - 1], hm[k]
-                den = up * dn * (up + dn) / 2.0
-                a[k] -= s * dn / den
-                b[k] += s * (up + dn) / den
-                if k < kb:
-                    c[k] -= s * up / den
-                else:   # ghost fill: node kb+1 carries node kb's value
-                    b[k] -= s * up / den
-            mat = np.diag(b) + np.diag(a[1:], -1) + np.diag(c[:-1], 1)
-            out[i, j, :n] = np.linalg.solve(mat, rhs[i, j, :n])
+    kb = kbot.reshape(-1).astype(np.int64)
+    s = (dt * kap).reshape(-1)
+    flat = out.reshape(-1, nz)
+    cols = np.nonzero(kb > 0)[0]
+    kk = np.arange(nz)
+    for lo in range(0, cols.size, 8192):
+        c_idx = cols[lo:lo + 8192]
+        m = c_idx.size
+        kbc, sc = kb[c_idx][:, None], s[c_idx][:, None]
+        live = kk[None, :] <= kbc                     # rows 0..kb of the system
+        a = np.zeros((m, nz))
+        b = np.ones((m, nz))
+        c = np.zeros((m, nz))
+        h0 = hm[0]
+        b[:, 0] += sc[:, 0] * 2.0 / h0 ** 2
+        c[:, 0] -= sc[:, 0] * 2.0 / h0 ** 2
+        if nz > 1:
+            hb = hm[-1]
+            a[:, nz - 1] -= sc[:, 0] * 2.0 / hb ** 2
+            b[:, nz - 1] += sc[:, 0] * 2.0 / hb ** 2
+        for k in range(1, nz - 1):
+            up, dn = hm[k - 1], hm[k]
+            den = up * dn * (up + dn) / 2.0
+            a[:, k] -= sc[:, 0] * dn / den
+            b[:, k] += sc[:, 0] * (up + dn) / den
+            interior = k < kbc[:, 0]
+            c[:, k] = np.where(interior, c[:, k] - sc[:, 0] * up / den, c[:, k])
+            b[:, k] = np.where(interior, b[:, k], b[:, k] - sc[:, 0] * up / den)
+        # rows beyond kb pass the right-hand side through (identity rows)
+        a = np.where(live, a, 0.0)
+        c = np.where(live, c, 0.0)
+        b = np.where(live, b, 1.0)
+        a[:, 0] = 0.0
+        c = np.where(kk[None, :] < kbc, c, 0.0)       # no coupling from row kb to kb + 1
+        mat = np.zeros((m, nz, nz))
+        mat[:, kk, kk] = b
+        mat[:, kk[1:], kk[:-1]] = a[:, 1:]
+        mat[:, kk[:-1], kk[1:]] = c[:, :-1]
+        flat[c_idx] = np.linalg.solve(mat, flat[c_idx][..., None])[..., 0]
     return out
 
 

@@ -357,7 +357,53 @@ def make_projection_case(seed=13):
     print("projection saved")
 
 
+def make_terms_case(seed=17):
+    """The reference's tracer-term decomposition (``terms_fn`` of
+    factory.py:762-764, dynamics/tendencies.py:74-92) on a moving float32
+    state of the 48x24x10 option-set grid with cold surface patches, so that
+    convection acts."""
+    grid = workloads.build_grid(48, 24, 10, land_lat=75.0)
+    T, S = workloads.initial_fields(grid, perturb_sigma=0.2)
+    kw = dict(workloads.PLAIN_OPTIONS)
+    kw.update(forcing=workloads.wind_forcing(grid), dt_bt=75.0, dtype="float64", return_params=True,
+              coastal_kappa_h_mask=np.asarray(grid.wet_mask), coastal_kappa_h=50.0,
+              coastal_kappa_v_mask=np.asarray(grid.wet_mask), coastal_kappa_v=2e-5)
+    out = make_solver_global(grid, _physics(workloads.PLAIN_PHYSICS), 1800.0, **kw)
+    terms_fn = out[4]
+    u, v, T0, S0, eta = _moving_state(grid, T, S, seed, amp_u=0.1, amp_eta=0.3)
+    rng = np.random.default_rng(seed + 1)
+    cold = (_smooth_noise(rng, (48, 24)) > 1.0) * np.asarray(grid.wet_mask)
+    T0 = T0.copy()
+    T0[:, :, :2] -= 4.0 * cold[:, :, None]
+    st = JaxStateG(*[_f32(a) for a in (u, v, T0, S0, eta)], np.zeros((48, 24)))
+    terms = terms_fn(st)
+    data = dict(_grid_arrays(grid))
+    data.update(in_u=_np(st.u), in_v=_np(st.v), in_T=_np(st.T), in_S=_np(st.S), in_eta=_np(st.eta),
+                coastal_kappa_h=np.float64(50.0), coastal_kappa_v=np.float64(2e-5),
+                terms=_np(terms), options=np.array(repr(workloads.PLAIN_OPTIONS)))
+    np.savez_compressed(os.path.join(HERE, "terms_48x24x10.npz"), **data)
+    print("terms saved", [float(np.abs(t).max()) for t in _np(terms)])
+
+
+def make_mld_case(seed=19):
+    """The reference's density-threshold mixed-layer depth
+    (diagnostics/mixed_layer.py:39-74) of perturbed thermocline columns with
+    the levels below the seafloor missing (NaN)."""
+    from zhenmode.model.diagnostics.mixed_layer import mixed_layer_depth
+    grid = workloads.build_grid(24, 16, 20, land_lat=70.0)
+    T, S = workloads.initial_fields(grid, perturb_sigma=0.2)
+    rng = np.random.default_rng(seed)
+    T = T + 0.3 * rng.standard_normal(T.shape)
+    wet3 = np.asarray(grid.wet_mask_3d)
+    mld = mixed_layer_depth(np.where(wet3 > 0.5, T, np.nan), np.where(wet3 > 0.5, S, np.nan), np.asarray(grid.z),
+                            ocean=np.asarray(grid.wet_mask) > 0.5)
+    np.savez_compressed(os.path.join(HERE, "mld_24x16x20.npz"), T=T, S=S, z=np.asarray(grid.z), wet3=wet3, mld=mld)
+    print("mld saved", np.nanmin(mld), np.nanmax(mld))
+
+
 def main():
+    make_terms_case()
+    make_mld_case()
     make_ledger_case()
     make_sponge_case()
     make_operator_case()

@@ -1,0 +1,56 @@
+"""Parity of the CUDA step with the float64 oracle at the full 720x360x50
+workload (the 0.5-degree plain FP32 option set), through the C ABI.
+
+One step from the initial state and one from a state two steps in (moving
+velocities, a displaced free surface): the relative L2 error of eta, u, v, T,
+S and of the density anomaly rho' (physics/eos.py:13-18) must each stay below
+1e-5, the bound for one production step.  The step being matched is
+_step_impl (src/zhenmode/model/solver/timestepping/step.py:341-458); the
+oracle restates it in float64 on the host cores (one to a few minutes per
+step).
+"""
+import numpy as np
+import pytest
+
+from oracle import step as ostep
+from tests import gpu_util as gu
+from zhenmode_b200 import workloads
+
+pytestmark = pytest.mark.gpu
+
+STEP_TOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def case():
+    from oracle.params import init_state
+    grid, physics, dt, kw, T, S = workloads.make_case("plain", 720, 360, 50, dtype="float32")
+    gpu, p = gu.build_pair(grid, physics, dt, kw)
+    return gpu, p, gu.f32(init_state(p, T, S))
+
+
+def _errors(got, want, p):
+    errs = gu.errors(got, want)
+    errs["rho_anomaly"] = gu.rel_l2(ostep.density_anomaly(got["T"], got["S"], p),
+                                    ostep.density_anomaly(want["T"], want["S"], p))
+    return errs
+
+
+def test_one_step_from_the_initial_state(case):
+    gpu, p, st0 = case
+    got = gu.run_steps(gpu, st0, 1)
+    want = ostep.step(dict(st0), p)
+    errs = _errors(got, want, p)
+    print("720x360x50 one step from rest, relative L2:", errs)
+    assert max(errs.values()) < STEP_TOL, errs
+
+
+def test_one_step_from_a_moving_state(case):
+    gpu, p, st0 = case
+    start = gu.f32(gu.run_steps(gpu, st0, 2))
+    assert np.abs(start["u"]).max() > 1e-3 and np.abs(start["eta"]).max() > 1e-3
+    got = gu.run_steps(gpu, start, 1)
+    want = ostep.step(dict(start), p)
+    errs = _errors(got, want, p)
+    print("720x360x50 one step from a state two steps in, relative L2:", errs)
+    assert max(errs.values()) < STEP_TOL, errs

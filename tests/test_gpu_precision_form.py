@@ -1,0 +1,64 @@
+"""The precision form (FP32 stencils, implicit vertical diffusion with one
+refinement step, float64 barotropic mode, seasonal wind stress and +-100 W/m^2
+heat flux blended on the device before every step) against the float64
+oracle over ten simulated days on a reduced 48x24x50 grid with the
+0.45-degree option set (the 800x400x50 form is timed by bench.py).
+
+The per-field relative L2 error (eta, u, v, T, S and the density anomaly)
+after one and ten days is printed and bounded; the oracle runs the same
+forcing sequence (inputs/forcing/seasonal.py:86-103 blend, float64) and
+solves the implicit backward-Euler systems directly.
+"""
+import numpy as np
+import pytest
+
+from oracle import params as oparams
+from oracle import seasonal
+from oracle import step as ostep
+from tests import gpu_util as gu
+from zhenmode_b200 import make_solver_global, workloads
+
+pytestmark = pytest.mark.gpu
+
+DAY_TOL = {1: 2e-5, 10: 2e-4}
+
+
+def _stacks(grid):
+    nx, ny = grid.nx, grid.ny
+    lat = np.radians(np.asarray(grid.lat))
+    tau0 = np.broadcast_to((0.1 * np.sin(2 * lat) * np.cos(lat))[None, :], (nx, ny))
+    phase = np.sin(2 * np.pi * (np.arange(12) + 0.5) / 12.0)
+    taux = np.stack([tau0 * (1 + 0.25 * p) for p in phase]).astype(np.float32)
+    qh = np.stack([np.broadcast_to(100.0 * p * np.cos(lat)[None, :], (nx, ny)) for p in phase]).astype(np.float32)
+    return taux, qh
+
+
+def test_precision_form_ten_days_against_the_oracle():
+    grid, physics, dt, kw, T, S = workloads.make_case("precision", 48, 24, 50, dtype="float32")
+    kw = dict(kw, vertical_diffusion="implicit")
+    step, init, _ = make_solver_global(grid, physics, dt, **kw)
+    okw = {k: v for k, v in kw.items() if k in oparams.SUPPORTED}
+    okw["dtype"] = "float64"
+    p = oparams.build_params(grid, physics, dt, **okw)
+    taux, qh = _stacks(grid)
+    st = init(T, S)
+    want = {k: getattr(st, k).double().cpu().numpy() for k in gu.FIELDS}
+    per_day = int(round(86400.0 / dt))
+    errs = {}
+    for n in range(10 * per_day):
+        day = n * dt / 86400.0
+        step.set_forcing_seasonal(tau_x=taux, q_heat=qh, day=day)
+        st = step(st)
+        p.tau_x_2d = seasonal.blend(taux.astype(np.float64), day)
+        p.Q_heat_2d = seasonal.blend(qh.astype(np.float64), day)
+        want = ostep.step(dict(want), p)
+        if (n + 1) % per_day == 0 and (n + 1) // per_day in DAY_TOL:
+            got = {k: getattr(st, k).double().cpu().numpy() for k in gu.FIELDS}
+            e = gu.errors(got, want)
+            e["rho_anomaly"] = gu.rel_l2(ostep.density_anomaly(got["T"], got["S"], p),
+                                         ostep.density_anomaly(want["T"], want["S"], p))
+            errs[(n + 1) // per_day] = e
+    for day, e in errs.items():
+        print(f"precision form 48x24x50, day {day}, relative L2 vs float64 oracle:",
+              {k: f"{v:.2e}" for k, v in e.items()})
+        assert max(e.values()) < DAY_TOL[day], (day, e)

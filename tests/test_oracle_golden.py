@@ -206,3 +206,32 @@ def test_ledger_matches_reference_budget_step():
                 if ref is not None:
                     scale = max(scale, float(np.max(np.abs(data[f"ledger{n}_{ref}"]))))
             assert err <= 1e-9 * scale, (n, key, err, scale)
+
+
+def _terms_case():
+    from zhenmode_b200 import workloads
+    data = load("terms_48x24x10")
+    grid = grid_from(data)
+    wm = np.asarray(grid.wet_mask)
+    kw = dict(workloads.PLAIN_OPTIONS)
+    kw.update(forcing=workloads.wind_forcing(grid), dt_bt=75.0,
+              coastal_kappa_h_mask=wm, coastal_kappa_h=float(data["coastal_kappa_h"]),
+              coastal_kappa_v_mask=wm, coastal_kappa_v=float(data["coastal_kappa_v"]))
+    state = {k: data["in_" + k] for k in ("u", "v", "T", "S", "eta")}
+    return data, grid, kw, state
+
+
+def test_tracer_terms_match_reference_terms_fn():
+    """terms_fn of factory.py:762-764 (dynamics/tendencies.py:74-92)."""
+    from zhenmode_b200 import workloads
+    data, grid, kw, state = _terms_case()
+    p = oparams.build_params(grid, workloads.PLAIN_PHYSICS, 1800.0, dtype="float64", **kw)
+    got = ostep.tracer_terms(state, p)
+    want = data["terms"]
+    assert got.shape == want.shape == (6,) + state["T"].shape
+    assert np.abs(want[3]).max() > 0, "the fixture must exercise convection"
+    for n, name in enumerate(("adv", "diff_h", "diff_v", "conv", "gm", "redi")):
+        if np.abs(want[n]).max() == 0:
+            assert np.abs(got[n]).max() == 0, name
+        else:
+            _check(name, got[n], want[n])

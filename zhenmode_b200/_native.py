@@ -109,6 +109,7 @@ EXPORTS = {
     "zm_ensemble_advance": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
                                            ctypes.POINTER(ctypes.c_int32)]),
     "zm_ensemble_destroy": (None, [ctypes.c_void_p]),
+    "zm_tracer_terms": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ZmState), ctypes.c_void_p]),
     "zm_budgets": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                   ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]),
     "zm_classify_state_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,

@@ -197,3 +197,72 @@ def fit(net, X, T, M, steps=2000, batch=8192, lr=1e-3, seed=0):
         sl = slice(a, min(n, a + 65536))
         losses.append(net.grad(X[sl], T[sl], M[sl])[0] * float(M[sl].sum().item()))
     return sum(losses) / float(M.sum().item())
+
+
+def mixed_layer_depth(T, S, z, wet3, ref_depth=10.0, density_delta=0.03):
+    """Density-threshold mixed-layer depth in metres, positive down, of every
+    column (diagnostics/mixed_layer.py:39-74, linear density of :14-35):
+    the depth of the first level at or below ``ref_depth`` whose density
+    exceeds the density at the level nearest ``ref_depth`` by
+    ``density_delta``; the deepest wet level where none does; NaN on land.
+    Levels below the seafloor (``wet3`` == 0) are the missing profile levels
+    of the reference.  Host NumPy over all columns at once; T, S and wet3 are
+    (nx, ny, nz) arrays, z the (nz,) node depths (negative down)."""
+    T = np.asarray(T, dtype=np.float64)
+    S = np.asarray(S, dtype=np.float64)
+    wet = np.asarray(wet3) > 0.5
+    depth = -np.asarray(z, dtype=np.float64)
+    rho = 1025.0 * (1.0 - 2.0e-4 * (T - 15.0) + 7.6e-4 * (S - 35.0))
+    ref_k = int(np.argmin(np.abs(depth - ref_depth)))
+    delta = rho - rho[..., ref_k:ref_k + 1]
+    hit = wet & (depth >= ref_depth)[None, None, :] & (delta >= density_delta)
+    first = np.argmax(hit, axis=-1)
+    nz = T.shape[-1]
+    deepest = nz - 1 - np.argmax(wet[..., ::-1], axis=-1)
+    k = np.where(hit.any(axis=-1), first, deepest)
+    mld = depth[k]
+    # the reference needs the level nearest ref_depth to be valid for any delta
+    ok = wet.any(axis=-1) & wet[..., ref_k]
+    return np.where(ok, mld, np.where(wet.any(axis=-1), depth[deepest], np.nan))
+
+
+def compare_with_plain(step, net, state, days, steps_per_day, grid):
+    """Run ``days`` simulated days from ``state`` with the plain closure and
+    with the network ``net`` (the plain closure judges the network), and
+    return per-day RMSEs over the wet columns of the daily-mean SST, SSS and
+    mixed-layer depth (from the daily-mean T and S) of the learned run
+    against the plain run, with the fallback-column count of the last step."""
+    import torch
+    wet2 = np.asarray(grid.wet_mask) > 0.5
+    wet3 = np.asarray(grid.wet_mask_3d)
+    z = np.asarray(grid.z)
+
+    def daily_means(closure):
+        step.set_closure(closure)
+        st, out = state, []
+        for _ in range(days):
+            accT = torch.zeros_like(state.T)
+            accS = torch.zeros_like(state.S)
+            for _ in range(steps_per_day):
+                st = step(st)
+                accT += st.T
+                accS += st.S
+            out.append((accT / steps_per_day, accS / steps_per_day))
+        fallback = step.closure_stats()[0] if closure is not None else 0
+        step.set_closure(None)
+        return out, fallback
+
+    plain, _ = daily_means(None)
+    learned, fallback = daily_means(net)
+    rmse = lambda a, b: float(np.sqrt(np.nanmean(((a - b)[wet2]) ** 2)))  # noqa: E731
+    res = {"sst_rmse_K": [], "sss_rmse_psu": [], "mld_rmse_m": [], "mld_mean_m": []}
+    for (tp, sp), (tl, sl) in zip(plain, learned):
+        tp, sp, tl, sl = (a.cpu().numpy() for a in (tp, sp, tl, sl))
+        res["sst_rmse_K"].append(rmse(tl[..., 0], tp[..., 0]))
+        res["sss_rmse_psu"].append(rmse(sl[..., 0], sp[..., 0]))
+        mp = mixed_layer_depth(tp, sp, z, wet3)
+        ml = mixed_layer_depth(tl, sl, z, wet3)
+        res["mld_rmse_m"].append(rmse(ml, mp))
+        res["mld_mean_m"].append(float(np.nanmean(mp[wet2])))
+    res["fallback_columns_last_step"] = int(fallback)
+    return res

@@ -1070,6 +1070,126 @@ void launch_tracer_adv(cudaStream_t s, const Dev& d, const float* T, const float
     k_tracer_adv_t<0><<<g, b, 0, s>>>(d, T, S, u, v, Fz, accT, accS, Tn, Sn, dts, first, last, topT, topS);
 }
 
+// Temperature-term decomposition of a state (dynamics/tendencies.py:74-92,
+// the terms_fn of factory.py:762-764), a read-only diagnosis outside the
+// step: advection (one evaluation of transport.py:365-475, limiter faces as
+// in k_tracer_adv_t), wet-face horizontal diffusion with kappa_h + coastal
+// (horizontal.py:217-243), vertical diffusion with kappa_v + coastal
+// (physics/vertical.py:45-53) and the interface-flux convective tendency
+// (physics/vertical.py:13-37, 63-82) with kappa_conv, each times the wet
+// mask.  One column per thread marching down; neighbours by global loads
+// (rows clamped at the walls, longitude wrapped).  T and S are anomalies:
+// every term is a difference operator of T, or (advection) a flux divergence
+// whose constant part cancels through the continuity inverse Fz.
+template <int LIM>
+__global__ void __launch_bounds__(128) k_tracer_terms(Dev d, const float* __restrict__ T,
+                                                      const float* __restrict__ S, const float* __restrict__ u,
+                                                      const float* __restrict__ v, const float* __restrict__ Fz,
+                                                      float* __restrict__ adv, float* __restrict__ dh,
+                                                      float* __restrict__ dv, float* __restrict__ conv) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= d.nx || j >= d.ny) return;
+  int ci[5], rj[5];  // columns i-2..i+2 (wrapped), rows j-2..j+2 (clamped)
+#pragma unroll
+  for (int o = 0; o < 5; ++o) {
+    int g = (i + o - 2) % d.nx;
+    ci[o] = g < 0 ? g + d.nx : g;
+    rj[o] = min(max(j + o - 2, 0), d.ny - 1);
+  }
+  uint64_t wx[5], wy[5];
+#pragma unroll
+  for (int o = 0; o < 5; ++o) {
+    wx[o] = wb(d, j, ci[o]);
+    wy[o] = wb(d, rj[o], i);
+  }
+  const long long base = idx2(d, j, i);
+  const uint64_t bits = wx[2];
+  const int kbt = kbot_of(bits);
+  const float ix = __ldg(d.inv_dx + base), ysc = d.inv_dy * __ldg(d.inv_cos + j);
+  const float kv = __ldg(d.kv2 + base);
+  const float cfn = j < d.ny - 1 ? __ldg(d.cfp + j) : 0.f, cfs = j > 0 ? __ldg(d.cfp + j - 1) : 0.f;
+  // convective interfaces of the column (k_tracer_rest's gates)
+  uint64_t unstable = 0ull, wetpair = 0ull;
+  for (int m = 0; m + 1 < d.nz; ++m) {
+    const long long a = (long long)m * d.plane + base, b = a + d.plane;
+    if (wetb(bits, m) && wetb(bits, m + 1)) {
+      wetpair |= 1ull << m;
+      if (kBeta * (ld(S, a) - ld(S, b)) > kAlpha * (ld(T, a) - ld(T, b))) unstable |= 1ull << m;
+    }
+  }
+  uint64_t allow = 0ull;
+  if (unstable && d.kappa_conv > 0.f) allow = d.localize_conv ? unstable : wetpair;
+  float fconv = 0.f;
+  for (int k = 0; k < d.nz; ++k) {
+    const long long pl = (long long)k * d.plane;
+    const float w0 = wetf(bits, k);
+    const float ck = ld(T, pl + base);
+    const float ckm = k > 0 ? ld(T, pl - d.plane + base) : ck;
+    const float ckp = k + 1 < d.nz ? ld(T, pl + d.plane + base) : ck;
+    float tx[5], ty[5], mx[5], my[5];
+#pragma unroll
+    for (int o = 0; o < 5; ++o) {
+      tx[o] = ld(T, pl + idx2(d, j, ci[o]));
+      ty[o] = ld(T, pl + idx2(d, rj[o], i));
+      mx[o] = wetf(wx[o], k);
+      my[o] = wetf(wy[o], k);
+    }
+    float a_ = 0.f;
+    if (w0 != 0.f) {
+      // x faces east (i, i+1) and west (i-1, i)
+      const float uc = ld(u, pl + base), ue = ld(u, pl + idx2(d, j, ci[3])), uw = ld(u, pl + idx2(d, j, ci[1]));
+      const float uxe = 0.5f * (uc + ue), uxw = 0.5f * (uw + uc);
+      const float fxe = uxe * ta_face_value<LIM>(uxe >= 0.f, tx[1], tx[2], tx[3], tx[4], mx[1], mx[2], mx[3], mx[4]) *
+                        (mx[2] * mx[3]);
+      const float fxw = uxw * ta_face_value<LIM>(uxw >= 0.f, tx[0], tx[1], tx[2], tx[3], mx[0], mx[1], mx[2], mx[3]) *
+                        (mx[1] * mx[2]);
+      // y faces north (j, j+1) and south (j-1, j); closed at the walls
+      float fyn = 0.f, fys = 0.f;
+      const float vc = ld(v, pl + base);
+      if (j < d.ny - 1) {
+        const float vy = 0.5f * (vc + ld(v, pl + idx2(d, rj[3], i)));
+        fyn = vy * ta_face_value<LIM>(vy >= 0.f, ty[1], ty[2], ty[3], ty[4], my[1], my[2], my[3], my[4]) *
+              (my[2] * my[3]) * cfn;
+      }
+      if (j > 0) {
+        const float vy = 0.5f * (ld(v, pl + idx2(d, rj[1], i)) + vc);
+        fys = vy * ta_face_value<LIM>(vy >= 0.f, ty[0], ty[1], ty[2], ty[3], my[0], my[1], my[2], my[3]) *
+              (my[1] * my[2]) * cfs;
+      }
+      const float h = (fxe - fxw) * ix + (fyn - fys) * ysc;
+      const float fz_k = ld(Fz, pl + base);
+      float up, dn = 0.f;
+      if (k == 0) {
+        up = fz_k * ck;
+      } else {
+        up = fz_k * (fz_k > 0.f ? ckm : ck) * (wetf(bits, k - 1) * w0);
+      }
+      if (k + 1 < d.nz) {
+        const float fz_n = ld(Fz, pl + d.plane + base);
+        const float tn = k + 1 <= kbt ? ckp : ck;
+        dn = fz_n * (fz_n > 0.f ? ck : tn) * (w0 * wetf(bits, k + 1));
+      }
+      a_ = -(h + (dn - up) * d.vc.inv_dz_node[k]) * w0;
+    }
+    adv[pl + base] = a_;
+    dh[pl + base] = hdiff(d, T, d.kh2, k, nb(d, j, i)) * w0;
+    dv[pl + base] = vdiff_c(d, k, bits, kv, ckm, ck, ckp) * w0;
+    float g = 0.f;
+    if (k + 1 < d.nz && ((allow >> k) & 1ull)) g = -d.kappa_conv * (ckp - ck) * d.vc.inv_dz_iface[k];
+    conv[pl + base] = (fconv - g) * d.vc.inv_dz_node[k] * w0;
+    fconv = g;
+  }
+}
+
+void launch_tracer_terms(cudaStream_t s, const Dev& d, const float* T, const float* S, const float* u,
+                         const float* v, const float* Fz, float* adv, float* dh, float* dv, float* conv) {
+  const dim3 b(32, 4), g((d.nx + 31) / 32, (d.ny + 3) / 4);
+  if (d.limiter == 2) k_tracer_terms<2><<<g, b, 0, s>>>(d, T, S, u, v, Fz, adv, dh, dv, conv);
+  else if (d.limiter == 1) k_tracer_terms<1><<<g, b, 0, s>>>(d, T, S, u, v, Fz, adv, dh, dv, conv);
+  else k_tracer_terms<0><<<g, b, 0, s>>>(d, T, S, u, v, Fz, adv, dh, dv, conv);
+}
+
 // Tracer residual of the N step (dynamics/tendencies.py:94-245) without the
 // diffusion pair that the residual adds and removes again: mean advection
 // rate + interface-flux convective mixing (physics/vertical.py:13-37, 63-82)

@@ -115,6 +115,8 @@ constexpr int IV_T = 64;
 void launch_implicit_vdiff(cudaStream_t s, const Dev& d, float* u, float* v, float* T, float* S, const float* u0,
                            const float* v0, const float* T0, const float* S0, float dth, const float* kap3);
 void launch_fz(cudaStream_t s, const Dev& d, const float* u, const float* v, float* Fz);
+void launch_tracer_terms(cudaStream_t s, const Dev& d, const float* T, const float* S, const float* u,
+                         const float* v, const float* Fz, float* adv, float* dh, float* dv, float* conv);
 __global__ void k_madv(Dev d, const float* u, const float* v, const float* Fz, float* Ayu, float* Ayv);
 __global__ void k_dealias_lon(Dev d, FftPlan plan, const float* Ayu, const float* Ayv, float* Au, float* Av,
                               int lines_per_block);

@@ -1522,6 +1522,26 @@ int zm_diagnostics(zm_solver* s, void* stream, const zm_state* in, const float* 
   return ZM_OK;
 }
 
+int zm_tracer_terms(zm_solver* s, void* stream, const zm_state* in, float* terms) {
+  if (!s || !in || !in->u || !in->v || !in->T || !in->S || !in->eta || !terms) return ZM_ERR_INVALID;
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t nref = (size_t)s->nx * s->ny * s->nz;
+  try {
+    // the caller's state goes to work buffers that are idle between steps
+    s->load(st, in, s->s2, s->frx);
+    launch_fz(st, s->d, s->s2.u, s->s2.v, s->Fz);
+    launch_tracer_terms(st, s->d, s->s2.T, s->s2.S, s->s2.u, s->s2.v, s->Fz, s->W1.u, s->W1.v, s->W1.T, s->W1.S);
+    s->check_launch();
+    const float* src[4] = {s->W1.u, s->W1.v, s->W1.T, s->W1.S};
+    for (int q = 0; q < 4; ++q) s->to_ref3(st, src[q], terms + q * nref, 0.f);
+    s->check_launch();
+    ZM_CUDA(cudaMemsetAsync(terms + 4 * nref, 0, 2 * nref * sizeof(float), st));  // GM, Redi: off
+  } catch (const Err& e) {
+    return fail(s, e);
+  }
+  return ZM_OK;
+}
+
 int zm_budgets(zm_solver* s, void* stream, const float* T, const float* S, double rho0, double cp, double* out) {
   if (!s || !T || !S || !out || !std::isfinite(rho0) || !std::isfinite(cp)) return ZM_ERR_INVALID;
   cudaStream_t st = (cudaStream_t)stream;

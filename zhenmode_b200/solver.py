@@ -705,7 +705,18 @@ def make_solver_global(grid, physics, dt, forcing=None,
         params.step = step
 
         def terms_fn(state):
-            raise NotImplementedError("tracer term decomposition is not implemented on the B200 path")
+            """(6, nx, ny, nz) float32 [adv, diff_h, diff_v, conv, gm, redi]
+            temperature terms of a state (factory.py:762-764,
+            dynamics/tendencies.py:74-92), on the state's side (a CUDA tensor
+            for a device state, a NumPy array for a host state)."""
+            import torch
+            fin, host = _device_fields(state, solver.shape)
+            out = torch.empty((6,) + tuple(solver.shape), dtype=torch.float32, device=fin[0].device)
+            stream = torch.cuda.current_stream(fin[0].device).cuda_stream
+            sin = _native.ZmState(*[t.data_ptr() for t in fin])
+            solver.check(solver.lib.zm_tracer_terms(solver.handle, ctypes.c_void_p(stream), ctypes.byref(sin),
+                                                    ctypes.c_void_p(out.data_ptr())), "zm_tracer_terms")
+            return out.cpu().numpy() if host else out
 
         result += [params, terms_fn]
     if dynamic_forcing:
