@@ -402,6 +402,74 @@ def run_precision(args):
     return 0
 
 
+def train_closure(step, st, dt, days):
+    """The learned closure trained on the plain model's own columns: `days`
+    simulated days of the plain step from `st`, 60 snapshots, at most 2M
+    rows, 3000 Adam steps of 8192 rows.  Returns (network, record, the state
+    at the end of the plain run)."""
+    import torch
+
+    from zhenmode_b200.closure import ClosureMLP, collect, fit
+    steps_per_day = int(round(86400.0 / dt))
+    nsteps = days * steps_per_day
+    every = max(1, nsteps // 60)
+    t0 = time.time()
+    X, Tt, M, end = collect(step, st, nsteps, every=every, max_rows=2_000_000, seed=0)
+    torch.cuda.synchronize()
+    t1 = time.time()
+    net = ClosureMLP(seed=0)
+    loss = fit(net, X, Tt, M, steps=3000, batch=8192, lr=1e-3)
+    torch.cuda.synchronize()
+    info = {"rows": int(X.shape[0]), "collect_days": days, "snapshots": nsteps // every,
+            "collect_s": round(t1 - t0, 1), "train_steps": 3000, "batch": 8192,
+            "train_s": round(time.time() - t1, 1), "loss_log10_kappa_mse": loss}
+    del X, Tt, M
+    return net, info, end
+
+
+def chosen_form(step, st, dt, grid, solver, args, plain_ms):
+    """The learned-closure form beside the plain one: train the network on
+    the plain model's columns, time the step with it (CUDA events around
+    zm_advance on the resident state, as for the plain line), and compare
+    10 simulated days of it with the plain run (daily-mean SST, SSS and
+    mixed-layer depth)."""
+    import ctypes
+
+    import torch
+
+    from zhenmode_b200 import _native
+    from zhenmode_b200.closure import compare_with_plain
+    net, info, end = train_closure(step, st, dt, args.closure_days)
+    steps_per_day = int(round(86400.0 / dt))
+    cmp = compare_with_plain(step, net, end, 10, steps_per_day, grid)
+    step.set_closure(net)
+    stream = torch.cuda.current_stream()
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    sin = _native.ZmState(*[t.data_ptr() for t in (end.u, end.v, end.T, end.S, end.eta)])
+    solver.check(solver.lib.zm_load_state(solver.handle, sptr, ctypes.byref(sin)), "zm_load_state")
+    solver.check(solver.lib.zm_advance(solver.handle, sptr, args.warmup), "zm_advance")
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    solver.check(solver.lib.zm_advance(solver.handle, sptr, args.steps), "zm_advance")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    prof = {}
+    for _ in range(PROFILE_STEPS):
+        for k, (pm, pc) in solver.profile(stream.cuda_stream).items():
+            am, ac = prof.get(k, (0.0, 0))
+            prof[k] = (am + pm / PROFILE_STEPS, pc)
+    fallback = step.closure_stats()[0]
+    step.set_closure(None)
+    return {"form": "learned", "ms_per_step": ms, "value": sim_years_per_day(ms, dt), "unit": "sim-years/day",
+            "speedup_vs_plain": plain_ms / ms, "target_speedup": 1.3,
+            "kernel_ms_per_step": {k: round(v[0], 4) for k, v in prof.items() if v[1] > 0},
+            "fallback_columns_last_step": int(fallback), "training": info,
+            "vs_plain_10_days": {"days": 10, "start": f"day {args.closure_days} of the plain training run", **cmp,
+                                 "sst_rmse_K_max": max(cmp["sst_rmse_K"]), "target_sst_rmse_K": 0.05}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -416,6 +484,8 @@ def main():
                          "2M rows) first, then time the step with it; projected: the plain step with the "
                          "column-divergence projection of the stage-2 advective velocity on")
     ap.add_argument("--closure-days", type=int, default=30)
+    ap.add_argument("--no-learned", action="store_true",
+                    help="plain form only: skip training and timing the learned-closure form beside it")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default launch shapes (profiling: no autotuner trial launches)")
     args = ap.parse_args()
@@ -456,21 +526,7 @@ def main():
     st = init_state(T_init=T, S_init=S)
     closure_info = None
     if args.form == "learned":
-        from zhenmode_b200.closure import ClosureMLP, collect, fit
-        steps_per_day = int(round(86400.0 / dt))
-        nsteps_c = args.closure_days * steps_per_day
-        every = max(1, nsteps_c // 60)
-        t0 = time.time()
-        X, Tt, M, _ = collect(step, st, nsteps_c, every=every, max_rows=2_000_000, seed=0)
-        torch.cuda.synchronize()
-        t1 = time.time()
-        net = ClosureMLP(seed=0)
-        loss = fit(net, X, Tt, M, steps=3000, batch=8192, lr=1e-3)
-        torch.cuda.synchronize()
-        closure_info = {"rows": int(X.shape[0]), "collect_days": args.closure_days, "snapshots": nsteps_c // every,
-                        "collect_s": round(t1 - t0, 1), "train_steps": 3000, "batch": 8192,
-                        "train_s": round(time.time() - t1, 1), "loss_log10_kappa_mse": loss}
-        del X, Tt, M
+        net, closure_info, _ = train_closure(step, st, dt, args.closure_days)
         step.set_closure(net)
     stream = torch.cuda.current_stream()
     sptr = ctypes.c_void_p(stream.cuda_stream)
@@ -543,6 +599,10 @@ def main():
         e2e = {"value": world * sim_years_per_day(ems, wl.dt), "unit": "sim-years/day", "ms_per_step": ems,
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes}
 
+    chosen = None
+    if args.form == "plain" and not args.no_learned and world == 1:
+        chosen = chosen_form(step, st, wl.dt, grid, solver, args, ms)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cms, desc = cpu_baseline()
@@ -558,8 +618,7 @@ def main():
                                        f"{solver.n_subcyc} barotropic subcycles, {solver.n_nu} nu_h subcycles",
                            "parallelism": f"replicas x{world}", "l2": "per-step working set >> L2 (no flush)",
                            "monitor_code": int(code.value), "form": args.form,
-                           "autotuned": {"nu_h_subcycles_per_pass": solver.tuned_shapes()[0],
-                                         "fft_lines_per_block": solver.tuned_shapes()[1]}},
+                           "autotuned": solver.launch_shapes()},
                 "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
                              "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                              "traffic": traffic, "algorithmic_bytes_per_launch": algo,
@@ -573,6 +632,8 @@ def main():
         if closure_info is not None:
             closure_info["fallback_columns_last_step"] = step.closure_stats()[0]
             line["closure"] = closure_info
+        if chosen is not None:
+            line["chosen_form"] = chosen
         if args.form == "projected":
             it = step.projection_stats()
             line["projection"] = {"cg_iterations": list(it[:3]), "refinement_solves": it[3],

@@ -133,7 +133,10 @@ int zm_create(const zm_grid* grid, const zm_params* params, zm_solver** out);
  * barotropic blocks of the resident kernel (0: streaming kernels), out[8] 1
  * when the polar cap of the barotropic mode is active (a band row is wet),
  * out[9] nu_h subcycles per temporally blocked pass (the halo width), out[10]
- * FFT lines per block.  Writes min(n, 11) values. */
+ * FFT lines per block, out[11] levels per block of the tracer-advection
+ * march, out[12] of the linear-finish march, out[13] tile rows of the
+ * vertical-transport march, out[14] of the pressure-gradient march.  Writes
+ * min(n, 15) values. */
 int zm_info(const zm_solver* s, int32_t* out, int32_t n);
 
 /* Copy a device state (reference layout) into the solver's resident state. */
@@ -293,8 +296,10 @@ int zm_mlp_train_step(zm_mlp_trainer* tr, void* stream, int32_t batch, const flo
 
 /* Autotuner: time, on the resident state and through stages that write only
  * work buffers, the launch shapes that change no result (the nu_h halo
- * width 3..6, i.e. subcycles per temporally blocked pass, and the FFT lines
- * per block 1..8) and keep the fastest; the next zm_advance recaptures its
+ * width 3..6, i.e. subcycles per temporally blocked pass, the FFT lines per
+ * block 1..8, the levels per block of the tracer-advection and linear-finish
+ * column marches 5..25, and the tile rows of the vertical-transport and
+ * pressure-gradient marches 4 or 8) and keep the fastest; the next zm_advance recaptures its
  * graphs.  zm_params.autotune = 1 runs it at the first zm_advance.  Writes
  * the choices when the pointers are given.  Synchronizes. */
 int zm_autotune(zm_solver* s, void* stream, int32_t* nu_halo, int32_t* fft_lines);

@@ -130,6 +130,8 @@ __device__ float2* fft_lines(float2* a, float2* b, const FftPlan& plan, int line
 __global__ void __launch_bounds__(256) k_dealias_lon(Dev d, FftPlan plan, const float* __restrict__ Ayu,
                                                      const float* __restrict__ Ayv, float* __restrict__ Au,
                                                      float* __restrict__ Av, int lines_per_block) {
+  pdl_trigger();
+  pdl_wait();  // the advection fields come from the preceding kernel
   extern __shared__ float2 fsm[];
   const int n = plan.n;
   float2* bufa = fsm;

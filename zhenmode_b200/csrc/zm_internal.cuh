@@ -60,6 +60,7 @@ struct Dev {
   const float* rot_s;          // sin(f dt/2)
   const float* wet2;           // 2-D wet mask (barotropic mode)
   const uint64_t* wbits;       // 3-D wet mask, one word per column
+  const unsigned char* nu_gate; // 3-D [nz][ny][P] face gates of the nu_h Laplacian (k_nu_gates)
   const float* kh2;            // kappa_h + coastal kappa_h
   const float* kv2;            // kappa_v + coastal kappa_v
   const float* tau_x;
@@ -80,6 +81,10 @@ struct Dev {
   float lambda_bulk, restore_S, ice_salt, ice_freeze;
   int localize_conv, limiter;  // limiter: 0 centered, 1 donor cell, 2 minmod (fct)
   int conservative_kv;
+  // launch shapes that change no result (chosen by the autotuner): levels per
+  // block of the tracer-advection and linear-step column marches, tile rows
+  // of the pressure-gradient and vertical-transport marches
+  int ta_kc, lt_kc, pg_rows, fz_rows;
   Vert vc;
 };
 

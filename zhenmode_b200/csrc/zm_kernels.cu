@@ -121,21 +121,20 @@ __device__ __forceinline__ float colv(const float* __restrict__ a, long long bas
 // metric term -(tan(lat)/R) du/dy), and the mirror ghost of the closed
 // walls folded in: at j = ny-1 the north neighbour equals u0, so aN = 0; at
 // j = 0, aS = 0.  The coefficients, scaled by nu_h dt_sub, are formed once
-// per pass.  Longitude wraps.  The lane's two columns are held as packed
-// pairs, so the update runs on the paired FP32 instructions (__ffma2_rn,
-// __fadd2_rn; the same roundings as the scalar form).  The wet flags of the
-// lane's cells are bits of a register; the neighbouring lanes' flags arrive by
-// shuffle and the neighbouring warps' through shared memory.  The state is
-// loaded after the coefficients are formed, so the two sets are not live
-// together during the set-up.
+// per pass from the face gates of the cell (k_nu_gates, built once per
+// solver: one byte per point) and per-row constants, so the set-up needs
+// no neighbour wet flags.  Longitude wraps.  The lane's two columns are held
+// as packed pairs, so the update runs on the paired FP32 instructions
+// (__ffma2_rn, __fadd2_rn; the same roundings as the scalar form).  Points
+// of the tile edge see their own values as the missing neighbours (their
+// results are discarded with the halo).
 __global__ void __launch_bounds__(32 * (NB_W / NB_R), 2)
 k_nu_tb(Dev d, const float* __restrict__ u, const float* __restrict__ v, float* __restrict__ uo,
         float* __restrict__ vo, float c, int nsub, int halo) {
   constexpr int NW = NB_W / NB_R;                 // warps per block
-  static_assert(2 * NB_R <= 32, "a lane's wet flags fit one register");
   const int TI = NB_W - 2 * halo;
   __shared__ float4 edge[2][NW][2][32];           // [parity][warp][0 bottom row, 1 top row][lane]
-  __shared__ unsigned swm[NW][32];                // each lane's wet-flag bits (coefficient setup)
+  pdl_trigger();
   const int lane = threadIdx.x, wp = threadIdx.y;
   const int k = blockIdx.z;
   const int gx0 = blockIdx.x * TI - halo, gy0 = blockIdx.y * TI - halo;
@@ -147,74 +146,40 @@ k_nu_tb(Dev d, const float* __restrict__ u, const float* __restrict__ v, float* 
     gi[h] = g < 0 ? g + d.nx : g;
   }
   const long long kb = (long long)k * d.plane;
-  // metric terms of the lane's cells, loaded first so that their latency
-  // overlaps the wet-flag loads
-  float ix2v[NB_R][2], tv[NB_R];
-#pragma unroll
-  for (int q = 0; q < NB_R; ++q) {
-    const int gj = gy0 + r0 + q;
-    const int gjc = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
-    tv[q] = __ldg(d.tanR + gjc);
-#pragma unroll
-    for (int h = 0; h < 2; ++h) ix2v[q][h] = __ldg(d.inv_dx2 + idx2(d, gjc, gi[h]));
-  }
-  // bit 2q + h of wm: cell (row r0 + q, column c0 + h) is wet at level k, read
-  // from the 32-bit half of the column's 64-bit wet word that holds bit k
-  // (little-endian: levels 0-31 in the first half)
-  unsigned wm = 0u;
-#pragma unroll
-  for (int q = 0; q < NB_R; ++q) {
-    int gj = gy0 + r0 + q;
-    gj = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
-#pragma unroll
-    for (int h = 0; h < 2; ++h)
-      wm |= ((__ldg(reinterpret_cast<const unsigned*>(d.wbits) + 2 * idx2(d, gj, gi[h]) + (k >> 5)) >> (k & 31)) & 1u)
-            << (2 * q + h);
-  }
-  const unsigned full = 0xffffffffu;
-  swm[wp][lane] = wm;
-  const unsigned wm_e = __shfl_down_sync(full, wm, 1);  // lane l + 1 (lane 31: its own, unused)
-  const unsigned wm_w = __shfl_up_sync(full, wm, 1);    // lane l - 1 (lane 0: its own, unused)
-  __syncthreads();
-  // flags of the rows just outside the strip; none beyond the tile's top and bottom rows
-  const unsigned wm_n = wp + 1 < NW ? swm[wp + 1][lane] : 0u;  // bits 0, 1: row r0 + NB_R
-  const unsigned wm_s = wp > 0 ? swm[wp - 1][lane] : 0u;       // bits 2 NB_R - 2, - 1: row r0 - 1
   const float cn = d.nu_h * c;
   // face coefficients, paired like the state: (column 2l, column 2l+1).  The
   // west and south ones are held negated (nW = -aW, nS = -aS) and negated back
   // in the update, an exact round trip: ptxas 12.9 allocates this form's
-  // registers differently, and it ran 4 % faster than holding aW, aS (timed
-  // before the metric terms were loaded ahead of the wet flags).
+  // registers differently, and it ran 4 % faster than holding aW, aS.
   float2 kE[NB_R], nW[NB_R], kN[NB_R], nS[NB_R];
 #pragma unroll
   for (int q = 0; q < NB_R; ++q) {
-    const int r = r0 + q;
-    const int gj = gy0 + r;
+    const int gj = gy0 + r0 + q;
+    const int gjc = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
     const bool n_in = gj < d.ny - 1;  // north neighbour inside the domain
     const bool s_in = gj > 0;
-    const float t = 0.5f * d.inv_dy * tv[q];
+    const float t = 0.5f * d.inv_dy * __ldg(d.tanR + gjc);
+    // aN with the north face open / closed, aS likewise (0 beyond the walls)
+    const float n1 = n_in ? (d.inv_dy2 - t) * cn : 0.f, n0 = n_in ? (0.f - t) * cn : 0.f;
+    const float s1 = s_in ? (d.inv_dy2 + t) * cn : 0.f, s0 = s_in ? (0.f + t) * cn : 0.f;
     float ce[2], cw[2], cnn[2], cs[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      const int b = 2 * q + h;
-      const bool w0 = (wm >> b) & 1u;
-      // neighbours outside the tile count as dry, as at the tile's own edge
-      const bool we = h == 0 ? ((wm >> (b + 1)) & 1u) : (lane < 31 && ((wm_e >> (2 * q)) & 1u));
-      const bool ww = h == 1 ? ((wm >> (b - 1)) & 1u) : (lane > 0 && ((wm_w >> (2 * q + 1)) & 1u));
-      const bool wn = n_in && (q + 1 < NB_R ? ((wm >> (b + 2)) & 1u) : ((wm_n >> h) & 1u));
-      const bool ws = s_in && (q > 0 ? ((wm >> (b - 2)) & 1u) : ((wm_s >> (2 * NB_R - 2 + h)) & 1u));
-      const float ix2 = ix2v[q][h];
-      const float cN = (w0 && wn) ? d.inv_dy2 : 0.f, cS = (w0 && ws) ? d.inv_dy2 : 0.f;
-      ce[h] = (w0 && we) ? ix2 * cn : 0.f;
-      cw[h] = (w0 && ww) ? ix2 * cn : 0.f;
-      cnn[h] = n_in ? (cN - t) * cn : 0.f;
-      cs[h] = s_in ? (cS + t) * cn : 0.f;
+      const int id2 = idx2(d, gjc, gi[h]);
+      const unsigned g = __ldg(d.nu_gate + kb + id2);
+      const float ax = __ldg(d.inv_dx2 + id2) * cn;
+      ce[h] = (g & 1u) ? ax : 0.f;
+      cw[h] = (g & 2u) ? ax : 0.f;
+      cnn[h] = (g & 4u) ? n1 : n0;
+      cs[h] = (g & 8u) ? s1 : s0;
     }
     kE[q] = make_float2(ce[0], ce[1]);
     nW[q] = make_float2(-cw[0], -cw[1]);
     kN[q] = make_float2(cnn[0], cnn[1]);
     nS[q] = make_float2(-cs[0], -cs[1]);
   }
+  const unsigned full = 0xffffffffu;
+  pdl_wait();  // u, v come from the preceding kernel
   // the lane's two columns as pairs: au[q] = (u[2l], u[2l+1]) of row q, av likewise
   float2 au[NB_R], av[NB_R];
 #pragma unroll
@@ -280,9 +245,28 @@ k_nu_tb(Dev d, const float* __restrict__ u, const float* __restrict__ v, float* 
   }
 }
 
+// Face gates of the nu_h Laplacian, one byte per point (built once per
+// solver): bit 0 east face (this cell and its east neighbour wet), bit 1
+// west, bit 2 north (inside the domain), bit 3 south.  Longitude wraps; the
+// closed walls have no face.
+__global__ void k_nu_gates(Dev d, unsigned char* __restrict__ gate) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (j >= d.ny || i >= d.P) return;
+  unsigned g = 0u;
+  if (i < d.nx && wetb(wb(d, j, i), k)) {
+    if (wetb(wb(d, j, east(d, i)), k)) g |= 1u;
+    if (wetb(wb(d, j, west(d, i)), k)) g |= 2u;
+    if (j < d.ny - 1 && wetb(wb(d, j + 1, i), k)) g |= 4u;
+    if (j > 0 && wetb(wb(d, j - 1, i), k)) g |= 8u;
+  }
+  gate[idx3(d, k, j, i)] = (unsigned char)g;
+}
+
 // Whole linear half step except the nu_h subcycles (timestepping/step.py:108-173,
 // legacy, mode split).  A block owns an LT_X x LT_Y tile of columns and marches
-// down LT_KC levels of them (the chunks of a column are separate blocks): u0,
+// down d.lt_kc levels of them (the chunks of a column are separate blocks): u0,
 // v0, T0, S0 of each level on the tile with a two-cell halo arrive in shared
 // memory by cp.async one level ahead, in LT_NB rotating buffers; the wet flags
 // are formed one level ahead from the cells' bitmasks, held in registers; the
@@ -294,7 +278,7 @@ k_nu_tb(Dev d, const float* __restrict__ u, const float* __restrict__ v, float* 
 // row is padded by itself in the reference.  Vertical diffusion takes the level
 // above from registers and the level below from the next buffer; then
 // land/ghost hold and the exact Coriolis rotation by f dt/2.
-constexpr int LT_X = 32, LT_Y = 8, LT_H = 2, LT_NB = 3, LT_KC = 10;
+constexpr int LT_X = 32, LT_Y = 8, LT_H = 2, LT_NB = 3;
 constexpr int LT_PX = LT_X + 2 * LT_H, LT_PY = LT_Y + 2 * LT_H;
 constexpr int LT_CELLS = LT_PX * LT_PY;
 static_assert(LT_CELLS <= 2 * LT_X * LT_Y, "two tile cells per thread at most");
@@ -377,12 +361,13 @@ __global__ void __launch_bounds__(LT_X * LT_Y, 4) k_lin_t(Dev d, const float* __
                                                          const float* __restrict__ S0, float* __restrict__ uo,
                                                          float* __restrict__ vo, float* __restrict__ To,
                                                          float* __restrict__ So, float dth) {
+  pdl_trigger();
   extern __shared__ float lt_smem[];
   LtTile& t = *reinterpret_cast<LtTile*>(lt_smem);
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = ty * LT_X + tx, nt = LT_X * LT_Y;
   const int i0 = blockIdx.x * LT_X, j0 = blockIdx.y * LT_Y;
-  const int k0 = blockIdx.z * LT_KC, k1 = min(d.nz, k0 + LT_KC);  // this block's levels
+  const int k0 = blockIdx.z * d.lt_kc, k1 = min(d.nz, k0 + d.lt_kc);  // this block's levels
   const int i = i0 + tx, j = j0 + ty;
   // threads outside the grid copy their tile cells, form their wet flags and
   // meet the barriers, nothing else
@@ -430,6 +415,7 @@ __global__ void __launch_bounds__(LT_X * LT_Y, 4) k_lin_t(Dev d, const float* __
       if (has1) pw[e1] = wetf(b1, k);
     }
   };
+  pdl_wait();  // the state comes from the preceding kernels
   issue(k0);
   issue(k0 + 1);
   wet_level(k0);
@@ -530,12 +516,12 @@ static_assert(sizeof(LtTile) <= 48 * 1024, "k_lin_t tile within the default dyna
 void launch_lin_t(cudaStream_t s, const Dev& d, const float* usub, const float* vsub, const float* u0,
                   const float* v0, const float* T0, const float* S0, float* uo, float* vo, float* To, float* So,
                   float dth, int implicit_v) {
-  const dim3 g((d.nx + LT_X - 1) / LT_X, (d.ny + LT_Y - 1) / LT_Y, (d.nz + LT_KC - 1) / LT_KC), b(LT_X, LT_Y);
+  const dim3 g((d.nx + LT_X - 1) / LT_X, (d.ny + LT_Y - 1) / LT_Y, (d.nz + d.lt_kc - 1) / d.lt_kc), b(LT_X, LT_Y);
   const int key = (d.nu_bi > 0.f ? 4 : 0) | (d.kappa_bi > 0.f ? 2 : 0) | (implicit_v ? 1 : 0);
   const size_t sm = sizeof(LtTile);
 #define ZM_LIN(K, UV, TS, IM)                                                                       \
   case K:                                                                                           \
-    k_lin_t<UV, TS, IM><<<g, b, sm, s>>>(d, usub, vsub, u0, v0, T0, S0, uo, vo, To, So, dth);       \
+    (void)launch_pdl(k_lin_t<UV, TS, IM>, g, b, sm, s, d, usub, vsub, u0, v0, T0, S0, uo, vo, To, So, dth); \
     break;
   switch (key) {
     ZM_LIN(0, false, false, false)
@@ -552,164 +538,269 @@ void launch_lin_t(cudaStream_t s, const Dev& d, const float* usub, const float* 
 
 // Backward-Euler vertical diffusion (extension: the implicit replacement of
 // the explicit L-step vertical diffusion).  The matrix is (I - s D2) with D2
-// the node-form operator of d2z on the wet levels 0..kbot (ghost fill below);
-// Thomas algorithm in FP32 plus one step of iterative refinement, residual
-// formed in FP32 against the original right-hand side.  Rows below the
-// deepest wet level are untouched.
-__device__ __forceinline__ void vcoef(const Dev& d, int k, int kb, float s, float& a, float& b, float& c) {
-  a = 0.f; c = 0.f; b = 1.f;
-  if (k == 0) { b += s * d.vc.d2_top; c = -s * d.vc.d2_top; return; }
-  if (k == d.nz - 1) { a = -s * d.vc.d2_bot; b += s * d.vc.d2_bot; return; }
-  a = -s * d.vc.d2_lo[k];
-  b += s * (d.vc.d2_lo[k] + d.vc.d2_hi[k]);
-  if (k < kb) c = -s * d.vc.d2_hi[k]; else b -= s * d.vc.d2_hi[k];
-}
+// the node-form operator of d2z on the wet levels 0..kbot (ghost fill below)
+// for u, v (nu_v) and T, S (kappa_v + coastal), or, with the learned closure,
+// the interface-flux operator with its diffusivity per interface for T and S.
+// Rows below the deepest wet level are identity rows (the value passes
+// through), as are all rows of a column with fewer than two wet levels.
+//
+// One warp solves one column's system for a pair of fields that share the
+// matrix (u and v, or T and S): lane l holds rows l and l + 32 (nz <= 64,
+// rows past nz are identity rows), and the system is reduced by parallel
+// cyclic reduction in six shuffle steps of distance 1, 2, ..., 32, each row
+// eliminating its neighbours at that distance, until every row is decoupled;
+// the solution is d / b.  One step of iterative refinement follows: the
+// residual r - A x of the FP32 solution against the original right-hand side
+// (neighbours by shuffle) is reduced with the elimination factors kept from
+// the first pass, and its solution is added.  The matrices are M-matrices
+// (diagonally dominant), which parallel cyclic reduction keeps at every step.
+// A block holds VP_C columns of one latitude row: their four fields (and the
+// closure's diffusivity) are loaded into shared memory with the columns
+// fastest (one sector of each level per field), the warps solve from there,
+// and the block writes the results back the same way, with the land hold and
+// the exact Coriolis rotation of u, v.
+constexpr int VP_C = 8;                  // columns per block
+constexpr int VP_T = 2 * VP_C * 32;      // one warp per (column, field pair)
+constexpr int VP_LD = VP_C + 1;          // shared row pitch
 
-// One thread per (column, field); lanes 2c and 2c+1 hold u and v (blockIdx.z
-// = 0: nu_v, node form of d2z with the ghost fill, then the land hold and the
-// exact Coriolis rotation, which swaps values within the lane pair) or T and S
-// (blockIdx.z = 1: kappa_v + coastal in the node form, or the learned
-// closure's diffusivity per interface kap3 in the interface-flux form, then
-// the land hold).  Each thread runs its own sequential Thomas sweeps (the two
-// fields of a pair repeat the same pivots).  The sweeps are latency-bound, so
-// the kernel is held to 32 registers for full occupancy: more independent
-// column chains in flight per SM outweigh a few spilled scalars and the
-// per-thread level arrays in local memory.  Passes over the n = kbot + 1 wet
-// levels:
-//   1. forward elimination, keeping 1 / pivot;
-//   2. back substitution: the FP32 solution x;
-//   3. the residual r - A x (r read again) and its forward elimination;
-//   4. back substitution of the correction e; x + e, hold, rotation, store.
-// The factor up / pivot is formed again where it is needed.
+struct VpTile {
+  float f[4][64][VP_LD];                 // u, v, T, S: right-hand sides in, solutions out
+  float kap[64][VP_LD];                  // closure diffusivity per interface (KAP)
+  float lo[64], hi[64], idzi[64], idzn[64];
+};
+
 template <bool KAP>
-__global__ void __launch_bounds__(IV_T, 32) k_implicit_vdiff(Dev d, float* __restrict__ u, float* __restrict__ v,
-                                                        float* __restrict__ T, float* __restrict__ S,
-                                                        const float* __restrict__ u0, const float* __restrict__ v0,
-                                                        const float* __restrict__ T0, const float* __restrict__ S0,
-                                                        float dth, const float* __restrict__ kap3) {
-  const int f = threadIdx.x & 1;
-  const int i = blockIdx.x * (IV_T / 2) + (threadIdx.x >> 1);
-  const int j = blockIdx.y;
-  const bool tracers = blockIdx.z == 1;
-  const bool in = i < d.nx;  // lanes past the last column run along (the pair exchange needs every lane) unstored
-  const long long base = idx2(d, j, in ? i : d.nx - 1);
-  float* __restrict__ fld = tracers ? (f ? S : T) : (f ? v : u);
-  const float* __restrict__ hold = tracers ? (f ? S0 : T0) : (f ? v0 : u0);
-  const bool kap = KAP && tracers;  // the u, v blocks of a closure launch keep nu_v
-  const uint64_t bits = wb(d, j, in ? i : d.nx - 1);
-  const int kb = kbot_of(bits);
-  const int n = kb > 0 && wetb(bits, 0) ? kb + 1 : 0;
-  const float sc = tracers ? __ldg(d.kv2 + base) * dth : d.nu_v * dth;
-  const long long pl = d.plane;
-  float x[ZM_MAXZ], inv[ZM_MAXZ], e[ZM_MAXZ], kq[KAP ? ZM_MAXZ : 1];
-  for (int k = 0; k < n; ++k) {
-    x[k] = fld[base + k * pl];
-    if (KAP && kap && k + 1 < n) kq[k] = __ldg(kap3 + base + k * pl);
+__global__ void __launch_bounds__(VP_T) k_vdiff_pcr(Dev d, float* __restrict__ u, float* __restrict__ v,
+                                                    float* __restrict__ T, float* __restrict__ S,
+                                                    const float* __restrict__ u0, const float* __restrict__ v0,
+                                                    const float* __restrict__ T0, const float* __restrict__ S0,
+                                                    float dth, const float* __restrict__ kap3) {
+  __shared__ VpTile t;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int i0 = blockIdx.x * VP_C, j = blockIdx.y;
+  const int nz = d.nz;
+  for (int e = tid; e < 64; e += VP_T) {
+    const bool in = e < nz;
+    t.lo[e] = in ? d.vc.d2_lo[e] : 0.f;
+    t.hi[e] = in ? d.vc.d2_hi[e] : 0.f;
+    t.idzi[e] = in ? d.vc.inv_dz_iface[e] : 0.f;
+    t.idzn[e] = in ? d.vc.inv_dz_node[e] : 0.f;
   }
-  // tridiagonal row k: lower lo, diagonal dg, upper up
-  auto row = [&](int k, float& lo, float& dg, float& up) {
-    if (KAP && kap) {
-      lo = k > 0 ? -dth * kq[k - 1] * d.vc.inv_dz_iface[k - 1] * d.vc.inv_dz_node[k] : 0.f;
-      up = k + 1 < n ? -dth * kq[k] * d.vc.inv_dz_iface[k] * d.vc.inv_dz_node[k] : 0.f;
-      dg = 1.f - lo - up;
-    } else {
-      vcoef(d, k, kb, sc, lo, dg, up);
-    }
-  };
-  // 1. forward elimination (lo = 0 in row 0, so its pivot is dg)
-  {
-    float cpp = 0.f, y = 0.f;
-    for (int k = 0; k < n; ++k) {
-      float lo, dg, up;
-      row(k, lo, dg, up);
-      const float iv = 1.f / (dg - lo * cpp);
-      cpp = up * iv;
-      y = (x[k] - lo * y) * iv;
-      x[k] = y;
-      inv[k] = iv;
+  // the block's columns, level-major with the columns fastest; rows past nz are zero
+  for (int e = tid; e < 4 * 64 * VP_C; e += VP_T) {
+    const int f = e / (64 * VP_C), rem = e - f * 64 * VP_C, k = rem / VP_C, c = rem - k * VP_C;
+    const int col = i0 + c;
+    const float* src = f == 0 ? u : (f == 1 ? v : (f == 2 ? T : S));
+    t.f[f][k][c] = (k < nz && col < d.nx) ? src[(long long)k * d.plane + idx2(d, j, col)] : 0.f;
+  }
+  if (KAP) {
+    for (int e = tid; e < 64 * VP_C; e += VP_T) {
+      const int k = e / VP_C, c = e - k * VP_C, col = i0 + c;
+      t.kap[k][c] = (k + 1 < nz && col < d.nx) ? __ldg(kap3 + (long long)k * d.plane + idx2(d, j, col)) : 0.f;
     }
   }
-  // 2. back substitution
-  for (int k = n - 2; k >= 0; --k) {
-    float lo, dg, up;
-    row(k, lo, dg, up);
-    x[k] -= (up * inv[k]) * x[k + 1];
-  }
-  // 3. residual of the FP32 solution, eliminated with the same factorization
-  {
-    float ep = 0.f, xm = 0.f, x0 = n > 0 ? x[0] : 0.f;
-    for (int k = 0; k < n; ++k) {
-      float lo, dg, up;
-      row(k, lo, dg, up);
-      const float xp = k + 1 < n ? x[k + 1] : 0.f;
-      float a = dg * x0;
-      if (k > 0) a += lo * xm;
-      if (k + 1 < n) a += up * xp;
-      ep = ((fld[base + k * pl] - a) - lo * ep) * inv[k];
-      e[k] = ep;
-      xm = x0;
-      x0 = xp;
-    }
-  }
-  // 4. back substitution of the correction; x + e, land hold, rotation
-  const float rc = tracers ? 0.f : __ldg(d.rot_c + base), rs = tracers ? 0.f : __ldg(d.rot_s + base);
-  float en = 0.f;
-  for (int k = d.nz - 1; k >= 0; --k) {
-    const long long id = base + k * pl;
-    const bool wet = wetb(bits, k);
-    float val = 0.f;
-    if (k < n) {
-      float ek = e[k];
-      if (k + 1 < n) {
-        float lo, dg, up;
-        row(k, lo, dg, up);
-        ek -= (up * inv[k]) * en;
+  __syncthreads();
+  const int c = warp % VP_C, sys = warp / VP_C;  // sys 0: u, v; 1: T, S
+  const int col = i0 + c;
+  if (col < d.nx) {
+    const int base = idx2(d, j, col);
+    const uint64_t bits = __ldg(d.wbits + base);
+    const int kb = kbot_of(bits);
+    const int n = (kb > 0 && wetb(bits, 0)) ? kb + 1 : 0;
+    const bool kap = KAP && sys == 1;
+    const float sc = sys ? __ldg(d.kv2 + base) * dth : d.nu_v * dth;
+    // row r of the system: lower a, diagonal b, upper c (identity beyond n)
+    auto row = [&](int r, float& a, float& b, float& cc) {
+      a = 0.f; b = 1.f; cc = 0.f;
+      if (r >= n) return;
+      if (kap) {
+        a = r > 0 ? -dth * t.kap[r - 1][c] * t.idzi[r - 1] * t.idzn[r] : 0.f;
+        cc = r + 1 < n ? -dth * t.kap[r][c] * t.idzi[r] * t.idzn[r] : 0.f;
+        b = 1.f - a - cc;
+      } else if (r == 0) {
+        b += sc * d.vc.d2_top;
+        cc = -sc * d.vc.d2_top;
+      } else if (r == nz - 1) {
+        a = -sc * d.vc.d2_bot;
+        b += sc * d.vc.d2_bot;
+      } else {
+        a = -sc * t.lo[r];
+        b += sc * (t.lo[r] + t.hi[r]);
+        if (r < kb) cc = -sc * t.hi[r];
+        else b -= sc * t.hi[r];
       }
-      en = ek;
-      val = x[k] + ek;
-    } else if (!tracers && wet) {
-      val = fld[id];
+    };
+    float a[2], b[2], cc[2], dA[2], dB[2], a0[2], b0[2], c0[2], rA[2], rB[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int r = lane + 32 * h;
+      row(r, a[h], b[h], cc[h]);
+      a0[h] = a[h];
+      b0[h] = b[h];
+      c0[h] = cc[h];
+      rA[h] = dA[h] = t.f[2 * sys][r][c];
+      rB[h] = dB[h] = t.f[2 * sys + 1][r][c];
     }
-    if (!wet) val = ld(hold, id);
-    if (tracers) {
-      if (in && (k < n || !wet)) fld[id] = val;
-    } else {
-      const float other = __shfl_xor_sync(0xffffffffu, val, 1);
-      const float uu = f ? other : val, vv = f ? val : other;
-      if (in) fld[id] = f ? -rs * uu + rc * vv : rc * uu + rs * vv;
+    const unsigned full = 0xffffffffu;
+    float K1[6][2], K2[6][2];
+#pragma unroll
+    for (int st = 0; st < 6; ++st) {
+      const int dd = 1 << st;
+      const int lp = (lane + dd) & 31, lm = (lane - dd) & 31;
+      const bool up0 = lane + dd < 32;  // row lane + dd lies in slot 0
+      const bool dn = lane >= dd;       // row lane - dd lies in slot 0
+      float qa[2][2], qb[2][2], qc[2][2], qA[2][2], qB[2][2];  // [slot][+, -] at distance dd
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        qa[h][0] = __shfl_sync(full, a[h], lp);
+        qb[h][0] = __shfl_sync(full, b[h], lp);
+        qc[h][0] = __shfl_sync(full, cc[h], lp);
+        qA[h][0] = __shfl_sync(full, dA[h], lp);
+        qB[h][0] = __shfl_sync(full, dB[h], lp);
+        qa[h][1] = __shfl_sync(full, a[h], lm);
+        qb[h][1] = __shfl_sync(full, b[h], lm);
+        qc[h][1] = __shfl_sync(full, cc[h], lm);
+        qA[h][1] = __shfl_sync(full, dA[h], lm);
+        qB[h][1] = __shfl_sync(full, dB[h], lm);
+      }
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        // rows r + dd (p) and r - dd (m) of this slot; identity rows outside 0..63.
+        // Slot 0: r + dd is in slot 0 of lane l + dd, or slot 1 of lane
+        // l + dd - 32; r - dd in slot 0 of lane l - dd, or outside.  Slot 1:
+        // r + dd in slot 1 of lane l + dd, or outside; r - dd in slot 1 of
+        // lane l - dd, or slot 0 of lane l - dd + 32.
+        const bool has_p = h == 0 || up0, has_m = h == 1 || dn;
+        const bool p1 = h == 1 || !up0, m1 = h == 1 && dn;  // the neighbour sits in slot 1
+        const float ap = has_p ? (p1 ? qa[1][0] : qa[0][0]) : 0.f;
+        const float bp = has_p ? (p1 ? qb[1][0] : qb[0][0]) : 1.f;
+        const float cp = has_p ? (p1 ? qc[1][0] : qc[0][0]) : 0.f;
+        const float Ap = has_p ? (p1 ? qA[1][0] : qA[0][0]) : 0.f;
+        const float Bp = has_p ? (p1 ? qB[1][0] : qB[0][0]) : 0.f;
+        const float am = has_m ? (m1 ? qa[1][1] : qa[0][1]) : 0.f;
+        const float bm = has_m ? (m1 ? qb[1][1] : qb[0][1]) : 1.f;
+        const float cm = has_m ? (m1 ? qc[1][1] : qc[0][1]) : 0.f;
+        const float Am = has_m ? (m1 ? qA[1][1] : qA[0][1]) : 0.f;
+        const float Bm = has_m ? (m1 ? qB[1][1] : qB[0][1]) : 0.f;
+        const float k1 = a[h] / bm, k2 = cc[h] / bp;
+        K1[st][h] = k1;
+        K2[st][h] = k2;
+        b[h] = b[h] - cm * k1 - ap * k2;
+        a[h] = -am * k1;
+        cc[h] = -cp * k2;
+        dA[h] = dA[h] - Am * k1 - Ap * k2;
+        dB[h] = dB[h] - Bm * k1 - Bp * k2;
+      }
     }
+    float xA[2], xB[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      xA[h] = dA[h] / b[h];
+      xB[h] = dB[h] / b[h];
+    }
+    // one refinement step: residual of the FP32 solution, reduced with the same factors
+    {
+      const int lp = (lane + 1) & 31, lm = (lane - 1) & 31;
+      float nA[2][2], nB[2][2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        nA[h][0] = __shfl_sync(full, xA[h], lp);
+        nB[h][0] = __shfl_sync(full, xB[h], lp);
+        nA[h][1] = __shfl_sync(full, xA[h], lm);
+        nB[h][1] = __shfl_sync(full, xB[h], lm);
+      }
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        // x[r + 1], x[r - 1] (rows past the ends carry zero coefficients)
+        const float pA = (h == 0 && lane == 31) ? nA[1][0] : nA[h][0];
+        const float pB = (h == 0 && lane == 31) ? nB[1][0] : nB[h][0];
+        const float mA = (h == 1 && lane == 0) ? nA[0][1] : nA[h][1];
+        const float mB = (h == 1 && lane == 0) ? nB[0][1] : nB[h][1];
+        dA[h] = rA[h] - (a0[h] * mA + b0[h] * xA[h] + c0[h] * pA);
+        dB[h] = rB[h] - (a0[h] * mB + b0[h] * xB[h] + c0[h] * pB);
+      }
+    }
+#pragma unroll
+    for (int st = 0; st < 6; ++st) {
+      const int dd = 1 << st;
+      const int lp = (lane + dd) & 31, lm = (lane - dd) & 31;
+      const bool up0 = lane + dd < 32;
+      const bool dn = lane >= dd;
+      float qA[2][2], qB[2][2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        qA[h][0] = __shfl_sync(full, dA[h], lp);
+        qB[h][0] = __shfl_sync(full, dB[h], lp);
+        qA[h][1] = __shfl_sync(full, dA[h], lm);
+        qB[h][1] = __shfl_sync(full, dB[h], lm);
+      }
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const bool has_p = h == 0 || up0, has_m = h == 1 || dn;
+        const bool p1 = h == 1 || !up0, m1 = h == 1 && dn;
+        const float Ap = has_p ? (p1 ? qA[1][0] : qA[0][0]) : 0.f;
+        const float Bp = has_p ? (p1 ? qB[1][0] : qB[0][0]) : 0.f;
+        const float Am = has_m ? (m1 ? qA[1][1] : qA[0][1]) : 0.f;
+        const float Bm = has_m ? (m1 ? qB[1][1] : qB[0][1]) : 0.f;
+        dA[h] = dA[h] - Am * K1[st][h] - Ap * K2[st][h];
+        dB[h] = dB[h] - Bm * K1[st][h] - Bp * K2[st][h];
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int r = lane + 32 * h;
+      t.f[2 * sys][r][c] = xA[h] + dA[h] / b[h];
+      t.f[2 * sys + 1][r][c] = xB[h] + dB[h] / b[h];
+    }
+  }
+  __syncthreads();
+  // write back: land hold on dry levels, exact rotation of u, v by f dt/2
+  for (int e = tid; e < nz * VP_C; e += VP_T) {
+    const int k = e / VP_C, cq = e - k * VP_C, cl = i0 + cq;
+    if (cl >= d.nx) continue;
+    const int base = idx2(d, j, cl);
+    const long long id = (long long)k * d.plane + base;
+    const bool wet = wetb(__ldg(d.wbits + base), k);
+    const float uu = wet ? t.f[0][k][cq] : ld(u0, id), vv = wet ? t.f[1][k][cq] : ld(v0, id);
+    const float rc = __ldg(d.rot_c + base), rs = __ldg(d.rot_s + base);
+    u[id] = rc * uu + rs * vv;
+    v[id] = -rs * uu + rc * vv;
+    T[id] = wet ? t.f[2][k][cq] : ld(T0, id);
+    S[id] = wet ? t.f[3][k][cq] : ld(S0, id);
   }
 }
 
 void launch_implicit_vdiff(cudaStream_t s, const Dev& d, float* u, float* v, float* T, float* S, const float* u0,
                            const float* v0, const float* T0, const float* S0, float dth, const float* kap3) {
-  const dim3 g((d.nx + IV_T / 2 - 1) / (IV_T / 2), d.ny, 2);
-  if (kap3) k_implicit_vdiff<true><<<g, IV_T, 0, s>>>(d, u, v, T, S, u0, v0, T0, S0, dth, kap3);
-  else k_implicit_vdiff<false><<<g, IV_T, 0, s>>>(d, u, v, T, S, u0, v0, T0, S0, dth, kap3);
+  const dim3 g((d.nx + VP_C - 1) / VP_C, d.ny);
+  if (kap3) k_vdiff_pcr<true><<<g, VP_T, 0, s>>>(d, u, v, T, S, u0, v0, T0, S0, dth, kap3);
+  else k_vdiff_pcr<false><<<g, VP_T, 0, s>>>(d, u, v, T, S, u0, v0, T0, S0, dth, kap3);
 }
 
 // ------------------------------------------------------------------ transport
 // Interface volume transport Fz[k] = sum_{m>=k} div_h[m] dz_node[m]
 // (dynamics/transport.py:110-133 with the face-flux divergence of
 // numerics/horizontal.py:255-281); Fz[nz] = 0 is implicit.  A block owns a
-// FZ_X x FZ_Y tile of columns and marches up from the bottom level: each
+// FZ_X x RY tile of columns (RY = d.fz_rows) and marches up from the bottom level: each
 // level's u and v on the tile and a one-cell halo arrive in shared memory by
 // cp.async, FZ_NB - 1 levels ahead, so each value is fetched once; one column
 // per thread accumulates the sum.
-constexpr int FZ_X = 32, FZ_Y = 4, FZ_NB = 4;  // tile columns, tile rows, level buffers
-constexpr int FZ_PX = FZ_X + 2, FZ_PY = FZ_Y + 2;
-constexpr int FZ_CELLS = FZ_PX * FZ_PY;
-static_assert(FZ_CELLS <= 2 * FZ_X * FZ_Y, "two tile cells per thread at most");
+constexpr int FZ_X = 32, FZ_NB = 4;  // tile columns, level buffers
+constexpr int FZ_PX = FZ_X + 2;
 
-__global__ void __launch_bounds__(FZ_X * FZ_Y) k_fz(Dev d, const float* __restrict__ u, const float* __restrict__ v,
+template <int RY>
+__global__ void __launch_bounds__(FZ_X * RY) k_fz(Dev d, const float* __restrict__ u, const float* __restrict__ v,
                                                     float* __restrict__ Fz) {
+  constexpr int FZ_PY = RY + 2, FZ_CELLS = FZ_PX * FZ_PY;
+  static_assert(FZ_CELLS <= 2 * FZ_X * RY, "two tile cells per thread at most");
+  pdl_trigger();
   __shared__ float su[FZ_NB][FZ_PY][FZ_PX], sv[FZ_NB][FZ_PY][FZ_PX];
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * FZ_X + tx;
-  const int i0 = blockIdx.x * FZ_X, j0 = blockIdx.y * FZ_Y;
+  const int i0 = blockIdx.x * FZ_X, j0 = blockIdx.y * RY;
   const int i = i0 + tx, j = j0 + ty;
   // threads outside the grid copy their tile cells and meet the barriers, nothing else
   const bool in = i < d.nx && j < d.ny;
-  const int e0 = tid, e1 = tid + FZ_X * FZ_Y;
+  const int e0 = tid, e1 = tid + FZ_X * RY;
   const bool has1 = e1 < FZ_CELLS;
   const int s0 = tile_cell<FZ_PX>(d, e0, i0, j0), s1 = has1 ? tile_cell<FZ_PX>(d, e1, i0, j0) : 0;
   auto issue = [&](int q) {  // the q-th level from the bottom into buffer q % FZ_NB; one commit group per call
@@ -735,6 +826,7 @@ __global__ void __launch_bounds__(FZ_X * FZ_Y) k_fz(Dev d, const float* __restri
   const float cf_n = __ldg(d.cfp + jc), cf_s = jc > 0 ? __ldg(d.cfp + jc - 1) : 0.f;
   const float yscale = d.inv_dy * __ldg(d.inv_cos + jc);
   float acc = 0.f;
+  pdl_wait();  // u, v come from the preceding kernel
 #pragma unroll
   for (int q = 0; q < FZ_NB - 1; ++q) issue(q);
   const int r = ty + 1, c = tx + 1;
@@ -759,7 +851,10 @@ __global__ void __launch_bounds__(FZ_X * FZ_Y) k_fz(Dev d, const float* __restri
 }
 
 void launch_fz(cudaStream_t s, const Dev& d, const float* u, const float* v, float* Fz) {
-  k_fz<<<dim3((d.nx + FZ_X - 1) / FZ_X, (d.ny + FZ_Y - 1) / FZ_Y), dim3(FZ_X, FZ_Y), 0, s>>>(d, u, v, Fz);
+  if (d.fz_rows == 8)
+    (void)launch_pdl(k_fz<8>, dim3((d.nx + FZ_X - 1) / FZ_X, (d.ny + 7) / 8), dim3(FZ_X, 8), 0, s, d, u, v, Fz);
+  else
+    (void)launch_pdl(k_fz<4>, dim3((d.nx + FZ_X - 1) / FZ_X, (d.ny + 3) / 4), dim3(FZ_X, 4), 0, s, d, u, v, Fz);
 }
 
 // Raw advective-form momentum advection -(u d/dx + v d/dy + w d/dz) of u and
@@ -815,11 +910,13 @@ __device__ __forceinline__ void adv_point(const Dev& d, const float* __restrict_
 __global__ void __launch_bounds__(256) k_madv(Dev d, const float* __restrict__ u, const float* __restrict__ v,
                                               const float* __restrict__ Fz, float* __restrict__ Ayu,
                                               float* __restrict__ Ayv) {
+  pdl_trigger();
   __shared__ float su[MADV_TY + 4][32];
   __shared__ float sv[MADV_TY + 4][32];
   const int i = blockIdx.x * 32 + threadIdx.x;
   const int j0 = blockIdx.y * MADV_TY;
   const int k = blockIdx.z;
+  pdl_wait();  // u, v, Fz come from the preceding kernels
   for (int r = threadIdx.y; r < MADV_TY + 4; r += blockDim.y) {
     int jj = j0 - 2 + r;
     jj = jj < 0 ? 0 : (jj >= d.ny ? d.ny - 1 : jj);
@@ -857,7 +954,7 @@ __device__ __forceinline__ float minmod_slope(float cm, float c0, float cp, floa
 
 // Tracer advection substep (dynamics/tendencies.py:111-140 with
 // _advection_scalar, dynamics/transport.py:365-475).  A block owns a
-// TA_X x TA_Y tile of columns and marches down TA_KC levels of them (the
+// TA_X x TA_Y tile of columns and marches down d.ta_kc levels of them (the
 // chunks of a column are separate blocks, so the grid fills the GPU in even
 // waves): T, S, u, v of each
 // level on the tile with a two-cell halo (for the minmod slopes of the face
@@ -868,7 +965,7 @@ __device__ __forceinline__ float minmod_slope(float cm, float c0, float cp, floa
 // from registers and the level below from the next buffer.  Rows beyond the
 // closed walls are loaded from the clamped row, which is the edge padding of
 // transport.py:199-290; longitude wraps.
-constexpr int TA_H = 2, TA_NB = 3, TA_KC = 10;
+constexpr int TA_H = 2, TA_NB = 3;
 constexpr int TA_PX = TA_X + 2 * TA_H, TA_PY = TA_Y + 2 * TA_H;
 constexpr int TA_CELLS = TA_PX * TA_PY;
 static_assert(TA_CELLS <= 2 * TA_X * TA_Y, "two tile cells per thread at most");
@@ -949,6 +1046,7 @@ __global__ void __launch_bounds__(TA_X * TA_Y, 5) k_tracer_adv_t(Dev d, const fl
                                                                  float dts, int first, int last,
                                                                  float* __restrict__ topT,
                                                                  float* __restrict__ topS) {
+  pdl_trigger();
   __shared__ TaTile t;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TA_X + tx;
   const int i0 = blockIdx.x * TA_X, j0 = blockIdx.y * TA_Y;
@@ -960,7 +1058,7 @@ __global__ void __launch_bounds__(TA_X * TA_Y, 5) k_tracer_adv_t(Dev d, const fl
   const bool has1 = e1 < TA_CELLS;
   const int s0 = tile_cell<TA_PX, TA_H>(d, e0, i0, j0), s1 = has1 ? tile_cell<TA_PX, TA_H>(d, e1, i0, j0) : 0;
   const uint64_t b0 = __ldg(d.wbits + s0), b1 = has1 ? __ldg(d.wbits + s1) : 0ull;
-  const int k0 = blockIdx.z * TA_KC, k1 = min(d.nz, k0 + TA_KC);  // this block's levels
+  const int k0 = blockIdx.z * d.ta_kc, k1 = min(d.nz, k0 + d.ta_kc);  // this block's levels
   auto issue = [&](int k) {  // level k into buffer k % TA_NB; one commit group per call
     if (k < d.nz && k <= k1) {  // level k1 only for the column neighbour below the chunk
       const long long off = (long long)k * d.plane;
@@ -985,6 +1083,7 @@ __global__ void __launch_bounds__(TA_X * TA_Y, 5) k_tracer_adv_t(Dev d, const fl
       if (has1) pw[e1] = wetf(b1, k);
     }
   };
+  pdl_wait();  // the tracers, velocities and Fz come from the preceding kernels
   issue(k0);
   issue(k0 + 1);
   wet_level(k0);
@@ -1061,13 +1160,9 @@ __global__ void __launch_bounds__(TA_X * TA_Y, 5) k_tracer_adv_t(Dev d, const fl
 void launch_tracer_adv(cudaStream_t s, const Dev& d, const float* T, const float* S, const float* u, const float* v,
                        const float* Fz, float* accT, float* accS, float* Tn, float* Sn, float dts, int first, int last,
                        float* topT, float* topS) {
-  const dim3 g((d.nx + TA_X - 1) / TA_X, (d.ny + TA_Y - 1) / TA_Y, (d.nz + TA_KC - 1) / TA_KC), b(TA_X, TA_Y);
-  if (d.limiter == 2)
-    k_tracer_adv_t<2><<<g, b, 0, s>>>(d, T, S, u, v, Fz, accT, accS, Tn, Sn, dts, first, last, topT, topS);
-  else if (d.limiter == 1)
-    k_tracer_adv_t<1><<<g, b, 0, s>>>(d, T, S, u, v, Fz, accT, accS, Tn, Sn, dts, first, last, topT, topS);
-  else
-    k_tracer_adv_t<0><<<g, b, 0, s>>>(d, T, S, u, v, Fz, accT, accS, Tn, Sn, dts, first, last, topT, topS);
+  const dim3 g((d.nx + TA_X - 1) / TA_X, (d.ny + TA_Y - 1) / TA_Y, (d.nz + d.ta_kc - 1) / d.ta_kc), b(TA_X, TA_Y);
+  auto kern = d.limiter == 2 ? k_tracer_adv_t<2> : (d.limiter == 1 ? k_tracer_adv_t<1> : k_tracer_adv_t<0>);
+  (void)launch_pdl(kern, g, b, 0, s, d, T, S, u, v, Fz, accT, accS, Tn, Sn, dts, first, last, topT, topS);
 }
 
 // Temperature-term decomposition of a state (dynamics/tendencies.py:74-92,
@@ -1223,11 +1318,13 @@ __device__ __forceinline__ void rest_store(const Dev& d, const RestArgs& a, long
 
 template <bool ST2>
 __global__ void __launch_bounds__(128) k_tracer_rest(Dev d, RestArgs a) {
+  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= d.nx || j >= d.ny) return;
   const long long base = idx2(d, j, i);
   const uint64_t bits = wb(d, j, i);
+  pdl_wait();  // the evaluation state and the advection rates come from the preceding kernels
   const int nz = d.nz;
   // static-instability gates of the evaluation state, in difference form:
   // rho[m] > rho[m+1]  <=>  beta (S[m]-S[m+1]) > alpha (T[m]-T[m+1]).
@@ -1355,8 +1452,7 @@ __global__ void __launch_bounds__(128) k_tracer_rest(Dev d, RestArgs a) {
 
 // The RK stage is a template argument (stage 2 also reads dT1, dS1).
 void launch_tracer_rest(dim3 g, dim3 b, cudaStream_t s, const Dev& d, const RestArgs& a) {
-  if (a.stage == 1) k_tracer_rest<false><<<g, b, 0, s>>>(d, a);
-  else k_tracer_rest<true><<<g, b, 0, s>>>(d, a);
+  (void)launch_pdl(a.stage == 1 ? k_tracer_rest<false> : k_tracer_rest<true>, g, b, 0, s, d, a);
 }
 
 // ------------------------------------------------------------------ pressure
@@ -1380,7 +1476,7 @@ __device__ __forceinline__ float drho(const Dev& d, float Ta, float Sa, float wa
 // in differences), one column per thread.  Modes: 0 the barotropic forcing
 // F_rho and the depth-mean velocity; 1 and 2 the P part of the momentum
 // residual with the RK combination of the first and second stage.  A block
-// owns a PG_X x PG_Y tile of columns and marches down the levels together:
+// owns a PG_X x RY tile of columns (RY = d.pg_rows) and marches down the levels together:
 // each level's T and S on the tile and a one-cell halo (rows clamped at the
 // closed walls like north()/south(), longitude wrapped like east()/west())
 // arrive in shared memory by cp.async, PG_NB - 1 levels ahead of the one being
@@ -1388,22 +1484,23 @@ __device__ __forceinline__ float drho(const Dev& d, float Ta, float Sa, float wa
 // the arithmetic.  Each thread keeps its column's density differences to the
 // four neighbours and their downward accumulation in registers.  Modes 1 and
 // 2 need the depth integral before the first output level, so the per-level
-// gradient goes to a scratch field (read back by the same thread, normally
-// from L2).
-constexpr int PG_X = 32, PG_Y = 4, PG_NB = 4;  // tile columns, tile rows, level buffers
-constexpr int PG_PX = PG_X + 2, PG_PY = PG_Y + 2;
-constexpr int PG_CELLS = PG_PX * PG_PY;
-static_assert(PG_CELLS <= 2 * PG_X * PG_Y, "two tile cells per thread at most");
+// gradient goes to a scratch field and the depth mean to a 2-D one; the
+// output pass over all points is k_pgf_out.
+constexpr int PG_X = 32, PG_NB = 4;  // tile columns, level buffers
+constexpr int PG_PX = PG_X + 2;
 
-template <int MODE>
-__global__ void __launch_bounds__(PG_X * PG_Y) k_pgf(Dev d, PgfArgs a) {
+template <int MODE, int RY>
+__global__ void __launch_bounds__(PG_X * RY) k_pgf(Dev d, PgfArgs a) {
+  constexpr int PG_PY = RY + 2, PG_CELLS = PG_PX * PG_PY;
+  static_assert(PG_CELLS <= 2 * PG_X * RY, "two tile cells per thread at most");
+  pdl_trigger();
   __shared__ float sT[PG_NB][PG_PY][PG_PX], sS[PG_NB][PG_PY][PG_PX];
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * PG_X + tx;
-  const int i0 = blockIdx.x * PG_X, j0 = blockIdx.y * PG_Y;
+  const int i0 = blockIdx.x * PG_X, j0 = blockIdx.y * RY;
   const int i = i0 + tx, j = j0 + ty;
   // threads outside the grid copy their tile cells and meet the barriers, nothing else
   const bool in = i < d.nx && j < d.ny;
-  const int e0 = tid, e1 = tid + PG_X * PG_Y;
+  const int e0 = tid, e1 = tid + PG_X * RY;
   const bool has1 = e1 < PG_CELLS;
   const int s0 = tile_cell<PG_PX>(d, e0, i0, j0), s1 = has1 ? tile_cell<PG_PX>(d, e1, i0, j0) : 0;
   auto issue = [&](int k) {  // level k into buffer k % PG_NB; one commit group per call
@@ -1432,6 +1529,7 @@ __global__ void __launch_bounds__(PG_X * PG_Y) k_pgf(Dev d, PgfArgs a) {
   float pe = 0.f, pw = 0.f, pn = 0.f, ps = 0.f;       // p[e]-p[c], p[c]-p[w], p[n]-p[c], p[c]-p[s]
   float de0 = 0.f, dw0 = 0.f, dn0 = 0.f, ds0 = 0.f;   // density differences at the level above
   float gx_prev = 0.f, gy_prev = 0.f, fx = 0.f, fy = 0.f;
+  pdl_wait();  // T, S and the momentum parts come from the preceding kernels
 #pragma unroll
   for (int q = 0; q < PG_NB - 1; ++q) issue(q);
   const int r = ty + 1, c = tx + 1;
@@ -1489,52 +1587,83 @@ __global__ void __launch_bounds__(PG_X * PG_Y) k_pgf(Dev d, PgfArgs a) {
     a.vbt0[cc] = sv;
     return;
   }
-  // second pass; the next level's inputs are loaded before this level's
-  // stores (the argument pointers may alias, so later loads would wait)
-  constexpr bool m2 = MODE == 2;
-  float qx = a.gsx[cc], qy = a.gsy[cc], qAu = ld(a.Au, cc), qAv = ld(a.Av, cc), qu = ld(a.u1, cc), qv = ld(a.v1, cc);
-  float qpu = m2 ? ld(a.Ppu, cc) : 0.f, qpv = m2 ? ld(a.Ppv, cc) : 0.f;
-#pragma unroll 1
-  for (int k = 0; k < d.nz; ++k) {
-    const long long id = (long long)k * d.plane + cc;
-    float nx_ = 0.f, ny_ = 0.f, nAu = 0.f, nAv = 0.f, nu = 0.f, nv = 0.f, npu = 0.f, npv = 0.f;
-    if (k + 1 < d.nz) {
-      const long long nid = id + d.plane;
-      nx_ = a.gsx[nid];
-      ny_ = a.gsy[nid];
-      nAu = ld(a.Au, nid);
-      nAv = ld(a.Av, nid);
-      nu = ld(a.u1, nid);
-      nv = ld(a.v1, nid);
-      if (m2) {
-        npu = ld(a.Ppu, nid);
-        npv = ld(a.Ppv, nid);
-      }
-    }
-    const float w = wetf(m0, k);
-    const float Pu = (qx - Fx) * w;
-    const float Pv = (qy - Fy) * w;
-    const float Au = qAu, Av = qAv, u1 = qu, v1 = qv;
-    if (MODE == 1) {
-      a.Pu[id] = Pu;
-      a.Pv[id] = Pv;
-      a.uo[id] = u1 + (Au + Pu) * a.dt;
-      a.vo[id] = v1 + (Av + Pv) * a.dt;
-    } else {
-      const float dec = (k == d.nz - 1 && w != 0.f) ? a.bottom_decay : 1.f;
-      a.uo[id] = (u1 + 0.5f * ((Au + qpu) + (Au + Pu)) * a.dt) * dec;
-      a.vo[id] = (v1 + 0.5f * ((Av + qpv) + (Av + Pv)) * a.dt) * dec;
-    }
-    qx = nx_; qy = ny_; qAu = nAu; qAv = nAv; qu = nu; qv = nv; qpu = npu; qpv = npv;
+  // modes 1 and 2: the output pass needs the depth mean before the first
+  // level, so it is its own fully parallel kernel (k_pgf_out)
+  a.Fxs[cc] = Fx;
+  a.Fys[cc] = Fy;
+}
+
+// Output pass of k_pgf modes 1 and 2, four consecutive points of a row per
+// thread with float4 loads and stores (P % 4 == 0):
+//   P = wm (pgf - F_rho) from the per-level gradient and the depth mean;
+//   mode 1: stores P and up = u1 + dt (A + P);
+//   mode 2: u2 = (u1 + dt/2 ((A + Pp) + (A + P))) * exp(-r_bot dt) at the
+//   deepest level (the implicit drag), wet points.
+template <int MODE>
+__global__ void __launch_bounds__(256) k_pgf_out(Dev d, PgfArgs a) {
+  pdl_trigger();
+  const int p4 = d.P >> 2;
+  const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;  // float4 index in [nz][ny][P/4]
+  if (f >= (long long)d.nz * d.ny * p4) return;
+  const int q = (int)(f % p4);
+  const long long kj = f / p4;
+  const int j = (int)(kj % d.ny), k = (int)(kj / d.ny);
+  const int i0 = 4 * q;
+  if (i0 >= d.nx) return;
+  const int c = idx2(d, j, i0);
+  const long long id = (long long)k * d.plane + c;
+  const ulonglong2 b01 = __ldg(reinterpret_cast<const ulonglong2*>(d.wbits + c));
+  const ulonglong2 b23 = __ldg(reinterpret_cast<const ulonglong2*>(d.wbits + c + 2));
+  const float4 w = make_float4(wetf(b01.x, k), wetf(b01.y, k), wetf(b23.x, k), wetf(b23.y, k));
+  pdl_wait();  // the gradient scratch and the momentum parts come from the preceding kernels
+  const float4 gx = *reinterpret_cast<const float4*>(a.gsx + id), gy = *reinterpret_cast<const float4*>(a.gsy + id);
+  const float4 Fx = *reinterpret_cast<const float4*>(a.Fxs + c), Fy = *reinterpret_cast<const float4*>(a.Fys + c);
+  const float4 Au = __ldg(reinterpret_cast<const float4*>(a.Au + id));
+  const float4 Av = __ldg(reinterpret_cast<const float4*>(a.Av + id));
+  const float4 u1 = __ldg(reinterpret_cast<const float4*>(a.u1 + id));
+  const float4 v1 = __ldg(reinterpret_cast<const float4*>(a.v1 + id));
+  const float4 Pu = make_float4((gx.x - Fx.x) * w.x, (gx.y - Fx.y) * w.y, (gx.z - Fx.z) * w.z, (gx.w - Fx.w) * w.w);
+  const float4 Pv = make_float4((gy.x - Fy.x) * w.x, (gy.y - Fy.y) * w.y, (gy.z - Fy.z) * w.z, (gy.w - Fy.w) * w.w);
+  const float dt = a.dt;
+  if (MODE == 1) {
+    *reinterpret_cast<float4*>(a.Pu + id) = Pu;
+    *reinterpret_cast<float4*>(a.Pv + id) = Pv;
+    *reinterpret_cast<float4*>(a.uo + id) =
+        make_float4(u1.x + (Au.x + Pu.x) * dt, u1.y + (Au.y + Pu.y) * dt, u1.z + (Au.z + Pu.z) * dt,
+                    u1.w + (Au.w + Pu.w) * dt);
+    *reinterpret_cast<float4*>(a.vo + id) =
+        make_float4(v1.x + (Av.x + Pv.x) * dt, v1.y + (Av.y + Pv.y) * dt, v1.z + (Av.z + Pv.z) * dt,
+                    v1.w + (Av.w + Pv.w) * dt);
+  } else {
+    const float4 pu = __ldg(reinterpret_cast<const float4*>(a.Ppu + id));
+    const float4 pv = __ldg(reinterpret_cast<const float4*>(a.Ppv + id));
+    const bool bot = k == d.nz - 1;
+    const float4 dec = make_float4(bot && w.x != 0.f ? a.bottom_decay : 1.f, bot && w.y != 0.f ? a.bottom_decay : 1.f,
+                                   bot && w.z != 0.f ? a.bottom_decay : 1.f, bot && w.w != 0.f ? a.bottom_decay : 1.f);
+    *reinterpret_cast<float4*>(a.uo + id) = make_float4((u1.x + 0.5f * ((Au.x + pu.x) + (Au.x + Pu.x)) * dt) * dec.x,
+                                                         (u1.y + 0.5f * ((Au.y + pu.y) + (Au.y + Pu.y)) * dt) * dec.y,
+                                                         (u1.z + 0.5f * ((Au.z + pu.z) + (Au.z + Pu.z)) * dt) * dec.z,
+                                                         (u1.w + 0.5f * ((Au.w + pu.w) + (Au.w + Pu.w)) * dt) * dec.w);
+    *reinterpret_cast<float4*>(a.vo + id) = make_float4((v1.x + 0.5f * ((Av.x + pv.x) + (Av.x + Pv.x)) * dt) * dec.x,
+                                                         (v1.y + 0.5f * ((Av.y + pv.y) + (Av.y + Pv.y)) * dt) * dec.y,
+                                                         (v1.z + 0.5f * ((Av.z + pv.z) + (Av.z + Pv.z)) * dt) * dec.z,
+                                                         (v1.w + 0.5f * ((Av.w + pv.w) + (Av.w + Pv.w)) * dt) * dec.w);
   }
 }
 
 // The mode is a template argument: each launch runs only its own passes.
 void launch_pgf(cudaStream_t s, const Dev& d, const PgfArgs& a) {
-  const dim3 g((d.nx + PG_X - 1) / PG_X, (d.ny + PG_Y - 1) / PG_Y), b(PG_X, PG_Y);
-  if (a.mode == 0) k_pgf<0><<<g, b, 0, s>>>(d, a);
-  else if (a.mode == 1) k_pgf<1><<<g, b, 0, s>>>(d, a);
-  else k_pgf<2><<<g, b, 0, s>>>(d, a);
+  const int ry = d.pg_rows == 8 ? 8 : 4;
+  const dim3 g((d.nx + PG_X - 1) / PG_X, (d.ny + ry - 1) / ry), b(PG_X, ry);
+  if (ry == 8)
+    (void)launch_pdl(a.mode == 0 ? k_pgf<0, 8> : (a.mode == 1 ? k_pgf<1, 8> : k_pgf<2, 8>), g, b, 0, s, d, a);
+  else
+    (void)launch_pdl(a.mode == 0 ? k_pgf<0, 4> : (a.mode == 1 ? k_pgf<1, 4> : k_pgf<2, 4>), g, b, 0, s, d, a);
+  if (a.mode != 0) {
+    const long long n4 = (long long)d.nz * d.ny * (d.P / 4);
+    (void)launch_pdl(a.mode == 1 ? k_pgf_out<1> : k_pgf_out<2>, dim3((unsigned)((n4 + 255) / 256)), dim3(256), 0, s,
+                     d, a);
+  }
 }
 
 // Seasonal forcing blend (inputs/forcing/seasonal.py:86-103): the current
@@ -1556,11 +1685,13 @@ __global__ void k_forcing_blend(Dev d, const float* __restrict__ stack, int prev
 __global__ void k_bt_forcing(Dev d, const float* __restrict__ frx, const float* __restrict__ fry,
                              double* __restrict__ Fx, double* __restrict__ Fy, const float* __restrict__ eta32,
                              double* __restrict__ eta64) {
+  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= d.nx || j >= d.ny) return;
   const int c = idx2(d, j, i);
   const double scale = 1.0 / (1025.0 * (double)d.H_sw);
+  pdl_wait();  // F_rho comes from the preceding kernel
   Fx[c] = (double)frx[c] + (double)__ldg(d.tau_x + c) * scale;
   Fy[c] = (double)fry[c] + (double)__ldg(d.tau_y + c) * scale;
   eta64[c] = (double)eta32[c];
@@ -1573,6 +1704,8 @@ __global__ void __launch_bounds__(256) k_cap3_means(Dev d, const float* __restri
                                                     const double* __restrict__ ubt, const double* __restrict__ ubt0,
                                                     const double* __restrict__ vbt, const double* __restrict__ vbt0,
                                                     float* __restrict__ means, int nb_rows) {
+  pdl_trigger();
+  pdl_wait();  // the projected fields come from the preceding kernels
   __shared__ float red[5][256];
   const int r = blockIdx.x;  // band row index
   const int k = blockIdx.y;
@@ -1629,9 +1762,11 @@ __global__ void __launch_bounds__(256) k_final(Dev d, const float* __restrict__ 
                                                const float* __restrict__ means, const float* __restrict__ wts,
                                                int nb_rows, float* __restrict__ uo, float* __restrict__ vo,
                                                float* __restrict__ To, float* __restrict__ So) {
+  pdl_trigger();
   ZM_POINT_IDX
   const int c = idx2(d, j, i);
   const bool wet = wetb(wb(d, j, i), k);
+  pdl_wait();  // every input comes from the preceding kernels
   if (!wet) {
     uo[id] = ld(u0, id);
     vo[id] = (j == 0 || j == d.ny - 1) ? 0.f : ld(v0, id);

@@ -7,6 +7,32 @@
 
 namespace zm {
 
+// Programmatic dependent launch.  A kernel launched by launch_pdl may begin
+// while the kernel before it on the stream (or in the captured graph)
+// finishes its last blocks: its blocks run the set-up that reads only static
+// arrays (grid metrics, masks, face gates), then pdl_wait(), which returns
+// once the preceding grid has completed and its memory is visible.  Every
+// kernel launched this way calls pdl_wait() before it reads or writes any
+// array that a preceding kernel writes or reads.  pdl_trigger() lets the
+// next kernel's launch begin once every block of this one has started.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <class... K, class... A>
+inline cudaError_t launch_pdl(void (*kern)(K...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, A... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, static_cast<K>(args)...);
+}
+
 struct FftPlan {
   int n, nstages, keep;
   int radix[24];
@@ -21,6 +47,7 @@ struct PgfArgs {
   const float *T, *S, *u1, *v1, *Au, *Av, *Ppu, *Ppv;
   float *Pu, *Pv, *uo, *vo, *frx, *fry;
   float *gsx, *gsy;  // per-level gradient scratch (modes 1 and 2)
+  float *Fxs, *Fys;  // depth-mean gradient per column (modes 1 and 2, 2-D)
   double *ubt0, *vbt0;
   float dt, bottom_decay;
   int mode;
@@ -107,11 +134,11 @@ __global__ void k_forcing_blend(Dev d, const float* stack, int prev, int cur, in
                                 float w_next, float* out);
 __global__ void k_barrier_probe(unsigned* bar, unsigned* err, unsigned expected, unsigned max_polls);
 __global__ void k_nu_tb(Dev d, const float* u, const float* v, float* uo, float* vo, float c, int nsub, int halo);
+__global__ void k_nu_gates(Dev d, unsigned char* gate);
 void launch_lin_t(cudaStream_t s, const Dev& d, const float* usub, const float* vsub, const float* u0,
                   const float* v0, const float* T0, const float* S0, float* uo, float* vo, float* To, float* So,
                   float dth, int implicit_v);
-// threads per block of k_implicit_vdiff (two per column) and its launch
-constexpr int IV_T = 64;
+// the implicit vertical solve (k_vdiff_pcr) of a state in place
 void launch_implicit_vdiff(cudaStream_t s, const Dev& d, float* u, float* v, float* T, float* S, const float* u0,
                            const float* v0, const float* T0, const float* S0, float dth, const float* kap3);
 void launch_fz(cudaStream_t s, const Dev& d, const float* u, const float* v, float* Fz);

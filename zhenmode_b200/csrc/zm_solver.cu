@@ -64,6 +64,7 @@ struct zm_solver {
   float *accT = nullptr, *accS = nullptr, *TsA = nullptr, *SsA = nullptr, *TsB = nullptr, *SsB = nullptr;
   float *dT1 = nullptr, *dS1 = nullptr, *Tp = nullptr, *Sp = nullptr, *Pu = nullptr, *Pv = nullptr;
   float *gsx = nullptr, *gsy = nullptr;  // pressure-gradient scratch
+  float *pfx = nullptr, *pfy = nullptr;  // its depth mean per column
   // budget snapshot: cell areas (reference layout), node thicknesses, partials
   double *area64 = nullptr, *width64 = nullptr, *bpart = nullptr, *bout = nullptr;
   int bblocks = 0;
@@ -182,7 +183,7 @@ struct zm_solver {
         const int nsub = std::min(nu_halo, n_nu - done);
         const Fields4& o = (pass % 2 == 0) ? W1 : W2;
         pb(ZM_K_NU_SUB, s);
-        k_nu_tb<<<grd, blk, 0, s>>>(d, a, c, o.u, o.v, dts, nsub, nu_halo);
+        ZM_CUDA(launch_pdl(k_nu_tb, grd, blk, 0, s, d, a, c, o.u, o.v, dts, nsub, nu_halo));
         pe(s);
         a = o.u;
         c = o.v;
@@ -248,9 +249,12 @@ struct zm_solver {
   void pgf(cudaStream_t s, PgfArgs a) {
     a.gsx = gsx;
     a.gsy = gsy;
+    a.Fxs = pfx;
+    a.Fys = pfy;
     pb(ZM_K_PGF, s);
     launch_pgf(s, d, a);
     pe(s);
+    if (a.mode != 0) ++launch_count;  // launch_pgf adds the output pass (k_pgf_out)
     check_launch();
   }
 
@@ -262,11 +266,13 @@ struct zm_solver {
     pe(s);
     const dim3 m(32, 8);
     pb(ZM_K_MADV, s);
-    k_madv<<<dim3((nx + 31) / 32, (ny + MADV_TY - 1) / MADV_TY, nz), m, 0, s>>>(d, src.u, src.v, Fz, Ayu, Ayv);
+    ZM_CUDA(launch_pdl(k_madv, dim3((nx + 31) / 32, (ny + MADV_TY - 1) / MADV_TY, nz), m, 0, s, d, src.u, src.v,
+                       Fz, Ayu, Ayv));
     pe(s);
     const int nlines = ny * nz;
     pb(ZM_K_DEALIAS, s);
-    k_dealias_lon<<<(nlines + fft_lines - 1) / fft_lines, 256, fft_smem, s>>>(d, fft, Ayu, Ayv, Au, Av, fft_lines);
+    ZM_CUDA(launch_pdl(k_dealias_lon, dim3((nlines + fft_lines - 1) / fft_lines), dim3(256), fft_smem, s, d, fft,
+                       Ayu, Ayv, Au, Av, fft_lines));
     pe(s);
     check_launch();
   }
@@ -413,7 +419,7 @@ struct zm_solver {
     pgf(s, a);
     const dim3 c(32, 8);
     pb(ZM_K_BAROTROPIC, s);
-    k_bt_forcing<<<grid2(c), c, 0, s>>>(d, frx, fry, Fx, Fy, eta_in, eta64[0]);
+    ZM_CUDA(launch_pdl(k_bt_forcing, grid2(c), c, 0, s, d, frx, fry, Fx, Fy, eta_in, eta64[0]));
     pe(s);
     double *ubt_fin, *vbt_fin;
     if (bt_blocks > 0) {
@@ -466,14 +472,13 @@ struct zm_solver {
     }
     if (cap_rows > 0) {
       pb(ZM_K_FINAL, s);
-      k_cap3_means<<<dim3(2 * cap_nb, nz), 256, 0, s>>>(d, s3.u, s3.v, s3.T, s3.S, ubt_fin, ubt0, vbt_fin, vbt0,
-                                                       means, cap_nb);
+      ZM_CUDA(launch_pdl(k_cap3_means, dim3(2 * cap_nb, nz), dim3(256), 0, s, d, s3.u, s3.v, s3.T, s3.S, ubt_fin,
+                         ubt0, vbt_fin, vbt0, means, cap_nb));
       pe(s);
     }
     pb(ZM_K_FINAL, s);
-    k_final<<<grid3(c), c, 0, s>>>(d, s3.u, s3.v, s3.T, s3.S, ubt_fin, ubt0, vbt_fin, vbt0, held.u, held.v,
-                                   held.T, held.S, means, wts, cap_rows > 0 ? cap_nb : 0, out.u, out.v, out.T,
-                                   out.S);
+    ZM_CUDA(launch_pdl(k_final, grid3(c), c, 0, s, d, s3.u, s3.v, s3.T, s3.S, ubt_fin, ubt0, vbt_fin, vbt0, held.u,
+                       held.v, held.T, held.S, means, wts, cap_rows > 0 ? cap_nb : 0, out.u, out.v, out.T, out.S));
     pe(s);
     check_launch();
   }
@@ -522,7 +527,9 @@ struct zm_solver {
 
   // Time the launch shapes that change no result on the resident state,
   // through stages that only write work buffers, and keep the fastest:
-  // nu_h halo width (3..NB_T) and FFT lines per block (1..8).
+  // nu_h halo width (3..NB_T), FFT lines per block (1..8), levels per block
+  // of the tracer-advection and linear-finish column marches, tile rows of
+  // the vertical-transport and pressure-gradient marches.
   void autotune(cudaStream_t s) {
     cudaEvent_t e0, e1;
     ZM_CUDA(cudaEventCreate(&e0));
@@ -567,6 +574,37 @@ struct zm_solver {
       }
       fft_lines = pick;
       fft_smem = (size_t)2 * pick * nx * sizeof(float2);
+      // column-march shapes: levels per block of the tracer advection and of
+      // the linear finish, tile rows of the vertical transport and of the
+      // pressure gradient (every point's arithmetic is the same in each)
+      auto tune = [&](int& field, std::initializer_list<int> cands, auto&& run) {
+        float b = 1e30f;
+        int keep = field;
+        for (int cand : cands) {
+          field = cand;
+          const float ms = time_ms(run);
+          if (ms < b) {
+            b = ms;
+            keep = cand;
+          }
+        }
+        field = keep;
+      };
+      const float dts = (float)(dt / adv_nsub);
+      launch_fz(s, d, in.u, in.v, Fz);
+      tune(d.ta_kc, {5, 8, 10, 13, 17, 25}, [&] {
+        launch_tracer_adv(s, d, in.T, in.S, in.u, in.v, Fz, accT, accS, TsA, SsA, dts, 1, 0, nullptr, nullptr);
+      });
+      const float dth = (float)(dt / 2.0);
+      tune(d.lt_kc, {5, 8, 10, 13, 17, 25}, [&] {
+        launch_lin_t(s, d, in.u, in.v, in.u, in.v, in.T, in.S, s1.u, s1.v, s1.T, s1.S, dth, vdiff || closure_on);
+      });
+      tune(d.fz_rows, {4, 8}, [&] { launch_fz(s, d, in.u, in.v, Fz); });
+      PgfArgs pa{};
+      pa.T = in.T; pa.S = in.S; pa.u1 = in.u; pa.v1 = in.v; pa.frx = frx; pa.fry = fry; pa.ubt0 = ubt0;
+      pa.vbt0 = vbt0; pa.gsx = gsx; pa.gsy = gsy; pa.Fxs = pfx; pa.Fys = pfy; pa.mode = 0;
+      tune(d.pg_rows, {4, 8}, [&] { launch_pgf(s, d, pa); });
+      check_launch();
     } catch (...) {
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
@@ -741,6 +779,18 @@ void build(zm_solver* s, const zm_grid* g, const zm_params* p) {
   d.inv_dx_d = s->upload(inv_dx_d); d.fcor_d = s->upload(fc_d);
   d.wbits = s->upload(bits);
   d.wet2 = s->upload(to_int2(g->wet_mask, nx, ny, P, 0.0));
+  {  // face gates of the nu_h Laplacian, one byte per point
+    unsigned char* gate = s->alloc<unsigned char>(s->n3);
+    const dim3 b(32, 8), gr((P + 31) / 32, (ny + 7) / 8, nz);
+    k_nu_gates<<<gr, b>>>(d, gate);
+    ZM_CUDA(cudaGetLastError());
+    ZM_CUDA(cudaDeviceSynchronize());
+    d.nu_gate = gate;
+  }
+  d.ta_kc = 10;
+  d.lt_kc = 10;
+  d.pg_rows = 4;
+  d.fz_rows = 4;
   {
     std::vector<float> kh = to_int2(p->coastal_kappa_h, nx, ny, P, 0.0);
     std::vector<float> kv = to_int2(p->coastal_kappa_v, nx, ny, P, 0.0);
@@ -886,6 +936,7 @@ void build(zm_solver* s, const zm_grid* g, const zm_params* p) {
   s->accT = s->f3(); s->accS = s->f3(); s->TsA = s->f3(); s->SsA = s->f3(); s->TsB = s->f3(); s->SsB = s->f3();
   s->dT1 = s->f3(); s->dS1 = s->f3(); s->Tp = s->f3(); s->Sp = s->f3(); s->Pu = s->f3(); s->Pv = s->f3();
   s->gsx = s->f3(); s->gsy = s->f3();
+  s->pfx = s->f2(); s->pfy = s->f2();
   s->up = s->f3(); s->vp = s->f3();
   s->frx = s->f2(); s->fry = s->f2();
   s->means = s->alloc<float>((size_t)4 * 2 * std::max(nb, 1) * nz);
@@ -1143,9 +1194,10 @@ int zm_create(const zm_grid* grid, const zm_params* params, zm_solver** out) {
 
 int zm_info(const zm_solver* s, int32_t* out, int32_t n) {
   if (!s || !out) return ZM_ERR_INVALID;
-  const int32_t v[11] = {s->n_subcyc, s->n_nu, s->adv_nsub, s->conv_nsub, s->P, (int32_t)(s->bytes >> 20),
-                         s->kernels_per_step, s->bt_blocks, s->bt.cap_active, s->nu_halo, s->fft_lines};
-  for (int q = 0; q < n && q < 11; ++q) out[q] = v[q];
+  const int32_t v[15] = {s->n_subcyc, s->n_nu, s->adv_nsub, s->conv_nsub, s->P, (int32_t)(s->bytes >> 20),
+                         s->kernels_per_step, s->bt_blocks, s->bt.cap_active, s->nu_halo, s->fft_lines,
+                         s->d.ta_kc, s->d.lt_kc, s->d.fz_rows, s->d.pg_rows};
+  for (int q = 0; q < n && q < 15; ++q) out[q] = v[q];
   return ZM_OK;
 }
 
