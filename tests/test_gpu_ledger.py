@@ -73,7 +73,7 @@ def test_ledger_step_equals_plain_step():
     """The audited step advances the state exactly like the graphed step."""
     import torch
     data, params, st = _setup()
-    step = params["step"]
+    step = params.step
     plain = step(st)
     audited, _ = ledger.make_budget_step(params)(st)
     for k in ("u", "v", "T", "S", "eta"):

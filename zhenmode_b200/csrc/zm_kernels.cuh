@@ -170,7 +170,9 @@ struct ProjArgs {
   const double* minv;   // Jacobi inverse diagonal [ny][P], or null (no preconditioner)
   const double* rarea;  // 1 / area on wet columns, 0 elsewhere
   const double* b;      // right-hand side -(coldiv / (dt g)) area
-  double *psi, *x, *r, *z, *p0, *p1, *Ap;
+  double *psi, *x;
+  double *r[2], *s[2], *w[2];  // residual, search direction's product and A M r, by iteration parity
+  double *u, *p;               // M r and the search direction of the own cell
   double* part;         // [blocks][ZM_PJ_SUMS] block partial sums
   unsigned *bar, *err;
   int* stats;           // iterations of each solve (3), refinement solves run
