@@ -538,243 +538,140 @@ void launch_lin_t(cudaStream_t s, const Dev& d, const float* usub, const float* 
 
 // Backward-Euler vertical diffusion (extension: the implicit replacement of
 // the explicit L-step vertical diffusion).  The matrix is (I - s D2) with D2
-// the node-form operator of d2z on the wet levels 0..kbot (ghost fill below)
-// for u, v (nu_v) and T, S (kappa_v + coastal), or, with the learned closure,
-// the interface-flux operator with its diffusivity per interface for T and S.
-// Rows below the deepest wet level are identity rows (the value passes
-// through), as are all rows of a column with fewer than two wet levels.
-//
-// One warp solves one column's system for a pair of fields that share the
-// matrix (u and v, or T and S): lane l holds rows l and l + 32 (nz <= 64,
-// rows past nz are identity rows), and the system is reduced by parallel
-// cyclic reduction in six shuffle steps of distance 1, 2, ..., 32, each row
-// eliminating its neighbours at that distance, until every row is decoupled;
-// the solution is d / b.  One step of iterative refinement follows: the
-// residual r - A x of the FP32 solution against the original right-hand side
-// (neighbours by shuffle) is reduced with the elimination factors kept from
-// the first pass, and its solution is added.  The matrices are M-matrices
-// (diagonally dominant), which parallel cyclic reduction keeps at every step.
-// A block holds VP_C columns of one latitude row: their four fields (and the
-// closure's diffusivity) are loaded into shared memory with the columns
-// fastest (one sector of each level per field), the warps solve from there,
-// and the block writes the results back the same way, with the land hold and
-// the exact Coriolis rotation of u, v.
-constexpr int VP_C = 8;                  // columns per block
-constexpr int VP_T = 2 * VP_C * 32;      // one warp per (column, field pair)
-constexpr int VP_LD = VP_C + 1;          // shared row pitch
+// the node-form operator of d2z on the wet levels 0..kbot (ghost fill below);
+// Thomas algorithm in FP32 plus one step of iterative refinement, residual
+// formed in FP32 against the original right-hand side.  Rows below the
+// deepest wet level are untouched.
+__device__ __forceinline__ void vcoef(const Dev& d, int k, int kb, float s, float& a, float& b, float& c) {
+  a = 0.f; c = 0.f; b = 1.f;
+  if (k == 0) { b += s * d.vc.d2_top; c = -s * d.vc.d2_top; return; }
+  if (k == d.nz - 1) { a = -s * d.vc.d2_bot; b += s * d.vc.d2_bot; return; }
+  a = -s * d.vc.d2_lo[k];
+  b += s * (d.vc.d2_lo[k] + d.vc.d2_hi[k]);
+  if (k < kb) c = -s * d.vc.d2_hi[k]; else b -= s * d.vc.d2_hi[k];
+}
 
-struct VpTile {
-  float f[4][64][VP_LD];                 // u, v, T, S: right-hand sides in, solutions out
-  float kap[64][VP_LD];                  // closure diffusivity per interface (KAP)
-  float lo[64], hi[64], idzi[64], idzn[64];
-};
-
+// One thread per (column, field); lanes 2c and 2c+1 hold u and v (blockIdx.z
+// = 0: nu_v, node form of d2z with the ghost fill, then the land hold and the
+// exact Coriolis rotation, which swaps values within the lane pair) or T and S
+// (blockIdx.z = 1: kappa_v + coastal in the node form, or the learned
+// closure's diffusivity per interface kap3 in the interface-flux form, then
+// the land hold).  Each thread runs its own sequential Thomas sweeps (the two
+// fields of a pair repeat the same pivots).  The sweeps are latency-bound, so
+// the kernel is held to 32 registers for full occupancy: more independent
+// column chains in flight per SM outweigh a few spilled scalars and the
+// per-thread level arrays in local memory.  Passes over the n = kbot + 1 wet
+// levels:
+//   1. forward elimination, keeping 1 / pivot;
+//   2. back substitution: the FP32 solution x;
+//   3. the residual r - A x (r read again) and its forward elimination;
+//   4. back substitution of the correction e; x + e, hold, rotation, store.
+// The factor up / pivot is formed again where it is needed.
 template <bool KAP>
-__global__ void __launch_bounds__(VP_T) k_vdiff_pcr(Dev d, float* __restrict__ u, float* __restrict__ v,
-                                                    float* __restrict__ T, float* __restrict__ S,
-                                                    const float* __restrict__ u0, const float* __restrict__ v0,
-                                                    const float* __restrict__ T0, const float* __restrict__ S0,
-                                                    float dth, const float* __restrict__ kap3) {
-  __shared__ VpTile t;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int i0 = blockIdx.x * VP_C, j = blockIdx.y;
-  const int nz = d.nz;
-  for (int e = tid; e < 64; e += VP_T) {
-    const bool in = e < nz;
-    t.lo[e] = in ? d.vc.d2_lo[e] : 0.f;
-    t.hi[e] = in ? d.vc.d2_hi[e] : 0.f;
-    t.idzi[e] = in ? d.vc.inv_dz_iface[e] : 0.f;
-    t.idzn[e] = in ? d.vc.inv_dz_node[e] : 0.f;
+__global__ void __launch_bounds__(IV_T, 32) k_implicit_vdiff(Dev d, float* __restrict__ u, float* __restrict__ v,
+                                                        float* __restrict__ T, float* __restrict__ S,
+                                                        const float* __restrict__ u0, const float* __restrict__ v0,
+                                                        const float* __restrict__ T0, const float* __restrict__ S0,
+                                                        float dth, const float* __restrict__ kap3) {
+  const int f = threadIdx.x & 1;
+  const int i = blockIdx.x * (IV_T / 2) + (threadIdx.x >> 1);
+  const int j = blockIdx.y;
+  const bool tracers = blockIdx.z == 1;
+  const bool in = i < d.nx;  // lanes past the last column run along (the pair exchange needs every lane) unstored
+  const long long base = idx2(d, j, in ? i : d.nx - 1);
+  float* __restrict__ fld = tracers ? (f ? S : T) : (f ? v : u);
+  const float* __restrict__ hold = tracers ? (f ? S0 : T0) : (f ? v0 : u0);
+  const bool kap = KAP && tracers;  // the u, v blocks of a closure launch keep nu_v
+  const uint64_t bits = wb(d, j, in ? i : d.nx - 1);
+  const int kb = kbot_of(bits);
+  const int n = kb > 0 && wetb(bits, 0) ? kb + 1 : 0;
+  const float sc = tracers ? __ldg(d.kv2 + base) * dth : d.nu_v * dth;
+  const long long pl = d.plane;
+  float x[ZM_MAXZ], inv[ZM_MAXZ], e[ZM_MAXZ], kq[KAP ? ZM_MAXZ : 1];
+  for (int k = 0; k < n; ++k) {
+    x[k] = fld[base + k * pl];
+    if (KAP && kap && k + 1 < n) kq[k] = __ldg(kap3 + base + k * pl);
   }
-  // the block's columns, level-major with the columns fastest; rows past nz are zero
-  for (int e = tid; e < 4 * 64 * VP_C; e += VP_T) {
-    const int f = e / (64 * VP_C), rem = e - f * 64 * VP_C, k = rem / VP_C, c = rem - k * VP_C;
-    const int col = i0 + c;
-    const float* src = f == 0 ? u : (f == 1 ? v : (f == 2 ? T : S));
-    t.f[f][k][c] = (k < nz && col < d.nx) ? src[(long long)k * d.plane + idx2(d, j, col)] : 0.f;
-  }
-  if (KAP) {
-    for (int e = tid; e < 64 * VP_C; e += VP_T) {
-      const int k = e / VP_C, c = e - k * VP_C, col = i0 + c;
-      t.kap[k][c] = (k + 1 < nz && col < d.nx) ? __ldg(kap3 + (long long)k * d.plane + idx2(d, j, col)) : 0.f;
+  // tridiagonal row k: lower lo, diagonal dg, upper up
+  auto row = [&](int k, float& lo, float& dg, float& up) {
+    if (KAP && kap) {
+      lo = k > 0 ? -dth * kq[k - 1] * d.vc.inv_dz_iface[k - 1] * d.vc.inv_dz_node[k] : 0.f;
+      up = k + 1 < n ? -dth * kq[k] * d.vc.inv_dz_iface[k] * d.vc.inv_dz_node[k] : 0.f;
+      dg = 1.f - lo - up;
+    } else {
+      vcoef(d, k, kb, sc, lo, dg, up);
     }
-  }
-  __syncthreads();
-  const int c = warp % VP_C, sys = warp / VP_C;  // sys 0: u, v; 1: T, S
-  const int col = i0 + c;
-  if (col < d.nx) {
-    const int base = idx2(d, j, col);
-    const uint64_t bits = __ldg(d.wbits + base);
-    const int kb = kbot_of(bits);
-    const int n = (kb > 0 && wetb(bits, 0)) ? kb + 1 : 0;
-    const bool kap = KAP && sys == 1;
-    const float sc = sys ? __ldg(d.kv2 + base) * dth : d.nu_v * dth;
-    // row r of the system: lower a, diagonal b, upper c (identity beyond n)
-    auto row = [&](int r, float& a, float& b, float& cc) {
-      a = 0.f; b = 1.f; cc = 0.f;
-      if (r >= n) return;
-      if (kap) {
-        a = r > 0 ? -dth * t.kap[r - 1][c] * t.idzi[r - 1] * t.idzn[r] : 0.f;
-        cc = r + 1 < n ? -dth * t.kap[r][c] * t.idzi[r] * t.idzn[r] : 0.f;
-        b = 1.f - a - cc;
-      } else if (r == 0) {
-        b += sc * d.vc.d2_top;
-        cc = -sc * d.vc.d2_top;
-      } else if (r == nz - 1) {
-        a = -sc * d.vc.d2_bot;
-        b += sc * d.vc.d2_bot;
-      } else {
-        a = -sc * t.lo[r];
-        b += sc * (t.lo[r] + t.hi[r]);
-        if (r < kb) cc = -sc * t.hi[r];
-        else b -= sc * t.hi[r];
-      }
-    };
-    float a[2], b[2], cc[2], dA[2], dB[2], a0[2], b0[2], c0[2], rA[2], rB[2];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int r = lane + 32 * h;
-      row(r, a[h], b[h], cc[h]);
-      a0[h] = a[h];
-      b0[h] = b[h];
-      c0[h] = cc[h];
-      rA[h] = dA[h] = t.f[2 * sys][r][c];
-      rB[h] = dB[h] = t.f[2 * sys + 1][r][c];
-    }
-    const unsigned full = 0xffffffffu;
-    float K1[6][2], K2[6][2];
-#pragma unroll
-    for (int st = 0; st < 6; ++st) {
-      const int dd = 1 << st;
-      const int lp = (lane + dd) & 31, lm = (lane - dd) & 31;
-      const bool up0 = lane + dd < 32;  // row lane + dd lies in slot 0
-      const bool dn = lane >= dd;       // row lane - dd lies in slot 0
-      float qa[2][2], qb[2][2], qc[2][2], qA[2][2], qB[2][2];  // [slot][+, -] at distance dd
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        qa[h][0] = __shfl_sync(full, a[h], lp);
-        qb[h][0] = __shfl_sync(full, b[h], lp);
-        qc[h][0] = __shfl_sync(full, cc[h], lp);
-        qA[h][0] = __shfl_sync(full, dA[h], lp);
-        qB[h][0] = __shfl_sync(full, dB[h], lp);
-        qa[h][1] = __shfl_sync(full, a[h], lm);
-        qb[h][1] = __shfl_sync(full, b[h], lm);
-        qc[h][1] = __shfl_sync(full, cc[h], lm);
-        qA[h][1] = __shfl_sync(full, dA[h], lm);
-        qB[h][1] = __shfl_sync(full, dB[h], lm);
-      }
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        // rows r + dd (p) and r - dd (m) of this slot; identity rows outside 0..63.
-        // Slot 0: r + dd is in slot 0 of lane l + dd, or slot 1 of lane
-        // l + dd - 32; r - dd in slot 0 of lane l - dd, or outside.  Slot 1:
-        // r + dd in slot 1 of lane l + dd, or outside; r - dd in slot 1 of
-        // lane l - dd, or slot 0 of lane l - dd + 32.
-        const bool has_p = h == 0 || up0, has_m = h == 1 || dn;
-        const bool p1 = h == 1 || !up0, m1 = h == 1 && dn;  // the neighbour sits in slot 1
-        const float ap = has_p ? (p1 ? qa[1][0] : qa[0][0]) : 0.f;
-        const float bp = has_p ? (p1 ? qb[1][0] : qb[0][0]) : 1.f;
-        const float cp = has_p ? (p1 ? qc[1][0] : qc[0][0]) : 0.f;
-        const float Ap = has_p ? (p1 ? qA[1][0] : qA[0][0]) : 0.f;
-        const float Bp = has_p ? (p1 ? qB[1][0] : qB[0][0]) : 0.f;
-        const float am = has_m ? (m1 ? qa[1][1] : qa[0][1]) : 0.f;
-        const float bm = has_m ? (m1 ? qb[1][1] : qb[0][1]) : 1.f;
-        const float cm = has_m ? (m1 ? qc[1][1] : qc[0][1]) : 0.f;
-        const float Am = has_m ? (m1 ? qA[1][1] : qA[0][1]) : 0.f;
-        const float Bm = has_m ? (m1 ? qB[1][1] : qB[0][1]) : 0.f;
-        const float k1 = a[h] / bm, k2 = cc[h] / bp;
-        K1[st][h] = k1;
-        K2[st][h] = k2;
-        b[h] = b[h] - cm * k1 - ap * k2;
-        a[h] = -am * k1;
-        cc[h] = -cp * k2;
-        dA[h] = dA[h] - Am * k1 - Ap * k2;
-        dB[h] = dB[h] - Bm * k1 - Bp * k2;
-      }
-    }
-    float xA[2], xB[2];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      xA[h] = dA[h] / b[h];
-      xB[h] = dB[h] / b[h];
-    }
-    // one refinement step: residual of the FP32 solution, reduced with the same factors
-    {
-      const int lp = (lane + 1) & 31, lm = (lane - 1) & 31;
-      float nA[2][2], nB[2][2];
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        nA[h][0] = __shfl_sync(full, xA[h], lp);
-        nB[h][0] = __shfl_sync(full, xB[h], lp);
-        nA[h][1] = __shfl_sync(full, xA[h], lm);
-        nB[h][1] = __shfl_sync(full, xB[h], lm);
-      }
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        // x[r + 1], x[r - 1] (rows past the ends carry zero coefficients)
-        const float pA = (h == 0 && lane == 31) ? nA[1][0] : nA[h][0];
-        const float pB = (h == 0 && lane == 31) ? nB[1][0] : nB[h][0];
-        const float mA = (h == 1 && lane == 0) ? nA[0][1] : nA[h][1];
-        const float mB = (h == 1 && lane == 0) ? nB[0][1] : nB[h][1];
-        dA[h] = rA[h] - (a0[h] * mA + b0[h] * xA[h] + c0[h] * pA);
-        dB[h] = rB[h] - (a0[h] * mB + b0[h] * xB[h] + c0[h] * pB);
-      }
-    }
-#pragma unroll
-    for (int st = 0; st < 6; ++st) {
-      const int dd = 1 << st;
-      const int lp = (lane + dd) & 31, lm = (lane - dd) & 31;
-      const bool up0 = lane + dd < 32;
-      const bool dn = lane >= dd;
-      float qA[2][2], qB[2][2];
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        qA[h][0] = __shfl_sync(full, dA[h], lp);
-        qB[h][0] = __shfl_sync(full, dB[h], lp);
-        qA[h][1] = __shfl_sync(full, dA[h], lm);
-        qB[h][1] = __shfl_sync(full, dB[h], lm);
-      }
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const bool has_p = h == 0 || up0, has_m = h == 1 || dn;
-        const bool p1 = h == 1 || !up0, m1 = h == 1 && dn;
-        const float Ap = has_p ? (p1 ? qA[1][0] : qA[0][0]) : 0.f;
-        const float Bp = has_p ? (p1 ? qB[1][0] : qB[0][0]) : 0.f;
-        const float Am = has_m ? (m1 ? qA[1][1] : qA[0][1]) : 0.f;
-        const float Bm = has_m ? (m1 ? qB[1][1] : qB[0][1]) : 0.f;
-        dA[h] = dA[h] - Am * K1[st][h] - Ap * K2[st][h];
-        dB[h] = dB[h] - Bm * K1[st][h] - Bp * K2[st][h];
-      }
-    }
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int r = lane + 32 * h;
-      t.f[2 * sys][r][c] = xA[h] + dA[h] / b[h];
-      t.f[2 * sys + 1][r][c] = xB[h] + dB[h] / b[h];
+  };
+  // 1. forward elimination (lo = 0 in row 0, so its pivot is dg)
+  {
+    float cpp = 0.f, y = 0.f;
+    for (int k = 0; k < n; ++k) {
+      float lo, dg, up;
+      row(k, lo, dg, up);
+      const float iv = 1.f / (dg - lo * cpp);
+      cpp = up * iv;
+      y = (x[k] - lo * y) * iv;
+      x[k] = y;
+      inv[k] = iv;
     }
   }
-  __syncthreads();
-  // write back: land hold on dry levels, exact rotation of u, v by f dt/2
-  for (int e = tid; e < nz * VP_C; e += VP_T) {
-    const int k = e / VP_C, cq = e - k * VP_C, cl = i0 + cq;
-    if (cl >= d.nx) continue;
-    const int base = idx2(d, j, cl);
-    const long long id = (long long)k * d.plane + base;
-    const bool wet = wetb(__ldg(d.wbits + base), k);
-    const float uu = wet ? t.f[0][k][cq] : ld(u0, id), vv = wet ? t.f[1][k][cq] : ld(v0, id);
-    const float rc = __ldg(d.rot_c + base), rs = __ldg(d.rot_s + base);
-    u[id] = rc * uu + rs * vv;
-    v[id] = -rs * uu + rc * vv;
-    T[id] = wet ? t.f[2][k][cq] : ld(T0, id);
-    S[id] = wet ? t.f[3][k][cq] : ld(S0, id);
+  // 2. back substitution
+  for (int k = n - 2; k >= 0; --k) {
+    float lo, dg, up;
+    row(k, lo, dg, up);
+    x[k] -= (up * inv[k]) * x[k + 1];
+  }
+  // 3. residual of the FP32 solution, eliminated with the same factorization
+  {
+    float ep = 0.f, xm = 0.f, x0 = n > 0 ? x[0] : 0.f;
+    for (int k = 0; k < n; ++k) {
+      float lo, dg, up;
+      row(k, lo, dg, up);
+      const float xp = k + 1 < n ? x[k + 1] : 0.f;
+      float a = dg * x0;
+      if (k > 0) a += lo * xm;
+      if (k + 1 < n) a += up * xp;
+      ep = ((fld[base + k * pl] - a) - lo * ep) * inv[k];
+      e[k] = ep;
+      xm = x0;
+      x0 = xp;
+    }
+  }
+  // 4. back substitution of the correction; x + e, land hold, rotation
+  const float rc = tracers ? 0.f : __ldg(d.rot_c + base), rs = tracers ? 0.f : __ldg(d.rot_s + base);
+  float en = 0.f;
+  for (int k = d.nz - 1; k >= 0; --k) {
+    const long long id = base + k * pl;
+    const bool wet = wetb(bits, k);
+    float val = 0.f;
+    if (k < n) {
+      float ek = e[k];
+      if (k + 1 < n) {
+        float lo, dg, up;
+        row(k, lo, dg, up);
+        ek -= (up * inv[k]) * en;
+      }
+      en = ek;
+      val = x[k] + ek;
+    } else if (!tracers && wet) {
+      val = fld[id];
+    }
+    if (!wet) val = ld(hold, id);
+    if (tracers) {
+      if (in && (k < n || !wet)) fld[id] = val;
+    } else {
+      const float other = __shfl_xor_sync(0xffffffffu, val, 1);
+      const float uu = f ? other : val, vv = f ? val : other;
+      if (in) fld[id] = f ? -rs * uu + rc * vv : rc * uu + rs * vv;
+    }
   }
 }
 
 void launch_implicit_vdiff(cudaStream_t s, const Dev& d, float* u, float* v, float* T, float* S, const float* u0,
                            const float* v0, const float* T0, const float* S0, float dth, const float* kap3) {
-  const dim3 g((d.nx + VP_C - 1) / VP_C, d.ny);
-  if (kap3) k_vdiff_pcr<true><<<g, VP_T, 0, s>>>(d, u, v, T, S, u0, v0, T0, S0, dth, kap3);
-  else k_vdiff_pcr<false><<<g, VP_T, 0, s>>>(d, u, v, T, S, u0, v0, T0, S0, dth, kap3);
+  const dim3 g((d.nx + IV_T / 2 - 1) / (IV_T / 2), d.ny, 2);
+  if (kap3) k_implicit_vdiff<true><<<g, IV_T, 0, s>>>(d, u, v, T, S, u0, v0, T0, S0, dth, kap3);
+  else k_implicit_vdiff<false><<<g, IV_T, 0, s>>>(d, u, v, T, S, u0, v0, T0, S0, dth, kap3);
 }
 
 // ------------------------------------------------------------------ transport

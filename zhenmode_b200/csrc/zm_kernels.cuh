@@ -139,7 +139,8 @@ __global__ void k_nu_gates(Dev d, unsigned char* gate);
 void launch_lin_t(cudaStream_t s, const Dev& d, const float* usub, const float* vsub, const float* u0,
                   const float* v0, const float* T0, const float* S0, float* uo, float* vo, float* To, float* So,
                   float dth, int implicit_v);
-// the implicit vertical solve (k_vdiff_pcr) of a state in place
+// threads per block of k_implicit_vdiff (two per column) and its launch
+constexpr int IV_T = 64;
 void launch_implicit_vdiff(cudaStream_t s, const Dev& d, float* u, float* v, float* T, float* S, const float* u0,
                            const float* v0, const float* T0, const float* S0, float dth, const float* kap3);
 void launch_fz(cudaStream_t s, const Dev& d, const float* u, const float* v, float* Fz);
@@ -171,9 +172,7 @@ struct ProjArgs {
   const double* minv;   // Jacobi inverse diagonal [ny][P], or null (no preconditioner)
   const double* rarea;  // 1 / area on wet columns, 0 elsewhere
   const double* b;      // right-hand side -(coldiv / (dt g)) area
-  double *psi, *x;
-  double *r[2], *s[2], *w[2];  // residual, search direction's product and A M r, by iteration parity
-  double *u, *p;               // M r and the search direction of the own cell
+  double *psi, *x, *r, *z, *p0, *p1, *Ap;
   double* part;         // [blocks][ZM_PJ_SUMS] block partial sums
   unsigned *bar, *err;
   int* stats;           // iterations of each solve (3), refinement solves run

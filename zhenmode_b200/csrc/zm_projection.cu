@@ -33,10 +33,10 @@
 //    loop of jax's cg: x = 0, r = b, z = M r, p = z, gamma = <r, z>; while the
 //    squared residual (gamma without a preconditioner, <r, r> with one) is
 //    above max(tol^2 <b, b>, atol^2) and k < maxiter: alpha = gamma / <p, Ap>,
-//    x += alpha p, r -= alpha Ap, z = M r, beta = <r, z> / gamma, p = z + beta p,
-//    in the single-reduction arrangement of Chronopoulos and Gear (cg_solve):
-//    every elementwise update is formed again at the stencil points of the
-//    next product, so an iteration takes one grid barrier.  Dot products are summed per thread, per block in
+//    x += alpha p, r -= alpha Ap, z = M r, beta = <r, z> / gamma, p = z + beta p.
+//    The direction update is folded into the next product (each thread forms
+//    z + beta p at its stencil points and stores its own), so an iteration
+//    takes two grid barriers.  Dot products are summed per thread, per block in
 //    a fixed tree and over blocks in block order by every block, so all blocks
 //    take the same branches and the result does not depend on timing.  The
 //    whole working set (a dozen 2-D float64 fields) stays in L2.
@@ -139,82 +139,56 @@ __device__ __forceinline__ double apply_a(const Dev& d, const ProjArgs& a, int j
   return -(__ldg(a.sxy + g) * (fe - fw) + __ldg(a.sxy + n2 + g) * (fn - fs));
 }
 
-// One CG solve into x (zeroed by the caller, with r[0] = rhs written before a
-// barrier), in the single-reduction form of Chronopoulos and Gear: the
-// iterates, residuals and stopping tests of jax's loop (x = 0, r = b,
-// u = M r, p = u; alpha = <r, u> / <p, A p>, x += alpha p, r -= alpha A p,
-// beta = <r, u>_new / <r, u>; stop when <r, u> (or <r, r> with a
-// preconditioner) is at most atol2 or after niter updates), with the two
-// inner products of an iteration and <r, r> summed in one reduction:
-//   w = A u, gamma = <r, u>, delta = <w, u>,
-//   beta = gamma / gamma_old, alpha = gamma / (delta - beta gamma / alpha_old),
-//   p = u + beta p, s = w + beta s (s = A p), x += alpha p, r -= alpha s.
-// Sweep i forms, at every stencil point q of its cells, s_{i-1}, r_i and
-// u_i = M r_i from the stored r_{i-1}, w_{i-1}, s_{i-2} (double-buffered by
-// parity, so no neighbour sees a value written in the same sweep), then
-// w_i = A u_i at the cell, and stores the cell's own r_i, s_{i-1}, w_i, u_i,
-// p_{i-1} and x_i: one grid barrier per iteration.  Returns the number of
-// updates, or -1 if a grid barrier gave up.
-__device__ int cg_solve(const Dev& d, const ProjArgs& a, double* x, double atol2, int& red) {
+// One CG solve (jax loop) into x, which the caller has zeroed together with
+// a.p0, r = rhs and z = M rhs, followed by a barrier.  Returns the iteration
+// count, or -1 if a grid barrier gave up.
+__device__ int cg_solve(const Dev& d, const ProjArgs& a, double* x, double gamma, double rr, double atol2, int& red) {
   const bool ident = a.minv == nullptr;
   const int ncell = d.nx * d.ny;
   const int stride = gridDim.x * blockDim.x;
   const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
-  double alpha = 0.0, beta = 0.0, gamma_old = 0.0;
-  for (int i = 0;; ++i) {
-    const int cur = i & 1, prv = cur ^ 1;
-    const double* rp = a.r[prv];  // r_{i-1}
-    const double* wp = a.w[prv];  // w_{i-1}
-    const double* sp = a.s[cur];  // s_{i-2}
-    const double* r0 = a.r[0];    // r_0 (sweep 0)
-    double sums[3] = {0.0, 0.0, 0.0};
+  const double* pold = a.p0;
+  double* pnew = a.p1;
+  double beta = 0.0;
+  int k = 0;
+  while ((ident ? gamma : rr) > atol2 && k < a.niter) {
+    double s[1] = {0.0};
     for (int c = t0; c < ncell; c += stride) {
-      const int j = c / d.nx, ii = c - j * d.nx;
-      const int g = idx2(d, j, ii);
-      // u_i = M r_i at a stencil point, r_i formed from the stored iterates
-      auto u_at = [&](int h) {
-        double rv;
-        if (i == 0) {
-          rv = __ldcg(r0 + h);
-        } else {
-          const double sv = i == 1 ? __ldcg(wp + h) : fma(beta, __ldcg(sp + h), __ldcg(wp + h));
-          rv = __ldcg(rp + h) - alpha * sv;
-        }
-        return ident ? rv : rv * __ldg(a.minv + h);
-      };
-      double uc;
-      const double wv = apply_a(d, a, j, ii, u_at, uc);
-      double rc;
-      if (i == 0) {
-        rc = __ldcg(r0 + g);
-      } else {
-        const double sv = i == 1 ? __ldcg(wp + g) : fma(beta, __ldcg(sp + g), __ldcg(wp + g));
-        rc = __ldcg(rp + g) - alpha * sv;
-        const double pv = i == 1 ? __ldcg(a.u + g) : fma(beta, __ldcg(a.p + g), __ldcg(a.u + g));
-        a.s[prv][g] = sv;
-        a.p[g] = pv;
-        x[g] = __ldcg(x + g) + alpha * pv;
-        a.r[cur][g] = rc;
-      }
-      a.w[cur][g] = wv;
-      a.u[g] = uc;
-      sums[0] += rc * uc;
-      sums[1] += wv * uc;
-      sums[2] += rc * rc;
+      const int j = c / d.nx, i = c - j * d.nx;
+      double pc;
+      const double ap = apply_a(
+          d, a, j, i, [&](int g) { return fma(beta, __ldcg(pold + g), __ldcg(a.z + g)); }, pc);
+      const int g = idx2(d, j, i);
+      pnew[g] = pc;
+      a.Ap[g] = ap;
+      s[0] += pc * ap;
     }
-    double t[3];
-    if (!reduce(a, red, sums, t)) return -1;
-    const double gamma = t[0], delta = t[1], rr = t[2];
-    if (!((ident ? gamma : rr) > atol2) || i >= a.niter) return i;
-    if (i == 0) {
-      beta = 0.0;
-      alpha = gamma / delta;
-    } else {
-      beta = gamma / gamma_old;
-      alpha = gamma / (delta - beta * gamma / alpha);
+    double t[1];
+    if (!reduce(a, red, s, t)) return -1;
+    const double alpha = gamma / t[0];
+    double s2[2] = {0.0, 0.0};
+    for (int c = t0; c < ncell; c += stride) {
+      const int j = c / d.nx, i = c - j * d.nx;
+      const int g = idx2(d, j, i);
+      x[g] = __ldcg(x + g) + alpha * __ldcg(pnew + g);
+      const double rv = __ldcg(a.r + g) - alpha * __ldcg(a.Ap + g);
+      const double zv = ident ? rv : rv * __ldg(a.minv + g);
+      a.r[g] = rv;
+      a.z[g] = zv;
+      s2[0] += rv * zv;
+      s2[1] += rv * rv;
     }
-    gamma_old = gamma;
+    double t2[2];
+    if (!reduce(a, red, s2, t2)) return -1;
+    beta = t2[0] / gamma;
+    gamma = t2[0];
+    rr = t2[1];
+    double* tmp = const_cast<double*>(pold);
+    pold = pnew;
+    pnew = tmp;
+    ++k;
   }
+  return k;
 }
 
 }  // namespace
@@ -319,19 +293,24 @@ __global__ void __launch_bounds__(256) k_proj_rhs(Dev d, const float* __restrict
 }
 
 __global__ void __launch_bounds__(PJ_THREADS, 1) k_proj_cg(Dev d, ProjArgs a) {
+  const bool ident = a.minv == nullptr;
   const int ncell = d.nx * d.ny;
   const int stride = gridDim.x * blockDim.x;
   const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
   int red = 0;
-  // r = b, psi = 0; <b, b>, sum b^2 / area
+  // r = b, z = M b, psi = 0, p = 0; <b, b>, <b, z>, sum b^2 / area
   double s[3] = {0.0, 0.0, 0.0};
   for (int c = t0; c < ncell; c += stride) {
     const int j = c / d.nx, i = c - j * d.nx;
     const int g = idx2(d, j, i);
     const double bv = __ldcg(a.b + g);
-    a.r[0][g] = bv;
+    const double zv = ident ? bv : bv * __ldg(a.minv + g);
+    a.r[g] = bv;
+    a.z[g] = zv;
     a.psi[g] = 0.0;
+    a.p0[g] = 0.0;
     s[0] += bv * bv;
+    s[1] += bv * zv;
     s[2] += bv * bv * __ldg(a.rarea + g);
   }
   double t[3];
@@ -341,7 +320,7 @@ __global__ void __launch_bounds__(PJ_THREADS, 1) k_proj_cg(Dev d, ProjArgs a) {
   const double thresh = a.trtol2 * t[2];
   int it[3] = {0, 0, 0};
   int nref = 0;
-  it[0] = cg_solve(d, a, a.psi, a.tol2 * bb, red);
+  it[0] = cg_solve(d, a, a.psi, t[1], bb, a.tol2 * bb, red);
   if (it[0] < 0) return;
   for (int q = 0; q < a.refinements; ++q) {
     // residual of the corrected velocity: res = b - A psi
@@ -352,16 +331,20 @@ __global__ void __launch_bounds__(PJ_THREADS, 1) k_proj_cg(Dev d, ProjArgs a) {
       double pc;
       const double ap = apply_a(d, a, j, i, [&](int h) { return __ldcg(a.psi + h); }, pc);
       const double res = __ldcg(a.b + g) - ap;
-      a.r[0][g] = res;
+      const double zv = ident ? res : res * __ldg(a.minv + g);
+      a.r[g] = res;
+      a.z[g] = zv;
       a.x[g] = 0.0;
+      a.p0[g] = 0.0;
       s3[0] += res * res;
+      s3[1] += res * zv;
       s3[2] += res * res * __ldg(a.rarea + g);
     }
     double t3[3];
     if (!reduce(a, red, s3, t3)) return;
     if (!(t3[2] > thresh)) break;
     ++nref;
-    it[1 + q] = cg_solve(d, a, a.x, fmax(a.tol2 * t3[0], floor2), red);
+    it[1 + q] = cg_solve(d, a, a.x, t3[1], t3[0], fmax(a.tol2 * t3[0], floor2), red);
     if (it[1 + q] < 0) return;
     for (int c = t0; c < ncell; c += stride) {
       const int j = c / d.nx, i = c - j * d.nx;

@@ -1120,13 +1120,11 @@ void build(zm_solver* s, const zm_grid* g, const zm_params* p) {
     a.b = s->alloc<double>(s->n2);
     a.psi = s->alloc<double>(s->n2);
     a.x = s->alloc<double>(s->n2);
-    for (int q = 0; q < 2; ++q) {
-      a.r[q] = s->alloc<double>(s->n2);
-      a.s[q] = s->alloc<double>(s->n2);
-      a.w[q] = s->alloc<double>(s->n2);
-    }
-    a.u = s->alloc<double>(s->n2);
-    a.p = s->alloc<double>(s->n2);
+    a.r = s->alloc<double>(s->n2);
+    a.z = s->alloc<double>(s->n2);
+    a.p0 = s->alloc<double>(s->n2);
+    a.p1 = s->alloc<double>(s->n2);
+    a.Ap = s->alloc<double>(s->n2);
     a.part = s->alloc<double>((size_t)2 * s->pj_blocks * ZM_PJ_SUMS);
     unsigned* sync = s->alloc<unsigned>(4);
     a.bar = sync;
