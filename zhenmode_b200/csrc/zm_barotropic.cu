@@ -13,12 +13,7 @@
 //   3  (cap active only) publish band-row partial sums, grid barrier, cap eta*;
 //   4  momentum: adjoint gradient of eta*, u* = ubt + dt (-g grad eta* + F),
 //      backward-Euler Coriolis, implicit drag, wet mask; publish eta*, u, v;
-//   5  grid barrier, or, when no step of the loop needs a sum over all blocks
-//      (polar cap, sponge and eta relaxation all off), the publication of the
-//      block's subcycle count; the next subcycle's halo refresh then waits
-//      only for the (up to eight) blocks whose tiles its halo covers.  The
-//      published fields are double-buffered, so a block overwrites a buffer
-//      only after every neighbour has published the subcycle that read it.
+//   5  grid barrier.
 // The polar cap (numerics/horizontal.py:387-451) needs the wet-point zonal mean
 // of each band row; blocks write per-tile partial row sums and every reader
 // folds them in tile order, so the result does not depend on timing.  When no
@@ -177,27 +172,6 @@ __global__ void __launch_bounds__(BT_THREADS, 4) k_bt_loop(Dev d, BtArgs a) {
   const int i0 = xt * BT_TX, j0 = yt * BT_TY;
   const unsigned nblocks = gridDim.x;
   const bool cap = a.cap_active != 0;
-  const bool local_sync = !cap && !a.sponge && !a.relax;
-  // blocks whose tiles the two-cell halo covers (longitude wraps, rows end at the walls)
-  __shared__ int nbr[8];
-  __shared__ int nn;
-  if (tid == 0) {
-    const int nty = (int)(gridDim.x / a.ntx);
-    int m = 0;
-    for (int dy = -1; dy <= 1; ++dy)
-      for (int dx = -1; dx <= 1; ++dx) {
-        if (dx == 0 && dy == 0) continue;
-        const int y = yt + dy;
-        if (y < 0 || y >= nty) continue;
-        const int x = ((xt + dx) % a.ntx + a.ntx) % a.ntx;
-        const int b = y * a.ntx + x;
-        if (b == (int)blockIdx.x) continue;
-        bool seen = false;
-        for (int q = 0; q < m; ++q) seen = seen || nbr[q] == b;
-        if (!seen) nbr[m++] = b;
-      }
-    nn = m;
-  }
   constexpr int NC = BT_PX * BT_PY;
   constexpr int NR = (BT_TX + 2) * (BT_TY + 2);  // tile + one-cell ring
   constexpr int NT = BT_TX * BT_TY;
@@ -248,7 +222,6 @@ __global__ void __launch_bounds__(BT_THREADS, 4) k_bt_loop(Dev d, BtArgs a) {
   for (int n = 0; n < a.nsub; ++n) {
     const int pin = n & 1, pout = pin ^ 1;
     if (n > 0) {
-      if (local_sync && !wait_neighbours(a.flags, nbr, nn, (unsigned)n, a.err, ZM_BT_BARRIER_POLLS)) return;
       // 1: halo from the neighbours' published fields; caps on every cell
       if (cap) {
         band_means(a, t, 1, a.part_u[pin]);
@@ -354,15 +327,7 @@ __global__ void __launch_bounds__(BT_THREADS, 4) k_bt_loop(Dev d, BtArgs a) {
       band_partials(d, a, t, t.V, a.part_v[pout], xt);
     }
     // 5: the published fields are complete
-    if (local_sync) {
-      __syncthreads();
-      if (tid == 0) {
-        __threadfence();
-        st_release(a.flags + blockIdx.x, (unsigned)(n + 1));
-      }
-    } else if (!grid_barrier(a.bar, a.err, nblocks, ZM_BT_BARRIER_POLLS)) {
-      return;
-    }
+    if (!grid_barrier(a.bar, a.err, nblocks, ZM_BT_BARRIER_POLLS)) return;
   }
   // ---- outputs: capped velocities and the float32 free surface
   const int plast = a.nsub & 1;

@@ -85,7 +85,6 @@ struct BtArgs {
   float* eta_out;
   const float* wts;
   unsigned *bar, *err;
-  unsigned* flags;            // per block: subcycles published (neighbour synchronisation), zeroed per launch
   int ntx, nb, nsub, cap_active;
   double dtH, dtb, drag;
   // lateral sponge and eta relaxation (barotropic.py:22-41); off when the flags are 0

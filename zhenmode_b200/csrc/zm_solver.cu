@@ -428,7 +428,6 @@ struct zm_solver {
     if (bt_blocks > 0) {
       BtArgs a2 = bt;
       a2.eta_out = eta_out;
-      ZM_CUDA(cudaMemsetAsync(bt.flags, 0, (size_t)bt_blocks * sizeof(unsigned), s));
       coop_launch(s, ZM_K_BAROTROPIC, k_bt_loop, bt_blocks, BT_THREADS, bt_tile_smem(), d, a2);
       ubt_fin = bt.ubt_out;
       vbt_fin = bt.vbt_out;
@@ -1014,7 +1013,6 @@ void build(zm_solver* s, const zm_grid* g, const zm_params* p) {
     s->bt_sync = s->alloc<unsigned>(4);
     a.bar = s->bt_sync;
     a.err = s->bt_sync + 2;
-    a.flags = s->bt_blocks > 0 ? s->alloc<unsigned>((size_t)s->bt_blocks) : nullptr;
   }
   {
     // lateral sponge and eta relaxation (factory.py:456-521)

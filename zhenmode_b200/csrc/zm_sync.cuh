@@ -47,35 +47,4 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned* err, unsig
   return ok != 0;
 }
 
-// Publication of a block's subcycle count, and the bounded wait for the
-// counts of the neighbouring blocks (flags[b] >= target).  The caller's
-// __syncthreads before the release and after the wait order the block's
-// stores before the flag and the neighbours' stores before its loads.
-__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
-// Waits (one thread per neighbour, up to 8) until every listed neighbour has
-// published `target`; false (and *err set) if a wait ran out of polls or
-// another block reported an error.
-__device__ __forceinline__ bool wait_neighbours(const unsigned* flags, const int* nbr, int nn, unsigned target,
-                                                unsigned* err, unsigned max_polls) {
-  __shared__ int ok;
-  if (threadIdx.x == 0) ok = 1;
-  __syncthreads();
-  if ((int)threadIdx.x < nn) {
-    unsigned polls = 0;
-    while (ld_acquire(flags + nbr[threadIdx.x]) < target) {
-      if (++polls > max_polls || ld_acquire(err) != 0u) {
-        atomicOr(err, ZM_BT_ERR_BARRIER);
-        ok = 0;
-        break;
-      }
-      __nanosleep(32);
-    }
-  }
-  __syncthreads();
-  return ok != 0;
-}
-
 }  // namespace zm
