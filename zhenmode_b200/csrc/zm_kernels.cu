@@ -319,15 +319,10 @@ __global__ void k_nu_gates(Dev d, unsigned char* __restrict__ gate) {
 // row is padded by itself in the reference.  Vertical diffusion takes the level
 // above from registers and the level below from the next buffer; then
 // land/ghost hold and the exact Coriolis rotation by f dt/2.
-// LT_H rows of halo; the columns carry LT_HX = 4 of halo so that every tile
-// starts on a 16-byte boundary (the TMA rule), two more than the stencil
-// reaches.
-constexpr int LT_X = 32, LT_Y = 8, LT_H = 2, LT_HX = 4, LT_NB = 3;
-constexpr int LT_PX = LT_X + 2 * LT_HX, LT_PY = LT_Y + 2 * LT_H;
+constexpr int LT_X = 32, LT_Y = 8, LT_H = 2, LT_NB = 3;
+constexpr int LT_PX = LT_X + 2 * LT_H, LT_PY = LT_Y + 2 * LT_H;
 constexpr int LT_CELLS = LT_PX * LT_PY;
 static_assert(LT_CELLS <= 2 * LT_X * LT_Y, "two tile cells per thread at most");
-static_assert((LT_PX * 4) % 16 == 0 && (LT_PX * LT_PY * 4) % 128 == 0, "TMA tile rows and slabs aligned");
-constexpr unsigned LT_LEVEL_BYTES = 4u * LT_PX * LT_PY * 4u;  // u, v, T, S tiles of one level
 
 struct LtTile {
   float u[LT_NB][LT_PY][LT_PX], v[LT_NB][LT_PY][LT_PX], T[LT_NB][LT_PY][LT_PX], S[LT_NB][LT_PY][LT_PX];
@@ -335,7 +330,6 @@ struct LtTile {
   float w[2][LT_PY][LT_PX], kh[LT_PY][LT_PX], ix[LT_PY][LT_PX], ix2[LT_PY][LT_PX];
   float tanR[LT_PY], cfp[LT_PY], icos[LT_PY];
   int gj[LT_PY];
-  uint64_t bar[LT_NB];  // TMA completion of each level buffer
 };
 
 // Laplacian of a tile field at (r, c) (horizontal.py:181-215) with the wet
@@ -407,13 +401,9 @@ __global__ void __launch_bounds__(LT_X * LT_Y, 4) k_lin_t(Dev d, const float* __
                                                          const float* __restrict__ v0, const float* __restrict__ T0,
                                                          const float* __restrict__ S0, float* __restrict__ uo,
                                                          float* __restrict__ vo, float* __restrict__ To,
-                                                         float* __restrict__ So, float dth,
-                                                         const __grid_constant__ CUtensorMap mU,
-                                                         const __grid_constant__ CUtensorMap mV,
-                                                         const __grid_constant__ CUtensorMap mT,
-                                                         const __grid_constant__ CUtensorMap mS) {
+                                                         float* __restrict__ So, float dth) {
   pdl_trigger();
-  extern __shared__ __align__(128) float lt_smem[];
+  extern __shared__ float lt_smem[];
   LtTile& t = *reinterpret_cast<LtTile*>(lt_smem);
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = ty * LT_X + tx, nt = LT_X * LT_Y;
@@ -425,8 +415,7 @@ __global__ void __launch_bounds__(LT_X * LT_Y, 4) k_lin_t(Dev d, const float* __
   const bool in = i < d.nx && j < d.ny;
   const int e0 = tid, e1 = tid + nt;
   const bool has1 = e1 < LT_CELLS;
-  const int s0 = tile_cell<LT_PX, LT_HX, LT_H>(d, e0, i0, j0);
-  const int s1 = has1 ? tile_cell<LT_PX, LT_HX, LT_H>(d, e1, i0, j0) : 0;
+  const int s0 = tile_cell<LT_PX, LT_H>(d, e0, i0, j0), s1 = has1 ? tile_cell<LT_PX, LT_H>(d, e1, i0, j0) : 0;
   const uint64_t b0 = __ldg(d.wbits + s0), b1 = has1 ? __ldg(d.wbits + s1) : 0ull;
   (&t.kh[0][0])[e0] = __ldg(d.kh2 + s0);
   (&t.ix[0][0])[e0] = __ldg(d.inv_dx + s0);
@@ -443,50 +432,22 @@ __global__ void __launch_bounds__(LT_X * LT_Y, 4) k_lin_t(Dev d, const float* __
     t.cfp[tid] = __ldg(d.cfp + gj);
     t.icos[tid] = __ldg(d.inv_cos + gj);
   }
-  // Each level's u0, v0, T0, S0 tiles arrive by four TMA copies of the box
-  // starting at (i0 - LT_HX, j0 - LT_H); cells whose field point lies outside
-  // the grid read zeros there and are refilled from the clamped and wrapped
-  // point by the threads that own them.
-  auto outside = [&](int e) {
-    const int rr = e / LT_PX, c2 = e - rr * LT_PX;
-    const int x = i0 - LT_HX + c2, y = j0 - LT_H + rr;
-    return x < 0 || x >= d.nx || y < 0 || y >= d.ny;
-  };
-  const bool fix0 = outside(e0), fix1 = has1 && outside(e1);
-  if (tid == 0) {
-    for (int q = 0; q < LT_NB; ++q) mbar_init(&t.bar[q], 1);
-    mbar_fence_init();
-  }
-  __syncthreads();
-  auto issue = [&](int k) {  // level k into buffer k % LT_NB (one thread)
-    if (tid == 0 && k < d.nz && k <= k1) {  // level k1 only for the column neighbour below the chunk
+  auto issue = [&](int k) {  // level k into buffer k % LT_NB; one commit group per call
+    if (k < d.nz && k <= k1) {  // level k1 only for the column neighbour below the chunk
+      const long long off = (long long)k * d.plane;
       const int q = k % LT_NB;
-      fence_proxy_async();  // the refills of the buffer's previous level come first
-      mbar_expect_tx(&t.bar[q], LT_LEVEL_BYTES);
-      tma_level(&t.u[q][0][0], &mU, i0 - LT_HX, j0 - LT_H, k, &t.bar[q]);
-      tma_level(&t.v[q][0][0], &mV, i0 - LT_HX, j0 - LT_H, k, &t.bar[q]);
-      tma_level(&t.T[q][0][0], &mT, i0 - LT_HX, j0 - LT_H, k, &t.bar[q]);
-      tma_level(&t.S[q][0][0], &mS, i0 - LT_HX, j0 - LT_H, k, &t.bar[q]);
+      cp_async4(&t.u[q][0][0] + e0, u0 + off + s0);
+      cp_async4(&t.v[q][0][0] + e0, v0 + off + s0);
+      cp_async4(&t.T[q][0][0] + e0, T0 + off + s0);
+      cp_async4(&t.S[q][0][0] + e0, S0 + off + s0);
+      if (has1) {
+        cp_async4(&t.u[q][0][0] + e1, u0 + off + s1);
+        cp_async4(&t.v[q][0][0] + e1, v0 + off + s1);
+        cp_async4(&t.T[q][0][0] + e1, T0 + off + s1);
+        cp_async4(&t.S[q][0][0] + e1, S0 + off + s1);
+      }
     }
-  };
-  auto arrive = [&](int k) {  // wait for level k's copies, then refill this thread's outside cells
-    if (k >= d.nz || k > k1) return true;
-    const int q = k % LT_NB;
-    if (!mbar_wait(&t.bar[q], (unsigned)(((k - k0) / LT_NB) & 1), ZM_TMA_POLLS)) return false;
-    const long long off = (long long)k * d.plane;
-    if (fix0) {
-      (&t.u[q][0][0])[e0] = ld(u0, off + s0);
-      (&t.v[q][0][0])[e0] = ld(v0, off + s0);
-      (&t.T[q][0][0])[e0] = ld(T0, off + s0);
-      (&t.S[q][0][0])[e0] = ld(S0, off + s0);
-    }
-    if (fix1) {
-      (&t.u[q][0][0])[e1] = ld(u0, off + s1);
-      (&t.v[q][0][0])[e1] = ld(v0, off + s1);
-      (&t.T[q][0][0])[e1] = ld(T0, off + s1);
-      (&t.S[q][0][0])[e1] = ld(S0, off + s1);
-    }
-    return true;
+    cp_async_commit();
   };
   auto wet_level = [&](int k) {  // wet flags of level k into w[k % 2]
     if (k < d.nz) {
@@ -514,25 +475,22 @@ __global__ void __launch_bounds__(LT_X * LT_Y, 4) k_lin_t(Dev d, const float* __
     Tm = ld(T0, pid);
     Sm = ld(S0, pid);
   }
-  const int r = ty + LT_H, cc = tx + LT_HX;
+  const int r = ty + LT_H, cc = tx + LT_H;
   constexpr bool do_uv = UV, do_ts = TS;
   for (int k = k0; k < k1; ++k) {
-    // levels k and k + 1 in shared memory (level k arrived in the previous pass)
-    if ((k == k0 && !arrive(k)) || !arrive(k + 1)) {
-      atomicOr(d.kerr, ZM_KERR_TMA);
-      return;
-    }
-    __syncthreads();  // every refill is done, w[k % 2] is formed, the ring fields and level k - 1's buffers are free
+    cp_async_wait<0>();  // this thread's copies of levels k and k + 1 are done
+    __syncthreads();     // everyone's are, w[k % 2] is formed, the ring fields and level k - 1's buffers are free
     issue(k + 2);
     wet_level(k + 1);
     const int q = k % LT_NB, qn = (k + 1) % LT_NB;
     const float(*w)[LT_PX] = t.w[k & 1];
     if (do_uv || do_ts) {
-      // the one-cell ring around the interior, walked row by row so that a
-      // warp's shared-memory addresses are consecutive (no bank conflicts)
-      constexpr int RY = LT_Y + 2, RX = LT_X + 2;
-      for (int e = tid; e < RX * RY; e += nt) {
-        const int rr = 1 + e / RX, c2 = LT_HX - 1 + e % RX;
+      // the one-cell ring around the interior, walked over whole padded rows so
+      // that a warp's shared-memory addresses are consecutive (no bank conflicts)
+      constexpr int RY = LT_Y + 2;
+      for (int e = tid; e < LT_PX * RY; e += nt) {
+        const int rr = 1 + e / LT_PX, c2 = e % LT_PX;
+        if (c2 == 0 || c2 == LT_PX - 1) continue;
         if (do_uv) {
           t.Lu[rr][c2] = lap_s(d, t, w, t.u[q], rr, c2, false);
           t.Lv[rr][c2] = lap_s(d, t, w, t.v[q], rr, c2, false);
@@ -596,20 +554,16 @@ __global__ void __launch_bounds__(LT_X * LT_Y, 4) k_lin_t(Dev d, const float* __
 // The biharmonic and implicit-diffusion options are template arguments: a
 // launch carries only the operators its option set uses.
 static_assert(sizeof(LtTile) <= 48 * 1024, "k_lin_t tile within the default dynamic shared memory");
-cudaError_t launch_lin_t(cudaStream_t s, const Dev& d, const float* usub, const float* vsub, const float* u0,
-                         const float* v0, const float* T0, const float* S0, float* uo, float* vo, float* To, float* So,
-                         float dth, int implicit_v) {
+void launch_lin_t(cudaStream_t s, const Dev& d, const float* usub, const float* vsub, const float* u0,
+                  const float* v0, const float* T0, const float* S0, float* uo, float* vo, float* To, float* So,
+                  float dth, int implicit_v) {
   const dim3 g((d.nx + LT_X - 1) / LT_X, (d.ny + LT_Y - 1) / LT_Y, (d.nz + d.lt_kc - 1) / d.lt_kc), b(LT_X, LT_Y);
   const int key = (d.nu_bi > 0.f ? 4 : 0) | (d.kappa_bi > 0.f ? 2 : 0) | (implicit_v ? 1 : 0);
   const size_t sm = sizeof(LtTile);
-  CUtensorMap m[4];
-  const float* f[4] = {u0, v0, T0, S0};
-  for (int q = 0; q < 4; ++q)
-    if (!level_map(&m[q], f[q], d.P, d.ny, d.nz, LT_PX, LT_PY)) return cudaErrorInvalidValue;
-#define ZM_LIN(K, UV, TS, IM)                                                                                    \
-  case K:                                                                                                        \
-    return launch_pdl(k_lin_t<UV, TS, IM>, g, b, sm, s, d, usub, vsub, u0, v0, T0, S0, uo, vo, To, So, dth, m[0], \
-                      m[1], m[2], m[3]);
+#define ZM_LIN(K, UV, TS, IM)                                                                       \
+  case K:                                                                                           \
+    (void)launch_pdl(k_lin_t<UV, TS, IM>, g, b, sm, s, d, usub, vsub, u0, v0, T0, S0, uo, vo, To, So, dth); \
+    break;
   switch (key) {
     ZM_LIN(0, false, false, false)
     ZM_LIN(1, false, false, true)
@@ -621,7 +575,6 @@ cudaError_t launch_lin_t(cudaStream_t s, const Dev& d, const float* usub, const 
     ZM_LIN(7, true, true, true)
   }
 #undef ZM_LIN
-  return cudaErrorInvalidValue;
 }
 
 // Backward-Euler vertical diffusion (extension: the implicit replacement of

@@ -135,9 +135,9 @@ __global__ void k_forcing_blend(Dev d, const float* stack, int prev, int cur, in
 __global__ void k_barrier_probe(unsigned* bar, unsigned* err, unsigned expected, unsigned max_polls);
 __global__ void k_nu_tb(Dev d, const float* u, const float* v, float* uo, float* vo, float c, int nsub, int halo);
 __global__ void k_nu_gates(Dev d, unsigned char* gate);
-cudaError_t launch_lin_t(cudaStream_t s, const Dev& d, const float* usub, const float* vsub, const float* u0,
-                         const float* v0, const float* T0, const float* S0, float* uo, float* vo, float* To, float* So,
-                         float dth, int implicit_v);
+void launch_lin_t(cudaStream_t s, const Dev& d, const float* usub, const float* vsub, const float* u0,
+                  const float* v0, const float* T0, const float* S0, float* uo, float* vo, float* To, float* So,
+                  float dth, int implicit_v);
 // threads per block of k_implicit_vdiff (two per column) and its launch
 constexpr int IV_T = 64;
 void launch_implicit_vdiff(cudaStream_t s, const Dev& d, float* u, float* v, float* T, float* S, const float* u0,

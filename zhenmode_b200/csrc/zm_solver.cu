@@ -197,8 +197,8 @@ struct zm_solver {
       vsub = c;
     }
     pb(ZM_K_LIN_FINISH, s);
-    ZM_CUDA(launch_lin_t(s, d, usub, vsub, src.u, src.v, src.T, src.S, dst.u, dst.v, dst.T, dst.S, dth,
-                         vdiff || closure_on));
+    launch_lin_t(s, d, usub, vsub, src.u, src.v, src.T, src.S, dst.u, dst.v, dst.T, dst.S, dth,
+                 vdiff || closure_on);
     pe(s);
     if (vdiff || closure_on) {
       pb(ZM_K_IMPLICIT, s);
@@ -600,8 +600,7 @@ struct zm_solver {
       });
       const float dth = (float)(dt / 2.0);
       tune(d.lt_kc, {5, 8, 10, 13, 17, 25}, [&] {
-        ZM_CUDA(launch_lin_t(s, d, in.u, in.v, in.u, in.v, in.T, in.S, s1.u, s1.v, s1.T, s1.S, dth,
-                             vdiff || closure_on));
+        launch_lin_t(s, d, in.u, in.v, in.u, in.v, in.T, in.S, s1.u, s1.v, s1.T, s1.S, dth, vdiff || closure_on);
       });
       tune(d.fz_rows, {4, 8}, [&] { launch_fz(s, d, in.u, in.v, Fz); });
       PgfArgs pa{};
