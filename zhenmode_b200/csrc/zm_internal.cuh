@@ -20,9 +20,6 @@
 #include <stdint.h>
 
 #define ZM_MAXZ 64
-// in-kernel wait limits and the error bits of Dev::kerr
-#define ZM_TMA_POLLS (1u << 22)
-#define ZM_KERR_TMA 1u
 
 namespace zm {
 
@@ -88,7 +85,6 @@ struct Dev {
   // block of the tracer-advection and linear-step column marches, tile rows
   // of the pressure-gradient and vertical-transport marches
   int ta_kc, lt_kc, pg_rows, fz_rows;
-  unsigned* kerr;              // bounded in-kernel waits that gave up (ZM_KERR_*), read by zm_status
   Vert vc;
 };
 

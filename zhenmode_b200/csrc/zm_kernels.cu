@@ -3,7 +3,6 @@
 // Each kernel names the reference operator it computes (paths relative to the
 // ZhenMode source tree).  Layout and masks: see zm_internal.cuh.
 #include "zm_kernels.cuh"
-#include "zm_tma.cuh"
 
 namespace zm {
 
@@ -30,10 +29,10 @@ __device__ __forceinline__ void cp_async_wait() {
 // Plane offset of cell e of a padded column tile PX cells wide whose interior
 // starts at (i0, j0), with an H-cell halo: rows clamped at the closed walls
 // like north()/south(), longitude wrapped like east()/west().
-template <int PX, int H = 1, int HY = H>
+template <int PX, int H = 1>
 __device__ __forceinline__ int tile_cell(const Dev& d, int e, int i0, int j0) {
   const int rr = e / PX, cc = e - rr * PX;
-  const int gj = min(max(j0 - HY + rr, 0), d.ny - 1);
+  const int gj = min(max(j0 - H + rr, 0), d.ny - 1);
   int gi = (i0 - H + cc) % d.nx;
   if (gi < 0) gi += d.nx;
   return idx2(d, gj, gi);
@@ -903,23 +902,17 @@ __device__ __forceinline__ float minmod_slope(float cm, float c0, float cp, floa
 // from registers and the level below from the next buffer.  Rows beyond the
 // closed walls are loaded from the clamped row, which is the edge padding of
 // transport.py:199-290; longitude wraps.
-// TA_H rows of halo; the columns carry TA_HX = 4 of halo so that every
-// tile starts on a 16-byte boundary (the TMA rule), two more than the
-// stencil reaches.
-constexpr int TA_H = 2, TA_HX = 4, TA_NB = 3;
-constexpr int TA_PX = TA_X + 2 * TA_HX, TA_PY = TA_Y + 2 * TA_H;
+constexpr int TA_H = 2, TA_NB = 3;
+constexpr int TA_PX = TA_X + 2 * TA_H, TA_PY = TA_Y + 2 * TA_H;
 constexpr int TA_CELLS = TA_PX * TA_PY;
 static_assert(TA_CELLS <= 2 * TA_X * TA_Y, "two tile cells per thread at most");
-static_assert((TA_PX * 4) % 16 == 0 && (TA_PX * TA_PY * 4) % 128 == 0, "TMA tile rows and slabs aligned");
-constexpr unsigned TA_LEVEL_BYTES = 4u * TA_PX * TA_PY * 4u;  // T, S, u, v tiles of one level
 
-struct __align__(128) TaTile {
+struct TaTile {
   float T[TA_NB][TA_PY][TA_PX];
   float S[TA_NB][TA_PY][TA_PX];
   float u[TA_NB][TA_PY][TA_PX];
   float v[TA_NB][TA_PY][TA_PX];
   float w[2][TA_PY][TA_PX];
-  uint64_t bar[TA_NB];  // TMA completion of each level buffer
 };
 
 // Limited face value of one tracer (transport.py:199-290).  With the upwind
@@ -989,11 +982,7 @@ __global__ void __launch_bounds__(TA_X * TA_Y, 5) k_tracer_adv_t(Dev d, const fl
                                                                  float* __restrict__ Tn, float* __restrict__ Sn,
                                                                  float dts, int first, int last,
                                                                  float* __restrict__ topT,
-                                                                 float* __restrict__ topS,
-                                                                 const __grid_constant__ CUtensorMap mT,
-                                                                 const __grid_constant__ CUtensorMap mS,
-                                                                 const __grid_constant__ CUtensorMap mU,
-                                                                 const __grid_constant__ CUtensorMap mV) {
+                                                                 float* __restrict__ topS) {
   pdl_trigger();
   __shared__ TaTile t;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TA_X + tx;
@@ -1004,56 +993,25 @@ __global__ void __launch_bounds__(TA_X * TA_Y, 5) k_tracer_adv_t(Dev d, const fl
   const bool in = i < d.nx && j < d.ny;
   const int e0 = tid, e1 = tid + TA_X * TA_Y;
   const bool has1 = e1 < TA_CELLS;
-  const int s0 = tile_cell<TA_PX, TA_HX, TA_H>(d, e0, i0, j0);
-  const int s1 = has1 ? tile_cell<TA_PX, TA_HX, TA_H>(d, e1, i0, j0) : 0;
+  const int s0 = tile_cell<TA_PX, TA_H>(d, e0, i0, j0), s1 = has1 ? tile_cell<TA_PX, TA_H>(d, e1, i0, j0) : 0;
   const uint64_t b0 = __ldg(d.wbits + s0), b1 = has1 ? __ldg(d.wbits + s1) : 0ull;
   const int k0 = blockIdx.z * d.ta_kc, k1 = min(d.nz, k0 + d.ta_kc);  // this block's levels
-  // Each level's T, S, u, v tiles arrive by four TMA copies of the box
-  // starting at (i0 - TA_HX, j0 - TA_H).  Cells whose field point lies
-  // outside the grid (beyond the closed walls, across the periodic seam, in
-  // the row padding) read zeros there and are refilled from the clamped and
-  // wrapped point by the threads that own them.
-  auto outside = [&](int e) {
-    const int rr = e / TA_PX, c2 = e - rr * TA_PX;
-    const int x = i0 - TA_HX + c2, y = j0 - TA_H + rr;
-    return x < 0 || x >= d.nx || y < 0 || y >= d.ny;
-  };
-  const bool fix0 = outside(e0), fix1 = has1 && outside(e1);
-  if (tid == 0) {
-    for (int q = 0; q < TA_NB; ++q) mbar_init(&t.bar[q], 1);
-    mbar_fence_init();
-  }
-  __syncthreads();
-  auto issue = [&](int k) {  // level k into buffer k % TA_NB (one thread)
-    if (tid == 0 && k < d.nz && k <= k1) {  // level k1 only for the column neighbour below the chunk
+  auto issue = [&](int k) {  // level k into buffer k % TA_NB; one commit group per call
+    if (k < d.nz && k <= k1) {  // level k1 only for the column neighbour below the chunk
+      const long long off = (long long)k * d.plane;
       const int q = k % TA_NB;
-      fence_proxy_async();  // the refills of the buffer's previous level come first
-      mbar_expect_tx(&t.bar[q], TA_LEVEL_BYTES);
-      tma_level(&t.T[q][0][0], &mT, i0 - TA_HX, j0 - TA_H, k, &t.bar[q]);
-      tma_level(&t.S[q][0][0], &mS, i0 - TA_HX, j0 - TA_H, k, &t.bar[q]);
-      tma_level(&t.u[q][0][0], &mU, i0 - TA_HX, j0 - TA_H, k, &t.bar[q]);
-      tma_level(&t.v[q][0][0], &mV, i0 - TA_HX, j0 - TA_H, k, &t.bar[q]);
+      cp_async4(&t.T[q][0][0] + e0, T + off + s0);
+      cp_async4(&t.S[q][0][0] + e0, S + off + s0);
+      cp_async4(&t.u[q][0][0] + e0, u + off + s0);
+      cp_async4(&t.v[q][0][0] + e0, v + off + s0);
+      if (has1) {
+        cp_async4(&t.T[q][0][0] + e1, T + off + s1);
+        cp_async4(&t.S[q][0][0] + e1, S + off + s1);
+        cp_async4(&t.u[q][0][0] + e1, u + off + s1);
+        cp_async4(&t.v[q][0][0] + e1, v + off + s1);
+      }
     }
-  };
-  // wait for level k's copies, then refill this thread's outside cells
-  auto arrive = [&](int k) {
-    if (k >= d.nz || k > k1) return true;
-    const int q = k % TA_NB;
-    if (!mbar_wait(&t.bar[q], (unsigned)(((k - k0) / TA_NB) & 1), ZM_TMA_POLLS)) return false;
-    const long long off = (long long)k * d.plane;
-    if (fix0) {
-      (&t.T[q][0][0])[e0] = ld(T, off + s0);
-      (&t.S[q][0][0])[e0] = ld(S, off + s0);
-      (&t.u[q][0][0])[e0] = ld(u, off + s0);
-      (&t.v[q][0][0])[e0] = ld(v, off + s0);
-    }
-    if (fix1) {
-      (&t.T[q][0][0])[e1] = ld(T, off + s1);
-      (&t.S[q][0][0])[e1] = ld(S, off + s1);
-      (&t.u[q][0][0])[e1] = ld(u, off + s1);
-      (&t.v[q][0][0])[e1] = ld(v, off + s1);
-    }
-    return true;
+    cp_async_commit();
   };
   auto wet_level = [&](int k) {  // wet flags of level k into w[k % 2]
     if (k < d.nz) {
@@ -1071,18 +1029,14 @@ __global__ void __launch_bounds__(TA_X * TA_Y, 5) k_tracer_adv_t(Dev d, const fl
   const uint64_t bits = __ldg(d.wbits + base);
   const int kbt = kbot_of(bits);
   const float ix = __ldg(d.inv_dx + base), ysc = d.inv_dy * __ldg(d.inv_cos + jc);
-  const int r = ty + TA_H, cc = tx + TA_HX;
+  const int r = ty + TA_H, cc = tx + TA_H;
   // T, S of the level above and Fz of the current level
   float ckm = k0 > 0 ? ld(T, base + (long long)(k0 - 1) * d.plane) : 0.f;
   float skm = k0 > 0 ? ld(S, base + (long long)(k0 - 1) * d.plane) : 0.f;
   float fzk = ld(Fz, base + (long long)k0 * d.plane);
   for (int k = k0; k < k1; ++k) {
-    // levels k and k + 1 in shared memory (level k arrived in the previous pass)
-    if ((k == k0 && !arrive(k)) || !arrive(k + 1)) {
-      atomicOr(d.kerr, ZM_KERR_TMA);
-      return;
-    }
-    __syncthreads();  // every refill is done, w[k % 2] is formed, level k - 1's buffers are free
+    cp_async_wait<0>();  // this thread's copies of levels k and k + 1 are done
+    __syncthreads();     // everyone's are, w[k % 2] is formed, level k - 1's buffers are free
     issue(k + 2);
     wet_level(k + 1);
     const long long id = (long long)k * d.plane + base;
@@ -1140,18 +1094,12 @@ __global__ void __launch_bounds__(TA_X * TA_Y, 5) k_tracer_adv_t(Dev d, const fl
 
 // The face limiter is a template argument: the face arithmetic is specialised
 // instead of branching on it at every face.
-cudaError_t launch_tracer_adv(cudaStream_t s, const Dev& d, const float* T, const float* S, const float* u,
-                              const float* v,
+void launch_tracer_adv(cudaStream_t s, const Dev& d, const float* T, const float* S, const float* u, const float* v,
                        const float* Fz, float* accT, float* accS, float* Tn, float* Sn, float dts, int first, int last,
                        float* topT, float* topS) {
   const dim3 g((d.nx + TA_X - 1) / TA_X, (d.ny + TA_Y - 1) / TA_Y, (d.nz + d.ta_kc - 1) / d.ta_kc), b(TA_X, TA_Y);
   auto kern = d.limiter == 2 ? k_tracer_adv_t<2> : (d.limiter == 1 ? k_tracer_adv_t<1> : k_tracer_adv_t<0>);
-  CUtensorMap m[4];
-  const float* f[4] = {T, S, u, v};
-  for (int q = 0; q < 4; ++q)
-    if (!level_map(&m[q], f[q], d.P, d.ny, d.nz, TA_PX, TA_PY)) return cudaErrorInvalidValue;
-  return launch_pdl(kern, g, b, 0, s, d, T, S, u, v, Fz, accT, accS, Tn, Sn, dts, first, last, topT, topS, m[0], m[1],
-                    m[2], m[3]);
+  (void)launch_pdl(kern, g, b, 0, s, d, T, S, u, v, Fz, accT, accS, Tn, Sn, dts, first, last, topT, topS);
 }
 
 // Temperature-term decomposition of a state (dynamics/tendencies.py:74-92,

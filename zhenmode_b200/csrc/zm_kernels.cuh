@@ -148,10 +148,7 @@ void launch_tracer_terms(cudaStream_t s, const Dev& d, const float* T, const flo
 __global__ void k_madv(Dev d, const float* u, const float* v, const float* Fz, float* Ayu, float* Ayv);
 __global__ void k_dealias_lon(Dev d, FftPlan plan, const float* Ayu, const float* Ayv, float* Au, float* Av,
                               int lines_per_block);
-// The level tiles arrive by TMA; returns the launch error (or
-// cudaErrorInvalidValue when a tensor map cannot be encoded).
-cudaError_t launch_tracer_adv(cudaStream_t s, const Dev& d, const float* T, const float* S, const float* u,
-                              const float* v,
+void launch_tracer_adv(cudaStream_t s, const Dev& d, const float* T, const float* S, const float* u, const float* v,
                        const float* Fz, float* accT, float* accS, float* Tn, float* Sn, float dts, int first, int last,
                        float* topT, float* topS);
 void launch_tracer_rest(dim3 g, dim3 b, cudaStream_t s, const Dev& d, const RestArgs& a);

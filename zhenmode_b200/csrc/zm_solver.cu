@@ -233,8 +233,8 @@ struct zm_solver {
       float* nT = (n % 2 == 0) ? TsA : TsB;
       float* nS = (n % 2 == 0) ? SsA : SsB;
       pb(ZM_K_TRACER_ADV, s);
-      ZM_CUDA(launch_tracer_adv(s, d, cT, cS, u, v, Fz, accT, accS, nT, nS, dts, n == 0, n == adv_nsub - 1,
-                                ledger_on ? led_topT : nullptr, ledger_on ? led_topS : nullptr));
+      launch_tracer_adv(s, d, cT, cS, u, v, Fz, accT, accS, nT, nS, dts, n == 0, n == adv_nsub - 1,
+                        ledger_on ? led_topT : nullptr, ledger_on ? led_topS : nullptr);
       pe(s);
       cT = nT;
       cS = nS;
@@ -596,7 +596,7 @@ struct zm_solver {
       const float dts = (float)(dt / adv_nsub);
       launch_fz(s, d, in.u, in.v, Fz);
       tune(d.ta_kc, {5, 8, 10, 13, 17, 25}, [&] {
-        ZM_CUDA(launch_tracer_adv(s, d, in.T, in.S, in.u, in.v, Fz, accT, accS, TsA, SsA, dts, 1, 0, nullptr, nullptr));
+        launch_tracer_adv(s, d, in.T, in.S, in.u, in.v, Fz, accT, accS, TsA, SsA, dts, 1, 0, nullptr, nullptr);
       });
       const float dth = (float)(dt / 2.0);
       tune(d.lt_kc, {5, 8, 10, 13, 17, 25}, [&] {
@@ -791,7 +791,6 @@ void build(zm_solver* s, const zm_grid* g, const zm_params* p) {
     ZM_CUDA(cudaDeviceSynchronize());
     d.nu_gate = gate;
   }
-  d.kerr = s->alloc<unsigned>(1);
   d.ta_kc = 10;
   d.lt_kc = 10;
   d.pg_rows = 4;
@@ -1748,9 +1747,6 @@ int zm_status(zm_solver* s, int32_t* monitor_code) {
   e = cudaMemcpy(&berr, s->bt.err, sizeof(berr), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return fail(s, Err{ZM_ERR_CUDA, std::string("zm_status: ") + cudaGetErrorString(e)});
   if (berr) return fail(s, Err{ZM_ERR_TIMEOUT, "barotropic grid barrier timed out"});
-  e = cudaMemcpy(&berr, s->d.kerr, sizeof(berr), cudaMemcpyDeviceToHost);
-  if (e != cudaSuccess) return fail(s, Err{ZM_ERR_CUDA, cudaGetErrorString(e)});
-  if (berr) return fail(s, Err{ZM_ERR_TIMEOUT, "a tile copy (TMA) of a step kernel did not complete in time"});
   if (s->proj_on) {
     e = cudaMemcpy(&berr, s->pj.err, sizeof(berr), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return fail(s, Err{ZM_ERR_CUDA, std::string("zm_status: ") + cudaGetErrorString(e)});
