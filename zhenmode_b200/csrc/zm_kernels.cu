@@ -123,10 +123,7 @@ __device__ __forceinline__ float colv(const float* __restrict__ a, long long bas
 // j = 0, aS = 0.  The coefficients, scaled by nu_h dt_sub, are formed once
 // per pass from the face gates of the cell (k_nu_gates, built once per
 // solver: one byte per point) and per-row constants, so the set-up needs
-// no neighbour wet flags.  Longitude wraps.  The kernel is persistent: each
-// block walks tiles (blockIdx, + gridDim, ...), and while it runs the
-// subcycles of one tile the u, v of its next tile arrive in shared memory by
-// cp.async (each lane prefetches exactly the cells it will hold).  The lane's two columns are held
+// no neighbour wet flags.  Longitude wraps.  The lane's two columns are held
 // as packed pairs, so the update runs on the paired FP32 instructions
 // (__ffma2_rn, __fadd2_rn; the same roundings as the scalar form).  Points
 // of the tile edge see their own values as the missing neighbours (their
@@ -137,152 +134,115 @@ k_nu_tb(Dev d, const float* __restrict__ u, const float* __restrict__ v, float* 
   constexpr int NW = NB_W / NB_R;                 // warps per block
   const int TI = NB_W - 2 * halo;
   __shared__ float4 edge[2][NW][2][32];           // [parity][warp][0 bottom row, 1 top row][lane]
-  __shared__ float2 pre_u[NB_W][32], pre_v[NB_W][32];  // the next tile's u, v: [row][lane] column pairs
   pdl_trigger();
   const int lane = threadIdx.x, wp = threadIdx.y;
+  const int k = blockIdx.z;
+  const int gx0 = blockIdx.x * TI - halo, gy0 = blockIdx.y * TI - halo;
   const int c0 = 2 * lane, r0 = wp * NB_R;
-  const int ntx = (d.nx + TI - 1) / TI, nty = (d.ny + TI - 1) / TI;
-  const int ntiles = ntx * nty * d.nz;
+  int gi[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    int g = (gx0 + c0 + h) % d.nx;
+    gi[h] = g < 0 ? g + d.nx : g;
+  }
+  const long long kb = (long long)k * d.plane;
   const float cn = d.nu_h * c;
-  const unsigned full = 0xffffffffu;
-  const float2 m1 = make_float2(-1.f, -1.f);
-  // the lane's cells of a tile: columns gi[0..1], rows gj (clamped) of its strip
-  auto tile_origin = [&](int tile, int& gx0, int& gy0, int& k) {
-    const int xt = tile % ntx, rest = tile / ntx;
-    gx0 = xt * TI - halo;
-    gy0 = (rest % nty) * TI - halo;
-    k = rest / nty;
-  };
-  auto cols = [&](int gx0, int (&gi)[2]) {
+  // face coefficients, paired like the state: (column 2l, column 2l+1).  The
+  // west and south ones are held negated (nW = -aW, nS = -aS) and negated back
+  // in the update, an exact round trip: ptxas 12.9 allocates this form's
+  // registers differently, and it ran 4 % faster than holding aW, aS.
+  float2 kE[NB_R], nW[NB_R], kN[NB_R], nS[NB_R];
+#pragma unroll
+  for (int q = 0; q < NB_R; ++q) {
+    const int gj = gy0 + r0 + q;
+    const int gjc = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
+    const bool n_in = gj < d.ny - 1;  // north neighbour inside the domain
+    const bool s_in = gj > 0;
+    const float t = 0.5f * d.inv_dy * __ldg(d.tanR + gjc);
+    // aN with the north face open / closed, aS likewise (0 beyond the walls)
+    const float n1 = n_in ? (d.inv_dy2 - t) * cn : 0.f, n0 = n_in ? (0.f - t) * cn : 0.f;
+    const float s1 = s_in ? (d.inv_dy2 + t) * cn : 0.f, s0 = s_in ? (0.f + t) * cn : 0.f;
+    float ce[2], cw[2], cnn[2], cs[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      int g = (gx0 + c0 + h) % d.nx;
-      gi[h] = g < 0 ? g + d.nx : g;
+      const int id2 = idx2(d, gjc, gi[h]);
+      const unsigned g = __ldg(d.nu_gate + kb + id2);
+      const float ax = __ldg(d.inv_dx2 + id2) * cn;
+      ce[h] = (g & 1u) ? ax : 0.f;
+      cw[h] = (g & 2u) ? ax : 0.f;
+      cnn[h] = (g & 4u) ? n1 : n0;
+      cs[h] = (g & 8u) ? s1 : s0;
     }
-  };
-  // this lane's u, v of a tile into shared memory, asynchronously (own cells only)
-  auto prefetch = [&](int tile) {
-    if (tile < ntiles) {
-      int gx0, gy0, k, gi[2];
-      tile_origin(tile, gx0, gy0, k);
-      cols(gx0, gi);
-      const long long kb = (long long)k * d.plane;
-#pragma unroll
-      for (int q = 0; q < NB_R; ++q) {
-        int gj = gy0 + r0 + q;
-        gj = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
-        const long long row = kb + (long long)gj * d.P;
-        cp_async4(&pre_u[r0 + q][lane].x, u + row + gi[0]);
-        cp_async4(&pre_u[r0 + q][lane].y, u + row + gi[1]);
-        cp_async4(&pre_v[r0 + q][lane].x, v + row + gi[0]);
-        cp_async4(&pre_v[r0 + q][lane].y, v + row + gi[1]);
-      }
-    }
-    cp_async_commit();
-  };
-  pdl_wait();  // u, v come from the preceding kernel
-  prefetch(blockIdx.x);
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    int gx0, gy0, k, gi[2];
-    tile_origin(tile, gx0, gy0, k);
-    cols(gx0, gi);
-    const long long kb = (long long)k * d.plane;
-    // face coefficients, paired like the state: (column 2l, column 2l+1).  The
-    // west and south ones are held negated (nW = -aW, nS = -aS) and negated
-    // back in the update, an exact round trip (ptxas allocates this form's
-    // registers differently; it ran 4 % faster than holding aW, aS)
-    float2 kE[NB_R], nW[NB_R], kN[NB_R], nS[NB_R];
-#pragma unroll
-    for (int q = 0; q < NB_R; ++q) {
-      const int gj = gy0 + r0 + q;
-      const int gjc = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
-      const bool n_in = gj < d.ny - 1;  // north neighbour inside the domain
-      const bool s_in = gj > 0;
-      const float t = 0.5f * d.inv_dy * __ldg(d.tanR + gjc);
-      // aN with the north face open / closed, aS likewise (0 beyond the walls)
-      const float n1 = n_in ? (d.inv_dy2 - t) * cn : 0.f, n0 = n_in ? (0.f - t) * cn : 0.f;
-      const float s1 = s_in ? (d.inv_dy2 + t) * cn : 0.f, s0 = s_in ? (0.f + t) * cn : 0.f;
-      float ce[2], cw[2], cnn[2], cs[2];
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int id2 = idx2(d, gjc, gi[h]);
-        const unsigned g = __ldg(d.nu_gate + kb + id2);
-        const float ax = __ldg(d.inv_dx2 + id2) * cn;
-        ce[h] = (g & 1u) ? ax : 0.f;
-        cw[h] = (g & 2u) ? ax : 0.f;
-        cnn[h] = (g & 4u) ? n1 : n0;
-        cs[h] = (g & 8u) ? s1 : s0;
-      }
-      kE[q] = make_float2(ce[0], ce[1]);
-      nW[q] = make_float2(-cw[0], -cw[1]);
-      kN[q] = make_float2(cnn[0], cnn[1]);
-      nS[q] = make_float2(-cs[0], -cs[1]);
-    }
-    // this tile's u, v (this lane's own prefetched cells), then the next tile's prefetch
-    cp_async_wait<0>();
-    float2 au[NB_R], av[NB_R];
-#pragma unroll
-    for (int q = 0; q < NB_R; ++q) {
-      au[q] = pre_u[r0 + q][lane];
-      av[q] = pre_v[r0 + q][lane];
-    }
-    prefetch(tile + gridDim.x);
-    for (int s = 0; s < nsub; ++s) {
-      const int p = s & 1;
-      edge[p][wp][0][lane] = make_float4(au[0].x, au[0].y, av[0].x, av[0].y);
-      edge[p][wp][1][lane] = make_float4(au[NB_R - 1].x, au[NB_R - 1].y, av[NB_R - 1].x, av[NB_R - 1].y);
-      __syncthreads();
-      // rows just outside the strip (the tile edge reuses the strip's own row)
-      const float4 nt = edge[p][wp + 1 < NW ? wp + 1 : wp][wp + 1 < NW ? 0 : 1][lane];
-      const float4 sb = edge[p][wp > 0 ? wp - 1 : wp][wp > 0 ? 1 : 0][lane];
-      float2 su = make_float2(sb.x, sb.y), sv = make_float2(sb.z, sb.w);
-#pragma unroll
-      for (int q = 0; q < NB_R; ++q) {
-        const float2 nu = q + 1 < NB_R ? au[q + 1] : make_float2(nt.x, nt.y);
-        const float2 nv = q + 1 < NB_R ? av[q + 1] : make_float2(nt.z, nt.w);
-        // east of (2l, 2l+1) is (2l+1, 2l+2), west is (2l-1, 2l); the outside
-        // columns come from the neighbouring lanes (lanes 0 and 31 get their
-        // own values: tile-edge error)
-        const float2 eu = make_float2(au[q].y, __shfl_down_sync(full, au[q].x, 1));
-        const float2 wu = make_float2(__shfl_up_sync(full, au[q].y, 1), au[q].x);
-        const float2 ev = make_float2(av[q].y, __shfl_down_sync(full, av[q].x, 1));
-        const float2 wv = make_float2(__shfl_up_sync(full, av[q].y, 1), av[q].x);
-        // u0 + aE (uE - u0) + aW (uW - u0) + aN (uN - u0) + aS (uS - u0) on packed pairs
-        const float2 ncu = __fmul2_rn(au[q], m1), ncv = __fmul2_rn(av[q], m1);
-        float2 ou = __ffma2_rn(kE[q], __fadd2_rn(eu, ncu), au[q]);
-        float2 ov = __ffma2_rn(kE[q], __fadd2_rn(ev, ncv), av[q]);
-        ou = __ffma2_rn(make_float2(-nW[q].x, -nW[q].y), __fadd2_rn(wu, ncu), ou);
-        ov = __ffma2_rn(make_float2(-nW[q].x, -nW[q].y), __fadd2_rn(wv, ncv), ov);
-        ou = __ffma2_rn(kN[q], __fadd2_rn(nu, ncu), ou);
-        ov = __ffma2_rn(kN[q], __fadd2_rn(nv, ncv), ov);
-        ou = __ffma2_rn(make_float2(-nS[q].x, -nS[q].y), __fadd2_rn(su, ncu), ou);
-        ov = __ffma2_rn(make_float2(-nS[q].x, -nS[q].y), __fadd2_rn(sv, ncv), ov);
-        su = au[q];
-        sv = av[q];
-        au[q] = ou;
-        av[q] = ov;
-      }
-    }
-    // write the exact interior
-#pragma unroll
-    for (int q = 0; q < NB_R; ++q) {
-      const int r = r0 + q;
-      const int gj = gy0 + r;
-      if (r < halo || r >= NB_W - halo || gj >= d.ny) continue;
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int col = c0 + h;
-        const int ix = gx0 + col;
-        if (col < halo || col >= NB_W - halo || ix >= d.nx) continue;
-        const long long id = kb + (long long)gj * d.P + ix;
-        uo[id] = h == 0 ? au[q].x : au[q].y;
-        vo[id] = h == 0 ? av[q].x : av[q].y;
-      }
-    }
-    // the edge buffers of the last subcycle are read before the next tile's first exchange
-    __syncthreads();
+    kE[q] = make_float2(ce[0], ce[1]);
+    nW[q] = make_float2(-cw[0], -cw[1]);
+    kN[q] = make_float2(cnn[0], cnn[1]);
+    nS[q] = make_float2(-cs[0], -cs[1]);
   }
-  cp_async_wait<0>();
+  const unsigned full = 0xffffffffu;
+  pdl_wait();  // u, v come from the preceding kernel
+  // the lane's two columns as pairs: au[q] = (u[2l], u[2l+1]) of row q, av likewise
+  float2 au[NB_R], av[NB_R];
+#pragma unroll
+  for (int q = 0; q < NB_R; ++q) {
+    int gj = gy0 + r0 + q;
+    gj = gj < 0 ? 0 : (gj >= d.ny ? d.ny - 1 : gj);
+    const long long id0 = kb + (long long)gj * d.P + gi[0], id1 = kb + (long long)gj * d.P + gi[1];
+    au[q] = make_float2(ld(u, id0), ld(u, id1));
+    av[q] = make_float2(ld(v, id0), ld(v, id1));
+  }
+  const float2 m1 = make_float2(-1.f, -1.f);
+  for (int s = 0; s < nsub; ++s) {
+    const int p = s & 1;
+    edge[p][wp][0][lane] = make_float4(au[0].x, au[0].y, av[0].x, av[0].y);
+    edge[p][wp][1][lane] = make_float4(au[NB_R - 1].x, au[NB_R - 1].y, av[NB_R - 1].x, av[NB_R - 1].y);
+    __syncthreads();
+    // rows just outside the strip (the tile edge reuses the strip's own row)
+    const float4 nt = edge[p][wp + 1 < NW ? wp + 1 : wp][wp + 1 < NW ? 0 : 1][lane];
+    const float4 sb = edge[p][wp > 0 ? wp - 1 : wp][wp > 0 ? 1 : 0][lane];
+    float2 su = make_float2(sb.x, sb.y), sv = make_float2(sb.z, sb.w);
+#pragma unroll
+    for (int q = 0; q < NB_R; ++q) {
+      const float2 nu = q + 1 < NB_R ? au[q + 1] : make_float2(nt.x, nt.y);
+      const float2 nv = q + 1 < NB_R ? av[q + 1] : make_float2(nt.z, nt.w);
+      // east of (2l, 2l+1) is (2l+1, 2l+2), west is (2l-1, 2l); the outside
+      // columns come from the neighbouring lanes (lanes 0 and 31 get their
+      // own values: tile-edge error)
+      const float2 eu = make_float2(au[q].y, __shfl_down_sync(full, au[q].x, 1));
+      const float2 wu = make_float2(__shfl_up_sync(full, au[q].y, 1), au[q].x);
+      const float2 ev = make_float2(av[q].y, __shfl_down_sync(full, av[q].x, 1));
+      const float2 wv = make_float2(__shfl_up_sync(full, av[q].y, 1), av[q].x);
+      // u0 + aE (uE - u0) + aW (uW - u0) + aN (uN - u0) + aS (uS - u0) on packed pairs
+      const float2 ncu = __fmul2_rn(au[q], m1), ncv = __fmul2_rn(av[q], m1);
+      float2 ou = __ffma2_rn(kE[q], __fadd2_rn(eu, ncu), au[q]);
+      float2 ov = __ffma2_rn(kE[q], __fadd2_rn(ev, ncv), av[q]);
+      ou = __ffma2_rn(make_float2(-nW[q].x, -nW[q].y), __fadd2_rn(wu, ncu), ou);
+      ov = __ffma2_rn(make_float2(-nW[q].x, -nW[q].y), __fadd2_rn(wv, ncv), ov);
+      ou = __ffma2_rn(kN[q], __fadd2_rn(nu, ncu), ou);
+      ov = __ffma2_rn(kN[q], __fadd2_rn(nv, ncv), ov);
+      ou = __ffma2_rn(make_float2(-nS[q].x, -nS[q].y), __fadd2_rn(su, ncu), ou);
+      ov = __ffma2_rn(make_float2(-nS[q].x, -nS[q].y), __fadd2_rn(sv, ncv), ov);
+      su = au[q];
+      sv = av[q];
+      au[q] = ou;
+      av[q] = ov;
+    }
+  }
+  // write the exact interior
+#pragma unroll
+  for (int q = 0; q < NB_R; ++q) {
+    const int r = r0 + q;
+    const int gj = gy0 + r;
+    if (r < halo || r >= NB_W - halo || gj >= d.ny) continue;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int col = c0 + h;
+      const int ix = gx0 + col;
+      if (col < halo || col >= NB_W - halo || ix >= d.nx) continue;
+      const long long id = kb + (long long)gj * d.P + ix;
+      uo[id] = h == 0 ? au[q].x : au[q].y;
+      vo[id] = h == 0 ? av[q].x : av[q].y;
+    }
+  }
 }
 
 // Face gates of the nu_h Laplacian, one byte per point (built once per

@@ -41,7 +41,6 @@ struct Fields4 {
 struct zm_solver {
   Dev d{};
   int device = 0;
-  int num_sms = 148;
   int nx = 0, ny = 0, nz = 0, P = 0;
   size_t n2 = 0, n3 = 0;
   int n_subcyc = 1, n_nu = 1, adv_nsub = 1, conv_nsub = 1;
@@ -178,9 +177,7 @@ struct zm_solver {
       const float* c = src.v;
       const int TI = NB_W - 2 * nu_halo;
       const dim3 blk(32, NB_W / NB_R);
-      // persistent blocks, two per SM, walking the tiles
-      const long long ntiles = (long long)((nx + TI - 1) / TI) * ((ny + TI - 1) / TI) * nz;
-      const dim3 grd((unsigned)std::min<long long>(ntiles, 2LL * num_sms));
+      const dim3 grd((nx + TI - 1) / TI, (ny + TI - 1) / TI, nz);
       int done = 0, pass = 0;
       while (done < n_nu) {
         const int nsub = std::min(nu_halo, n_nu - done);
@@ -715,7 +712,6 @@ void build(zm_solver* s, const zm_grid* g, const zm_params* p) {
   require(fft_factor(nx, plan), ZM_ERR_UNSUPPORTED, "nx must be a product of 2, 3 and 5 (longitude FFT filter)");
 
   cudaGetDevice(&s->device);
-  cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, s->device);
   s->nx = nx; s->ny = ny; s->nz = nz;
   s->P = (nx + 3) / 4 * 4;
   const int P = s->P;
