@@ -328,6 +328,60 @@ __device__ __forceinline__ float hdiff_s(const Dev& d, const LtTile& t, const fl
   return (fe - fw) * t.ix[r][c] + (fn - fs) * d.inv_dy * t.icos[r];
 }
 
+// The two operators above on a pair of tile fields (u and v, or T and S) that
+// share every coefficient, on the paired FP32 instructions (__fadd2_rn,
+// __fmul2_rn, __ffma2_rn: each half rounds like the scalar operation).  The
+// wet gates are products of 0/1 flags, formed once per point, and a
+// difference a0 - ax enters as the exact negation of ax - a0.
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 pair(const float (*A)[LT_PX], const float (*B)[LT_PX], int r, int c) {
+  return make_float2(A[r][c], B[r][c]);
+}
+
+__device__ __forceinline__ float2 lap2(const Dev& d, const LtTile& t, const float (*w)[LT_PX],
+                                      const float (*A)[LT_PX], const float (*B)[LT_PX], int r, int c, bool mirror) {
+  const float2 m1 = f2(-1.f);
+  const float2 a0 = pair(A, B, r, c), ae = pair(A, B, r, c + 1), aw = pair(A, B, r, c - 1);
+  float2 an = pair(A, B, r + 1, c), as = pair(A, B, r - 1, c);
+  if (mirror) {
+    if (t.gj[r] == d.ny - 1) an = a0;
+    if (t.gj[r] == 0) as = a0;
+  }
+  const float w0 = w[r][c];
+  const float ge = w0 * w[r][c + 1], gw = w0 * w[r][c - 1], gn = w[r + 1][c] * w0, gs = w0 * w[r - 1][c];
+  const float2 na0 = __fmul2_rn(a0, m1);
+  // d2x = ((ae - a0) ge - (a0 - aw) gw) / dx^2, d2y likewise / dy^2
+  const float2 d2x = __fmul2_rn(__ffma2_rn(__fadd2_rn(aw, na0), f2(gw), __fmul2_rn(__fadd2_rn(ae, na0), f2(ge))),
+                                f2(t.ix2[r][c]));
+  const float2 d2y = __fmul2_rn(__ffma2_rn(__fadd2_rn(as, na0), f2(gs), __fmul2_rn(__fadd2_rn(an, na0), f2(gn))),
+                                f2(d.inv_dy2));
+  const float2 ddy = __fmul2_rn(__fadd2_rn(an, __fmul2_rn(as, m1)), f2(0.5f * d.inv_dy));
+  return __ffma2_rn(ddy, f2(-t.tanR[r]), __fadd2_rn(d2x, d2y));
+}
+
+__device__ __forceinline__ float2 hdiff2(const Dev& d, const LtTile& t, const float (*w)[LT_PX],
+                                        const float (*A)[LT_PX], const float (*B)[LT_PX], int r, int c, bool unit) {
+  const float2 m1 = f2(-1.f);
+  const float2 a0 = pair(A, B, r, c);
+  const float k0 = unit ? 1.f : t.kh[r][c];
+  const float ke = unit ? 1.f : t.kh[r][c + 1], kw = unit ? 1.f : t.kh[r][c - 1];
+  const float kn = unit ? 1.f : t.kh[r + 1][c], ks = unit ? 1.f : t.kh[r - 1][c];
+  const float w0 = w[r][c];
+  const int gj = t.gj[r];
+  // face coefficients: 0.5 (k + k') / dx (or cos_face / dy) times the face gate
+  const float ce = 0.5f * (k0 + ke) * t.ix[r][c] * (w0 * w[r][c + 1]);
+  const float cw = 0.5f * (kw + k0) * t.ix[r][c - 1] * (w[r][c - 1] * w0);
+  const float cn = gj < d.ny - 1 ? 0.5f * (k0 + kn) * d.inv_dy * (w0 * w[r + 1][c]) * t.cfp[r] : 0.f;
+  const float cs = gj > 0 ? 0.5f * (ks + k0) * d.inv_dy * (w[r - 1][c] * w0) * t.cfp[r - 1] : 0.f;
+  const float2 na0 = __fmul2_rn(a0, m1);
+  // (fe - fw) / dx + (fn - fs) / (dy cos), with fw = (a0 - aw) cw = -(aw - a0) cw
+  const float2 x = __ffma2_rn(__fadd2_rn(pair(A, B, r, c - 1), na0), f2(cw),
+                              __fmul2_rn(__fadd2_rn(pair(A, B, r, c + 1), na0), f2(ce)));
+  const float2 y = __ffma2_rn(__fadd2_rn(pair(A, B, r - 1, c), na0), f2(cs),
+                              __fmul2_rn(__fadd2_rn(pair(A, B, r + 1, c), na0), f2(cn)));
+  return __ffma2_rn(x, f2(t.ix[r][c]), __fmul2_rn(y, f2(d.inv_dy * t.icos[r])));
+}
+
 // Node-form d2/dz2 with zero-flux ends (numerics/vertical.py:275-293) and the
 // tracer vertical diffusion at a wet level k of a column, from its values at
 // k - 1 (am), k (a0) and k + 1 (ap): the column is ghost-filled below kbot
@@ -451,12 +505,14 @@ __global__ void __launch_bounds__(LT_X * LT_Y, 4) k_lin_t(Dev d, const float* __
         const int rr = 1 + e / LT_PX, c2 = e % LT_PX;
         if (c2 == 0 || c2 == LT_PX - 1) continue;
         if (do_uv) {
-          t.Lu[rr][c2] = lap_s(d, t, w, t.u[q], rr, c2, false);
-          t.Lv[rr][c2] = lap_s(d, t, w, t.v[q], rr, c2, false);
+          const float2 L = lap2(d, t, w, t.u[q], t.v[q], rr, c2, false);
+          t.Lu[rr][c2] = L.x;
+          t.Lv[rr][c2] = L.y;
         }
         if (do_ts) {
-          t.LT[rr][c2] = hdiff_s(d, t, w, t.T[q], rr, c2, true);
-          t.LS[rr][c2] = hdiff_s(d, t, w, t.S[q], rr, c2, true);
+          const float2 L = hdiff2(d, t, w, t.T[q], t.S[q], rr, c2, true);
+          t.LT[rr][c2] = L.x;
+          t.LS[rr][c2] = L.y;
         }
       }
       __syncthreads();
@@ -472,18 +528,14 @@ __global__ void __launch_bounds__(LT_X * LT_Y, 4) k_lin_t(Dev d, const float* __
       T = Tc;
       S = Sc;
     } else {
-      T = Tc + hdiff_s(d, t, w, t.T[q], r, cc, false) * dth;
-      S = Sc + hdiff_s(d, t, w, t.S[q], r, cc, false) * dth;
-      if (do_ts) {
-        T = T - d.kappa_bi * hdiff_s(d, t, w, t.LT, r, cc, true) * dth;
-        S = S - d.kappa_bi * hdiff_s(d, t, w, t.LS, r, cc, true) * dth;
-      }
-      u = ld(usub, id);
-      v = ld(vsub, id);
-      if (do_uv) {
-        u = u - d.nu_bi * lap_s(d, t, w, t.Lu, r, cc, true) * dth;
-        v = v - d.nu_bi * lap_s(d, t, w, t.Lv, r, cc, true) * dth;
-      }
+      float2 ts = __ffma2_rn(hdiff2(d, t, w, t.T[q], t.S[q], r, cc, false), f2(dth), make_float2(Tc, Sc));
+      if (do_ts) ts = __ffma2_rn(hdiff2(d, t, w, t.LT, t.LS, r, cc, true), f2(-d.kappa_bi * dth), ts);
+      float2 uv = make_float2(ld(usub, id), ld(vsub, id));
+      if (do_uv) uv = __ffma2_rn(lap2(d, t, w, t.Lu, t.Lv, r, cc, true), f2(-d.nu_bi * dth), uv);
+      T = ts.x;
+      S = ts.y;
+      u = uv.x;
+      v = uv.y;
       if (!IMPL) {
         const bool below = k + 1 < d.nz;  // level k + 1 sits in buffer qn
         const float up = below ? t.u[qn][r][cc] : uc, vp = below ? t.v[qn][r][cc] : vc;

@@ -103,6 +103,8 @@ struct zm_solver {
   float *tau_x = nullptr, *tau_y = nullptr, *qheat = nullptr;
   unsigned int* flags = nullptr;
   cudaStream_t cap_stream = nullptr;  // graphs are captured here, launched on the caller's stream
+  cudaStream_t side = nullptr;        // the second branch of the N step (momentum advection)
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   bool graphs_ready = false;
   // set while an ensemble captures this member: the cooperative barotropic
@@ -154,6 +156,9 @@ struct zm_solver {
     for (int g = 0; g < 2; ++g)
       if (graph[g]) cudaGraphExecDestroy(graph[g]);
     if (cap_stream) cudaStreamDestroy(cap_stream);
+    if (side) cudaStreamDestroy(side);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
     for (void* p : allocs) cudaFree(p);
   }
 
@@ -264,6 +269,10 @@ struct zm_solver {
     pb(ZM_K_FZ, s);
     launch_fz(s, d, src.u, src.v, Fz);
     pe(s);
+    momentum_advection_rest(s, src);
+  }
+  // ... its part after the vertical transport Fz: advection and the dealias filter
+  void momentum_advection_rest(cudaStream_t s, const Fields4& src) {
     const dim3 m(32, 8);
     pb(ZM_K_MADV, s);
     ZM_CUDA(launch_pdl(k_madv, dim3((nx + 31) / 32, (ny + MADV_TY - 1) / MADV_TY, nz), m, 0, s, d, src.u, src.v,
@@ -385,9 +394,20 @@ struct zm_solver {
 
   // Nonlinear RK2 step N(dt): src -> dst.
   void nonlinear(cudaStream_t s, const Fields4& src, const Fields4& dst) {
-    momentum_advection_part(s, src);
+    pb(ZM_K_FZ, s);
+    launch_fz(s, d, src.u, src.v, Fz);
+    pe(s);
+    // The momentum advection and its filter (latency-bound) and the stage-1
+    // tracer residual (issue-bound) depend only on the state and Fz: they run
+    // on two streams (two branches of the captured graph) and join before
+    // the pressure part that needs both.
+    ZM_CUDA(cudaEventRecord(ev_fork, s));
+    ZM_CUDA(cudaStreamWaitEvent(side, ev_fork, 0));
+    momentum_advection_rest(side, src);
+    ZM_CUDA(cudaEventRecord(ev_join, side));
     // stage 1: tracers at the old velocity, momentum with the predicted tracers
     tracer_residual(s, 1, src.u, src.v, src.T, src.S, src.T, src.S, Tp, Sp);
+    ZM_CUDA(cudaStreamWaitEvent(s, ev_join, 0));
     PgfArgs a{};
     a.T = Tp; a.S = Sp; a.u1 = src.u; a.v1 = src.v; a.Au = Au; a.Av = Av;
     a.Pu = Pu; a.Pv = Pv; a.uo = up; a.vo = vp; a.dt = (float)dt; a.mode = 1;
@@ -1164,6 +1184,9 @@ void build(zm_solver* s, const zm_grid* g, const zm_params* p) {
     s->bout = s->alloc<double>(ZM_BUDGET_SUMS * 2);
   }
   ZM_CUDA(cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking));
+  ZM_CUDA(cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking));
+  ZM_CUDA(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
+  ZM_CUDA(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
   ZM_CUDA(cudaDeviceSynchronize());
 }
 
