@@ -135,8 +135,8 @@ int zm_create(const zm_grid* grid, const zm_params* params, zm_solver** out);
  * out[9] nu_h subcycles per temporally blocked pass (the halo width), out[10]
  * FFT lines per block, out[11] levels per block of the tracer-advection
  * march, out[12] of the linear-finish march, out[13] tile rows of the
- * vertical-transport march, out[14] of the pressure-gradient march.  Writes
- * min(n, 15) values. */
+ * vertical-transport march, out[14] of the pressure-gradient march, out[15]
+ * warps per nu_h tile (8 or 16).  Writes min(n, 16) values. */
 int zm_info(const zm_solver* s, int32_t* out, int32_t n);
 
 /* Copy a device state (reference layout) into the solver's resident state. */
@@ -296,7 +296,8 @@ int zm_mlp_train_step(zm_mlp_trainer* tr, void* stream, int32_t batch, const flo
 
 /* Autotuner: time, on the resident state and through stages that write only
  * work buffers, the launch shapes that change no result (the nu_h halo
- * width 3..6, i.e. subcycles per temporally blocked pass, the FFT lines per
+ * width 3..6, i.e. subcycles per temporally blocked pass, with 8 or 16 warps
+ * per nu_h tile, the FFT lines per
  * block 1..8, the levels per block of the tracer-advection and linear-finish
  * column marches 5..25, and the tile rows of the vertical-transport and
  * pressure-gradient marches 4 or 8) and keep the fastest; the next zm_advance recaptures its

@@ -104,14 +104,15 @@ __device__ __forceinline__ float colv(const float* __restrict__ a, long long bas
 
 // ------------------------------------------------------------------ L half step
 // nu_h Laplacian subcycles on (u, v) (timestepping/step.py:94-107), several
-// subcycles per pass on one level.  A block covers an NB_W x NB_W tile with
-// 32 x (NB_W / NB_R) threads: lane l of warp w holds columns 2l, 2l+1 of rows
+// subcycles per pass on one level.  A block covers an NB_W wide, NW * NB_R
+// high tile with 32 x NW threads (NW = 8 or 16 warps, chosen by the
+// autotuner): lane l of warp w holds columns 2l, 2l+1 of rows
 // NB_R w .. NB_R w + NB_R - 1 in registers, as (u, v) pairs, with their face
 // coefficients.  East/west neighbours move between lanes by shuffles; the
 // rows above and below a warp's strip pass through shared memory, double
 // buffered, so one barrier per subcycle suffices.  Values at the tile edge
 // are wrong, and the error enters one cell per subcycle: after nsub <= halo
-// subcycles the inner (NB_W - 2 halo)^2 points are exact (halo <= NB_T is a
+// subcycles the inner (NB_W - 2 halo) x (NW NB_R - 2 halo) points are exact (halo <= NB_T is a
 // launch parameter chosen by the autotuner).
 //
 // The Laplacian of numerics/horizontal.py:181-215 is rewritten per point as
@@ -128,16 +129,17 @@ __device__ __forceinline__ float colv(const float* __restrict__ a, long long bas
 // (__ffma2_rn, __fadd2_rn; the same roundings as the scalar form).  Points
 // of the tile edge see their own values as the missing neighbours (their
 // results are discarded with the halo).
-__global__ void __launch_bounds__(32 * (NB_W / NB_R), 2)
+template <int NW>
+__global__ void __launch_bounds__(32 * NW, 16 / NW)
 k_nu_tb(Dev d, const float* __restrict__ u, const float* __restrict__ v, float* __restrict__ uo,
         float* __restrict__ vo, float c, int nsub, int halo) {
-  constexpr int NW = NB_W / NB_R;                 // warps per block
-  const int TI = NB_W - 2 * halo;
+  constexpr int NH = NW * NB_R;                   // tile rows
+  const int TI = NB_W - 2 * halo, TJ = NH - 2 * halo;
   __shared__ float4 edge[2][NW][2][32];           // [parity][warp][0 bottom row, 1 top row][lane]
   pdl_trigger();
   const int lane = threadIdx.x, wp = threadIdx.y;
   const int k = blockIdx.z;
-  const int gx0 = blockIdx.x * TI - halo, gy0 = blockIdx.y * TI - halo;
+  const int gx0 = blockIdx.x * TI - halo, gy0 = blockIdx.y * TJ - halo;
   const int c0 = 2 * lane, r0 = wp * NB_R;
   int gi[2];
 #pragma unroll
@@ -232,7 +234,7 @@ k_nu_tb(Dev d, const float* __restrict__ u, const float* __restrict__ v, float* 
   for (int q = 0; q < NB_R; ++q) {
     const int r = r0 + q;
     const int gj = gy0 + r;
-    if (r < halo || r >= NB_W - halo || gj >= d.ny) continue;
+    if (r < halo || r >= NH - halo || gj >= d.ny) continue;
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int col = c0 + h;
@@ -797,6 +799,14 @@ __global__ void __launch_bounds__(FZ_X * RY) k_fz(Dev d, const float* __restrict
     acc += div * d.vc.dz_node[k];
     Fz[(long long)k * d.plane + cc] = acc;
   }
+}
+
+cudaError_t launch_nu_tb(cudaStream_t s, const Dev& d, int warps, const float* u, const float* v, float* uo,
+                         float* vo, float c, int nsub, int halo) {
+  const int TI = NB_W - 2 * halo, TJ = warps * NB_R - 2 * halo;
+  const dim3 grd((d.nx + TI - 1) / TI, (d.ny + TJ - 1) / TJ, d.nz);
+  if (warps == 16) return launch_pdl(k_nu_tb<16>, grd, dim3(32, 16), 0, s, d, u, v, uo, vo, c, nsub, halo);
+  return launch_pdl(k_nu_tb<8>, grd, dim3(32, 8), 0, s, d, u, v, uo, vo, c, nsub, halo);
 }
 
 void launch_fz(cudaStream_t s, const Dev& d, const float* u, const float* v, float* Fz) {

@@ -133,7 +133,9 @@ __global__ void k_budget_final(const double* partial, int nblocks, double* out);
 __global__ void k_forcing_blend(Dev d, const float* stack, int prev, int cur, int next, float w_prev, float w_cur,
                                 float w_next, float* out);
 __global__ void k_barrier_probe(unsigned* bar, unsigned* err, unsigned expected, unsigned max_polls);
-__global__ void k_nu_tb(Dev d, const float* u, const float* v, float* uo, float* vo, float c, int nsub, int halo);
+// the temporally blocked nu_h subcycles with 8 or 16 warps per tile (NB_W x 8 warps * NB_R)
+cudaError_t launch_nu_tb(cudaStream_t s, const Dev& d, int warps, const float* u, const float* v, float* uo,
+                         float* vo, float c, int nsub, int halo);
 __global__ void k_nu_gates(Dev d, unsigned char* gate);
 void launch_lin_t(cudaStream_t s, const Dev& d, const float* usub, const float* vsub, const float* u0,
                   const float* v0, const float* T0, const float* S0, float* uo, float* vo, float* To, float* So,

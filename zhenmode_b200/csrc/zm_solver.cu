@@ -70,6 +70,7 @@ struct zm_solver {
   int bblocks = 0;
   // learned vertical-mixing closure (off until zm_set_closure)
   int nu_halo = NB_T;            // nu_h subcycles per pass (autotuned)
+  int nu_warps = 8;              // warps (tile rows / NB_R) of the nu_h tiles (autotuned)
   bool want_tune = false;
   bool tuned = false;
   bool closure_on = false;
@@ -180,15 +181,12 @@ struct zm_solver {
       const float dts = (float)(dt / 2.0 / n_nu);
       const float* a = src.u;
       const float* c = src.v;
-      const int TI = NB_W - 2 * nu_halo;
-      const dim3 blk(32, NB_W / NB_R);
-      const dim3 grd((nx + TI - 1) / TI, (ny + TI - 1) / TI, nz);
       int done = 0, pass = 0;
       while (done < n_nu) {
         const int nsub = std::min(nu_halo, n_nu - done);
         const Fields4& o = (pass % 2 == 0) ? W1 : W2;
         pb(ZM_K_NU_SUB, s);
-        ZM_CUDA(launch_pdl(k_nu_tb, grd, blk, 0, s, d, a, c, o.u, o.v, dts, nsub, nu_halo));
+        ZM_CUDA(launch_nu_tb(s, d, nu_warps, a, c, o.u, o.v, dts, nsub, nu_halo));
         pe(s);
         a = o.u;
         c = o.v;
@@ -568,16 +566,20 @@ struct zm_solver {
       const Fields4& in = st[cur];
       if (d.nu_h != 0.f) {
         float best = 1e30f;
-        int pick = nu_halo;
-        for (int h = 3; h <= NB_T; ++h) {
-          nu_halo = h;
-          const float ms = time_ms([&] { linear_half(s, in, s1); });
-          if (ms < best) {
-            best = ms;
-            pick = h;
+        int pick = nu_halo, pick_w = nu_warps;
+        for (int wq : {8, 16})
+          for (int h = 3; h <= NB_T; ++h) {
+            nu_halo = h;
+            nu_warps = wq;
+            const float ms = time_ms([&] { linear_half(s, in, s1); });
+            if (ms < best) {
+              best = ms;
+              pick = h;
+              pick_w = wq;
+            }
           }
-        }
         nu_halo = pick;
+        nu_warps = pick_w;
       }
       float best = 1e30f;
       int pick = fft_lines;
@@ -1217,10 +1219,10 @@ int zm_create(const zm_grid* grid, const zm_params* params, zm_solver** out) {
 
 int zm_info(const zm_solver* s, int32_t* out, int32_t n) {
   if (!s || !out) return ZM_ERR_INVALID;
-  const int32_t v[15] = {s->n_subcyc, s->n_nu, s->adv_nsub, s->conv_nsub, s->P, (int32_t)(s->bytes >> 20),
+  const int32_t v[16] = {s->n_subcyc, s->n_nu, s->adv_nsub, s->conv_nsub, s->P, (int32_t)(s->bytes >> 20),
                          s->kernels_per_step, s->bt_blocks, s->bt.cap_active, s->nu_halo, s->fft_lines,
-                         s->d.ta_kc, s->d.lt_kc, s->d.fz_rows, s->d.pg_rows};
-  for (int q = 0; q < n && q < 15; ++q) out[q] = v[q];
+                         s->d.ta_kc, s->d.lt_kc, s->d.fz_rows, s->d.pg_rows, s->nu_warps};
+  for (int q = 0; q < n && q < 16; ++q) out[q] = v[q];
   return ZM_OK;
 }
 

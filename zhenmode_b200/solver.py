@@ -208,9 +208,10 @@ class _Solver:
 
     def launch_shapes(self):
         """Every launch shape the autotuner chooses, by name."""
-        info = (ctypes.c_int32 * 15)()
-        self.lib.zm_info(self.handle, info, 15)
-        return {"nu_h_subcycles_per_pass": int(info[9]), "fft_lines_per_block": int(info[10]),
+        info = (ctypes.c_int32 * 16)()
+        self.lib.zm_info(self.handle, info, 16)
+        return {"nu_h_subcycles_per_pass": int(info[9]), "nu_h_warps_per_tile": int(info[15]),
+                "fft_lines_per_block": int(info[10]),
                 "tracer_adv_levels_per_block": int(info[11]), "linear_finish_levels_per_block": int(info[12]),
                 "fz_tile_rows": int(info[13]), "pgf_tile_rows": int(info[14])}
 
