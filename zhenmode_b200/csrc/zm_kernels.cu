@@ -876,6 +876,8 @@ __global__ void __launch_bounds__(256) k_madv(Dev d, const float* __restrict__ u
   const int j0 = blockIdx.y * MADV_TY;
   const int k = blockIdx.z;
   pdl_wait();  // u, v, Fz come from the preceding kernels
+  // rows unrolled by four so that their (independent, latency-bound) loads overlap
+#pragma unroll 4
   for (int r = threadIdx.y; r < MADV_TY + 4; r += blockDim.y) {
     int jj = j0 - 2 + r;
     jj = jj < 0 ? 0 : (jj >= d.ny ? d.ny - 1 : jj);
