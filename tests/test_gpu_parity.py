@@ -93,7 +93,10 @@ def test_steps_match_reference_goldens(name):
     got_n = gu.run_steps(gpu, state, nsteps)
     want_n = {k: data[f"out{nsteps}_{k}"] for k in gu.FIELDS}
     errs = gu.errors(got_n, want_n)
-    assert max(errs.values()) < 10 * STEP_TOL, errs
+    print(name, nsteps, "steps, relative L2:", errs)
+    # Each step rounds the state to float32 and adds at most STEP_TOL against the
+    # float64 reference; over n steps the differences add at most linearly.
+    assert max(errs.values()) < nsteps * STEP_TOL, errs
 
 
 def test_production_options_at_reduced_size():
