@@ -377,6 +377,7 @@ def run_precision(args):
     solver.check(solver.lib.zm_status(solver.handle, ctypes.byref(code)), "zm_status")
     nsteps = days * per_day
     ms = total_ms / nsteps
+    audit = budget_audit_day(step, out, taux, qh, (days * per_day + max(args.warmup, 3)), per_day, dt)
     heat = [d[4] for d in daily]
     salt = [d[5] for d in daily]
     drift = lambda v: max(abs(v[i + 1] - v[i]) / abs(v[i]) for i in range(len(v) - 1))
@@ -393,13 +394,37 @@ def run_precision(args):
                        "form": "precision", "monitor_code": int(code.value)},
             "budgets": {"heat_content_J": heat, "salt_content_kg": salt,
                         "max_relative_change_per_day": {"heat": drift(heat), "salt": drift(salt)},
-                        "total_volume_m3": daily[-1][6], "sums": "float64, compensated, fixed order"},
+                        "total_volume_m3": daily[-1][6], "sums": "float64, compensated, fixed order",
+                        "ledger_day_after": audit},
             "roofline": {"bound": "hbm", "step_stage_bytes": bstep, "step_frac": bstep / (ms * 1e-3) / 1e9 / peak,
                          "peak": peak, "peak_kind": peak_kind, "unit": "GB/s"},
             "gpu_launches": nsteps * (solver.kernels_per_step() + 3), "clocks": clk, "e2e": None,
             "cpu_baseline": None}
     print(json.dumps(line))
     return 0
+
+
+def budget_audit_day(step, fields, taux, qh, n0, per_day, dt):
+    """One more simulated day of the precision form through the stage/source
+    ledger (the reference's budget audit step): per quantity (heat J, salt kg,
+    volume m^3) the observed change of the day, the summed source inputs
+    (surface heat and salt fluxes, restoring, sponge), and the budget residual
+    observed - sources with its ratio to the change scale."""
+    from zhenmode_b200 import JaxStateG, ledger
+
+    advance = ledger.make_budget_step(step)
+    st = JaxStateG(*fields, 0.0)
+    total = ledger.empty_budget()
+    for n in range(per_day):
+        step.set_forcing_seasonal(tau_x=taux, q_heat=qh, day=(n0 + n) * dt / 86400.0)
+        st, led = advance(st)
+        total = ledger.accumulate_budget(total, led)
+    names = ("heat_J", "salt_kg", "volume_m3")
+    obs, src, res, scale = (total["observed_change"], total["source_inputs"].sum(axis=0),
+                            total["budget_residual"], total["change_scale"])
+    return {n: {"observed_change": float(obs[i]), "source_inputs": float(src[i]), "residual": float(res[i]),
+                "residual_over_change_scale": float(abs(res[i]) / scale[i]) if scale[i] > 0 else None}
+            for i, n in enumerate(names)}
 
 
 def train_closure(step, st, dt, days):

@@ -876,8 +876,6 @@ __global__ void __launch_bounds__(256) k_madv(Dev d, const float* __restrict__ u
   const int j0 = blockIdx.y * MADV_TY;
   const int k = blockIdx.z;
   pdl_wait();  // u, v, Fz come from the preceding kernels
-  // rows unrolled by four so that their (independent, latency-bound) loads overlap
-#pragma unroll 4
   for (int r = threadIdx.y; r < MADV_TY + 4; r += blockDim.y) {
     int jj = j0 - 2 + r;
     jj = jj < 0 ? 0 : (jj >= d.ny ? d.ny - 1 : jj);
@@ -932,8 +930,7 @@ constexpr int TA_CELLS = TA_PX * TA_PY;
 static_assert(TA_CELLS <= 2 * TA_X * TA_Y, "two tile cells per thread at most");
 
 struct TaTile {
-  float T[TA_NB][TA_PY][TA_PX];
-  float S[TA_NB][TA_PY][TA_PX];
+  float2 ts[TA_NB][TA_PY][TA_PX];  // (T, S) of a cell, side by side for the paired FP32 face arithmetic
   float u[TA_NB][TA_PY][TA_PX];
   float v[TA_NB][TA_PY][TA_PX];
   float w[2][TA_PY][TA_PX];
@@ -957,43 +954,56 @@ __device__ __forceinline__ float ta_face_value(bool pos, float cm, float c0, flo
   return 0.5f * (c0 + c1);
 }
 
-// T and S fluxes through the x face between tile columns cc and cc+1 of row r
+// Minmod slopes of T and S at once (dynamics/transport.py:199-213): the
+// differences on the paired FP32 instructions, the sign test per tracer.
+__device__ __forceinline__ float2 minmod_slope2(float2 cm, float2 c0, float2 cp) {
+  const float2 m1 = f2(-1.f);
+  const float2 l = __ffma2_rn(cm, m1, c0), r = __ffma2_rn(c0, m1, cp);
+  const float mx = fminf(fabsf(l.x), fabsf(r.x)), my = fminf(fabsf(l.y), fabsf(r.y));
+  return make_float2((l.x > 0.f && r.x > 0.f) ? mx : ((l.x < 0.f && r.x < 0.f) ? -mx : 0.f),
+                     (l.y > 0.f && r.y > 0.f) ? my : ((l.y < 0.f && r.y < 0.f) ? -my : 0.f));
+}
+
+// Limited (T, S) face state, the paired form of ta_face_value.  The wet
+// weights are 0 or 1, so applying their product once to both slopes rounds
+// like the per-tracer product s w0 wm wp.
+template <int LIM>
+__device__ __forceinline__ float2 ta_face_value2(bool pos, float2 cm, float2 c0, float2 c1, float2 cp, float wm,
+                                                 float w0, float w1, float wp) {
+  if (LIM == 2) {
+    const float2 a = pos ? cm : cp, b = pos ? c0 : c1, c = pos ? c1 : c0;
+    const float wgt = pos ? w0 * wm * w1 : w1 * wp * w0;
+    return __ffma2_rn(f2(0.5f * wgt), minmod_slope2(a, b, c), b);
+  }
+  if (LIM == 1) return pos ? c0 : c1;
+  return __fmul2_rn(f2(0.5f), __fadd2_rn(c0, c1));
+}
+
+// (T, S) fluxes through the x face between tile columns cc and cc+1 of row r
 // of level buffer q (wet flags in buffer wq)
 template <int LIM>
-__device__ __forceinline__ void ta_faces_x(const TaTile& t, int q, int wq, int r, int cc, float& fT, float& fS) {
+__device__ __forceinline__ float2 ta_faces_x(const TaTile& t, int q, int wq, int r, int cc) {
   const float w0 = t.w[wq][r][cc], we = t.w[wq][r][cc + 1];
   const float ux = 0.5f * (t.u[q][r][cc] + t.u[q][r][cc + 1]);
   const bool pos = ux >= 0.f;
   const float wm = t.w[wq][r][cc - 1], wp = t.w[wq][r][cc + 2];
-  const float cT = ta_face_value<LIM>(pos, t.T[q][r][cc - 1], t.T[q][r][cc], t.T[q][r][cc + 1], t.T[q][r][cc + 2],
-                                      wm, w0, we, wp);
-  const float cS = ta_face_value<LIM>(pos, t.S[q][r][cc - 1], t.S[q][r][cc], t.S[q][r][cc + 1], t.S[q][r][cc + 2],
-                                      wm, w0, we, wp);
-  const float g = w0 * we;
-  fT = ux * cT * g;
-  fS = ux * cS * g;
+  const float2 c = ta_face_value2<LIM>(pos, t.ts[q][r][cc - 1], t.ts[q][r][cc], t.ts[q][r][cc + 1],
+                                       t.ts[q][r][cc + 2], wm, w0, we, wp);
+  return __fmul2_rn(f2(ux * (w0 * we)), c);
 }
 
-// T and S fluxes through the y face between tile rows r and r+1 (global rows
+// (T, S) fluxes through the y face between tile rows r and r+1 (global rows
 // gj, gj+1); zero through the closed walls
 template <int LIM>
-__device__ __forceinline__ void ta_faces_y(const Dev& d, const TaTile& t, int q, int wq, int r, int cc, int gj,
-                                           float& fT, float& fS) {
-  if (gj < 0 || gj >= d.ny - 1) {
-    fT = fS = 0.f;
-    return;
-  }
+__device__ __forceinline__ float2 ta_faces_y(const Dev& d, const TaTile& t, int q, int wq, int r, int cc, int gj) {
+  if (gj < 0 || gj >= d.ny - 1) return f2(0.f);
   const float w0 = t.w[wq][r][cc], wn = t.w[wq][r + 1][cc];
   const float vy = 0.5f * (t.v[q][r][cc] + t.v[q][r + 1][cc]);
   const bool pos = vy >= 0.f;
   const float wm = t.w[wq][r - 1][cc], wp = t.w[wq][r + 2][cc];
-  const float cT = ta_face_value<LIM>(pos, t.T[q][r - 1][cc], t.T[q][r][cc], t.T[q][r + 1][cc], t.T[q][r + 2][cc],
-                                      wm, w0, wn, wp);
-  const float cS = ta_face_value<LIM>(pos, t.S[q][r - 1][cc], t.S[q][r][cc], t.S[q][r + 1][cc], t.S[q][r + 2][cc],
-                                      wm, w0, wn, wp);
-  const float g = w0 * wn, cf = __ldg(d.cfp + gj);
-  fT = vy * cT * g * cf;
-  fS = vy * cS * g * cf;
+  const float2 c = ta_face_value2<LIM>(pos, t.ts[q][r - 1][cc], t.ts[q][r][cc], t.ts[q][r + 1][cc],
+                                       t.ts[q][r + 2][cc], wm, w0, wn, wp);
+  return __fmul2_rn(__fmul2_rn(f2(vy * (w0 * wn)), c), f2(__ldg(d.cfp + gj)));
 }
 
 template <int LIM>
@@ -1024,13 +1034,14 @@ __global__ void __launch_bounds__(TA_X * TA_Y, 5) k_tracer_adv_t(Dev d, const fl
     if (k < d.nz && k <= k1) {  // level k1 only for the column neighbour below the chunk
       const long long off = (long long)k * d.plane;
       const int q = k % TA_NB;
-      cp_async4(&t.T[q][0][0] + e0, T + off + s0);
-      cp_async4(&t.S[q][0][0] + e0, S + off + s0);
+      float* ts = &t.ts[q][0][0].x;
+      cp_async4(ts + 2 * e0, T + off + s0);
+      cp_async4(ts + 2 * e0 + 1, S + off + s0);
       cp_async4(&t.u[q][0][0] + e0, u + off + s0);
       cp_async4(&t.v[q][0][0] + e0, v + off + s0);
       if (has1) {
-        cp_async4(&t.T[q][0][0] + e1, T + off + s1);
-        cp_async4(&t.S[q][0][0] + e1, S + off + s1);
+        cp_async4(ts + 2 * e1, T + off + s1);
+        cp_async4(ts + 2 * e1 + 1, S + off + s1);
         cp_async4(&t.u[q][0][0] + e1, u + off + s1);
         cp_async4(&t.v[q][0][0] + e1, v + off + s1);
       }
@@ -1054,9 +1065,10 @@ __global__ void __launch_bounds__(TA_X * TA_Y, 5) k_tracer_adv_t(Dev d, const fl
   const int kbt = kbot_of(bits);
   const float ix = __ldg(d.inv_dx + base), ysc = d.inv_dy * __ldg(d.inv_cos + jc);
   const int r = ty + TA_H, cc = tx + TA_H;
-  // T, S of the level above and Fz of the current level
-  float ckm = k0 > 0 ? ld(T, base + (long long)(k0 - 1) * d.plane) : 0.f;
-  float skm = k0 > 0 ? ld(S, base + (long long)(k0 - 1) * d.plane) : 0.f;
+  // (T, S) of the level above and Fz of the current level
+  float2 cm = k0 > 0 ? make_float2(ld(T, base + (long long)(k0 - 1) * d.plane),
+                                   ld(S, base + (long long)(k0 - 1) * d.plane))
+                     : f2(0.f);
   float fzk = ld(Fz, base + (long long)k0 * d.plane);
   for (int k = k0; k < k1; ++k) {
     cp_async_wait<0>();  // this thread's copies of levels k and k + 1 are done
@@ -1068,50 +1080,41 @@ __global__ void __launch_bounds__(TA_X * TA_Y, 5) k_tracer_adv_t(Dev d, const fl
     if (!in) continue;
     const int q = k % TA_NB, qn = (k + 1) % TA_NB, wq = k & 1;
     const float w0 = t.w[wq][r][cc];
-    const float ck = t.T[q][r][cc], sk = t.S[q][r][cc];
+    const float2 ck = t.ts[q][r][cc];
     if (topT && k == 0) {  // ledger mode: the rigid-lid surface flux Fz[0] c[0] of the substep, summed
-      topT[base] = (first ? 0.f : topT[base]) + fzk * ck;
-      topS[base] = (first ? 0.f : topS[base]) + fzk * sk;
+      topT[base] = (first ? 0.f : topT[base]) + fzk * ck.x;
+      topS[base] = (first ? 0.f : topS[base]) + fzk * ck.y;
     }
-    float aT = 0.f, aS = 0.f;
+    float2 a = f2(0.f);
     if (w0 != 0.f) {
-      float fxeT, fxeS, fxwT, fxwS, fynT, fynS, fysT, fysS;
-      ta_faces_x<LIM>(t, q, wq, r, cc, fxeT, fxeS);
-      ta_faces_x<LIM>(t, q, wq, r, cc - 1, fxwT, fxwS);
-      ta_faces_y<LIM>(d, t, q, wq, r, cc, jc, fynT, fynS);
-      ta_faces_y<LIM>(d, t, q, wq, r - 1, cc, jc - 1, fysT, fysS);
-      const float hT = (fxeT - fxwT) * ix + (fynT - fysT) * ysc;
-      const float hS = (fxeS - fxwS) * ix + (fynS - fysS) * ysc;
-      const float fz_k = fzk;
-      float upT, upS, dnT = 0.f, dnS = 0.f;
+      const float2 m1 = f2(-1.f);
+      const float2 fxe = ta_faces_x<LIM>(t, q, wq, r, cc), fxw = ta_faces_x<LIM>(t, q, wq, r, cc - 1);
+      const float2 fyn = ta_faces_y<LIM>(d, t, q, wq, r, cc, jc), fys = ta_faces_y<LIM>(d, t, q, wq, r - 1, cc, jc - 1);
+      const float2 h = __ffma2_rn(__ffma2_rn(fxw, m1, fxe), f2(ix), __fmul2_rn(__ffma2_rn(fys, m1, fyn), f2(ysc)));
+      // vertical donor-cell fluxes through the top (up) and bottom (dn) faces;
+      // the wet weights are 0 or 1, so folding them into Fz rounds like the
+      // product Fz c g
+      float2 up, dn = f2(0.f);
       if (k == 0) {
-        upT = fz_k * ck;
-        upS = fz_k * sk;
+        up = __fmul2_rn(f2(fzk), ck);
       } else {
-        const float g = wetf(bits, k - 1) * w0;
-        upT = fz_k * (fz_k > 0.f ? ckm : ck) * g;
-        upS = fz_k * (fz_k > 0.f ? skm : sk) * g;
+        up = __fmul2_rn(f2(fzk * (wetf(bits, k - 1) * w0)), fzk > 0.f ? cm : ck);
       }
       if (k + 1 < d.nz) {
-        const float g = w0 * wetf(bits, k + 1);
-        const float fz_n = fzn;
         // ghost fill below the deepest wet level: node k+1 carries node k's value
-        const bool below = k + 1 <= kbt;
-        const float tn = below ? t.T[qn][r][cc] : ck, sn = below ? t.S[qn][r][cc] : sk;
-        dnT = fz_n * (fz_n > 0.f ? ck : tn) * g;
-        dnS = fz_n * (fz_n > 0.f ? sk : sn) * g;
+        const float2 cn = k + 1 <= kbt ? t.ts[qn][r][cc] : ck;
+        dn = __fmul2_rn(f2(fzn * (w0 * wetf(bits, k + 1))), fzn > 0.f ? ck : cn);
       }
-      aT = -(hT + (dnT - upT) * d.vc.inv_dz_node[k]) * w0;
-      aS = -(hS + (dnS - upS) * d.vc.inv_dz_node[k]) * w0;
+      a = __fmul2_rn(__ffma2_rn(__ffma2_rn(up, m1, dn), f2(d.vc.inv_dz_node[k]), h), f2(-w0));
     }
-    accT[id] = first ? aT : accT[id] + aT;
-    accS[id] = first ? aS : accS[id] + aS;
+    accT[id] = first ? a.x : accT[id] + a.x;
+    accS[id] = first ? a.y : accS[id] + a.y;
     if (!last) {
-      Tn[id] = ck + aT * dts;
-      Sn[id] = sk + aS * dts;
+      const float2 cnew = __ffma2_rn(a, f2(dts), ck);
+      Tn[id] = cnew.x;
+      Sn[id] = cnew.y;
     }
-    ckm = ck;
-    skm = sk;
+    cm = ck;
     fzk = fzn;
   }
 }
