@@ -42,15 +42,22 @@ __device__ __forceinline__ int band_of(int ny, int nb, int j) {
 
 constexpr int BT_PX = BT_TX + 2 * BT_H, BT_PY = BT_TY + 2 * BT_H;
 
+// Backward-Euler Coriolis with the implicit linear drag
+// (barotropic.py:86-265): u = (u* + fd v*) drag / (1 + fd^2), fd = f dt_bt.
+// The factor drag / (1 + fd^2) is static per cell; both paths form it here.
+__device__ __forceinline__ double bt_drag_factor(double fd, double drag) { return drag / (1.0 + fd * fd); }
+
 struct BtTile {
   double U[BT_PY][BT_PX], V[BT_PY][BT_PX];  // velocities (capped at the subcycle start)
   double E[BT_PY][BT_PX];                   // eta; overwritten in place by eta* on the tile + ring
   double ix[BT_PY][BT_PX];                  // 1/dx
   float w[BT_PY][BT_PX];                    // 2-D wet mask
   double cosl[BT_PY], cfp[BT_PY], cfm[BT_PY];
+  double iyc[BT_PY];                        // 1/(dy cos(lat)) of the row
   double mean[3][2 * ZM_BT_MAX_NB];         // band-row means: eta*, u, v
   double red[BT_THREADS];
-  double fx[BT_TY][BT_TX], fy[BT_TY][BT_TX], fc[BT_TY][BT_TX];  // forcing and f of the owned cells
+  double fx[BT_TY][BT_TX], fy[BT_TY][BT_TX];  // forcing of the owned cells
+  double fd[BT_TY][BT_TX], rd[BT_TY][BT_TX];  // f dt and drag / (1 + (f dt)^2) of the owned cells
   int gj[BT_PY];                            // global row, -1 beyond the walls
   int gx[BT_PX];                            // global column (periodic wrap)
   unsigned char own_c[BT_PX];               // column owned by this block
@@ -74,7 +81,7 @@ __device__ __forceinline__ double eta_new(const Dev& d, const BtArgs& a, const B
     const double ws = t.w[r - 1][c];
     fs = 0.5 * (t.V[r - 1][c] * ws + v0) * (ws * w0) * t.cfp[r - 1];
   }
-  const double div = div_x + (fn - fs) * d.inv_dy_d / t.cosl[r];
+  const double div = div_x + (fn - fs) * t.iyc[r];
   return (t.E[r][c] - a.dtH * div) * w0;
 }
 
@@ -165,6 +172,7 @@ __device__ bool refill(const Dev& d, const BtArgs& a, BtTile& t, const double* f
 size_t bt_tile_smem() { return sizeof(BtTile); }
 
 __global__ void __launch_bounds__(BT_THREADS, 4) k_bt_loop(Dev d, BtArgs a) {
+  grid_barrier_begin(a.bar);
   extern __shared__ double bt_smem[];
   BtTile& t = *reinterpret_cast<BtTile*>(bt_smem);
   const int tid = threadIdx.x, nt = blockDim.x;
@@ -188,6 +196,7 @@ __global__ void __launch_bounds__(BT_THREADS, 4) k_bt_loop(Dev d, BtArgs a) {
     t.cosl[r] = (double)__ldg(d.cosl + jc);
     t.cfp[r] = (double)__ldg(d.cfp + jc);
     t.cfm[r] = (double)__ldg(d.cfm + jc);
+    t.iyc[r] = d.inv_dy_d / t.cosl[r];
   }
   __syncthreads();
   for (int e = tid; e < NC; e += nt) {
@@ -209,13 +218,15 @@ __global__ void __launch_bounds__(BT_THREADS, 4) k_bt_loop(Dev d, BtArgs a) {
     const int r = e / BT_TX, c = e - r * BT_TX;
     const int gj = t.gj[r + BT_H];
     if (gj < 0 || !t.own_c[c + BT_H]) {
-      t.fx[r][c] = t.fy[r][c] = t.fc[r][c] = 0.0;
+      t.fx[r][c] = t.fy[r][c] = t.fd[r][c] = t.rd[r][c] = 0.0;
       continue;
     }
     const int g = idx2(d, gj, t.gx[c + BT_H]);
     t.fx[r][c] = a.Fx[g];
     t.fy[r][c] = a.Fy[g];
-    t.fc[r][c] = __ldg(d.fcor_d + g);
+    const double fd = __ldg(d.fcor_d + g) * a.dtb;
+    t.fd[r][c] = fd;
+    t.rd[r][c] = bt_drag_factor(fd, a.drag);
   }
   __syncthreads();
   const double g9 = 9.81;
@@ -304,13 +315,12 @@ __global__ void __launch_bounds__(BT_THREADS, 4) k_bt_loop(Dev d, BtArgs a) {
       double dyp = 0.0, dym = 0.0;
       if (j < d.ny - 1) dyp = (t.E[r + 1][c] - e0) * (w0 * t.w[r + 1][c]) * t.cfp[r];
       if (j > 0) dym = (e0 - t.E[r - 1][c]) * (w0 * t.w[r - 1][c]) * t.cfm[r];
-      const double gy = (d.inv_dy_d / t.cosl[r]) * 0.5 * (dyp + dym);
+      const double gy = t.iyc[r] * 0.5 * (dyp + dym);
       const double us = t.U[r][c] + a.dtb * (-g9 * gx + t.fx[r - BT_H][c - BT_H]);
       const double vs = t.V[r][c] + a.dtb * (-g9 * gy + t.fy[r - BT_H][c - BT_H]);
-      const double fd = t.fc[r - BT_H][c - BT_H] * a.dtb;
-      const double den = 1.0 + fd * fd;
-      double un = (us + fd * vs) / den * a.drag * w0;
-      double vn = (vs - fd * us) / den * a.drag * w0;
+      const double fd = t.fd[r - BT_H][c - BT_H], rd = t.rd[r - BT_H][c - BT_H];
+      double un = (us + fd * vs) * rd * w0;
+      double vn = (vs - fd * us) * rd * w0;
       if (a.sponge) {
         un *= a.es[g];
         vn *= a.es[g];
@@ -378,7 +388,7 @@ __global__ void __launch_bounds__(256) k_bt_eta(Dev d, const double* __restrict_
     const double ws = __ldg(d.wet2 + cs);
     fs = 0.5 * (vbt[cs] * ws + v0) * (ws * w0) * (double)__ldg(d.cfp + j - 1);
   }
-  const double div = div_x + (fn - fs) * d.inv_dy_d / (double)__ldg(d.cosl + j);
+  const double div = div_x + (fn - fs) * (d.inv_dy_d / (double)__ldg(d.cosl + j));
   eta_o[c] = (eta[c] - dtH * div) * w0;
 }
 
@@ -406,10 +416,9 @@ __global__ void __launch_bounds__(256) k_bt_vel(Dev d, const double* __restrict_
   const double gy = (d.inv_dy_d / (double)__ldg(d.cosl + j)) * 0.5 * (dyp + dym);
   const double us = ubt[c] + dtb * (-9.81 * gx + Fx[c]);
   const double vs = vbt[c] + dtb * (-9.81 * gy + Fy[c]);
-  const double fd = __ldg(d.fcor_d + c) * dtb;
-  const double den = 1.0 + fd * fd;
-  double un = (us + fd * vs) / den * drag * w0;
-  double vn = (vs - fd * us) / den * drag * w0;
+  const double fd = __ldg(d.fcor_d + c) * dtb, rd = bt_drag_factor(fd, drag);
+  double un = (us + fd * vs) * rd * w0;
+  double vn = (vs - fd * us) * rd * w0;
   if (sv) {
     un *= sv[c];
     vn *= sv[c];
@@ -500,6 +509,7 @@ __global__ void __launch_bounds__(256) k_eta_to_float(Dev d, const double* __res
 // gridDim.x blocks arrive, so with expected > gridDim.x every block gives up
 // after max_polls polls and records ZM_BT_ERR_BARRIER.
 __global__ void k_barrier_probe(unsigned* bar, unsigned* err, unsigned expected, unsigned max_polls) {
+  grid_barrier_begin(bar);
   grid_barrier(bar, err, expected, max_polls);
 }
 

@@ -293,6 +293,7 @@ __global__ void __launch_bounds__(256) k_proj_rhs(Dev d, const float* __restrict
 }
 
 __global__ void __launch_bounds__(PJ_THREADS, 1) k_proj_cg(Dev d, ProjArgs a) {
+  grid_barrier_begin(a.bar);
   const bool ident = a.minv == nullptr;
   const int ncell = d.nx * d.ny;
   const int stride = gridDim.x * blockDim.x;
