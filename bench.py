@@ -422,8 +422,16 @@ def budget_audit_day(step, fields, taux, qh, n0, per_day, dt):
     names = ("heat_J", "salt_kg", "volume_m3")
     obs, src, res, scale = (total["observed_change"], total["source_inputs"].sum(axis=0),
                             total["budget_residual"], total["change_scale"])
+    # what the fixed-node inventory leaves outside the sources (the reference
+    # ledger reports these as diagnostics, not sources): the advective flux
+    # through the rigid-lid surface, the eta x surface-tracer change, and the
+    # closure of the stage decomposition (observed - sum of stage changes)
+    advb, disp, dec = (total["advection_boundary_changes"], total["surface_displacement_tracer_change"],
+                       total["decomposition_residual"])
     return {n: {"observed_change": float(obs[i]), "source_inputs": float(src[i]), "residual": float(res[i]),
-                "residual_over_change_scale": float(abs(res[i]) / scale[i]) if scale[i] > 0 else None}
+                "residual_over_change_scale": float(abs(res[i]) / scale[i]) if scale[i] > 0 else None,
+                "surface_advective_flux": float(advb[i]), "surface_displacement_tracer_change": float(disp[i]),
+                "stage_decomposition_residual": float(dec[i])}
             for i, n in enumerate(names)}
 
 
@@ -624,6 +632,27 @@ def main():
         e2e = {"value": world * sim_years_per_day(ems, wl.dt), "unit": "sim-years/day", "ms_per_step": ems,
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes}
 
+    # the reference runtime's call (run_loop.py:56): step(JaxStateG) on device
+    # tensors in the reference layout, each call loading the state through the
+    # ABI, running the step graph and storing the result into new tensors
+    dropin = None
+    if args.e2e_steps > 0:
+        cur = step(st)
+        torch.cuda.synchronize()
+        e4 = torch.cuda.Event(enable_timing=True)
+        e5 = torch.cuda.Event(enable_timing=True)
+        t_host = time.perf_counter()
+        e4.record(stream)
+        for _ in range(args.e2e_steps):
+            cur = step(cur)
+        e5.record(stream)
+        torch.cuda.synchronize()
+        t_host = (time.perf_counter() - t_host) * 1e3 / args.e2e_steps
+        dms = max_over_ranks(e4.elapsed_time(e5) / args.e2e_steps)
+        dropin = {"ms_per_call": dms, "host_ms_per_call": t_host, "over_resident_step_ms": dms - ms,
+                  "call": "step(JaxStateG of CUDA tensors), reference layout in and out"}
+        del cur
+
     chosen = None
     if args.form == "plain" and not args.no_learned and world == 1:
         chosen = chosen_form(step, st, wl.dt, grid, solver, args, ms)
@@ -659,6 +688,8 @@ def main():
             line["closure"] = closure_info
         if chosen is not None:
             line["chosen_form"] = chosen
+        if dropin is not None:
+            line["dropin_step_call"] = dropin
         if args.form == "projected":
             it = step.projection_stats()
             line["projection"] = {"cg_iterations": list(it[:3]), "refinement_solves": it[3],

@@ -139,10 +139,13 @@ def _moving(p, T, S, seed=5, amp=0.1):
     return st
 
 
-@pytest.mark.parametrize("shape", [(24, 16, 6), (90, 45, 15), (180, 24, 10)])
+@pytest.mark.parametrize("shape", [(24, 16, 6), (90, 45, 15), (180, 24, 10), (360, 20, 6), (720, 16, 4),
+                                   (800, 12, 4)])
 def test_momentum_advection_part_matches_oracle(shape):
     """Dealiased advection + wind part of the momentum residual (stage 4),
-    including grids whose longitude mask drops the +-nx/3 bins."""
+    including grids whose longitude mask drops the +-nx/3 bins; widths 180,
+    360, 720 and 800 take the register-resident filter, 24 and 90 the
+    shared-memory one."""
     from oracle.params import RHO_0
     grid, physics, dt, kw, T, S = workloads.make_case("plain", *shape, dtype="float32")
     gpu, p = gu.build_pair(grid, physics, dt, kw)

@@ -41,6 +41,9 @@ struct FftPlan {
   const int* base_tab;          // Stockham output base of each butterfly
   const float2* stage_tw;       // exp(-2 pi i (k r n / (ns R) mod n) / n) per butterfly and r >= 1
   const unsigned char* keepbin; // 1 where bin m survives the 2/3 rule, m < n
+  // register-resident form for n = r1 r2 r3 (0 when n has no supported split)
+  int r1, r2, r3;
+  const float2* tw_full;        // exp(-2 pi i j / n), j < n (float64-derived)
 };
 
 struct PgfArgs {
@@ -150,6 +153,13 @@ void launch_tracer_terms(cudaStream_t s, const Dev& d, const float* T, const flo
 __global__ void k_madv(Dev d, const float* u, const float* v, const float* Fz, float* Ayu, float* Ayv);
 __global__ void k_dealias_lon(Dev d, FftPlan plan, const float* Ayu, const float* Ayv, float* Au, float* Av,
                               int lines_per_block);
+// the longitude dealias filter: the register-resident kernel when the plan
+// has a split of nx, else the shared-memory Stockham kernel; `lines` lines per
+// block (the register form takes at most 4), stockham_smem its shared memory
+cudaError_t launch_dealias(cudaStream_t s, const Dev& d, const FftPlan& plan, const float* Ayu, const float* Ayv,
+                           float* Au, float* Av, int lines, size_t stockham_smem, bool pdl);
+// the (r1, r2, r3) split of n the register-resident filter supports, or false
+bool fft_reg_split(int n, int& r1, int& r2, int& r3);
 void launch_tracer_adv(cudaStream_t s, const Dev& d, const float* T, const float* S, const float* u, const float* v,
                        const float* Fz, float* accT, float* accS, float* Tn, float* Sn, float dts, int first, int last,
                        float* topT, float* topS);

@@ -276,10 +276,8 @@ struct zm_solver {
     ZM_CUDA(launch_pdl(k_madv, dim3((nx + 31) / 32, (ny + MADV_TY - 1) / MADV_TY, nz), m, 0, s, d, src.u, src.v,
                        Fz, Ayu, Ayv));
     pe(s);
-    const int nlines = ny * nz;
     pb(ZM_K_DEALIAS, s);
-    ZM_CUDA(launch_pdl(k_dealias_lon, dim3((nlines + fft_lines - 1) / fft_lines), dim3(256), fft_smem, s, d, fft,
-                       Ayu, Ayv, Au, Av, fft_lines));
+    ZM_CUDA(launch_dealias(s, d, fft, Ayu, Ayv, Au, Av, fft_lines, fft_smem, true));
     pe(s);
     check_launch();
   }
@@ -936,6 +934,15 @@ void build(zm_solver* s, const zm_grid* g, const zm_params* p) {
     }
   }
   plan.keepbin = s->upload(keepbin);
+  // twiddles of the register-resident form, exp(-2 pi i j / nx)
+  if (fft_reg_split(nx, plan.r1, plan.r2, plan.r3)) {
+    std::vector<float2> tw(nx);
+    for (int j = 0; j < nx; ++j) {
+      const double a = -2.0 * kPi * (double)j / nx;
+      tw[j] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    plan.tw_full = s->upload(tw);
+  }
   s->fft = plan;
   s->fft_lines = std::max(1, std::min(4, (int)((200 * 1024 / sizeof(float2)) / (2 * nx))));
   s->fft_smem = (size_t)2 * s->fft_lines * nx * sizeof(float2);
@@ -1504,9 +1511,8 @@ int zm_run_stage(zm_solver* s, void* stream, int32_t stage, const zm_state* in, 
       s->project(st, s->st[a].u, s->st[a].v);
       s->copy_uv(st, s->st[a].u, s->st[a].v, s->st[a], s->st[b]);
     } else {
-      const int nlines = s->ny * s->nz;
-      k_dealias_lon<<<(nlines + s->fft_lines - 1) / s->fft_lines, 256, s->fft_smem, st>>>(
-          s->d, s->fft, s->st[a].u, s->st[a].v, s->Au, s->Av, s->fft_lines);
+      ZM_CUDA(launch_dealias(st, s->d, s->fft, s->st[a].u, s->st[a].v, s->Au, s->Av, s->fft_lines, s->fft_smem,
+                             false));
       s->check_launch();
       s->copy_uv(st, s->Au, s->Av, s->st[a], s->st[b]);
     }
