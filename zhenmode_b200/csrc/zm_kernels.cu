@@ -1430,10 +1430,11 @@ void launch_tracer_rest(dim3 g, dim3 b, cudaStream_t s, const Dev& d, const Rest
 //   mode 2: u2 = (u1 + dt/2 ((A + Pp) + (A + P))) * exp(-r_bot dt) at k = nz-1
 
 
-__device__ __forceinline__ float drho(const Dev& d, float Ta, float Sa, float wa, float Tb, float Sb, float wb_) {
-  // rho'(a) wa - rho'(b) wb in difference form when both are wet
-  if (wa != 0.f && wb_ != 0.f) return kRho0 * (-kAlpha * (Ta - Tb) + kBeta * (Sa - Sb));
-  return rho_anom(Ta, Sa) * wa - rho_anom(Tb, Sb) * wb_;
+__device__ __forceinline__ float drho(float Ta, float Sa, float wa, float Tb, float Sb, float wb_) {
+  // rho'(a) wa - rho'(b) wb in difference form: with wet flags of 0 or 1 the
+  // products wa Ta, wb Tb are exact, so this is rho0 (-alpha (Ta - Tb) +
+  // beta (Sa - Sb)) when both are wet and rho'(a) wa - rho'(b) wb otherwise
+  return kRho0 * (-kAlpha * (wa * Ta - wb_ * Tb) + kBeta * (wa * Sa - wb_ * Sb));
 }
 
 // Pressure-gradient kernel (physics/pressure.py:32-97, legacy trapezoid form,
@@ -1493,22 +1494,39 @@ __global__ void __launch_bounds__(PG_X * RY) k_pgf(Dev d, PgfArgs a) {
   float pe = 0.f, pw = 0.f, pn = 0.f, ps = 0.f;       // p[e]-p[c], p[c]-p[w], p[n]-p[c], p[c]-p[s]
   float de0 = 0.f, dw0 = 0.f, dn0 = 0.f, ds0 = 0.f;   // density differences at the level above
   float gx_prev = 0.f, gy_prev = 0.f, fx = 0.f, fy = 0.f;
+  // wet flags of the column and its neighbours, bit 0 = the current level
+  uint64_t f0 = m0, fe = me, fw = mw, fn = mn, fs = ms;
+  float w0_prev = 0.f;
+  // mode 0: the depth mean velocity (transport.py:135-143) along the same march
+  double su = 0.0, sv = 0.0;
+  float u_prev = 0.f, v_prev = 0.f;
+  constexpr float kInvRho0 = 1.f / kRho0;
   pdl_wait();  // T, S and the momentum parts come from the preceding kernels
 #pragma unroll
   for (int q = 0; q < PG_NB - 1; ++q) issue(q);
   const int r = ty + 1, c = tx + 1;
+  float* gsx = MODE != 0 ? a.gsx + cc : nullptr;  // this column's gradient scratch, one plane per level
+  float* gsy = MODE != 0 ? a.gsy + cc : nullptr;
   for (int k = 0; k < d.nz; ++k) {
     cp_async_wait<PG_NB - 2>();  // this thread's copies of level k are done
     __syncthreads();             // everyone's are, and level k - 1's buffer is free
     issue(k + PG_NB - 1);
     if (!in) continue;
+    float uk = 0.f, vk = 0.f;
+    if (MODE == 0) {  // loads in flight while the level's differences are formed
+      uk = ld(a.u1, (long long)k * d.plane + cc);
+      vk = ld(a.v1, (long long)k * d.plane + cc);
+    }
     const int b = k % PG_NB;
     const float Tc = sT[b][r][c], Sc = sS[b][r][c];
-    const float w0 = wetf(m0, k), we = wetf(me, k), ww = wetf(mw, k), wn = wetf(mn, k), ws = wetf(ms, k);
-    const float de = drho(d, sT[b][r][c + 1], sS[b][r][c + 1], we, Tc, Sc, w0);
-    const float dw = drho(d, Tc, Sc, w0, sT[b][r][c - 1], sS[b][r][c - 1], ww);
-    const float dn = drho(d, sT[b][r + 1][c], sS[b][r + 1][c], wn, Tc, Sc, w0);
-    const float ds = drho(d, Tc, Sc, w0, sT[b][r - 1][c], sS[b][r - 1][c], ws);
+    const float w0 = (float)(unsigned)(f0 & 1ull), we = (float)(unsigned)(fe & 1ull),
+                ww = (float)(unsigned)(fw & 1ull), wn = (float)(unsigned)(fn & 1ull),
+                ws = (float)(unsigned)(fs & 1ull);
+    f0 >>= 1; fe >>= 1; fw >>= 1; fn >>= 1; fs >>= 1;
+    const float de = drho(sT[b][r][c + 1], sS[b][r][c + 1], we, Tc, Sc, w0);
+    const float dw = drho(Tc, Sc, w0, sT[b][r][c - 1], sS[b][r][c - 1], ww);
+    const float dn = drho(sT[b][r + 1][c], sS[b][r + 1][c], wn, Tc, Sc, w0);
+    const float ds = drho(Tc, Sc, w0, sT[b][r - 1][c], sS[b][r - 1][c], ws);
     if (k > 0) {
       const float h = kG * 0.5f * d.vc.dz3d[k - 1];
       pe += (de0 + de) * h;
@@ -1520,16 +1538,25 @@ __global__ void __launch_bounds__(PG_X * RY) k_pgf(Dev d, PgfArgs a) {
     const float gx = hx * (pe * w0 * we + pw * w0 * ww);
     const float gy = hy * ((has_n ? pn * w0 * wn : 0.f) * cfp + (has_s ? ps * w0 * ws : 0.f) * cfm);
     if (k > 0) {
-      const float wif = wetf(m0, k - 1) * w0 * d.vc.dz3d[k - 1];
+      const float wif = w0_prev * w0 * d.vc.dz3d[k - 1];
       fx += 0.5f * (gx_prev + gx) * wif;
       fy += 0.5f * (gy_prev + gy) * wif;
+      if (MODE == 0) {
+        su += (double)(0.5f * (u_prev + uk) * d.vc.dznorm[k - 1]);
+        sv += (double)(0.5f * (v_prev + vk) * d.vc.dznorm[k - 1]);
+      }
     }
+    w0_prev = w0;
     gx_prev = gx;
     gy_prev = gy;
+    u_prev = uk;
+    v_prev = vk;
     if (MODE != 0) {
-      const long long id = (long long)k * d.plane + cc;
-      a.gsx[id] = -gx / kRho0;
-      a.gsy[id] = -gy / kRho0;
+      // -g / rho0 by the float reciprocal of rho0 (within one rounding of the quotient)
+      *gsx = -gx * kInvRho0;
+      *gsy = -gy * kInvRho0;
+      gsx += d.plane;
+      gsy += d.plane;
     }
   }
   if (!in) return;
@@ -1538,15 +1565,6 @@ __global__ void __launch_bounds__(PG_X * RY) k_pgf(Dev d, PgfArgs a) {
   if (MODE == 0) {
     a.frx[cc] = Fx;
     a.fry[cc] = Fy;
-    double su = 0.0, sv = 0.0;
-    float u_prev = ld(a.u1, cc), v_prev = ld(a.v1, cc);
-    for (int k = 1; k < d.nz; ++k) {
-      const float uk = ld(a.u1, (long long)k * d.plane + cc), vk = ld(a.v1, (long long)k * d.plane + cc);
-      su += (double)(0.5f * (u_prev + uk) * d.vc.dznorm[k - 1]);
-      sv += (double)(0.5f * (v_prev + vk) * d.vc.dznorm[k - 1]);
-      u_prev = uk;
-      v_prev = vk;
-    }
     a.ubt0[cc] = su;
     a.vbt0[cc] = sv;
     return;
