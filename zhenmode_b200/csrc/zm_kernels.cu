@@ -1048,11 +1048,15 @@ __global__ void __launch_bounds__(TA_X * TA_Y, 5) k_tracer_adv_t(Dev d, const fl
     }
     cp_async_commit();
   };
-  auto wet_level = [&](int k) {  // wet flags of level k into w[k % 2]
+  // wet flags of the two tile cells, bit 0 = the next level wet_level forms
+  uint64_t rb0 = b0 >> k0, rb1 = b1 >> k0;
+  auto wet_level = [&](int k) {  // wet flags of level k into w[k % 2]; called for k0, k0 + 1, ... in turn
     if (k < d.nz) {
       float* pw = &t.w[k & 1][0][0];
-      pw[e0] = wetf(b0, k);
-      if (has1) pw[e1] = wetf(b1, k);
+      pw[e0] = (float)(unsigned)(rb0 & 1ull);
+      if (has1) pw[e1] = (float)(unsigned)(rb1 & 1ull);
+      rb0 >>= 1;
+      rb1 >>= 1;
     }
   };
   pdl_wait();  // the tracers, velocities and Fz come from the preceding kernels
@@ -1070,6 +1074,9 @@ __global__ void __launch_bounds__(TA_X * TA_Y, 5) k_tracer_adv_t(Dev d, const fl
                                    ld(S, base + (long long)(k0 - 1) * d.plane))
                      : f2(0.f);
   float fzk = ld(Fz, base + (long long)k0 * d.plane);
+  // the column's own wet flags: level k - 1 in wup, level k + 1 in bit 1 of cb
+  float wup = k0 > 0 ? wetf(bits, k0 - 1) : 0.f;
+  uint64_t cb = bits >> k0;
   for (int k = k0; k < k1; ++k) {
     cp_async_wait<0>();  // this thread's copies of levels k and k + 1 are done
     __syncthreads();     // everyone's are, w[k % 2] is formed, level k - 1's buffers are free
@@ -1098,12 +1105,12 @@ __global__ void __launch_bounds__(TA_X * TA_Y, 5) k_tracer_adv_t(Dev d, const fl
       if (k == 0) {
         up = __fmul2_rn(f2(fzk), ck);
       } else {
-        up = __fmul2_rn(f2(fzk * (wetf(bits, k - 1) * w0)), fzk > 0.f ? cm : ck);
+        up = __fmul2_rn(f2(fzk * (wup * w0)), fzk > 0.f ? cm : ck);
       }
       if (k + 1 < d.nz) {
         // ghost fill below the deepest wet level: node k+1 carries node k's value
         const float2 cn = k + 1 <= kbt ? t.ts[qn][r][cc] : ck;
-        dn = __fmul2_rn(f2(fzn * (w0 * wetf(bits, k + 1))), fzn > 0.f ? ck : cn);
+        dn = __fmul2_rn(f2(fzn * (w0 * (float)(unsigned)((cb >> 1) & 1ull))), fzn > 0.f ? ck : cn);
       }
       a = __fmul2_rn(__ffma2_rn(__ffma2_rn(up, m1, dn), f2(d.vc.inv_dz_node[k]), h), f2(-w0));
     }
@@ -1116,6 +1123,8 @@ __global__ void __launch_bounds__(TA_X * TA_Y, 5) k_tracer_adv_t(Dev d, const fl
     }
     cm = ck;
     fzk = fzn;
+    wup = (float)(unsigned)(cb & 1ull);
+    cb >>= 1;
   }
 }
 
@@ -1430,11 +1439,13 @@ void launch_tracer_rest(dim3 g, dim3 b, cudaStream_t s, const Dev& d, const Rest
 //   mode 2: u2 = (u1 + dt/2 ((A + Pp) + (A + P))) * exp(-r_bot dt) at k = nz-1
 
 
-__device__ __forceinline__ float drho(float Ta, float Sa, float wa, float Tb, float Sb, float wb_) {
-  // rho'(a) wa - rho'(b) wb in difference form: with wet flags of 0 or 1 the
-  // products wa Ta, wb Tb are exact, so this is rho0 (-alpha (Ta - Tb) +
-  // beta (Sa - Sb)) when both are wet and rho'(a) wa - rho'(b) wb otherwise
-  return kRho0 * (-kAlpha * (wa * Ta - wb_ * Tb) + kBeta * (wa * Sa - wb_ * Sb));
+__device__ __forceinline__ float drho(float2 a, float wa, float2 b, float wb_) {
+  // rho'(a) wa - rho'(b) wb in difference form, a = (Ta, Sa): with wet flags
+  // of 0 or 1 the products are exact, so this is rho0 (-alpha (Ta - Tb) +
+  // beta (Sa - Sb)) when both are wet and rho'(a) wa - rho'(b) wb otherwise;
+  // the T and S differences on one paired instruction
+  const float2 dd = __ffma2_rn(f2(wa), a, __fmul2_rn(f2(-wb_), b));
+  return kRho0 * (-kAlpha * dd.x + kBeta * dd.y);
 }
 
 // Pressure-gradient kernel (physics/pressure.py:32-97, legacy trapezoid form,
@@ -1459,7 +1470,7 @@ __global__ void __launch_bounds__(PG_X * RY) k_pgf(Dev d, PgfArgs a) {
   constexpr int PG_PY = RY + 2, PG_CELLS = PG_PX * PG_PY;
   static_assert(PG_CELLS <= 2 * PG_X * RY, "two tile cells per thread at most");
   pdl_trigger();
-  __shared__ float sT[PG_NB][PG_PY][PG_PX], sS[PG_NB][PG_PY][PG_PX];
+  __shared__ float2 sTS[PG_NB][PG_PY][PG_PX];  // (T, S) of a cell side by side
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * PG_X + tx;
   const int i0 = blockIdx.x * PG_X, j0 = blockIdx.y * RY;
   const int i = i0 + tx, j = j0 + ty;
@@ -1471,13 +1482,12 @@ __global__ void __launch_bounds__(PG_X * RY) k_pgf(Dev d, PgfArgs a) {
   auto issue = [&](int k) {  // level k into buffer k % PG_NB; one commit group per call
     if (k < d.nz) {
       const long long off = (long long)k * d.plane;
-      float* bt = &sT[k % PG_NB][0][0];
-      float* bs = &sS[k % PG_NB][0][0];
-      cp_async4(bt + e0, a.T + off + s0);
-      cp_async4(bs + e0, a.S + off + s0);
+      float* ts = &sTS[k % PG_NB][0][0].x;
+      cp_async4(ts + 2 * e0, a.T + off + s0);
+      cp_async4(ts + 2 * e0 + 1, a.S + off + s0);
       if (has1) {
-        cp_async4(bt + e1, a.T + off + s1);
-        cp_async4(bs + e1, a.S + off + s1);
+        cp_async4(ts + 2 * e1, a.T + off + s1);
+        cp_async4(ts + 2 * e1 + 1, a.S + off + s1);
       }
     }
     cp_async_commit();
@@ -1518,15 +1528,15 @@ __global__ void __launch_bounds__(PG_X * RY) k_pgf(Dev d, PgfArgs a) {
       vk = ld(a.v1, (long long)k * d.plane + cc);
     }
     const int b = k % PG_NB;
-    const float Tc = sT[b][r][c], Sc = sS[b][r][c];
+    const float2 tc = sTS[b][r][c];
     const float w0 = (float)(unsigned)(f0 & 1ull), we = (float)(unsigned)(fe & 1ull),
                 ww = (float)(unsigned)(fw & 1ull), wn = (float)(unsigned)(fn & 1ull),
                 ws = (float)(unsigned)(fs & 1ull);
     f0 >>= 1; fe >>= 1; fw >>= 1; fn >>= 1; fs >>= 1;
-    const float de = drho(sT[b][r][c + 1], sS[b][r][c + 1], we, Tc, Sc, w0);
-    const float dw = drho(Tc, Sc, w0, sT[b][r][c - 1], sS[b][r][c - 1], ww);
-    const float dn = drho(sT[b][r + 1][c], sS[b][r + 1][c], wn, Tc, Sc, w0);
-    const float ds = drho(Tc, Sc, w0, sT[b][r - 1][c], sS[b][r - 1][c], ws);
+    const float de = drho(sTS[b][r][c + 1], we, tc, w0);
+    const float dw = drho(tc, w0, sTS[b][r][c - 1], ww);
+    const float dn = drho(sTS[b][r + 1][c], wn, tc, w0);
+    const float ds = drho(tc, w0, sTS[b][r - 1][c], ws);
     if (k > 0) {
       const float h = kG * 0.5f * d.vc.dz3d[k - 1];
       pe += (de0 + de) * h;
