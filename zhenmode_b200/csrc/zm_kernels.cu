@@ -464,11 +464,15 @@ __global__ void __launch_bounds__(LT_X * LT_Y, 4) k_lin_t(Dev d, const float* __
     }
     cp_async_commit();
   };
-  auto wet_level = [&](int k) {  // wet flags of level k into w[k % 2]
+  // wet flags of the two tile cells, bit 0 = the next level wet_level forms
+  uint64_t rb0 = b0 >> k0, rb1 = b1 >> k0;
+  auto wet_level = [&](int k) {  // wet flags of level k into w[k % 2]; called for k0, k0 + 1, ... in turn
     if (k < d.nz) {
       float* pw = &t.w[k & 1][0][0];
-      pw[e0] = wetf(b0, k);
-      if (has1) pw[e1] = wetf(b1, k);
+      pw[e0] = (float)(unsigned)(rb0 & 1ull);
+      if (has1) pw[e1] = (float)(unsigned)(rb1 & 1ull);
+      rb0 >>= 1;
+      rb1 >>= 1;
     }
   };
   pdl_wait();  // the state comes from the preceding kernels
@@ -777,6 +781,9 @@ __global__ void __launch_bounds__(FZ_X * RY) k_fz(Dev d, const float* __restrict
   const float cf_n = __ldg(d.cfp + jc), cf_s = jc > 0 ? __ldg(d.cfp + jc - 1) : 0.f;
   const float yscale = d.inv_dy * __ldg(d.inv_cos + jc);
   float acc = 0.f;
+  // wet flags with level nz - 1 in bit 63, shifted up one level per iteration (the march runs upwards)
+  const int up = 64 - d.nz;
+  uint64_t f0 = m0 << up, fe = me << up, fw = mw << up, fn = mn << up, fs = ms << up;
   pdl_wait();  // u, v come from the preceding kernel
 #pragma unroll
   for (int q = 0; q < FZ_NB - 1; ++q) issue(q);
@@ -788,13 +795,16 @@ __global__ void __launch_bounds__(FZ_X * RY) k_fz(Dev d, const float* __restrict
     if (!in) continue;
     const int k = d.nz - 1 - q, bq = q % FZ_NB;
     const float uc = su[bq][r][c], ue = su[bq][r][c + 1], uw = su[bq][r][c - 1];
-    const float w0 = wetf(m0, k);
-    const float fxe = 0.5f * (uc + ue) * w0 * wetf(me, k);
-    const float fxw = 0.5f * (uw + uc) * wetf(mw, k) * w0;
+    const float w0 = (float)(unsigned)(f0 >> 63), we = (float)(unsigned)(fe >> 63),
+                ww = (float)(unsigned)(fw >> 63), wn = (float)(unsigned)(fn >> 63),
+                ws = (float)(unsigned)(fs >> 63);
+    f0 <<= 1; fe <<= 1; fw <<= 1; fn <<= 1; fs <<= 1;
+    const float fxe = 0.5f * (uc + ue) * w0 * we;
+    const float fxw = 0.5f * (uw + uc) * ww * w0;
     float fyn = 0.f, fys = 0.f;
     const float vc = sv[bq][r][c];
-    if (jc < d.ny - 1) fyn = 0.5f * (vc + sv[bq][r + 1][c]) * w0 * wetf(mn, k) * cf_n;
-    if (jc > 0) fys = 0.5f * (sv[bq][r - 1][c] + vc) * wetf(ms, k) * w0 * cf_s;
+    if (jc < d.ny - 1) fyn = 0.5f * (vc + sv[bq][r + 1][c]) * w0 * wn * cf_n;
+    if (jc > 0) fys = 0.5f * (sv[bq][r - 1][c] + vc) * ws * w0 * cf_s;
     const float div = (fxe - fxw) * idx_c + (fyn - fys) * yscale;
     acc += div * d.vc.dz_node[k];
     Fz[(long long)k * d.plane + cc] = acc;
