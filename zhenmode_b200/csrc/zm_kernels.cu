@@ -969,9 +969,13 @@ __device__ __forceinline__ float ta_face_value(bool pos, float cm, float c0, flo
 __device__ __forceinline__ float2 minmod_slope2(float2 cm, float2 c0, float2 cp) {
   const float2 m1 = f2(-1.f);
   const float2 l = __ffma2_rn(cm, m1, c0), r = __ffma2_rn(c0, m1, cp);
+  // l and r of one sign <=> l r > 0 (both differences of float32 tracer
+  // anomalies, so the product underflows only where both are below 1e-19, and
+  // the slope dropped there is below that too); NaN compares false, as in the
+  // sign form
+  const float2 lr = __fmul2_rn(l, r);
   const float mx = fminf(fabsf(l.x), fabsf(r.x)), my = fminf(fabsf(l.y), fabsf(r.y));
-  return make_float2((l.x > 0.f && r.x > 0.f) ? mx : ((l.x < 0.f && r.x < 0.f) ? -mx : 0.f),
-                     (l.y > 0.f && r.y > 0.f) ? my : ((l.y < 0.f && r.y < 0.f) ? -my : 0.f));
+  return make_float2(lr.x > 0.f ? copysignf(mx, l.x) : 0.f, lr.y > 0.f ? copysignf(my, l.y) : 0.f);
 }
 
 // Limited (T, S) face state, the paired form of ta_face_value.  The wet
