@@ -15,8 +15,10 @@ step).  The per-step working set (~3 GB) is far larger than the 126 MB L2, so
 no flush is needed between iterations.
 
 `--impl reference` times the CPU restatement of the reference algorithm
-(``oracle/``, float64 NumPy, one thread) on a bounded sample: the same option
-set on a 180x90x50 grid, scaled per grid point to 720x360x50.
+(``oracle/``, float64 NumPy) on every host core, one spawned process per core,
+each on a bounded sample: the same option set on a 180x90x50 grid (smaller
+when many steps are asked for), scaled per grid point to 720x360x50; the
+default line's `cpu_baseline` is the same on one core.
 """
 from __future__ import annotations
 
@@ -51,7 +53,7 @@ PROFILE_STEPS = 5
 # DRAM bytes per launch measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum)
 # for a kernel class on a grid, as summarised under profiles/; null for others.
 # ncu dram__bytes_read.sum + dram__bytes_write.sum of one full-size k_nu_tb launch (6 subcycles)
-NCU_TRAFFIC_BYTES = {((720, 360, 50), "nu_sub"): 106823424 + 63360256}
+NCU_TRAFFIC_BYTES = {((720, 360, 50), "nu_sub"): 117752832 + 65883136}
 
 
 def algo_fields_per_launch(cls, launches_per_step, n_nu):
