@@ -1521,9 +1521,15 @@ __global__ void __launch_bounds__(PG_X * RY) k_pgf(Dev d, PgfArgs a) {
   // wet flags of the column and its neighbours, bit 0 = the current level
   uint64_t f0 = m0, fe = me, fw = mw, fn = mn, fs = ms;
   float w0_prev = 0.f;
-  // mode 0: the depth mean velocity (transport.py:135-143) along the same march
+  // mode 0: the depth mean velocity (transport.py:135-143) along the same march,
+  // each level's u, v loaded one level ahead
   double su = 0.0, sv = 0.0;
   float u_prev = 0.f, v_prev = 0.f;
+  float u_next = 0.f, v_next = 0.f;
+  if (MODE == 0 && in) {
+    u_next = ld(a.u1, cc);
+    v_next = ld(a.v1, cc);
+  }
   constexpr float kInvRho0 = 1.f / kRho0;
   pdl_wait();  // T, S and the momentum parts come from the preceding kernels
 #pragma unroll
@@ -1537,9 +1543,13 @@ __global__ void __launch_bounds__(PG_X * RY) k_pgf(Dev d, PgfArgs a) {
     issue(k + PG_NB - 1);
     if (!in) continue;
     float uk = 0.f, vk = 0.f;
-    if (MODE == 0) {  // loads in flight while the level's differences are formed
-      uk = ld(a.u1, (long long)k * d.plane + cc);
-      vk = ld(a.v1, (long long)k * d.plane + cc);
+    if (MODE == 0) {  // this level's u, v arrived during the previous level; the next ones are in flight
+      uk = u_next;
+      vk = v_next;
+      if (k + 1 < d.nz) {
+        u_next = ld(a.u1, (long long)(k + 1) * d.plane + cc);
+        v_next = ld(a.v1, (long long)(k + 1) * d.plane + cc);
+      }
     }
     const int b = k % PG_NB;
     const float2 tc = sTS[b][r][c];
