@@ -831,98 +831,84 @@ void launch_fz(cudaStream_t s, const Dev& d, const float* u, const float* v, flo
 // of the dealias filter, [1,4,6,4,1]/16 on edge-held rows
 // (numerics/horizontal.py:283-305).  The longitude 2/3-rule half runs in the
 // FFT kernel; the two filters act on different axes and commute.
-//
-// One block: 32 columns x MADV_TY (60) output rows of one level.  The
-// advection is formed on MV_RY = MADV_TY + 4 rows (the filter's 2-row halo on
-// each side); the level's (u, v) and wet flags on those rows with a one-cell
-// halo are first staged in shared memory (rows clamped at the closed walls,
-// longitude wrapped), so each neighbour value is one shared load; the column's
-// values one level up and down come from global memory (ghost-filled below the
-// deepest wet level, numerics/vertical.py:122-135, 267-272).  Rows beyond the
-// walls repeat the wall row's advection, which is the filter's edge padding.
-constexpr int MV_RY = MADV_TY + 4, MV_PX = 32 + 2, MV_PY = MV_RY + 2, MV_CELLS = MV_PX * MV_PY;
+__device__ __forceinline__ void adv_point(const Dev& d, const float* __restrict__ u, const float* __restrict__ v,
+                                          const float* __restrict__ Fz, int k, int j, int i, float& au, float& av) {
+  const Nb n = nb(d, j, i);
+  const long long b = (long long)k * d.plane;
+  const uint64_t m0 = wb(d, j, i);
+  const float w0 = wetf(m0, k);
+  if (w0 == 0.f) { au = 0.f; av = 0.f; return; }
+  const float we = wetf(wb(d, j, n.ie), k), ww = wetf(wb(d, j, n.iw), k);
+  const float wn = wetf(wb(d, n.jn, i), k), ws = wetf(wb(d, n.js, i), k);
+  const long long c = b + idx2(d, j, i);
+  const float uc = ld(u, c), vc = ld(v, c);
+  const float ue = ld(u, b + idx2(d, j, n.ie)), uw = ld(u, b + idx2(d, j, n.iw));
+  const float un = ld(u, b + idx2(d, n.jn, i)), us = ld(u, b + idx2(d, n.js, i));
+  const float ve = ld(v, b + idx2(d, j, n.ie)), vw = ld(v, b + idx2(d, j, n.iw));
+  const float vn = ld(v, b + idx2(d, n.jn, i)), vs = ld(v, b + idx2(d, n.js, i));
+  const float hx = __ldg(d.inv_dx + idx2(d, j, i)) * 0.5f, hy = d.inv_dy * 0.5f;
+  const float dudx = hx * ((ue - uc) * w0 * we + (uc - uw) * w0 * ww);
+  const float dvdx = hx * ((ve - vc) * w0 * we + (vc - vw) * w0 * ww);
+  const float dudy = hy * ((un - uc) * wn * w0 + (uc - us) * w0 * ws);
+  const float dvdy = hy * ((vn - vc) * wn * w0 + (vc - vs) * w0 * ws);
+  // d/dz of the ghost-filled column (numerics/vertical.py:267-272)
+  const int kb = kbot_of(m0);
+  const long long base = idx2(d, j, i);
+  float dudz, dvdz;
+  if (k == 0) {
+    const float inv = d.vc.ddz_inv[0];
+    dudz = (colv(u, base, d.plane, 1, kb) - colv(u, base, d.plane, 0, kb)) * inv;
+    dvdz = (colv(v, base, d.plane, 1, kb) - colv(v, base, d.plane, 0, kb)) * inv;
+  } else if (k == d.nz - 1) {
+    const float inv = d.vc.ddz_inv[k];
+    dudz = (colv(u, base, d.plane, k, kb) - colv(u, base, d.plane, k - 1, kb)) * inv;
+    dvdz = (colv(v, base, d.plane, k, kb) - colv(v, base, d.plane, k - 1, kb)) * inv;
+  } else {
+    const float inv = d.vc.ddz_inv[k];
+    dudz = (colv(u, base, d.plane, k + 1, kb) - colv(u, base, d.plane, k - 1, kb)) * inv;
+    dvdz = (colv(v, base, d.plane, k + 1, kb) - colv(v, base, d.plane, k - 1, kb)) * inv;
+  }
+  const float w = -ld(Fz, c) * w0;  // dynamics/transport.py:149-166
+  au = -(uc * dudx + vc * dudy + w * dudz);
+  av = -(uc * dvdx + vc * dvdy + w * dvdz);
+}
 
+// One block: 32 columns x MADV_TY (60) rows of one level.  The 8 warps take 8
+// of the 64 rows (tile and a 2-row halo on each side) per pass, so the halo
+// adds 7 % of the point work (50 % with 8-row tiles).
 __global__ void __launch_bounds__(256) k_madv(Dev d, const float* __restrict__ u, const float* __restrict__ v,
                                               const float* __restrict__ Fz, float* __restrict__ Ayu,
                                               float* __restrict__ Ayv) {
   pdl_trigger();
-  __shared__ float2 suv[MV_PY][MV_PX];   // (u, v) of the level
-  __shared__ float swt[MV_PY][MV_PX];    // its wet flags
-  __shared__ float2 say[MV_RY][32];      // the advection before the filter
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
-  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * MADV_TY;
+  __shared__ float su[MADV_TY + 4][32];
+  __shared__ float sv[MADV_TY + 4][32];
+  const int i = blockIdx.x * 32 + threadIdx.x;
+  const int j0 = blockIdx.y * MADV_TY;
   const int k = blockIdx.z;
-  const long long kp = (long long)k * d.plane;
   pdl_wait();  // u, v, Fz come from the preceding kernels
-  for (int e = tid; e < MV_CELLS; e += 256) {
-    const int pr = e / MV_PX, pc = e - pr * MV_PX;
-    const int gj = min(max(j0 - 3 + pr, 0), d.ny - 1);
-    int gi = i0 - 1 + pc;
-    gi = gi < 0 ? gi + d.nx : (gi >= d.nx ? gi - d.nx : gi);
-    const long long c2 = idx2(d, gj, gi);
-    (&suv[0][0])[e] = make_float2(ld(u, kp + c2), ld(v, kp + c2));
-    (&swt[0][0])[e] = wetf(__ldg(d.wbits + c2), k);
-  }
-  __syncthreads();
-  const int i = i0 + tx, pc = tx + 1;
-  const float hy = d.inv_dy * 0.5f;
-  for (int r = ty; r < MV_RY; r += 8) {
-    const int pr = r + 1;
-    const int jj = min(max(j0 - 2 + r, 0), d.ny - 1);
+  for (int r = threadIdx.y; r < MADV_TY + 4; r += blockDim.y) {
+    int jj = j0 - 2 + r;
+    jj = jj < 0 ? 0 : (jj >= d.ny ? d.ny - 1 : jj);
     float au = 0.f, av = 0.f;
-    const float w0 = swt[pr][pc];
-    if (i < d.nx && w0 != 0.f) {
-      const float we = swt[pr][pc + 1], ww = swt[pr][pc - 1];
-      const float wn = swt[pr + 1][pc], ws = swt[pr - 1][pc];
-      const float2 c = suv[pr][pc], e = suv[pr][pc + 1], w = suv[pr][pc - 1];
-      const float2 n = suv[pr + 1][pc], so = suv[pr - 1][pc];
-      const float uc = c.x, vc = c.y;
-      const long long base = idx2(d, jj, i);
-      const float hx = __ldg(d.inv_dx + base) * 0.5f;
-      const float dudx = hx * ((e.x - uc) * w0 * we + (uc - w.x) * w0 * ww);
-      const float dvdx = hx * ((e.y - vc) * w0 * we + (vc - w.y) * w0 * ww);
-      const float dudy = hy * ((n.x - uc) * wn * w0 + (uc - so.x) * w0 * ws);
-      const float dvdy = hy * ((n.y - vc) * wn * w0 + (vc - so.y) * w0 * ws);
-      // d/dz of the ghost-filled column: below the deepest wet level kb the
-      // column repeats its value there, so the level below a wet point is its
-      // own value when k = kb
-      const int kb = kbot_of(__ldg(d.wbits + base));
-      float dudz, dvdz;
-      if (k == 0) {
-        const float inv = d.vc.ddz_inv[0];
-        const long long id1 = base + (0 < kb ? d.plane : 0);
-        dudz = (ld(u, id1) - uc) * inv;
-        dvdz = (ld(v, id1) - vc) * inv;
-      } else if (k == d.nz - 1) {
-        const float inv = d.vc.ddz_inv[k];
-        const long long idm = kp - d.plane + base;
-        dudz = (uc - ld(u, idm)) * inv;
-        dvdz = (vc - ld(v, idm)) * inv;
-      } else {
-        const float inv = d.vc.ddz_inv[k];
-        const long long idp = kp + (k < kb ? d.plane : 0) + base, idm = kp - d.plane + base;
-        dudz = (ld(u, idp) - ld(u, idm)) * inv;
-        dvdz = (ld(v, idp) - ld(v, idm)) * inv;
-      }
-      const float wz = -ld(Fz, kp + base) * w0;  // dynamics/transport.py:149-166
-      au = -(uc * dudx + vc * dudy + wz * dudz);
-      av = -(uc * dvdx + vc * dvdy + wz * dvdz);
-    }
-    say[r][tx] = make_float2(au, av);
+    if (i < d.nx) adv_point(d, u, v, Fz, k, jj, i, au, av);
+    su[r][threadIdx.x] = au;
+    sv[r][threadIdx.x] = av;
   }
   __syncthreads();
-  // rows j-2..j+2 clamped to the domain: with the tile formed on clamped rows
+  // rows j-2..j+2 clamped to the domain: with the tile loaded on clamped rows
   // the clamp is already applied at the tile edges except inside the tile.
   auto row = [&](int jj) { jj = jj < 0 ? 0 : (jj >= d.ny ? d.ny - 1 : jj); return jj - (j0 - 2); };
-  if (i >= d.nx) return;
-  for (int jr = ty; jr < MADV_TY; jr += 8) {
+  const int t = threadIdx.x;
+  for (int jr = threadIdx.y; jr < MADV_TY; jr += blockDim.y) {
     const int j = j0 + jr;
-    if (j >= d.ny) break;
-    const float2 a0 = say[row(j - 2)][tx], a1 = say[row(j - 1)][tx], a2 = say[row(j)][tx];
-    const float2 a3 = say[row(j + 1)][tx], a4 = say[row(j + 2)][tx];
-    const long long id = kp + idx2(d, j, i);
-    Ayu[id] = (a0.x + 4.f * a1.x + 6.f * a2.x + 4.f * a3.x + a4.x) / 16.f;
-    Ayv[id] = (a0.y + 4.f * a1.y + 6.f * a2.y + 4.f * a3.y + a4.y) / 16.f;
+    if (i >= d.nx || j >= d.ny) continue;
+    const float fu = (su[row(j - 2)][t] + 4.f * su[row(j - 1)][t] + 6.f * su[row(j)][t] + 4.f * su[row(j + 1)][t] +
+                      su[row(j + 2)][t]) / 16.f;
+    const float fv = (sv[row(j - 2)][t] + 4.f * sv[row(j - 1)][t] + 6.f * sv[row(j)][t] + 4.f * sv[row(j + 1)][t] +
+                      sv[row(j + 2)][t]) / 16.f;
+    const long long id = idx3(d, k, j, i);
+    Ayu[id] = fu;
+    Ayv[id] = fv;
   }
 }
 
