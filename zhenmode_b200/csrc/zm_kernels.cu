@@ -1009,15 +1009,15 @@ __device__ __forceinline__ float2 ta_faces_x(const TaTile& t, int q, int wq, int
 // (T, S) fluxes through the y face between tile rows r and r+1 (global rows
 // gj, gj+1); zero through the closed walls
 template <int LIM>
-__device__ __forceinline__ float2 ta_faces_y(const TaTile& t, int q, int wq, int r, int cc, bool open, float cf) {
-  if (!open) return f2(0.f);
+__device__ __forceinline__ float2 ta_faces_y(const Dev& d, const TaTile& t, int q, int wq, int r, int cc, int gj) {
+  if (gj < 0 || gj >= d.ny - 1) return f2(0.f);
   const float w0 = t.w[wq][r][cc], wn = t.w[wq][r + 1][cc];
   const float vy = 0.5f * (t.v[q][r][cc] + t.v[q][r + 1][cc]);
   const bool pos = vy >= 0.f;
   const float wm = t.w[wq][r - 1][cc], wp = t.w[wq][r + 2][cc];
   const float2 c = ta_face_value2<LIM>(pos, t.ts[q][r - 1][cc], t.ts[q][r][cc], t.ts[q][r + 1][cc],
                                        t.ts[q][r + 2][cc], wm, w0, wn, wp);
-  return __fmul2_rn(__fmul2_rn(f2(vy * (w0 * wn)), c), f2(cf));
+  return __fmul2_rn(__fmul2_rn(f2(vy * (w0 * wn)), c), f2(__ldg(d.cfp + gj)));
 }
 
 template <int LIM>
@@ -1082,10 +1082,6 @@ __global__ void __launch_bounds__(TA_X * TA_Y, 5) k_tracer_adv_t(Dev d, const fl
   const uint64_t bits = __ldg(d.wbits + base);
   const int kbt = kbot_of(bits);
   const float ix = __ldg(d.inv_dx + base), ysc = d.inv_dy * __ldg(d.inv_cos + jc);
-  // the column's y faces (rows jc, jc+1 and jc-1, jc): closed at the walls,
-  // else with the cosine of the face latitude
-  const bool yn_open = jc < d.ny - 1, ys_open = jc > 0;
-  const float cfn = yn_open ? __ldg(d.cfp + jc) : 0.f, cfs = ys_open ? __ldg(d.cfp + jc - 1) : 0.f;
   const int r = ty + TA_H, cc = tx + TA_H;
   // (T, S) of the level above and Fz of the current level
   float2 cm = k0 > 0 ? make_float2(ld(T, base + (long long)(k0 - 1) * d.plane),
@@ -1114,8 +1110,7 @@ __global__ void __launch_bounds__(TA_X * TA_Y, 5) k_tracer_adv_t(Dev d, const fl
     if (w0 != 0.f) {
       const float2 m1 = f2(-1.f);
       const float2 fxe = ta_faces_x<LIM>(t, q, wq, r, cc), fxw = ta_faces_x<LIM>(t, q, wq, r, cc - 1);
-      const float2 fyn = ta_faces_y<LIM>(t, q, wq, r, cc, yn_open, cfn);
-      const float2 fys = ta_faces_y<LIM>(t, q, wq, r - 1, cc, ys_open, cfs);
+      const float2 fyn = ta_faces_y<LIM>(d, t, q, wq, r, cc, jc), fys = ta_faces_y<LIM>(d, t, q, wq, r - 1, cc, jc - 1);
       const float2 h = __ffma2_rn(__ffma2_rn(fxw, m1, fxe), f2(ix), __fmul2_rn(__ffma2_rn(fys, m1, fyn), f2(ysc)));
       // vertical donor-cell fluxes through the top (up) and bottom (dn) faces;
       // the wet weights are 0 or 1, so folding them into Fz rounds like the
