@@ -2,8 +2,8 @@
 float64 oracle and with golden vectors of the reference's own step code.
 
 All calls go through the C ABI (``zm_run_stage`` / ``zm_step``).  The
-tolerances are relative L2 norms per field; the north-star bound for one
-production step is 1e-5.
+tolerances are relative L2 norms per field; one production step is held to
+1e-5.
 """
 import numpy as np
 import pytest
