@@ -154,7 +154,9 @@ int zm_store_state(zm_solver* s, void* stream, zm_state* out);
 int zm_step(zm_solver* s, void* stream, const zm_state* in, zm_state* out, int32_t nsteps);
 
 /* As zm_step with HOST pointers (pinned memory gives full copy bandwidth);
- * returns after the result is in `out`. */
+ * returns after the result is in `out`.  The copies run on a stream of the
+ * solver's own, ordered after the work already queued on `stream`, so that
+ * each field's layout change overlaps the next field's transfer. */
 int zm_step_host(zm_solver* s, void* stream, const zm_state* in, zm_state* out, int32_t nsteps);
 
 /* Replace the 2-D forcing fields (device float32 arrays, (nx, ny)); the

@@ -106,6 +106,10 @@ struct zm_solver {
   cudaStream_t cap_stream = nullptr;  // graphs are captured here, launched on the caller's stream
   cudaStream_t side = nullptr;        // the second branch of the N step (momentum advection)
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // host-buffer steps: the copies run on their own stream, one event per field
+  // each way, so that a field's layout change overlaps the next field's copy
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_copy[11] = {};
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   bool graphs_ready = false;
   // set while an ensemble captures this member: the cooperative barotropic
@@ -160,6 +164,9 @@ struct zm_solver {
     if (side) cudaStreamDestroy(side);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
+    for (cudaEvent_t e : ev_copy)
+      if (e) cudaEventDestroy(e);
     for (void* p : allocs) cudaFree(p);
   }
 
@@ -1417,22 +1424,46 @@ int zm_step_host(zm_solver* s, void* stream, const zm_state* in, zm_state* out, 
   if (!s || !in || !out) return ZM_ERR_INVALID;
   cudaStream_t st = (cudaStream_t)stream;
   try {
+    if (!s->copy_stream) {
+      ZM_CUDA(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
+      for (cudaEvent_t& e : s->ev_copy) ZM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    cudaStream_t cs = s->copy_stream;
+    cudaEvent_t* ev = s->ev_copy;  // [0] start, [1..5] inputs copied, [6..10] outputs laid out
     const size_t b3 = (size_t)s->nx * s->ny * s->nz * sizeof(float), b2 = (size_t)s->nx * s->ny * sizeof(float);
-    ZM_CUDA(cudaMemcpyAsync(s->ref.u, in->u, b3, cudaMemcpyHostToDevice, st));
-    ZM_CUDA(cudaMemcpyAsync(s->ref.v, in->v, b3, cudaMemcpyHostToDevice, st));
-    ZM_CUDA(cudaMemcpyAsync(s->ref.T, in->T, b3, cudaMemcpyHostToDevice, st));
-    ZM_CUDA(cudaMemcpyAsync(s->ref.S, in->S, b3, cudaMemcpyHostToDevice, st));
-    ZM_CUDA(cudaMemcpyAsync(s->ref_eta, in->eta, b2, cudaMemcpyHostToDevice, st));
-    zm_state dev{s->ref.u, s->ref.v, s->ref.T, s->ref.S, s->ref_eta};
-    s->load(st, &dev, s->st[s->cur], s->eta[s->cur]);
+    float* ref[5] = {s->ref.u, s->ref.v, s->ref.T, s->ref.S, s->ref_eta};
+    const float* hin[5] = {in->u, in->v, in->T, in->S, in->eta};
+    float* hout[5] = {out->u, out->v, out->T, out->S, out->eta};
+    Fields4& a = s->st[s->cur];
+    float* fin[4] = {a.u, a.v, a.T, a.S};
+    const float offs[4] = {0.f, 0.f, s->d.T_ref, s->d.S_ref};
+    // the copies start after the work already queued on the caller's stream
+    ZM_CUDA(cudaEventRecord(ev[0], st));
+    ZM_CUDA(cudaStreamWaitEvent(cs, ev[0], 0));
+    for (int f = 0; f < 5; ++f) {
+      ZM_CUDA(cudaMemcpyAsync(ref[f], hin[f], f < 4 ? b3 : b2, cudaMemcpyHostToDevice, cs));
+      ZM_CUDA(cudaEventRecord(ev[1 + f], cs));
+    }
+    const dim3 c(32, 8);
+    for (int f = 0; f < 5; ++f) {
+      ZM_CUDA(cudaStreamWaitEvent(st, ev[1 + f], 0));
+      if (f < 4) s->to_int3(st, ref[f], fin[f], offs[f]);
+      else k_ref_to_int2<<<s->grid2(c), c, 0, st>>>(s->d, ref[4], s->eta[s->cur]);
+    }
+    s->check_launch();
     int rc = zm_advance(s, stream, nsteps);
     if (rc) return rc;
-    s->store(st, s->st[s->cur], s->eta[s->cur], &dev);
-    ZM_CUDA(cudaMemcpyAsync(out->u, s->ref.u, b3, cudaMemcpyDeviceToHost, st));
-    ZM_CUDA(cudaMemcpyAsync(out->v, s->ref.v, b3, cudaMemcpyDeviceToHost, st));
-    ZM_CUDA(cudaMemcpyAsync(out->T, s->ref.T, b3, cudaMemcpyDeviceToHost, st));
-    ZM_CUDA(cudaMemcpyAsync(out->S, s->ref.S, b3, cudaMemcpyDeviceToHost, st));
-    ZM_CUDA(cudaMemcpyAsync(out->eta, s->ref_eta, b2, cudaMemcpyDeviceToHost, st));
+    Fields4& b = s->st[s->cur];
+    float* fout[4] = {b.u, b.v, b.T, b.S};
+    for (int f = 0; f < 5; ++f) {
+      if (f < 4) s->to_ref3(st, fout[f], ref[f], offs[f]);
+      else k_int_to_ref2<<<s->grid2(c), c, 0, st>>>(s->d, s->eta[s->cur], ref[4]);
+      ZM_CUDA(cudaEventRecord(ev[6 + f], st));
+      ZM_CUDA(cudaStreamWaitEvent(cs, ev[6 + f], 0));
+      ZM_CUDA(cudaMemcpyAsync(hout[f], ref[f], f < 4 ? b3 : b2, cudaMemcpyDeviceToHost, cs));
+    }
+    s->check_launch();
+    ZM_CUDA(cudaStreamSynchronize(cs));
     ZM_CUDA(cudaStreamSynchronize(st));
   } catch (const Err& e) {
     return fail(s, e);
